@@ -1,0 +1,220 @@
+/* lkg — B200-native batched pose scoring for LKlight GSO docking.
+ *
+ * C ABI of liblkg.so.  Two groups of entry points:
+ *
+ *  1. Drop-in replacements for the reference's CUDA C ABI (same names, same
+ *     signatures, same argument meaning, same 0 / -1 return convention and
+ *     the same stderr message on failure), so src/gpu_score.rs,
+ *     src/gpu_family.rs and src/gpu_field.rs link against liblkg unchanged.
+ *     Host buffers are borrowed for the call; device copies of the constant
+ *     receptor / ligand / field arrays are cached keyed on the host pointers,
+ *     as the reference's cache does (full_score.cu:350-387).
+ *
+ *  2. A handle API (lkg_*) for callers that batch many complexes: device-
+ *     resident complexes, one persistent launch per GSO step over all of them,
+ *     CUDA-graph capture, device pointers, an exact (FP64) parity mode and
+ *     enumerated status codes.  There is no CPU fallback anywhere: a missing
+ *     device or a failed launch is reported as an error.
+ *
+ * Pose layout everywhere: 7 doubles per pose (w, x, y, z, tx, ty, tz) — the
+ * unit quaternion then the translation, as full_score.cu:230 reads them.
+ */
+#ifndef LKG_H
+#define LKG_H
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---------------------------------------------------------------------- */
+/* Status codes                                                            */
+/* ---------------------------------------------------------------------- */
+typedef enum {
+    LKG_OK = 0,
+    LKG_ERR_ARG = 1,        /* bad argument / size */
+    LKG_ERR_OOM = 2,        /* device allocation failed */
+    LKG_ERR_LAUNCH = 3,     /* kernel launch / configuration failed */
+    LKG_ERR_TIMEOUT = 4,    /* a bounded device wait or host poll ran out */
+    LKG_ERR_DEVICE = 5,     /* sticky CUDA error or device fault */
+    LKG_ERR_CAPACITY = 6,   /* a fixed-capacity device structure overflowed */
+    LKG_ERR_NO_DEVICE = 7,  /* no CUDA device visible */
+    LKG_ERR_STATE = 8       /* call not valid in the handle's current state */
+} lkg_status;
+
+const char* lkg_status_string(int status);
+/* status / message of the last failing call on this thread */
+int lkg_last_status(void);
+const char* lkg_last_error(void);
+/* 1 when a usable CUDA device is present (replaces gpu_score.rs:226-232) */
+int lkg_device_available(void);
+const char* lkg_version(void);
+
+/* family flags (gpu_score.rs:15-21) and family ids */
+#define LKG_F_FAR 1u
+#define LKG_F_ELEC 2u
+#define LKG_F_CLASH 4u
+#define LKG_F_DESOLV 16u
+enum { LKG_DNA = 0, LKG_VDW = 1, LKG_PYDOCK = 2, LKG_CPYDOCK = 3 };
+
+/* ---------------------------------------------------------------------- */
+/* 1. Reference-compatible entry points                                    */
+/* ---------------------------------------------------------------------- */
+
+/* Replaces src/cuda/full_score.cu:359-371 (Rust decls src/gpu_score.rs:252-262,
+ * src/gpu_family.rs:209-221).  out[2k] = raw electrostatics of pose k (near
+ * clamped sum + far-field q*phi; multiply by 332/4 on the host), out[2k+1] =
+ * LJ (+ clash when LKG_F_CLASH).  flags: dna 7, pydock/cpydock 3, vdw 0; with
+ * no LKG_F_FAR, phi may be a dummy and its dims 0. */
+int cuda_batch_score(const float* phi, int nx, int ny, int nz, float ox, float oy, float oz, float sp,
+                     const float* r_coords, const float* r_ele, const float* r_svdw,
+                     const float* r_vdwr, const unsigned char* r_heavy, int nr,
+                     const int* cell_start, const int* cell_atoms, int ncx, int ncy, int ncz,
+                     float c_ox, float c_oy, float c_oz, float c_sp,
+                     const float* l_base, const double* poses, const float* l_ele,
+                     const float* l_svdw, const float* l_vdwr, const unsigned char* l_heavy,
+                     int nl, int N, unsigned flags, double* out);
+
+/* Replaces src/cuda/full_score.cu:571-581 (Rust decl src/gpu_family.rs:361-372).
+ * outS[k] = sum over receptor and ligand atoms of g(min d^2)*des, with the
+ * minimum taken over non-excluded opposite atoms (r_flag / l_flag == 0) and
+ * g(d2) = min(-10*sqrt(d2) + 65, asa) when 0 < d2 <= 6.4^2 and asa > 0.
+ * The minima, the reduction and the pose transform run in one fused kernel
+ * with no N x nr scratch.  l_ele is unused (as in the reference). */
+int cuda_cpydock_solv(const float* r_coords, const unsigned char* r_flag, int nr,
+                      const int* cell_start, const int* cell_atoms, int ncx, int ncy, int ncz,
+                      float c_ox, float c_oy, float c_oz, float c_sp,
+                      const float* l_base, const double* poses, const unsigned char* l_flag,
+                      const float* l_ele, int nl, int N,
+                      const float* r_des, const float* r_asa, const float* l_des, const float* l_asa,
+                      double* outS);
+
+/* Replaces src/cuda/full_score.cu:140-150 (Rust decl src/gpu_score.rs:159-168):
+ * one pose given as already-transformed ligand coordinates; per-atom outputs
+ * (dna terms: far field, clamped electrostatics, LJ, clash). */
+int cuda_full_score(const float* phi, int nx, int ny, int nz, float ox, float oy, float oz, float sp,
+                    const float* r_coords, const float* r_ele, const float* r_svdw,
+                    const float* r_vdwr, const unsigned char* r_heavy, int nr,
+                    const int* cell_start, const int* cell_atoms, int ncx, int ncy, int ncz,
+                    float c_ox, float c_oy, float c_oz, float c_sp,
+                    const float* l_coords, const float* l_ele, const float* l_svdw,
+                    const float* l_vdwr, const unsigned char* l_heavy, int nl,
+                    float* out_elec, float* out_vdw);
+
+/* Replaces src/cuda/far_field.cu:59-63 (Rust decl src/gpu_field.rs:20-33):
+ * *result = sum_j q_j * phi(x_j) by trilinear interpolation. */
+int cuda_far_field(const float* phi, int nx, int ny, int nz, float ox, float oy, float oz, float sp,
+                   const float* coords, const float* charges, int n, double* result);
+
+/* Drops every cached device copy made by the entry points above. */
+void lkg_compat_cache_clear(void);
+
+/* ---------------------------------------------------------------------- */
+/* 2. Handle API                                                           */
+/* ---------------------------------------------------------------------- */
+typedef struct lkg_ctx lkg_ctx;
+
+enum { LKG_PREC_FAST = 0,   /* f32 pair math, f64 transform and sums */
+       LKG_PREC_EXACT = 1   /* f64 pair math in the reference's operation order */ };
+
+/* One molecule, host arrays (borrowed for the call), f64 as the reference's
+ * models hold them.  vdw = vdW well depth (vdw_charges); heavy = dna clash
+ * flag; hyd = cpydock hydrogens array (1 = heavy; the exclusion mask is
+ * derived from it as cpydock.rs:808-819 does); des/asa = cpydock desolvation
+ * coefficient / reference ASA.  Unused arrays may be NULL. */
+typedef struct {
+    int32_t n;
+    const double* coords;   /* n x 3 */
+    const double* ele;
+    const double* vdw;
+    const double* radius;
+    const uint8_t* heavy;
+    const int32_t* hyd;
+    const double* des;
+    const double* asa;
+} lkg_mol;
+
+/* Receptor far field (optional, ReceptorField layout).  When NULL the
+ * library builds it (bit-identical to grid_dna.rs:44-149). */
+typedef struct {
+    const float* phi;       /* nx*ny*nz, x fastest */
+    int32_t nx, ny, nz;
+    double ox, oy, oz, spacing;
+} lkg_field;
+
+int lkg_ctx_create(int device, lkg_ctx** out);
+int lkg_ctx_destroy(lkg_ctx* ctx);
+int lkg_ctx_set_precision(lkg_ctx* ctx, int precision);
+/* Tile shape for subsequent launches (0 = autotuned / default). */
+int lkg_ctx_set_tiles(lkg_ctx* ctx, int threads_per_block, int cell_size_milli_angstrom);
+/* Work on this CUDA stream (cudaStream_t) instead of the context's own. */
+int lkg_ctx_set_stream(lkg_ctx* ctx, void* stream);
+void* lkg_ctx_stream(lkg_ctx* ctx);
+
+/* Upload one complex; returns its id in *complex_id. */
+int lkg_complex_add(lkg_ctx* ctx, int family, const lkg_mol* receptor, const lkg_mol* ligand,
+                    const lkg_field* field, int* complex_id);
+/* Receptor / ligand atom counts and near-cell geometry of a complex. */
+int lkg_complex_info(lkg_ctx* ctx, int complex_id, int* nr, int* nl, int* n_cells);
+
+/* Score::batch_energy for one complex, host buffers: poses N x 7 -> scores.
+ * parts (optional, N x 4): raw near+far electrostatics, LJ (+clash),
+ * desolvation sum, near pairs (d <= 10 A) counted by the kernel. */
+int lkg_score(lkg_ctx* ctx, int complex_id, int n_pose, const double* poses,
+              double* scores, double* parts);
+
+/* Device-pointer variant, asynchronous on the context stream. */
+int lkg_score_device(lkg_ctx* ctx, int complex_id, int n_pose, const double* d_poses,
+                     double* d_scores, double* d_parts);
+
+/* Many complexes in one persistent launch.  For item i: complex ids[i],
+ * counts[i] poses starting at pose offset sum(counts[:i]) of d_poses; scores
+ * and parts use the same offsets.  Device pointers, asynchronous. */
+int lkg_score_multi_device(lkg_ctx* ctx, int n_items, const int* complex_ids, const int* counts,
+                           const double* d_poses, double* d_scores, double* d_parts);
+
+/* Kernel launches made by this context so far (for launch accounting). */
+int64_t lkg_ctx_launches(lkg_ctx* ctx);
+
+/* ---------------------------------------------------------------------- */
+/* Setup helpers (host)                                                    */
+/* ---------------------------------------------------------------------- */
+/* Receptor far field, bit-identical to ReceptorField::build
+ * (grid_dna.rs:44-149).  Query dims with phi == NULL. */
+int lkg_field_build(const double* coords, const double* charges, int32_t n,
+                    double origin[3], int32_t dims[3], double* spacing, float* phi);
+/* Lee & Richards SASA, probe 1.4, 20 slices (lr_sasa.rs:277-291). */
+int lkg_lr_sasa(const double* coords, const double* radii, int32_t n, double* out);
+/* Self-avoiding random chain for synthetic receptors (see lkg_setup.cpp). */
+int lkg_synth_chain(uint64_t seed, int32_t n, double r0, double bond, double min_sep, int32_t patience,
+                    double* coords, double* r_final);
+
+/* rand 0.7.3 StdRng::seed_from_u64 stream (Rng::gen::<f64>) for callers
+ * that reproduce the reference's setup poses and GSO draws. */
+void* lkg_rng_new(uint64_t seed);
+double lkg_rng_f64(void* rng);
+void lkg_rng_free(void* rng);
+
+/* ---------------------------------------------------------------------- */
+/* GSO driver (GSO::run, lib.rs:66-78; Swarm / Glowworm, swarm.rs,         */
+/* glowworm.rs) over the batched scorer                                    */
+/* ---------------------------------------------------------------------- */
+typedef struct lkg_gso lkg_gso;
+/* n_groups groups of (complex, n_swarms[g] swarms x n_glow[g] glowworms);
+ * positions: all glowworms in group, swarm, glowworm order, 7 doubles each
+ * as initial_positions_*.dat holds them (tx ty tz qw qx qy qz); every swarm
+ * of group g draws from StdRng::seed_from_u64(seeds[g]). */
+int lkg_gso_create(lkg_ctx* ctx, int n_groups, const int* complex_ids, const int* n_swarms,
+                   const int* n_glow, const double* positions, const uint64_t* seeds, lkg_gso** out);
+/* steps x (score moved glowworms of all swarms in one launch group; move) */
+int lkg_gso_run(lkg_gso* gso, int steps);
+int lkg_gso_state(lkg_gso* gso, double* trans, double* rot, double* luc, double* scoring,
+                  double* vision, int32_t* nneigh);
+int64_t lkg_gso_scored(lkg_gso* gso);
+int lkg_gso_destroy(lkg_gso* gso);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,292 @@
+"""lkg: B200-native batched pose scoring for LKlight GSO docking.
+
+Python binding of liblkg.so (built in-tree by ``build.py``).  The compute
+path is the CUDA library; this module only marshals arrays.  There is no CPU
+fallback: if the library or a CUDA device is missing, calls raise.
+
+The ``Scorer`` class mirrors the reference's ``Score`` trait
+(src/scoring.rs:20-81: ``energy``, ``supports_batch``, ``batch_energy``) for
+the dna / vdw / pydock / cpydock families; ``compat`` exposes the
+reference-compatible C entry points (``cuda_batch_score`` ...).
+"""
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "liblkg.so")
+
+DNA, VDW, PYDOCK, CPYDOCK = 0, 1, 2, 3
+FAMILIES = {"dna": DNA, "vdw": VDW, "pydock": PYDOCK, "cpydock": CPYDOCK}
+FLAGS = {"dna": 7, "pydock": 3, "cpydock": 3, "vdw": 0}   # gpu_family.rs:187-194
+PREC_FAST, PREC_EXACT = 0, 1
+
+STATUS = {0: "ok", 1: "invalid argument", 2: "device out of memory", 3: "kernel launch failed",
+          4: "timed out", 5: "device error", 6: "device capacity exceeded", 7: "no CUDA device",
+          8: "invalid state"}
+
+
+class LkgError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__("lkg status %d (%s): %s" % (status, STATUS.get(status, "?"), msg))
+        self.status = status
+
+
+class Mol(C.Structure):
+    _fields_ = [("n", C.c_int32), ("coords", C.c_void_p), ("ele", C.c_void_p), ("vdw", C.c_void_p),
+                ("radius", C.c_void_p), ("heavy", C.c_void_p), ("hyd", C.c_void_p), ("des", C.c_void_p),
+                ("asa", C.c_void_p)]
+
+
+class Field(C.Structure):
+    _fields_ = [("phi", C.c_void_p), ("nx", C.c_int32), ("ny", C.c_int32), ("nz", C.c_int32),
+                ("ox", C.c_double), ("oy", C.c_double), ("oz", C.c_double), ("spacing", C.c_double)]
+
+
+_lib = None
+
+
+def build(force=False):
+    from importlib import util
+    spec = util.spec_from_file_location("_lkg_build", os.path.join(HERE, "build.py"))
+    mod = util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod.build(force=force)
+
+
+def lib():
+    """Load liblkg.so (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise OSError("liblkg.so not built (%s); run lklight-gpu_b200/build.py" % LIB_PATH)
+    L = C.CDLL(LIB_PATH)
+    P, I, I64, U64, D, F = C.c_void_p, C.c_int, C.c_int64, C.c_uint64, C.c_double, C.c_float
+    I32 = C.c_int32
+    sig = {
+        "lkg_status_string": (C.c_char_p, [I]), "lkg_last_status": (I, []),
+        "lkg_last_error": (C.c_char_p, []), "lkg_device_available": (I, []),
+        "lkg_version": (C.c_char_p, []),
+        "lkg_ctx_create": (I, [I, P]), "lkg_ctx_destroy": (I, [P]),
+        "lkg_ctx_set_precision": (I, [P, I]), "lkg_ctx_set_tiles": (I, [P, I, I]),
+        "lkg_ctx_set_stream": (I, [P, P]), "lkg_ctx_stream": (P, [P]), "lkg_ctx_launches": (I64, [P]),
+        "lkg_complex_add": (I, [P, I, P, P, P, P]), "lkg_complex_info": (I, [P, I, P, P, P]),
+        "lkg_score": (I, [P, I, I, P, P, P]), "lkg_score_device": (I, [P, I, I, P, P, P]),
+        "lkg_score_multi_device": (I, [P, I, P, P, P, P, P]),
+        "lkg_field_build": (I, [P, P, I32, P, P, P, P]), "lkg_lr_sasa": (I, [P, P, I32, P]),
+        "lkg_synth_chain": (I, [U64, I32, D, D, D, I32, P, P]),
+        "lkg_rng_new": (P, [U64]), "lkg_rng_f64": (D, [P]), "lkg_rng_free": (None, [P]),
+        "lkg_gso_create": (I, [P, I, P, P, P, P, P, P]), "lkg_gso_run": (I, [P, I]),
+        "lkg_gso_state": (I, [P, P, P, P, P, P, P]), "lkg_gso_scored": (I64, [P]),
+        "lkg_gso_destroy": (I, [P]), "lkg_compat_cache_clear": (None, []),
+        "cuda_batch_score": (I, [P, I, I, I, F, F, F, F, P, P, P, P, P, I, P, P, I, I, I, F, F, F, F,
+                                 P, P, P, P, P, P, I, I, C.c_uint, P]),
+        "cuda_cpydock_solv": (I, [P, P, I, P, P, I, I, I, F, F, F, F, P, P, P, P, I, I, P, P, P, P, P]),
+        "cuda_full_score": (I, [P, I, I, I, F, F, F, F, P, P, P, P, P, I, P, P, I, I, I, F, F, F, F,
+                                P, P, P, P, P, I, P, P]),
+        "cuda_far_field": (I, [P, I, I, I, F, F, F, F, P, P, I, P]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+def _check(status):
+    if status != 0:
+        raise LkgError(status, lib().lkg_last_error().decode())
+
+
+def ptr(a):
+    return None if a is None else C.c_void_p(a.ctypes.data)
+
+
+def _arr(a, dt):
+    return None if a is None else np.ascontiguousarray(a, dtype=dt)
+
+
+def device_available():
+    return bool(lib().lkg_device_available())
+
+
+def make_mol(m, keep):
+    """Build an lkg_mol from a dict of per-atom arrays (coords n x 3, ele,
+    vdw (well depth), radius, optional heavy / hyd / des / asa)."""
+    c = _arr(m["coords"], np.float64).reshape(-1, 3)
+    arrs = dict(coords=c, ele=_arr(m["ele"], np.float64), vdw=_arr(m["vdw"], np.float64),
+                radius=_arr(m["radius"], np.float64), heavy=_arr(m.get("heavy"), np.uint8),
+                hyd=_arr(m.get("hyd"), np.int32), des=_arr(m.get("des"), np.float64),
+                asa=_arr(m.get("asa"), np.float64))
+    keep.append(arrs)
+    return Mol(len(c), *[None if arrs[k] is None else arrs[k].ctypes.data
+                         for k in ("coords", "ele", "vdw", "radius", "heavy", "hyd", "des", "asa")])
+
+
+class Context:
+    """A device context: resident complexes, a stream, scratch buffers."""
+
+    def __init__(self, device=0, precision="fast", tile=0, cell=0.0):
+        h = C.c_void_p()
+        _check(lib().lkg_ctx_create(device, C.byref(h)))
+        self.h = h
+        self._keep = []
+        if precision != "fast":
+            _check(lib().lkg_ctx_set_precision(self.h, PREC_EXACT if precision == "exact" else PREC_FAST))
+        if tile or cell:
+            _check(lib().lkg_ctx_set_tiles(self.h, int(tile), int(round(cell * 1000))))
+
+    def set_precision(self, precision):
+        _check(lib().lkg_ctx_set_precision(self.h, PREC_EXACT if precision == "exact" else PREC_FAST))
+
+    def add_complex(self, family, rec, lig, field=None):
+        keep = []
+        r, l = make_mol(rec, keep), make_mol(lig, keep)
+        f = None
+        if field is not None:
+            phi = _arr(field["phi"], np.float32)
+            keep.append(phi)
+            nx, ny, nz = (int(v) for v in field["dims"])
+            f = Field(phi.ctypes.data, nx, ny, nz, *[float(v) for v in field["origin"]], float(field["spacing"]))
+        cid = C.c_int()
+        fam = FAMILIES[family] if isinstance(family, str) else family
+        _check(lib().lkg_complex_add(self.h, fam, C.byref(r), C.byref(l),
+                                     None if f is None else C.byref(f), C.byref(cid)))
+        return cid.value
+
+    def info(self, cid):
+        nr, nl, nc = C.c_int(), C.c_int(), C.c_int()
+        _check(lib().lkg_complex_info(self.h, cid, C.byref(nr), C.byref(nl), C.byref(nc)))
+        return nr.value, nl.value, nc.value
+
+    def score(self, cid, poses, parts=False):
+        """poses: N x 7 (w, x, y, z, tx, ty, tz) host array -> N scores
+        (and N x 4 parts: raw electrostatics, LJ, desolvation, near pairs)."""
+        p = _arr(poses, np.float64).reshape(-1, 7)
+        out = np.zeros(len(p))
+        pa = np.zeros((len(p), 4)) if parts else None
+        _check(lib().lkg_score(self.h, cid, len(p), ptr(p), ptr(out), ptr(pa)))
+        return (out, pa) if parts else out
+
+    def score_device(self, cid, n, d_poses, d_scores, d_parts=0):
+        _check(lib().lkg_score_device(self.h, cid, n, C.c_void_p(d_poses), C.c_void_p(d_scores),
+                                      C.c_void_p(d_parts) if d_parts else None))
+
+    def score_multi_device(self, ids, counts, d_poses, d_scores, d_parts=0):
+        ids = np.ascontiguousarray(ids, np.int32)
+        counts = np.ascontiguousarray(counts, np.int32)
+        _check(lib().lkg_score_multi_device(self.h, len(ids), ptr(ids), ptr(counts), C.c_void_p(d_poses),
+                                            C.c_void_p(d_scores), C.c_void_p(d_parts) if d_parts else None))
+
+    @property
+    def stream(self):
+        return lib().lkg_ctx_stream(self.h)
+
+    def set_stream(self, stream_ptr):
+        _check(lib().lkg_ctx_set_stream(self.h, C.c_void_p(stream_ptr)))
+
+    @property
+    def launches(self):
+        return lib().lkg_ctx_launches(self.h)
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().lkg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Scorer:
+    """The reference ``Score`` trait for one complex (src/scoring.rs:20-81)."""
+
+    def __init__(self, family, rec, lig, ctx=None, precision="fast"):
+        self.ctx = ctx or Context(precision=precision)
+        self.family = family
+        self.cid = self.ctx.add_complex(family, rec, lig)
+
+    def supports_batch(self):
+        return device_available()
+
+    def energy(self, translation, rotation):
+        """Score::energy for one pose: translation (3), rotation (w, x, y, z)."""
+        return float(self.batch_energy([translation], [rotation])[0])
+
+    def batch_energy(self, translations, rotations):
+        t = np.asarray(translations, np.float64).reshape(-1, 3)
+        q = np.asarray(rotations, np.float64).reshape(-1, 4)
+        return self.ctx.score(self.cid, np.hstack([q, t]))
+
+
+class GSO:
+    """Batched GSO over groups of (complex, swarms x glowworms)."""
+
+    def __init__(self, ctx, groups, positions, seeds):
+        self.ctx = ctx
+        ids = np.array([g[0] for g in groups], np.int32)
+        ns = np.array([g[1] for g in groups], np.int32)
+        ng = np.array([g[2] for g in groups], np.int32)
+        self.n = int((ns * ng).sum())
+        self._pos = _arr(positions, np.float64).reshape(-1, 7)
+        assert len(self._pos) == self.n
+        sd = np.ascontiguousarray(seeds, np.uint64)
+        h = C.c_void_p()
+        _check(lib().lkg_gso_create(ctx.h, len(ids), ptr(ids), ptr(ns), ptr(ng), ptr(self._pos), ptr(sd),
+                                    C.byref(h)))
+        self.h = h
+
+    def run(self, steps):
+        _check(lib().lkg_gso_run(self.h, steps))
+
+    def state(self):
+        n = self.n
+        t, r, luc, sc, vis = np.zeros((n, 3)), np.zeros((n, 4)), np.zeros(n), np.zeros(n), np.zeros(n)
+        nn = np.zeros(n, np.int32)
+        _check(lib().lkg_gso_state(self.h, ptr(t), ptr(r), ptr(luc), ptr(sc), ptr(vis), ptr(nn)))
+        return dict(translation=t, rotation=r, luciferin=luc, scoring=sc, vision=vis, neighbors=nn)
+
+    @property
+    def scored(self):
+        return lib().lkg_gso_scored(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().lkg_gso_destroy(self.h)
+
+
+class Rng:
+    """rand 0.7.3 ``StdRng::seed_from_u64`` (the product's copy)."""
+
+    def __init__(self, seed):
+        self.h = lib().lkg_rng_new(seed)
+
+    def f64(self):
+        return lib().lkg_rng_f64(self.h)
+
+    def __del__(self):
+        if getattr(self, "h", None):
+            lib().lkg_rng_free(self.h)
+
+
+def field_build(coords, charges):
+    """Receptor far field on the GPU, bit-identical to ReceptorField::build."""
+    c, q = _arr(coords, np.float64).reshape(-1, 3), _arr(charges, np.float64)
+    o, d, s = np.zeros(3), np.zeros(3, np.int32), C.c_double()
+    _check(lib().lkg_field_build(ptr(c), ptr(q), len(q), ptr(o), ptr(d), C.byref(s), None))
+    phi = np.zeros(int(np.prod(d.astype(np.int64))), np.float32)
+    _check(lib().lkg_field_build(ptr(c), ptr(q), len(q), ptr(o), ptr(d), C.byref(s), ptr(phi)))
+    return dict(phi=phi, dims=d, origin=o, spacing=s.value)
+
+
+def lr_sasa(coords, radii):
+    c, r = _arr(coords, np.float64).reshape(-1, 3), _arr(radii, np.float64)
+    out = np.zeros(len(r))
+    _check(lib().lkg_lr_sasa(ptr(c), ptr(r), len(r), ptr(out)))
+    return out

@@ -1,0 +1,113 @@
+// Internal types shared by the lkg kernels and the host runtime.
+//
+// Device layout of one complex (all arrays in HBM, built once per complex):
+//   receptor atoms sorted by a fine uniform cell grid (cell edge h, default
+//   10/3 A, cells x-fastest), so that one (z, y) row of consecutive x cells
+//   is one contiguous span of atoms [cell_start[row+cx0], cell_start[row+cx1+1]);
+//     rpos  float4 (x, y, z, q)              rpos64 double4 (same, f64)
+//     rpar  float4 (sqrt eps, r, heavy, excl) rpar64 double4 (sqrt eps, r, eps, heavy)
+//     rsolv float2 (des, asa)                rsolv64 double2
+//   ligand atoms sorted along a coarse Morton order of the reference frame
+//   (tiles of consecutive atoms are spatially compact), same three arrays;
+//   receptor far field phi (f32, x fastest, the ReceptorField layout).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace lkg {
+
+enum : unsigned { F_FAR = 1u, F_ELEC = 2u, F_CLASH = 4u, F_DESOLV = 16u };
+// LJ formula variants of the exact (f64) path:
+//   0: sqrt(eps_i)*sqrt(eps_j) * (p6^2 - 2 p6), f64::min cap   (dna, pydock)
+//   1: sqrt(eps_i*eps_j) * (p6^2 - 2 p6), cap by `if k > 1`     (vdw)
+//   2: as 1 with p6 = pow(r,6)/pow(d2,3)                          (cpydock)
+enum { LJ_SVDW = 0, LJ_SQRT = 1, LJ_POW = 2 };
+
+struct ComplexDev {
+    int nr, nl;
+    unsigned flags;          // F_* of this complex's family
+    int lj_form;             // LJ_* (exact path)
+    // receptor (sorted by fine cell)
+    const float4* rpos;
+    const float4* rpar;
+    const float2* rsolv;
+    const double4* rpos64;
+    const double4* rpar64;
+    const double2* rsolv64;
+    const int* rorig;        // sorted -> caller index
+    const int* cell_start;   // ncx*ncy*ncz + 1
+    int ncx, ncy, ncz;
+    float ox, oy, oz, h, inv_h;
+    // ligand (Morton-sorted)
+    const float4* lpos;
+    const float4* lpar;
+    const float2* lsolv;
+    const double4* lpos64;
+    const double4* lpar64;
+    const double2* lsolv64;
+    const int* lorig;
+    int ntiles;              // ceil(nl / tile)
+    // far field
+    const float* phi;
+    int fnx, fny, fnz;
+    float fox, foy, foz, fsp;
+    double fox64, foy64, foz64, fsp64;
+    // desolvation
+    int hcap;                // receptor-minimum hash capacity (power of two)
+    double solv_const;       // sum over asa<0 atoms of asa*des (CPU-grid semantics)
+};
+
+// One launch over a batch of (complex, pose range) items.
+struct LaunchParams {
+    const ComplexDev* cx;        // device array of complex descriptors
+    const int* item_complex;     // [n_items]
+    const int* item_pose0;       // [n_items] global pose offset
+    const int* item_npose;       // [n_items]
+    const long long* item_work0; // [n_items+1] cumulative work units
+    int n_items;
+    long long total_work;
+    int tile;                    // ligand atoms per work unit (non-desolv kernel)
+    const double* poses;         // global N x 7 (w,x,y,z,tx,ty,tz)
+    double* scores;              // [N] final score, or N x 2 raw (elec, vdw) when raw_pairs
+    double* parts;               // [N x 4] or null: elec_raw, vdw, solv, near pairs
+    int raw_pairs;               // compat: scores holds (elec_raw, vdw) pairs
+    int solv_only;               // compat cuda_cpydock_solv: scores[k] = S
+    // scratch (self-resetting between launches)
+    double* partials;            // [N x max_tiles x 4]
+    int* pose_counter;           // [N]
+    unsigned long long* work_counter;  // [2]: next unit, CTAs done
+    int* status;                 // [4]: error flags (capacity overflow, bad index)
+    int max_tiles;
+    // per-atom outputs (cuda_full_score): pose 0 of item 0, caller atom order
+    float* atom_elec;
+    float* atom_vdw;
+};
+
+constexpr double FACTOR = 332.0;
+constexpr double EPSILON = 4.0;
+constexpr float ES_CAP_F = (float)(4.0 / 332.0);
+constexpr double ES_CAP_D = 1.0 * 4.0 / 332.0;
+constexpr float NEAR_R = 10.0f;
+constexpr float SCAN_R = 10.001f;   // candidate radius (superset margin over 10 A)
+constexpr float SOLV2_F = 40.96f;   // 6.4^2 as the reference GPU writes it
+constexpr double SOLV2_D = 6.4 * 6.4;
+
+// launches (defined in lkg_kernels_*.cu)
+cudaError_t launch_score_fast(const LaunchParams& p, int threads, int blocks, cudaStream_t s);
+cudaError_t launch_desolv_fast(const LaunchParams& p, int threads, int blocks, int hcap, cudaStream_t s);
+cudaError_t launch_score_exact(const LaunchParams& p, int threads, int blocks, cudaStream_t s);
+cudaError_t launch_desolv_exact(const LaunchParams& p, int threads, int blocks, int hcap, cudaStream_t s);
+size_t desolv_smem_bytes(int hcap, bool exact);
+
+// GPU far-field builder (lkg_field.cu), bit-identical to the reference's
+// host builder: writes phi (n[0]*n[1]*n[2] floats) for receptor atoms
+// given in their original order.
+cudaError_t build_field_device(const double* d_coords, const double* d_q, int n,
+                               const double lo[3], const int dims[3], double spacing,
+                               float* d_phi, cudaStream_t s);
+// far-field sum for cuda_far_field
+cudaError_t launch_far_field_sum(const float* phi, int nx, int ny, int nz, float ox, float oy,
+                                 float oz, float sp, const float* coords, const float* q, int n,
+                                 double* d_result, cudaStream_t s);
+
+}  // namespace lkg

@@ -1,0 +1,655 @@
+// liblkg host runtime: contexts, device-resident complexes, persistent
+// launches over batches of complexes, and the lkg_* handle API.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <numeric>
+#include <thread>
+
+#include "lkg_runtime.h"
+
+namespace lkg {
+
+int max_blocks_score_fast(int threads);
+int max_blocks_desolv_fast(int threads, int hcap);
+int max_blocks_score_exact(int threads);
+int max_blocks_desolv_exact(int threads, int hcap);
+
+namespace {
+thread_local int t_status = 0;
+thread_local char t_msg[512] = "";
+}  // namespace
+
+int set_error(int status, const char* fmt, ...) {
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(t_msg, sizeof(t_msg), fmt, ap);
+    va_end(ap);
+    t_status = status;
+    return status;
+}
+
+int set_ok() {
+    t_status = 0;
+    t_msg[0] = 0;
+    return 0;
+}
+
+int cuda_to_status(cudaError_t e) {
+    switch (e) {
+        case cudaSuccess: return LKG_OK;
+        case cudaErrorMemoryAllocation: return LKG_ERR_OOM;
+        case cudaErrorNoDevice:
+        case cudaErrorInsufficientDriver: return LKG_ERR_NO_DEVICE;
+        case cudaErrorInvalidConfiguration:
+        case cudaErrorInvalidValue:
+        case cudaErrorLaunchOutOfResources:
+        case cudaErrorInvalidDeviceFunction:
+        case cudaErrorNoKernelImageForDevice: return LKG_ERR_LAUNCH;
+        default: return LKG_ERR_DEVICE;
+    }
+}
+
+// ReceptorField box geometry (grid_dna.rs:45-61)
+void field_geometry(const double* c, int n, double lo[3], int dims[3], double* spacing) {
+    const double RMAX = 30.0, S = 0.5;
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = std::fmin(mn[a], c[3 * i + a]);
+            mx[a] = std::fmax(mx[a], c[3 * i + a]);
+        }
+    for (int a = 0; a < 3; ++a) {
+        lo[a] = std::floor(mn[a] - RMAX - 2.0 * S);
+        double hi = std::ceil(mx[a] + RMAX + 2.0 * S);
+        dims[a] = (int)((hi - lo[a]) / S) + 1;
+    }
+    *spacing = S;
+}
+
+namespace {
+
+template <class T>
+cudaError_t upload(DBuf& b, const std::vector<T>& v, cudaStream_t s) {
+    cudaError_t e = b.reserve(v.size() * sizeof(T));
+    if (e != cudaSuccess) return e;
+    if (v.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+inline uint32_t spread3(uint32_t v) {
+    v &= 0x3ff;
+    v = (v | (v << 16)) & 0x030000FF;
+    v = (v | (v << 8)) & 0x0300F00F;
+    v = (v | (v << 4)) & 0x030C30C3;
+    v = (v | (v << 2)) & 0x09249249;
+    return v;
+}
+
+// receptor: sort by fine cell (x fastest), pack device arrays
+int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
+    ComplexDev& d = cr.d;
+    const int n = R.n;
+    const float h = ctx->cell_h, inv_h = 1.0f / h;
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            float v = (float)R.c[3 * i + a];
+            mn[a] = std::min(mn[a], v);
+            mx[a] = std::max(mx[a], v);
+        }
+    if (n == 0) { mn[0] = mn[1] = mn[2] = 0.f; mx[0] = mx[1] = mx[2] = 0.f; }
+    float o[3];
+    int nc[3];
+    for (int a = 0; a < 3; ++a) {
+        o[a] = std::floor(mn[a]) - 1.0f;
+        nc[a] = std::max(1, (int)std::floor((mx[a] - o[a]) * inv_h) + 2);
+    }
+    const size_t ncell = (size_t)nc[0] * nc[1] * nc[2];
+    if (ncell > (size_t)1 << 28) return set_error(LKG_ERR_ARG, "receptor cell grid too large (%zu cells)", ncell);
+    std::vector<int> cell_of(n), cs(ncell + 1, 0);
+    for (int i = 0; i < n; ++i) {
+        int ci[3];
+        for (int a = 0; a < 3; ++a)
+            ci[a] = std::min(std::max((int)std::floor(((float)R.c[3 * i + a] - o[a]) * inv_h), 0), nc[a] - 1);
+        cell_of[i] = (ci[2] * nc[1] + ci[1]) * nc[0] + ci[0];
+        cs[cell_of[i] + 1]++;
+    }
+    for (size_t k = 0; k < ncell; ++k) cs[k + 1] += cs[k];
+    std::vector<int> cur(cs.begin(), cs.end() - 1), order(n);
+    for (int i = 0; i < n; ++i) order[cur[cell_of[i]]++] = i;
+    std::vector<float4> pos(n), par(n);
+    std::vector<float2> sol(n);
+    std::vector<double4> pos64(n), par64(n);
+    std::vector<double2> sol64(n);
+    for (int k = 0; k < n; ++k) {
+        int i = order[k];
+        pos[k] = make_float4((float)R.c[3 * i], (float)R.c[3 * i + 1], (float)R.c[3 * i + 2], (float)R.q[i]);
+        par[k] = make_float4((float)R.svdw[i], (float)R.rad[i], R.heavy[i] ? 1.f : 0.f, R.excl[i] ? 1.f : 0.f);
+        sol[k] = make_float2((float)R.des[i], (float)R.asa[i]);
+        pos64[k] = make_double4(R.c[3 * i], R.c[3 * i + 1], R.c[3 * i + 2], R.q[i]);
+        par64[k] = make_double4(R.svdw[i], R.rad[i], R.eps[i], R.heavy[i] ? 1.0 : 0.0);
+        sol64[k] = make_double2(R.des[i], R.asa[i]);
+    }
+    cudaStream_t s = ctx->stream;
+    LKG_CK(upload(cr.rpos, pos, s), "upload receptor");
+    LKG_CK(upload(cr.rpar, par, s), "upload receptor");
+    LKG_CK(upload(cr.rsolv, sol, s), "upload receptor");
+    LKG_CK(upload(cr.rpos64, pos64, s), "upload receptor");
+    LKG_CK(upload(cr.rpar64, par64, s), "upload receptor");
+    LKG_CK(upload(cr.rsolv64, sol64, s), "upload receptor");
+    LKG_CK(upload(cr.rorig, order, s), "upload receptor");
+    LKG_CK(upload(cr.cell_start, cs, s), "upload receptor");
+    LKG_CK(cudaStreamSynchronize(s), "upload receptor");
+    d.nr = n;
+    d.rpos = cr.rpos.as<float4>(); d.rpar = cr.rpar.as<float4>(); d.rsolv = cr.rsolv.as<float2>();
+    d.rpos64 = cr.rpos64.as<double4>(); d.rpar64 = cr.rpar64.as<double4>(); d.rsolv64 = cr.rsolv64.as<double2>();
+    d.rorig = cr.rorig.as<int>(); d.cell_start = cr.cell_start.as<int>();
+    d.ncx = nc[0]; d.ncy = nc[1]; d.ncz = nc[2];
+    d.ox = o[0]; d.oy = o[1]; d.oz = o[2]; d.h = h; d.inv_h = inv_h;
+    cr.n_cells = (int)ncell;
+    // desolvation hash capacity: >= 2 x receptor atoms up to 16384 slots
+    int cap = 64;
+    while (cap < 2 * n && cap < 16384) cap <<= 1;
+    d.hcap = cap;
+    return set_ok();
+}
+
+// ligand: sort along a Morton curve of 4 A cells so tiles are compact
+int build_ligand(lkg_ctx* ctx, const MolIn& L, ComplexRec& cr) {
+    ComplexDev& d = cr.d;
+    const int n = L.n;
+    double mn[3] = {INFINITY, INFINITY, INFINITY};
+    for (int i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) mn[a] = std::min(mn[a], L.c[3 * i + a]);
+    std::vector<uint32_t> code(n);
+    for (int i = 0; i < n; ++i) {
+        uint32_t ci[3];
+        for (int a = 0; a < 3; ++a) ci[a] = (uint32_t)std::min(1023.0, std::floor((L.c[3 * i + a] - mn[a]) / 4.0));
+        code[i] = spread3(ci[0]) | (spread3(ci[1]) << 1) | (spread3(ci[2]) << 2);
+    }
+    std::vector<int> order(n);
+    std::iota(order.begin(), order.end(), 0);
+    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return code[a] < code[b]; });
+    std::vector<float4> pos(n), par(n);
+    std::vector<float2> sol(n);
+    std::vector<double4> pos64(n), par64(n);
+    std::vector<double2> sol64(n);
+    for (int k = 0; k < n; ++k) {
+        int i = order[k];
+        pos[k] = make_float4((float)L.c[3 * i], (float)L.c[3 * i + 1], (float)L.c[3 * i + 2], (float)L.q[i]);
+        par[k] = make_float4((float)L.svdw[i], (float)L.rad[i], L.heavy[i] ? 1.f : 0.f, L.excl[i] ? 1.f : 0.f);
+        sol[k] = make_float2((float)L.des[i], (float)L.asa[i]);
+        pos64[k] = make_double4(L.c[3 * i], L.c[3 * i + 1], L.c[3 * i + 2], L.q[i]);
+        par64[k] = make_double4(L.svdw[i], L.rad[i], L.eps[i], L.heavy[i] ? 1.0 : 0.0);
+        sol64[k] = make_double2(L.des[i], L.asa[i]);
+    }
+    cudaStream_t s = ctx->stream;
+    LKG_CK(upload(cr.lpos, pos, s), "upload ligand");
+    LKG_CK(upload(cr.lpar, par, s), "upload ligand");
+    LKG_CK(upload(cr.lsolv, sol, s), "upload ligand");
+    LKG_CK(upload(cr.lpos64, pos64, s), "upload ligand");
+    LKG_CK(upload(cr.lpar64, par64, s), "upload ligand");
+    LKG_CK(upload(cr.lsolv64, sol64, s), "upload ligand");
+    LKG_CK(upload(cr.lorig, order, s), "upload ligand");
+    LKG_CK(cudaStreamSynchronize(s), "upload ligand");
+    d.nl = n;
+    d.lpos = cr.lpos.as<float4>(); d.lpar = cr.lpar.as<float4>(); d.lsolv = cr.lsolv.as<float2>();
+    d.lpos64 = cr.lpos64.as<double4>(); d.lpar64 = cr.lpar64.as<double4>(); d.lsolv64 = cr.lsolv64.as<double2>();
+    d.lorig = cr.lorig.as<int>();
+    d.ntiles = std::max(1, (n + ctx->tile - 1) / ctx->tile);
+    return set_ok();
+}
+
+int build_field(lkg_ctx* ctx, const MolIn& R, const lkg_field* f, bool build, ComplexRec& cr) {
+    ComplexDev& d = cr.d;
+    cudaStream_t s = ctx->stream;
+    if (f && f->phi) {
+        size_t n = (size_t)f->nx * f->ny * f->nz;
+        LKG_CK(cr.phi.reserve(n * sizeof(float)), "field alloc");
+        LKG_CK(cudaMemcpyAsync(cr.phi.p, f->phi, n * sizeof(float), cudaMemcpyHostToDevice, s), "field upload");
+        d.fnx = f->nx; d.fny = f->ny; d.fnz = f->nz;
+        d.fox64 = f->ox; d.foy64 = f->oy; d.foz64 = f->oz; d.fsp64 = f->spacing;
+    } else if (build && R.n > 0) {
+        double lo[3], sp;
+        int dims[3];
+        field_geometry(R.c.data(), R.n, lo, dims, &sp);
+        std::vector<double4> atoms;
+        for (int i = 0; i < R.n; ++i)
+            if (R.q[i] != 0.0) atoms.push_back(make_double4(R.c[3 * i], R.c[3 * i + 1], R.c[3 * i + 2], R.q[i]));
+        size_t n = (size_t)dims[0] * dims[1] * dims[2];
+        LKG_CK(cr.phi.reserve(n * sizeof(float)), "field alloc");
+        DBuf d_atoms;
+        LKG_CK(upload(d_atoms, atoms, s), "field atoms");
+        LKG_CK(build_field_device(d_atoms.as<double>(), nullptr, (int)atoms.size(), lo, dims, sp,
+                                  cr.phi.as<float>(), s), "field build");
+        ctx->launches++;
+        LKG_CK(cudaStreamSynchronize(s), "field build");
+        d.fnx = dims[0]; d.fny = dims[1]; d.fnz = dims[2];
+        d.fox64 = lo[0]; d.foy64 = lo[1]; d.foz64 = lo[2]; d.fsp64 = sp;
+    } else {
+        d.phi = nullptr; d.fnx = d.fny = d.fnz = 0;
+        d.fox = d.foy = d.foz = 0.f; d.fsp = 1.f;
+        return set_ok();
+    }
+    LKG_CK(cudaStreamSynchronize(s), "field upload");
+    d.phi = cr.phi.as<float>();
+    d.fox = (float)d.fox64; d.foy = (float)d.foy64; d.foz = (float)d.foz64; d.fsp = (float)d.fsp64;
+    return set_ok();
+}
+
+int sync_descriptors(lkg_ctx* ctx) {
+    if (!ctx->cx_dirty) return 0;
+    std::vector<ComplexDev> v;
+    for (auto& c : ctx->cx) v.push_back(c->d);
+    LKG_CK(upload(ctx->d_cx, v, ctx->stream), "descriptor upload");
+    LKG_CK(cudaStreamSynchronize(ctx->stream), "descriptor upload");
+    ctx->cx_dirty = false;
+    return 0;
+}
+
+int ensure_scratch(lkg_ctx* ctx, size_t n_poses, size_t max_tiles) {
+    if (n_poses <= ctx->cap_poses && max_tiles <= ctx->cap_tiles && ctx->status.p) return 0;
+    size_t np = std::max(n_poses, ctx->cap_poses), nt = std::max(max_tiles, ctx->cap_tiles);
+    np = std::max<size_t>(np, 1024);
+    LKG_CK(cudaStreamSynchronize(ctx->stream), "scratch");
+    LKG_CK(ctx->partials.reserve(np * nt * 4 * sizeof(double)), "scratch alloc");
+    LKG_CK(ctx->pose_counter.reserve(np * sizeof(int)), "scratch alloc");
+    LKG_CK(cudaMemset(ctx->pose_counter.p, 0, np * sizeof(int)), "scratch clear");
+    if (!ctx->work_counter.p) {
+        LKG_CK(ctx->work_counter.reserve(2 * sizeof(unsigned long long)), "scratch alloc");
+        LKG_CK(cudaMemset(ctx->work_counter.p, 0, 2 * sizeof(unsigned long long)), "scratch clear");
+        LKG_CK(ctx->status.reserve(4 * sizeof(int)), "scratch alloc");
+        LKG_CK(cudaMemset(ctx->status.p, 0, 4 * sizeof(int)), "scratch clear");
+    }
+    ctx->cap_poses = np;
+    ctx->cap_tiles = nt;
+    return 0;
+}
+
+int occupancy(lkg_ctx* ctx, bool desolv, bool exact, int threads, int hcap) {
+    Occupancy& o = desolv ? ctx->occ_desolv[exact] : ctx->occ_tiles[exact];
+    if (o.threads == threads && o.hcap == hcap && o.blocks > 0) return o.blocks;
+    int b;
+    if (desolv) b = exact ? max_blocks_desolv_exact(threads, hcap) : max_blocks_desolv_fast(threads, hcap);
+    else b = exact ? max_blocks_score_exact(threads) : max_blocks_score_fast(threads);
+    o.threads = threads; o.hcap = hcap; o.blocks = std::max(1, b);
+    return o.blocks;
+}
+
+}  // namespace
+
+int complex_create(lkg_ctx* ctx, int family, unsigned flags, int lj_form, const MolIn& rec,
+                   const MolIn& lig, const lkg_field* field, bool build_field_flag, double solv_const,
+                   int* out_id) {
+    if (cudaSetDevice(ctx->device) != cudaSuccess) return set_error(LKG_ERR_DEVICE, "cudaSetDevice failed");
+    auto cr = std::make_unique<ComplexRec>();
+    cr->family = family;
+    int st;
+    if ((st = build_receptor(ctx, rec, *cr))) return st;
+    if ((st = build_ligand(ctx, lig, *cr))) return st;
+    if ((st = build_field(ctx, rec, field, build_field_flag && (flags & F_FAR), *cr))) return st;
+    cr->d.flags = flags;
+    cr->d.lj_form = lj_form;
+    cr->d.solv_const = solv_const;
+    ctx->cx.push_back(std::move(cr));
+    ctx->cx_dirty = true;
+    *out_id = (int)ctx->cx.size() - 1;
+    return set_ok();
+}
+
+int complex_set_ligand(lkg_ctx* ctx, int id, const MolIn& lig) {
+    if (id < 0 || id >= (int)ctx->cx.size()) return set_error(LKG_ERR_ARG, "bad complex id %d", id);
+    int st = build_ligand(ctx, lig, *ctx->cx[id]);
+    ctx->cx_dirty = true;
+    return st;
+}
+
+int launch_items(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, const double* d_poses,
+                 double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e,
+                 float* atom_v) {
+    if (n_items <= 0) return set_ok();
+    for (int i = 0; i < n_items; ++i) {
+        if (ids[i] < 0 || ids[i] >= (int)ctx->cx.size()) return set_error(LKG_ERR_ARG, "bad complex id %d", ids[i]);
+        if (counts[i] < 0) return set_error(LKG_ERR_ARG, "negative pose count");
+    }
+    int st;
+    if ((st = sync_descriptors(ctx))) return st;
+    const bool exact = ctx->precision == LKG_PREC_EXACT;
+    size_t n_poses = 0, max_tiles = 1;
+    for (int i = 0; i < n_items; ++i) {
+        n_poses += (size_t)counts[i];
+        max_tiles = std::max<size_t>(max_tiles, (size_t)ctx->cx[ids[i]]->d.ntiles);
+    }
+    if (n_poses == 0) return set_ok();
+    if ((st = ensure_scratch(ctx, n_poses, max_tiles))) return st;
+    // two groups: tile kernel and fused-desolvation kernel
+    for (int grp = 0; grp < 2; ++grp) {
+        std::vector<int> ic, ip0, inp;
+        std::vector<long long> w0{0};
+        long long pose0 = 0;
+        int hcap = 64;
+        for (int i = 0; i < n_items; ++i) {
+            const ComplexDev& d = ctx->cx[ids[i]]->d;
+            bool des = (d.flags & F_DESOLV) != 0;
+            if (des == (grp == 1) && counts[i] > 0) {
+                ic.push_back(ids[i]);
+                ip0.push_back((int)pose0);
+                inp.push_back(counts[i]);
+                long long units = des ? (long long)counts[i] : (long long)counts[i] * d.ntiles;
+                w0.push_back(w0.back() + units);
+                hcap = std::max(hcap, d.hcap);
+            }
+            pose0 += counts[i];
+        }
+        if (ic.empty()) continue;
+        const int ni = (int)ic.size();
+        size_t bytes = (size_t)ni * 3 * sizeof(int) + (size_t)(ni + 1) * sizeof(long long) + 64;
+        LKG_CK(ctx->h_items.reserve(bytes * 2), "item staging");
+        LKG_CK(ctx->d_items.reserve(bytes * 2), "item staging");
+        // group 1 uses the second half so both tables can be in flight
+        char* hb = ctx->h_items.as<char>() + (grp ? bytes : 0);
+        char* db = ctx->d_items.as<char>() + (grp ? bytes : 0);
+        long long* hw = (long long*)hb;
+        int* hi = (int*)(hb + (size_t)(ni + 1) * sizeof(long long));
+        memcpy(hw, w0.data(), (ni + 1) * sizeof(long long));
+        memcpy(hi, ic.data(), ni * sizeof(int));
+        memcpy(hi + ni, ip0.data(), ni * sizeof(int));
+        memcpy(hi + 2 * ni, inp.data(), ni * sizeof(int));
+        LKG_CK(cudaMemcpyAsync(db, hb, bytes, cudaMemcpyHostToDevice, ctx->stream), "item upload");
+        LaunchParams p{};
+        p.cx = ctx->d_cx.as<ComplexDev>();
+        p.item_work0 = (const long long*)db;
+        p.item_complex = (const int*)(db + (size_t)(ni + 1) * sizeof(long long));
+        p.item_pose0 = p.item_complex + ni;
+        p.item_npose = p.item_complex + 2 * ni;
+        p.n_items = ni;
+        p.total_work = w0.back();
+        p.tile = ctx->tile;
+        p.poses = d_poses;
+        p.scores = d_scores;
+        p.parts = d_parts;
+        p.raw_pairs = raw_pairs;
+        p.solv_only = solv_only;
+        p.partials = ctx->partials.as<double>();
+        p.pose_counter = ctx->pose_counter.as<int>();
+        p.work_counter = ctx->work_counter.as<unsigned long long>();
+        p.status = ctx->status.as<int>();
+        p.max_tiles = (int)ctx->cap_tiles;
+        p.atom_elec = atom_e;
+        p.atom_vdw = atom_v;
+        cudaError_t e;
+        if (grp == 0) {
+            int threads = ctx->tile;
+            long long blocks = (long long)ctx->sm_count * occupancy(ctx, false, exact, threads, 0);
+            blocks = std::max(1LL, std::min(blocks, p.total_work));
+            e = exact ? launch_score_exact(p, threads, (int)blocks, ctx->stream)
+                      : launch_score_fast(p, threads, (int)blocks, ctx->stream);
+        } else {
+            int threads = ctx->desolv_threads;
+            size_t smem = desolv_smem_bytes(hcap, exact);
+            if (smem > 227 * 1024) return set_error(LKG_ERR_CAPACITY, "desolvation hash too large");
+            long long blocks = (long long)ctx->sm_count * occupancy(ctx, true, exact, threads, hcap);
+            blocks = std::max(1LL, std::min(blocks, p.total_work));
+            e = exact ? launch_desolv_exact(p, threads, (int)blocks, hcap, ctx->stream)
+                      : launch_desolv_fast(p, threads, (int)blocks, hcap, ctx->stream);
+        }
+        if (e != cudaSuccess) return set_error(cuda_to_status(e), "score launch: %s", cudaGetErrorString(e));
+        ctx->launches++;
+    }
+    return set_ok();
+}
+
+int wait_stream(lkg_ctx* ctx, double timeout_s) {
+    // bounded host poll: the kernels hold no unbounded waits, but a device
+    // that stops answering must still surface as an error, not a hang
+    auto t0 = std::chrono::steady_clock::now();
+    int spins = 0;
+    for (;;) {
+        cudaError_t e = cudaStreamQuery(ctx->stream);
+        if (e == cudaSuccess) return set_ok();
+        if (e != cudaErrorNotReady) return set_error(cuda_to_status(e), "stream: %s", cudaGetErrorString(e));
+        double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (el > timeout_s) return set_error(LKG_ERR_TIMEOUT, "stream did not finish within %.0f s", timeout_s);
+        if (++spins < 2000) std::this_thread::yield();
+        else std::this_thread::sleep_for(std::chrono::microseconds(50));
+    }
+}
+
+int check_status(lkg_ctx* ctx) {
+    int h[4] = {0, 0, 0, 0};
+    LKG_CK(cudaMemcpy(h, ctx->status.p, sizeof(h), cudaMemcpyDeviceToHost), "status read");
+    if (h[0] & 1) {
+        cudaMemset(ctx->status.p, 0, sizeof(h));
+        return set_error(LKG_ERR_CAPACITY, "desolvation hash overflow (too many receptor atoms within 6.4 A of one pose)");
+    }
+    return set_ok();
+}
+
+}  // namespace lkg
+
+using namespace lkg;
+
+// ---------------------------------------------------------------------------
+// C ABI: status, device, context, complexes, scoring
+// ---------------------------------------------------------------------------
+extern "C" {
+
+const char* lkg_status_string(int s) {
+    switch (s) {
+        case LKG_OK: return "ok";
+        case LKG_ERR_ARG: return "invalid argument";
+        case LKG_ERR_OOM: return "device out of memory";
+        case LKG_ERR_LAUNCH: return "kernel launch failed";
+        case LKG_ERR_TIMEOUT: return "timed out";
+        case LKG_ERR_DEVICE: return "device error";
+        case LKG_ERR_CAPACITY: return "device capacity exceeded";
+        case LKG_ERR_NO_DEVICE: return "no CUDA device";
+        case LKG_ERR_STATE: return "invalid state";
+        default: return "unknown status";
+    }
+}
+
+int lkg_last_status(void) { return t_status; }
+const char* lkg_last_error(void) { return t_msg; }
+const char* lkg_version(void) { return "lkg 0.1 (sm_100a)"; }
+
+int lkg_device_available(void) {
+    int n = 0;
+    return cudaGetDeviceCount(&n) == cudaSuccess && n > 0 ? 1 : 0;
+}
+
+int lkg_ctx_create(int device, lkg_ctx** out) {
+    if (!out) return set_error(LKG_ERR_ARG, "null out");
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return set_error(LKG_ERR_NO_DEVICE, "no CUDA device");
+    if (device < 0 || device >= n) return set_error(LKG_ERR_ARG, "device %d out of range", device);
+    LKG_CK(cudaSetDevice(device), "cudaSetDevice");
+    auto* c = new lkg_ctx();
+    c->device = device;
+    cudaDeviceGetAttribute(&c->sm_count, cudaDevAttrMultiProcessorCount, device);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) { delete c; return set_error(cuda_to_status(e), "stream create: %s", cudaGetErrorString(e)); }
+    c->own_stream = true;
+    *out = c;
+    return set_ok();
+}
+
+int lkg_ctx_destroy(lkg_ctx* ctx) {
+    if (!ctx) return set_ok();
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return set_ok();
+}
+
+int lkg_ctx_set_precision(lkg_ctx* ctx, int precision) {
+    if (!ctx || (precision != LKG_PREC_FAST && precision != LKG_PREC_EXACT))
+        return set_error(LKG_ERR_ARG, "bad precision");
+    ctx->precision = precision;
+    return set_ok();
+}
+
+int lkg_ctx_set_tiles(lkg_ctx* ctx, int threads, int cell_milli) {
+    if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
+    if (threads) {
+        if (threads < 32 || threads > 256 || threads % 32) return set_error(LKG_ERR_ARG, "tile must be 32..256, multiple of 32");
+        if (!ctx->cx.empty() && threads != ctx->tile) return set_error(LKG_ERR_STATE, "tile fixed once complexes exist");
+        ctx->tile = threads;
+    }
+    if (cell_milli) {
+        if (cell_milli < 1500 || cell_milli > 10000) return set_error(LKG_ERR_ARG, "cell edge must be 1.5..10 A");
+        if (!ctx->cx.empty()) return set_error(LKG_ERR_STATE, "cell edge fixed once complexes exist");
+        ctx->cell_h = cell_milli / 1000.0f;
+    }
+    return set_ok();
+}
+
+int lkg_ctx_set_stream(lkg_ctx* ctx, void* stream) {
+    if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
+    cudaStreamSynchronize(ctx->stream);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
+    ctx->stream = (cudaStream_t)stream;
+    ctx->own_stream = false;
+    return set_ok();
+}
+
+void* lkg_ctx_stream(lkg_ctx* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
+int64_t lkg_ctx_launches(lkg_ctx* ctx) { return ctx ? ctx->launches : 0; }
+
+}  // extern "C"
+
+namespace {
+
+int mol_from_api(const lkg_mol* m, int family, bool receptor_side, MolIn& out, double* solv_const) {
+    (void)receptor_side;
+    if (!m || m->n < 0 || (m->n > 0 && (!m->coords || !m->ele || !m->vdw || !m->radius)))
+        return set_error(LKG_ERR_ARG, "molecule arrays missing");
+    const int n = m->n;
+    out.n = n;
+    out.c.assign(m->coords, m->coords + 3 * n);
+    out.q.assign(m->ele, m->ele + n);
+    out.eps.assign(m->vdw, m->vdw + n);
+    out.svdw.resize(n);
+    for (int i = 0; i < n; ++i) out.svdw[i] = std::sqrt(out.eps[i]);
+    out.rad.assign(m->radius, m->radius + n);
+    out.heavy.assign(n, 0);
+    if (m->heavy) out.heavy.assign(m->heavy, m->heavy + n);
+    out.excl.assign(n, 0);
+    out.des.assign(n, 0.0);
+    out.asa.assign(n, 0.0);
+    if (family == LKG_CPYDOCK) {
+        if (!m->hyd || !m->des || !m->asa) return set_error(LKG_ERR_ARG, "cpydock needs hyd, des and asa");
+        // C-binary exclusion view of the hydrogens array (cpydock.rs:808-819)
+        for (int i = 0; i < n; ++i) out.excl[i] = (i % 2 == 0 && m->hyd[i / 2] != 0) ? 1 : 0;
+        out.des.assign(m->des, m->des + n);
+        out.asa.assign(m->asa, m->asa + n);
+        for (int i = 0; i < n; ++i)
+            if (out.asa[i] < 0.0) *solv_const += out.asa[i] * out.des[i];
+    }
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lkg_complex_add(lkg_ctx* ctx, int family, const lkg_mol* rec, const lkg_mol* lig,
+                    const lkg_field* field, int* complex_id) {
+    if (!ctx || !complex_id) return set_error(LKG_ERR_ARG, "null argument");
+    unsigned flags;
+    int lj;
+    switch (family) {
+        case LKG_DNA: flags = F_FAR | F_ELEC | F_CLASH; lj = LJ_SVDW; break;
+        case LKG_PYDOCK: flags = F_FAR | F_ELEC; lj = LJ_SVDW; break;
+        case LKG_VDW: flags = 0; lj = LJ_SQRT; break;
+        case LKG_CPYDOCK: flags = F_FAR | F_ELEC | F_DESOLV; lj = LJ_POW; break;
+        default: return set_error(LKG_ERR_ARG, "unknown family %d", family);
+    }
+    MolIn R, L;
+    double solv_const = 0.0;
+    int st;
+    if ((st = mol_from_api(rec, family, true, R, &solv_const))) return st;
+    if ((st = mol_from_api(lig, family, false, L, &solv_const))) return st;
+    if (L.n == 0) return set_error(LKG_ERR_ARG, "empty ligand");
+    return complex_create(ctx, family, flags, lj, R, L, field, true, solv_const, complex_id);
+}
+
+int lkg_complex_info(lkg_ctx* ctx, int id, int* nr, int* nl, int* n_cells) {
+    if (!ctx || id < 0 || id >= (int)ctx->cx.size()) return set_error(LKG_ERR_ARG, "bad complex id");
+    if (nr) *nr = ctx->cx[id]->d.nr;
+    if (nl) *nl = ctx->cx[id]->d.nl;
+    if (n_cells) *n_cells = ctx->cx[id]->n_cells;
+    return set_ok();
+}
+
+int lkg_score_device(lkg_ctx* ctx, int id, int n, const double* d_poses, double* d_scores, double* d_parts) {
+    if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
+    if (n == 0) return set_ok();
+    if (n < 0 || !d_poses || !d_scores) return set_error(LKG_ERR_ARG, "bad pose buffer");
+    cudaSetDevice(ctx->device);
+    return launch_items(ctx, 1, &id, &n, d_poses, d_scores, d_parts, 0, 0, nullptr, nullptr);
+}
+
+int lkg_score_multi_device(lkg_ctx* ctx, int n_items, const int* ids, const int* counts,
+                           const double* d_poses, double* d_scores, double* d_parts) {
+    if (!ctx || n_items < 0 || (n_items && (!ids || !counts))) return set_error(LKG_ERR_ARG, "bad items");
+    cudaSetDevice(ctx->device);
+    return launch_items(ctx, n_items, ids, counts, d_poses, d_scores, d_parts, 0, 0, nullptr, nullptr);
+}
+
+int lkg_score(lkg_ctx* ctx, int id, int n, const double* poses, double* scores, double* parts) {
+    if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
+    if (n == 0) return set_ok();
+    if (n < 0 || !poses || !scores) return set_error(LKG_ERR_ARG, "bad pose buffer");
+    cudaSetDevice(ctx->device);
+    const size_t pb = (size_t)n * 7 * sizeof(double), ob = (size_t)n * sizeof(double), qb = (size_t)n * 4 * sizeof(double);
+    LKG_CK(ctx->h_poses.reserve(pb), "staging");
+    LKG_CK(ctx->h_out.reserve(ob + qb), "staging");
+    LKG_CK(ctx->d_poses.reserve(pb), "staging");
+    LKG_CK(ctx->d_scores.reserve(ob), "staging");
+    LKG_CK(ctx->d_parts.reserve(qb), "staging");
+    memcpy(ctx->h_poses.p, poses, pb);
+    LKG_CK(cudaMemcpyAsync(ctx->d_poses.p, ctx->h_poses.p, pb, cudaMemcpyHostToDevice, ctx->stream), "pose upload");
+    int st = launch_items(ctx, 1, &id, &n, ctx->d_poses.as<double>(), ctx->d_scores.as<double>(),
+                          parts ? ctx->d_parts.as<double>() : nullptr, 0, 0, nullptr, nullptr);
+    if (st) return st;
+    LKG_CK(cudaMemcpyAsync(ctx->h_out.p, ctx->d_scores.p, ob, cudaMemcpyDeviceToHost, ctx->stream), "score readback");
+    if (parts)
+        LKG_CK(cudaMemcpyAsync(ctx->h_out.as<char>() + ob, ctx->d_parts.p, qb, cudaMemcpyDeviceToHost, ctx->stream),
+               "parts readback");
+    if ((st = wait_stream(ctx, 300.0))) return st;
+    if ((st = check_status(ctx))) return st;
+    memcpy(scores, ctx->h_out.p, ob);
+    if (parts) memcpy(parts, ctx->h_out.as<char>() + ob, qb);
+    return set_ok();
+}
+
+int lkg_field_build(const double* coords, const double* charges, int32_t n, double origin[3],
+                    int32_t dims[3], double* spacing, float* phi) {
+    if (!coords || !charges || n <= 0 || !origin || !dims || !spacing) return set_error(LKG_ERR_ARG, "bad field args");
+    int d[3];
+    field_geometry(coords, n, origin, d, spacing);
+    for (int a = 0; a < 3; ++a) dims[a] = d[a];
+    if (!phi) return set_ok();
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return set_error(LKG_ERR_NO_DEVICE, "no CUDA device");
+    std::vector<double4> atoms;
+    for (int i = 0; i < n; ++i)
+        if (charges[i] != 0.0) atoms.push_back(make_double4(coords[3 * i], coords[3 * i + 1], coords[3 * i + 2], charges[i]));
+    size_t np = (size_t)d[0] * d[1] * d[2];
+    DBuf d_atoms, d_phi;
+    LKG_CK(upload(d_atoms, atoms, 0), "field atoms");
+    LKG_CK(d_phi.reserve(np * sizeof(float)), "field alloc");
+    LKG_CK(build_field_device(d_atoms.as<double>(), nullptr, (int)atoms.size(), origin, d, *spacing,
+                              d_phi.as<float>(), 0), "field build");
+    LKG_CK(cudaMemcpy(phi, d_phi.p, np * sizeof(float), cudaMemcpyDeviceToHost), "field readback");
+    return set_ok();
+}
+
+}  // extern "C"

@@ -1,0 +1,126 @@
+// Host runtime types of liblkg (context, device-resident complexes).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "../../include/lkg.h"
+#include "lkg_internal.h"
+
+namespace lkg {
+
+int set_error(int status, const char* fmt, ...);
+int set_ok();
+int cuda_to_status(cudaError_t e);
+
+#define LKG_CK(call, what)                                                                    \
+    do {                                                                                      \
+        cudaError_t e_ = (call);                                                              \
+        if (e_ != cudaSuccess) return ::lkg::set_error(::lkg::cuda_to_status(e_), "%s: %s", \
+                                                       what, cudaGetErrorString(e_));         \
+    } while (0)
+
+// owning device allocation
+struct DBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    DBuf() = default;
+    DBuf(const DBuf&) = delete;
+    DBuf& operator=(const DBuf&) = delete;
+    ~DBuf() { release(); }
+    void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
+    cudaError_t reserve(size_t n) {  // grow-only, contents not kept
+        if (n <= bytes && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, n ? n : 16);
+        if (e == cudaSuccess) bytes = n ? n : 16;
+        else p = nullptr;
+        return e;
+    }
+    template <class T> T* as() const { return (T*)p; }
+};
+
+// pinned host allocation
+struct HBuf {
+    void* p = nullptr;
+    size_t bytes = 0;
+    HBuf() = default;
+    HBuf(const HBuf&) = delete;
+    HBuf& operator=(const HBuf&) = delete;
+    ~HBuf() { if (p) cudaFreeHost(p); }
+    cudaError_t reserve(size_t n) {
+        if (n <= bytes && p) return cudaSuccess;
+        if (p) cudaFreeHost(p);
+        p = nullptr; bytes = 0;
+        cudaError_t e = cudaMallocHost(&p, n ? n : 16);
+        if (e == cudaSuccess) bytes = n ? n : 16;
+        return e;
+    }
+    template <class T> T* as() const { return (T*)p; }
+};
+
+// one molecule in the library's unified host form (f64, caller order)
+struct MolIn {
+    int n = 0;
+    std::vector<double> c, q, svdw, eps, rad, des, asa;
+    std::vector<uint8_t> heavy, excl;
+};
+
+// device arrays of one complex; `d` points into them
+struct ComplexRec {
+    int family = -1;
+    DBuf rpos, rpar, rsolv, rpos64, rpar64, rsolv64, rorig, cell_start;
+    DBuf lpos, lpar, lsolv, lpos64, lpar64, lsolv64, lorig;
+    DBuf phi;
+    ComplexDev d{};
+    int n_cells = 0;
+};
+
+struct Occupancy { int threads = 0, hcap = 0, blocks = 0; };
+
+}  // namespace lkg
+
+struct lkg_ctx {
+    int device = 0;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    int precision = LKG_PREC_FAST;
+    int tile = 128;                 // ligand atoms per work unit
+    int desolv_threads = 512;
+    float cell_h = 10.0f / 3.0f;    // fine receptor cell edge (A)
+    std::vector<std::unique_ptr<lkg::ComplexRec>> cx;
+    lkg::DBuf d_cx;                 // ComplexDev[] on the device
+    bool cx_dirty = true;
+    // scratch (self-resetting between launches)
+    lkg::DBuf partials, pose_counter, work_counter, status;
+    size_t cap_poses = 0, cap_tiles = 0;
+    // item tables
+    lkg::DBuf d_items;
+    lkg::HBuf h_items;
+    // host-buffer call staging
+    lkg::DBuf d_poses, d_scores, d_parts;
+    lkg::HBuf h_poses, h_out;
+    int64_t launches = 0;
+    lkg::Occupancy occ_tiles[2], occ_desolv[2];
+};
+
+namespace lkg {
+// build + upload one complex (receptor / ligand already in unified form);
+// field: either provided (phi host pointer + geometry) or built on the GPU
+int complex_create(lkg_ctx* ctx, int family, unsigned flags, int lj_form, const MolIn& rec,
+                   const MolIn& lig, const lkg_field* field, bool build_field, double solv_const,
+                   int* out_id);
+// replace the ligand of an existing complex (cuda_full_score)
+int complex_set_ligand(lkg_ctx* ctx, int id, const MolIn& lig);
+// one persistent launch group over items; device pointers
+int launch_items(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, const double* d_poses,
+                 double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e,
+                 float* atom_v);
+int wait_stream(lkg_ctx* ctx, double timeout_s);
+int check_status(lkg_ctx* ctx);
+void field_geometry(const double* coords, int n, double lo[3], int dims[3], double* spacing);
+}  // namespace lkg

@@ -1,0 +1,548 @@
+// Fused pose-scoring kernels (sm_100a).
+//
+// One work unit = one tile of ligand atoms of one pose of one complex; one
+// thread per ligand atom.  Per atom, in one pass:
+//   (a) rigid transform x' = R(q) x + t in f64 (full_score.cu:255-268);
+//   (b) far field q_j * phi(x') by trilinear interpolation
+//       (full_score.cu:27-51 / grid_dna.rs:159-197);
+//   (c) near scan over receptor atoms within 10 A: the fine cell grid turns
+//       every (z, y) cell row inside the 10 A sphere into one contiguous span
+//       of position-sorted receptor atoms, trimmed in x to the sphere, read
+//       as coalesced float4 through the read-only path; for d^2 <= 100 the
+//       clamped electrostatics, the capped Lennard-Jones and the heavy-atom
+//       clash penalty (full_score.cu:296-315, dna.rs:947-968);
+//   (d) cpydock only: the ligand atom's minimum distance to non-excluded
+//       receptor atoms in registers and the receptor atoms' minima in a
+//       shared-memory hash (atomicMin), reduced in the same kernel
+//       (full_score.cu:477-569 merged; cpydock.rs:615-668).
+// Per-pose sums: registers -> warp shuffles -> one shared array per block ->
+// per-tile partials; the last tile of a pose to finish sums the partials in
+// tile order, so results do not depend on scheduling (bitwise reproducible).
+// Work units are fetched from a global counter by persistent blocks; the
+// counters reset themselves at the end of each launch.
+#pragma once
+#include "lkg_internal.h"
+
+namespace lkg {
+
+// ------------------------------------------------------------------------
+// precision traits
+// ------------------------------------------------------------------------
+template <typename R> struct Tr;
+template <> struct Tr<float> {
+    __device__ static float4 rpos(const ComplexDev& c, int k) { return __ldg(c.rpos + k); }
+    __device__ static float4 rpar(const ComplexDev& c, int k) { return __ldg(c.rpar + k); }
+    __device__ static float2 rsolv(const ComplexDev& c, int k) { return __ldg(c.rsolv + k); }
+    __device__ static float4 lpos(const ComplexDev& c, int j) { return __ldg(c.lpos + j); }
+    __device__ static float4 lpar(const ComplexDev& c, int j) { return __ldg(c.lpar + j); }
+    __device__ static float2 lsolv(const ComplexDev& c, int j) { return __ldg(c.lsolv + j); }
+};
+template <> struct Tr<double> {
+    __device__ static double4 rpos(const ComplexDev& c, int k) { return c.rpos64[k]; }
+    __device__ static double4 rpar(const ComplexDev& c, int k) { return c.rpar64[k]; }
+    __device__ static double2 rsolv(const ComplexDev& c, int k) { return c.rsolv64[k]; }
+    __device__ static double4 lpos(const ComplexDev& c, int j) { return c.lpos64[j]; }
+    __device__ static double4 lpar(const ComplexDev& c, int j) { return c.lpar64[j]; }
+    __device__ static double2 lsolv(const ComplexDev& c, int j) { return c.lsolv64[j]; }
+};
+
+// ------------------------------------------------------------------------
+// transform
+// ------------------------------------------------------------------------
+struct Rot { double m00, m01, m02, m10, m11, m12, m20, m21, m22, tx, ty, tz; };
+
+__device__ __forceinline__ Rot pose_matrix(const double* __restrict__ pq) {
+    // qt.rs:67-74 / full_score.cu:259-265; no normalisation (as the reference)
+    double w = pq[0], x = pq[1], y = pq[2], z = pq[3];
+    Rot r;
+    r.m00 = 1. - 2. * (y * y + z * z); r.m01 = 2. * (x * y - w * z); r.m02 = 2. * (x * z + w * y);
+    r.m10 = 2. * (x * y + w * z); r.m11 = 1. - 2. * (x * x + z * z); r.m12 = 2. * (y * z - w * x);
+    r.m20 = 2. * (x * z - w * y); r.m21 = 2. * (y * z + w * x); r.m22 = 1. - 2. * (x * x + y * y);
+    r.tx = pq[4]; r.ty = pq[5]; r.tz = pq[6];
+    return r;
+}
+
+__device__ __forceinline__ void apply(const Rot& r, double vx, double vy, double vz,
+                                      double& x, double& y, double& z) {
+    // rot3_apply (qt.rs:122-128) then + t, left to right
+    x = r.m00 * vx + r.m01 * vy + r.m02 * vz + r.tx;
+    y = r.m10 * vx + r.m11 * vy + r.m12 * vz + r.ty;
+    z = r.m20 * vx + r.m21 * vy + r.m22 * vz + r.tz;
+}
+
+// ------------------------------------------------------------------------
+// far field
+// ------------------------------------------------------------------------
+__device__ __forceinline__ float sample_phi(const ComplexDev& c, float x, float y, float z) {
+    float fx = (x - c.fox) / c.fsp, fy = (y - c.foy) / c.fsp, fz = (z - c.foz) / c.fsp;
+    // in the box iff 0 <= f < n - 1 per axis (ix + 1 < n); compared in float
+    // so that inf / NaN / huge coordinates never reach the integer index
+    if (!(fx >= 0.f && fy >= 0.f && fz >= 0.f && fx < (float)(c.fnx - 1) && fy < (float)(c.fny - 1) &&
+          fz < (float)(c.fnz - 1)))
+        return 0.f;
+    int ix = (int)fx, iy = (int)fy, iz = (int)fz;
+    if (ix + 1 >= c.fnx || iy + 1 >= c.fny || iz + 1 >= c.fnz) return 0.f;
+    float tx = fx - ix, ty = fy - iy, tz = fz - iz;
+    size_t sy = (size_t)c.fnx, sz = (size_t)c.fnx * c.fny;
+    const float* p = c.phi + (size_t)iz * sz + (size_t)iy * sy + ix;
+    float c000 = __ldg(p), c100 = __ldg(p + 1), c010 = __ldg(p + sy), c110 = __ldg(p + sy + 1);
+    float c001 = __ldg(p + sz), c101 = __ldg(p + sz + 1), c011 = __ldg(p + sz + sy), c111 = __ldg(p + sz + sy + 1);
+    float c00 = c000 * (1.f - tx) + c100 * tx, c10 = c010 * (1.f - tx) + c110 * tx;
+    float c01 = c001 * (1.f - tx) + c101 * tx, c11 = c011 * (1.f - tx) + c111 * tx;
+    float c0 = c00 * (1.f - ty) + c10 * ty, c1 = c01 * (1.f - ty) + c11 * ty;
+    return c0 * (1.f - tz) + c1 * tz;
+}
+
+__device__ __forceinline__ double sample_phi(const ComplexDev& c, double x, double y, double z) {
+    // grid_dna.rs:159-197 including the `tx as f32` weights
+    double s = c.fsp64;
+    double fx = (x - c.fox64) / s, fy = (y - c.foy64) / s, fz = (z - c.foz64) / s;
+    double ix = floor(fx), iy = floor(fy), iz = floor(fz);
+    if (ix < 0.0 || iy < 0.0 || iz < 0.0) return 0.0;
+    if (!(ix < (double)(c.fnx - 1) && iy < (double)(c.fny - 1) && iz < (double)(c.fnz - 1))) return 0.0;
+    long long ix0 = (long long)ix, iy0 = (long long)iy, iz0 = (long long)iz;
+    if (ix0 + 1 >= c.fnx || iy0 + 1 >= c.fny || iz0 + 1 >= c.fnz) return 0.0;
+    double tx = (double)(float)(fx - ix), ty = (double)(float)(fy - iy), tz = (double)(float)(fz - iz);
+    size_t sy = (size_t)c.fnx, sz = (size_t)c.fnx * c.fny;
+    const float* p = c.phi + (size_t)iz0 * sz + (size_t)iy0 * sy + ix0;
+    double c000 = p[0], c100 = p[1], c010 = p[sy], c110 = p[sy + 1];
+    double c001 = p[sz], c101 = p[sz + 1], c011 = p[sz + sy], c111 = p[sz + sy + 1];
+    double c00 = c000 * (1.0 - tx) + c100 * tx;
+    double c10 = c010 * (1.0 - tx) + c110 * tx;
+    double c01 = c001 * (1.0 - tx) + c101 * tx;
+    double c11 = c011 * (1.0 - tx) + c111 * tx;
+    double c0 = c00 * (1.0 - ty) + c10 * ty;
+    double c1 = c01 * (1.0 - ty) + c11 * ty;
+    return c0 * (1.0 - tz) + c1 * tz;
+}
+
+// ------------------------------------------------------------------------
+// near scan: visit every receptor atom whose fine cell intersects the
+// SCAN_R sphere around (x, y, z); rows are trimmed to the sphere.
+// ------------------------------------------------------------------------
+template <typename F>
+__device__ __forceinline__ void scan_rows(const ComplexDev& c, float x, float y, float z, F&& visit) {
+    const float R = SCAN_R, R2 = SCAN_R * SCAN_R;
+    int cz0 = max(0, (int)floorf((z - R - c.oz) * c.inv_h));
+    int cz1 = min(c.ncz - 1, (int)floorf((z + R - c.oz) * c.inv_h));
+    for (int cz = cz0; cz <= cz1; ++cz) {
+        float zlo = c.oz + cz * c.h;
+        float dzm = fmaxf(0.f, fmaxf(zlo - z, z - (zlo + c.h)));
+        float remz = R2 - dzm * dzm;
+        if (remz < 0.f) continue;
+        float wy = sqrtf(remz);
+        int cy0 = max(0, (int)floorf((y - wy - c.oy) * c.inv_h));
+        int cy1 = min(c.ncy - 1, (int)floorf((y + wy - c.oy) * c.inv_h));
+        for (int cy = cy0; cy <= cy1; ++cy) {
+            float ylo = c.oy + cy * c.h;
+            float dym = fmaxf(0.f, fmaxf(ylo - y, y - (ylo + c.h)));
+            float rem = remz - dym * dym;
+            if (rem < 0.f) continue;
+            float wx = sqrtf(rem);
+            int cx0 = max(0, (int)floorf((x - wx - c.ox) * c.inv_h));
+            int cx1 = min(c.ncx - 1, (int)floorf((x + wx - c.ox) * c.inv_h));
+            if (cx0 > cx1) continue;
+            int row = (cz * c.ncy + cy) * c.ncx;
+            int b = __ldg(c.cell_start + row + cx0), e = __ldg(c.cell_start + row + cx1 + 1);
+            for (int k = b; k < e; ++k) visit(k);
+        }
+    }
+}
+
+// ------------------------------------------------------------------------
+// pair terms
+// ------------------------------------------------------------------------
+struct AtomAcc {
+    double elec, vdw;   // per-atom sums
+    int np;             // near pairs
+};
+
+__device__ __forceinline__ void pair_fast(unsigned flags, float qj, float svj, float rj, bool hj,
+                                          const float4& a, const float4& pr, float d2,
+                                          float& elec, float& vdw) {
+    float ir2 = __frcp_rn(d2);
+    if (flags & F_ELEC) {
+        float ae = qj * a.w * ir2;
+        ae = fminf(fmaxf(ae, -ES_CAP_F), ES_CAP_F);
+        elec += ae;
+    }
+    float sv = svj * pr.x;
+    float rr = rj + pr.y;
+    float rr2 = rr * rr;
+    float p6 = rr2 * rr2 * rr2 * (ir2 * ir2 * ir2);
+    // (sv*p6)*(p6-2): finite for sv == 0 even where p6^2 would overflow
+    float vp = fminf(sv * p6 * (p6 - 2.f), 1.0f);
+    if ((flags & F_CLASH) && hj && pr.z != 0.f) {
+        float d = sqrtf(d2);
+        float dmin = 0.75f * rr;
+        if (d < dmin) vp += 6.f * (dmin - d);
+    }
+    vdw += vp;
+}
+
+__device__ __forceinline__ double powi6(double x) { double x2 = x * x; double x4 = x2 * x2; return x2 * x4; }
+__device__ __forceinline__ double powi3(double x) { double x2 = x * x; return x * x2; }
+
+__device__ __forceinline__ void pair_exact(unsigned flags, int lj_form, double qj, double svj, double rj,
+                                           double epsj, bool hj, const double4& a, const double4& pr,
+                                           double d2, double& elec, double& vdw) {
+    // dna.rs:947-968, pydock.rs:415-424, vdw.rs:129-137, cpydock.rs:630-639
+    if (flags & F_ELEC) {
+        double ae = qj * a.w / d2;
+        if (ae < -ES_CAP_D) ae = -ES_CAP_D;
+        if (ae > ES_CAP_D) ae = ES_CAP_D;
+        elec += ae;
+    }
+    if (lj_form == LJ_SVDW) {
+        double vdw_e = svj * pr.x;
+        double vdw_r = rj + pr.y;
+        double p6 = powi6(vdw_r) / powi3(d2);
+        double v = fmin(vdw_e * (p6 * p6 - 2.0 * p6), 1.0);
+        if ((flags & F_CLASH) && hj && pr.w != 0.0) {
+            double d = sqrt(d2);
+            double dmin = 0.75 * vdw_r;
+            if (d < dmin) v += 6.0 * (dmin - d);
+        }
+        vdw += v;
+    } else {
+        double ve = sqrt(epsj * pr.z);
+        double vr = rj + pr.y;
+        double p6 = (lj_form == LJ_POW) ? pow(vr, 6.0) / pow(d2, 3.0) : powi6(vr) / powi3(d2);
+        double k = ve * (p6 * p6 - 2.0 * p6);
+        vdw += (k > 1.0) ? 1.0 : k;
+    }
+}
+
+// g(min d^2) of the desolvation sum (cpydock.rs:648-668)
+__device__ __forceinline__ float solv_term(float d2, float asa) {
+    if (d2 <= SOLV2_F && d2 > 0.f && asa > 0.f) return fminf(-10.f * sqrtf(d2) + 65.f, asa);
+    return 0.f;
+}
+__device__ __forceinline__ double solv_term(double d2, double asa) {
+    double sv = 0.0;
+    if (d2 <= SOLV2_D && d2 > 0.0 && asa > 0.0) sv = -10.0 * sqrt(d2) + 65.0;
+    if (sv > asa && asa > 0.0) sv = asa;
+    return sv;
+}
+
+// receptor-minimum hash in shared memory (open addressing, bounded probes)
+template <typename R> struct MinHash;
+template <> struct MinHash<float> {
+    int* keys; int* vals; int cap;
+    __device__ void init(char* smem, int cap_) {
+        cap = cap_; keys = (int*)smem; vals = keys + cap;
+        for (int s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = -1; vals[s] = 0x7f7fffff; }
+    }
+    __device__ bool insert(int k, float d2) {
+        unsigned h = ((unsigned)k * 2654435761u) & (unsigned)(cap - 1);
+        for (int probe = 0; probe < cap; ++probe) {
+            int prev = atomicCAS(keys + h, -1, k);
+            if (prev == -1 || prev == k) { atomicMin(vals + h, __float_as_int(d2)); return true; }
+            h = (h + 1) & (unsigned)(cap - 1);
+        }
+        return false;
+    }
+    __device__ float value(int s) const { return __int_as_float(vals[s]); }
+};
+template <> struct MinHash<double> {
+    int* keys; unsigned long long* vals; int cap;
+    __device__ void init(char* smem, int cap_) {
+        cap = cap_; vals = (unsigned long long*)smem; keys = (int*)(vals + cap);
+        for (int s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = -1; vals[s] = 0x7fefffffffffffffull; }
+    }
+    __device__ bool insert(int k, double d2) {
+        unsigned h = ((unsigned)k * 2654435761u) & (unsigned)(cap - 1);
+        for (int probe = 0; probe < cap; ++probe) {
+            int prev = atomicCAS(keys + h, -1, k);
+            if (prev == -1 || prev == k) {
+                atomicMin(vals + h, (unsigned long long)__double_as_longlong(d2));
+                return true;
+            }
+            h = (h + 1) & (unsigned)(cap - 1);
+        }
+        return false;
+    }
+    __device__ double value(int s) const { return __longlong_as_double((long long)vals[s]); }
+};
+
+// ------------------------------------------------------------------------
+// per-atom work
+// ------------------------------------------------------------------------
+template <typename R> struct Atom;
+
+// f32 path: f64 transform cast to f32 as the reference kernel does
+template <> struct Atom<float> {
+    template <bool DESOLV>
+    __device__ static void run(const ComplexDev& c, const Rot& rot, int j, AtomAcc& acc,
+                               float& min_l, MinHash<float>* hash, int* status,
+                               float* out_e, float* out_v) {
+        float4 b = Tr<float>::lpos(c, j);
+        float4 lp = Tr<float>::lpar(c, j);
+        double xd, yd, zd;
+        apply(rot, (double)b.x, (double)b.y, (double)b.z, xd, yd, zd);
+        float x = (float)xd, y = (float)yd, z = (float)zd;
+        const float qj = b.w, svj = lp.x, rj = lp.y;
+        const bool hj = lp.z != 0.f, lf = lp.w != 0.f;
+        const unsigned flags = c.flags;
+        float elec = 0.f, vdw = 0.f;
+        if ((flags & F_FAR) && qj != 0.f) elec += qj * sample_phi(c, x, y, z);
+        int np = 0;
+        scan_rows(c, x, y, z, [&](int k) {
+            float4 a = Tr<float>::rpos(c, k);
+            float dx = x - a.x, dy = y - a.y, dz = z - a.z;
+            float d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 <= 100.f) {
+                float4 pr = Tr<float>::rpar(c, k);
+                ++np;
+                pair_fast(flags, qj, svj, rj, hj, a, pr, d2, elec, vdw);
+                if (DESOLV && !lf && pr.w == 0.f) {
+                    min_l = fminf(min_l, d2);
+                    if (d2 <= SOLV2_F && !hash->insert(k, d2)) atomicOr(status, 1);
+                }
+            }
+        });
+        acc.elec += (double)elec;
+        acc.vdw += (double)vdw;
+        acc.np += np;
+        if (out_e) { int o = c.lorig[j]; out_e[o] = elec; out_v[o] = vdw; }
+    }
+};
+
+// f64 path: the reference CPU grid arithmetic
+template <> struct Atom<double> {
+    template <bool DESOLV>
+    __device__ static void run(const ComplexDev& c, const Rot& rot, int j, AtomAcc& acc,
+                               double& min_l, MinHash<double>* hash, int* status,
+                               float* out_e, float* out_v) {
+        double4 b = Tr<double>::lpos(c, j);
+        double4 lp = Tr<double>::lpar(c, j);
+        double x, y, z;
+        apply(rot, b.x, b.y, b.z, x, y, z);
+        const double qj = b.w, svj = lp.x, rj = lp.y, epsj = lp.z;
+        const bool hj = lp.w != 0.0;
+        const bool lf = DESOLV ? (Tr<float>::lpar(c, j).w != 0.f) : false;
+        const unsigned flags = c.flags;
+        const int lj_form = c.lj_form;
+        double elec = 0.0, vdw = 0.0, far = 0.0;
+        if ((flags & F_FAR) && qj != 0.0) far = qj * sample_phi(c, x, y, z);
+        int np = 0;
+        scan_rows(c, (float)x, (float)y, (float)z, [&](int k) {
+            double4 a = Tr<double>::rpos(c, k);
+            double dx = x - a.x, dy = y - a.y, dz = z - a.z;
+            double d2 = dx * dx + dy * dy + dz * dz;
+            if (d2 <= 100.0) {
+                double4 pr = Tr<double>::rpar(c, k);
+                ++np;
+                pair_exact(flags, lj_form, qj, svj, rj, epsj, hj, a, pr, d2, elec, vdw);
+                if (DESOLV && !lf && __ldg(&c.rpar[k].w) == 0.f) {
+                    min_l = fmin(min_l, d2);
+                    if (d2 <= SOLV2_D && !hash->insert(k, d2)) atomicOr(status, 1);
+                }
+            }
+        });
+        acc.elec += elec + far;
+        acc.vdw += vdw;
+        acc.np += np;
+        if (out_e) { int o = c.lorig[j]; out_e[o] = (float)(elec + far); out_v[o] = (float)vdw; }
+    }
+};
+
+// ------------------------------------------------------------------------
+// reductions
+// ------------------------------------------------------------------------
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ long long warp_sum(long long v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// block sum of NV doubles into thread 0 (fixed order -> deterministic)
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV], double (*sred)[32]) {
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) v[i] = warp_sum(v[i]);
+    if (lane == 0)
+#pragma unroll
+        for (int i = 0; i < NV; ++i) sred[i][wid] = v[i];
+    __syncthreads();
+    if (threadIdx.x == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            double s = 0.0;
+            for (int w = 0; w < nw; ++w) s += sred[i][w];
+            v[i] = s;
+        }
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ int find_item(const long long* __restrict__ work0, int n_items, long long w) {
+    int lo = 0, hi = n_items - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (__ldg(work0 + mid) <= w) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// final per-pose output (family combination: gpu_score.rs:326-331,
+// gpu_family.rs:283-308, cpydock.rs:789-791; CPU-grid cpydock adds the
+// constant asa<0 term, cpydock.rs:648-668)
+__device__ __forceinline__ void write_pose(const LaunchParams& p, const ComplexDev& c, long long g,
+                                           double elec, double vdw, double solv, double np) {
+    if (p.raw_pairs) { p.scores[2 * g] = elec; p.scores[2 * g + 1] = vdw; }
+    else if (p.solv_only) { p.scores[g] = solv; }
+    else {
+        double s;
+        double ek = elec * FACTOR / EPSILON;
+        if (c.flags & F_DESOLV) {
+            double st = solv + c.solv_const;
+            s = (ek + 0.1 * vdw - st) * -1.0;
+            solv = st;
+        } else if (!(c.flags & F_ELEC)) {
+            s = vdw * -1.0;
+        } else {
+            s = -(ek + vdw);
+        }
+        p.scores[g] = s;
+    }
+    if (p.parts) {
+        p.parts[4 * g] = elec; p.parts[4 * g + 1] = vdw; p.parts[4 * g + 2] = solv; p.parts[4 * g + 3] = np;
+    }
+}
+
+__device__ __forceinline__ void finish_launch(const LaunchParams& p) {
+    if (threadIdx.x == 0) {
+        unsigned long long d = atomicAdd(p.work_counter + 1, 1ull);
+        if (d == gridDim.x - 1) { p.work_counter[0] = 0ull; p.work_counter[1] = 0ull; }
+    }
+}
+
+// ------------------------------------------------------------------------
+// kernel 1: tiles of ligand atoms (dna / pydock / vdw and compat flags)
+// ------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(256) k_score_tiles(LaunchParams p) {
+    __shared__ long long s_work;
+    __shared__ double s_red[4][32];
+    for (;;) {
+        if (threadIdx.x == 0) s_work = (long long)atomicAdd(p.work_counter, 1ull);
+        __syncthreads();
+        const long long w = s_work;
+        __syncthreads();
+        if (w >= p.total_work) break;
+        const int b = find_item(p.item_work0, p.n_items, w);
+        const ComplexDev& c = p.cx[__ldg(p.item_complex + b)];
+        const long long local = w - __ldg(p.item_work0 + b);
+        const int pose = (int)(local / c.ntiles), tile = (int)(local % c.ntiles);
+        const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
+        const int j = tile * p.tile + threadIdx.x;
+        AtomAcc acc{0.0, 0.0, 0};
+        if (j < c.nl && threadIdx.x < p.tile) {
+            const Rot rot = pose_matrix(p.poses + 7 * g);
+            R dummy_min = (R)0;
+            const bool atom_out = p.atom_elec && b == 0 && pose == 0;
+            Atom<R>::template run<false>(c, rot, j, acc, dummy_min, nullptr, p.status,
+                                         atom_out ? p.atom_elec : nullptr, atom_out ? p.atom_vdw : nullptr);
+        }
+        double v[3] = {acc.elec, acc.vdw, (double)acc.np};
+        block_sum<3>(v, s_red);
+        if (threadIdx.x == 0) {
+            double* part = p.partials + ((size_t)g * p.max_tiles + tile) * 4;
+            part[0] = v[0]; part[1] = v[1]; part[2] = 0.0; part[3] = v[2];
+            __threadfence();
+            int done = atomicAdd(p.pose_counter + g, 1);
+            if (done == c.ntiles - 1) {
+                __threadfence();
+                double e = 0.0, vv = 0.0, np = 0.0;
+                const double* pp = p.partials + (size_t)g * p.max_tiles * 4;
+                for (int t = 0; t < c.ntiles; ++t) {
+                    e += __ldcg(pp + 4 * t); vv += __ldcg(pp + 4 * t + 1); np += __ldcg(pp + 4 * t + 3);
+                }
+                write_pose(p, c, g, e, vv, 0.0, np);
+                p.pose_counter[g] = 0;
+            }
+        }
+    }
+    finish_launch(p);
+}
+
+// ------------------------------------------------------------------------
+// kernel 2: one block per pose, cpydock desolvation fused
+// ------------------------------------------------------------------------
+template <typename R>
+__global__ void __launch_bounds__(512) k_score_desolv(LaunchParams p) {
+    extern __shared__ __align__(16) char smem[];
+    __shared__ long long s_work;
+    __shared__ double s_red[4][32];
+    __shared__ long long s_fix[32];
+    for (;;) {
+        if (threadIdx.x == 0) s_work = (long long)atomicAdd(p.work_counter, 1ull);
+        __syncthreads();
+        const long long w = s_work;
+        __syncthreads();
+        if (w >= p.total_work) break;
+        const int b = find_item(p.item_work0, p.n_items, w);
+        const ComplexDev& c = p.cx[__ldg(p.item_complex + b)];
+        const int pose = (int)(w - __ldg(p.item_work0 + b));
+        const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
+        MinHash<R> hash;
+        hash.init(smem, c.hcap);
+        __syncthreads();
+        const Rot rot = pose_matrix(p.poses + 7 * g);
+        AtomAcc acc{0.0, 0.0, 0};
+        double solv_l = 0.0;
+        const bool want_pairs = !p.solv_only;
+        for (int j = threadIdx.x; j < c.nl; j += blockDim.x) {
+            R min_l = (R)1e30;
+            AtomAcc a1{0.0, 0.0, 0};
+            Atom<R>::template run<true>(c, rot, j, a1, min_l, &hash, p.status, nullptr, nullptr);
+            if (want_pairs) { acc.elec += a1.elec; acc.vdw += a1.vdw; }
+            acc.np += a1.np;
+            if (sizeof(R) == 4) {
+                float2 ls = Tr<float>::lsolv(c, j);
+                solv_l += (double)(solv_term((float)min_l, ls.y) * ls.x);
+            } else {
+                double2 ls = c.lsolv64[j];
+                solv_l += solv_term((double)min_l, ls.y) * ls.x;
+            }
+        }
+        __syncthreads();
+        // receptor side: fixed-point sum over hash slots (slot order depends on
+        // insertion races; integer sums do not)
+        long long fix = 0;
+        for (int s = threadIdx.x; s < c.hcap; s += blockDim.x) {
+            int k = hash.keys[s];
+            if (k < 0) continue;
+            double term;
+            if (sizeof(R) == 4) {
+                float2 rs = Tr<float>::rsolv(c, k);
+                term = (double)(solv_term((float)hash.value(s), rs.y) * rs.x);
+            } else {
+                double2 rs = c.rsolv64[k];
+                term = solv_term((double)hash.value(s), rs.y) * rs.x;
+            }
+            fix += __double2ll_rn(term * 4294967296.0);
+        }
+        fix = warp_sum(fix);
+        if ((threadIdx.x & 31) == 0) s_fix[threadIdx.x >> 5] = fix;
+        double v[4] = {acc.elec, acc.vdw, solv_l, (double)acc.np};
+        block_sum<4>(v, s_red);   // contains __syncthreads: s_fix is complete
+        if (threadIdx.x == 0) {
+            long long f = 0;
+            for (int i = 0; i < (int)((blockDim.x + 31) >> 5); ++i) f += s_fix[i];
+            double solv = v[2] + (double)f * (1.0 / 4294967296.0);
+            write_pose(p, c, g, v[0], v[1], solv, v[3]);
+        }
+        __syncthreads();
+    }
+    finish_launch(p);
+}
+
+}  // namespace lkg

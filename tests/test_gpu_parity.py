@@ -1,0 +1,244 @@
+"""GPU parity: the sm_100a kernels, called through liblkg's C ABI, against the
+oracle (CPU restatement of the reference's CPU grid path) on the same inputs.
+
+Tolerances: the fast path (f32 pair math) must agree within 1e-5 relative,
+denominator max(|E|, 1); the exact path (f64 pair math in the reference's
+operation order) within 1e-11 (only the summation order differs); integer
+and bit-level results (far-field grid, near-pair counts) exactly.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from tests.lkg_helpers import azp_model, compat, config0, config0_cpydock, lkg, random_poses, rel_err, synth
+
+pytestmark = pytest.mark.gpu
+
+FAST_TOL = 1e-5
+EXACT_TOL = 1e-11
+
+
+@pytest.fixture(scope="module")
+def ctx():
+    c = lkg.Context()
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def ctx_exact():
+    c = lkg.Context(precision="exact")
+    yield c
+    c.close()
+
+
+def _azp_poses(n=24, seed=3):
+    return random_poses(n, [0, 0, 0], 6.0, seed)
+
+
+# ---------------------------------------------------------------- far field
+def test_field_builder_bitwise_equals_reference_builder():
+    rec, _ = azp_model("dna")
+    g = lkg.field_build(rec["coords"], rec["ele"])
+    o = oracle.Field(rec["coords"], rec["ele"])
+    assert np.array_equal(g["dims"], o.dims) and np.array_equal(g["origin"], o.origin)
+    assert np.array_equal(g["phi"].view(np.uint32), o.phi.view(np.uint32))
+
+
+def test_field_builder_bitwise_synthetic_receptor():
+    m = synth.globule(3000, 77)
+    g = lkg.field_build(m["coords"], m["ele"])
+    o = oracle.Field(m["coords"], m["ele"])
+    assert np.array_equal(g["phi"].view(np.uint32), o.phi.view(np.uint32))
+
+
+def test_field_unit_charge_kat_on_gpu_field():
+    # grid_dna.rs:217-233 on the GPU-built field, sampled by cuda_far_field
+    g = lkg.field_build(np.zeros((1, 3)), np.ones(1))
+    for x, exp, tol in ((12.0, 1 / 144, 1e-4), (-12.0, 1 / 144, 1e-4), (28.0, 1 / 784, 1e-5), (5.0, 0.0, 1e-9),
+                        (35.0, 0.0, 1e-9)):
+        v = compat.far_field(g, np.array([[x, 0.0, 0.0]]), np.ones(1))
+        assert abs(v - exp) < tol
+
+
+# ---------------------------------------------------------------- families
+@pytest.mark.parametrize("family", ["dna", "pydock", "vdw", "cpydock"])
+def test_family_fast_matches_oracle_1azp(ctx, family):
+    rec, lig = azp_model(family)
+    m = oracle.Model(family, rec, lig)
+    poses = _azp_poses()
+    ref, rparts = m.batch_energy_grid(poses, parts=True)
+    cid = ctx.add_complex(family, rec, lig)
+    got, parts = ctx.score(cid, poses, parts=True)
+    assert rel_err(got, ref).max() < FAST_TOL
+    assert np.all(np.abs(parts[:, 3] - rparts[:, 4]) <= 2)  # near pairs (f32 boundary cases only)
+
+
+@pytest.mark.parametrize("family", ["dna", "pydock", "vdw", "cpydock"])
+def test_family_exact_matches_oracle_1azp(ctx_exact, family):
+    rec, lig = azp_model(family)
+    m = oracle.Model(family, rec, lig)
+    poses = _azp_poses(16, 5)
+    ref, rparts = m.batch_energy_grid(poses, parts=True)
+    cid = ctx_exact.add_complex(family, rec, lig)
+    got, parts = ctx_exact.score(cid, poses, parts=True)
+    assert rel_err(got, ref).max() < EXACT_TOL
+    assert np.array_equal(parts[:, 3], rparts[:, 4])  # near-pair counts exactly
+
+
+def test_identity_pose_reproduces_reference_pins(ctx_exact):
+    # dna 1AZP at the identity pose: src/dna.rs:1150 pins -1211.6718762645426
+    rec, lig = azp_model("dna")
+    cid = ctx_exact.add_complex("dna", rec, lig)
+    got = ctx_exact.score(cid, np.array([[1, 0, 0, 0, 0, 0, 0.0]]))[0]
+    assert abs(got - (-1211.6718762645426)) / 1211.67 < 1e-12
+
+
+# ---------------------------------------------------------------- config 0
+def test_config0_fast_200_poses(ctx):
+    c0 = config0()
+    m = oracle.Model("dna", c0["rec"], c0["lig"])
+    pos = synth.to_kernel_poses(synth.setup_poses(c0["rec"]["coords"], 1, 200, 42))
+    ref, rparts = m.batch_energy_grid(pos, parts=True)
+    cid = ctx.add_complex("dna", c0["rec"], c0["lig"])
+    got, parts = ctx.score(cid, pos, parts=True)
+    assert rel_err(got, ref).max() < FAST_TOL
+    assert rparts[:, 4].sum() > 0
+    # rerun: bitwise reproducible
+    assert np.array_equal(got, ctx.score(cid, pos))
+
+
+def test_config1_cpydock_fast(ctx):
+    c1 = config0_cpydock()
+    m = oracle.Model("cpydock", c1["rec"], c1["lig"])
+    pos = synth.to_kernel_poses(synth.setup_poses(c1["rec"]["coords"], 2, 20, 7))
+    ref, rparts = m.batch_energy_grid(pos, parts=True)
+    cid = ctx.add_complex("cpydock", c1["rec"], c1["lig"])
+    got, parts = ctx.score(cid, pos, parts=True)
+    assert rel_err(got, ref).max() < FAST_TOL
+    assert np.abs(parts[:, 2] - rparts[:, 3]).max() < 1e-3 * max(1.0, np.abs(rparts[:, 3]).max())
+
+
+# ---------------------------------------------------------------- compat ABI
+def _compat_inputs(family):
+    rec, lig = azp_model(family)
+    heavy = rec.get("heavy")
+    R = compat.CudaReceptor(rec["coords"], rec["ele"], np.sqrt(rec["vdw"]), rec["radius"],
+                            heavy if family == "dna" else None)
+    L = compat.CudaLigand(lig["coords"], lig["ele"], np.sqrt(lig["vdw"]), lig["radius"],
+                          lig.get("heavy") if family == "dna" else None)
+    return rec, lig, R, L
+
+
+@pytest.mark.parametrize("family", ["dna", "pydock", "vdw"])
+def test_cuda_batch_score_matches_oracle(family):
+    rec, lig, R, L = _compat_inputs(family)
+    field = None
+    if family != "vdw":
+        f = oracle.Field(rec["coords"], rec["ele"])
+        field = dict(phi=f.phi, dims=f.dims, origin=f.origin, spacing=f.spacing)
+    poses = _azp_poses(12, 9)
+    got = compat.batch_scores(field, R, L, poses, lkg.FLAGS[family])
+    ref = oracle.Model(family, rec, lig).batch_energy_grid(poses)
+    assert rel_err(got, ref).max() < FAST_TOL
+
+
+def test_cuda_cpydock_solv_matches_oracle_desolvation():
+    rec, lig, R, L = _compat_inputs("cpydock")
+    poses = _azp_poses(12, 11)
+    s = compat.cpydock_solv(R, L, poses, compat.cpy_flag(rec["hyd"]), compat.cpy_flag(lig["hyd"]),
+                            rec["des"], rec["asa"], lig["des"], lig["asa"])
+    _, parts = oracle.Model("cpydock", rec, lig).batch_energy_grid(poses, parts=True)
+    # the reference GPU solv omits the constant asa<0 term of the CPU path
+    const = float((rec["asa"] * rec["des"])[rec["asa"] < 0].sum() + (lig["asa"] * lig["des"])[lig["asa"] < 0].sum())
+    assert np.abs(s - (parts[:, 3] - const)).max() < 1e-3 * max(1.0, np.abs(parts[:, 3]).max())
+
+
+def test_cuda_full_score_per_atom_sums():
+    rec, lig, R, L = _compat_inputs("dna")
+    f = oracle.Field(rec["coords"], rec["ele"])
+    field = dict(phi=f.phi, dims=f.dims, origin=f.origin, spacing=f.spacing)
+    t = np.array([1.0, -2.0, 3.0])
+    lc = lig["coords"] + t
+    oe, ov = compat.full_score(field, R, lc, L)
+    e, parts = oracle.Model("dna", rec, lig).energy_grid(t, [1, 0, 0, 0], parts=True)
+    assert abs(oe.astype(np.float64).sum() - (parts[0] + parts[1])) < 1e-5 * max(1.0, abs(parts[0] + parts[1]))
+    assert abs(ov.astype(np.float64).sum() - parts[2]) < 1e-5 * max(1.0, abs(parts[2]))
+
+
+def test_cuda_far_field_matches_oracle():
+    rec, lig = azp_model("pydock")
+    f = oracle.Field(rec["coords"], rec["ele"])
+    field = dict(phi=f.phi, dims=f.dims, origin=f.origin, spacing=f.spacing)
+    xyz = lig["coords"] + np.array([3.0, 1.0, -2.0])
+    got = compat.far_field(field, xyz, lig["ele"])
+    ref = sum(q * f.sample(*p) for p, q in zip(xyz, lig["ele"]) if q != 0)
+    assert abs(got - ref) < 1e-5 * max(1.0, abs(ref))
+
+
+# ---------------------------------------------------------------- batching
+def test_multi_complex_launch_equals_single(ctx):
+    import torch
+    cids, posesets = [], []
+    for fam, seed in (("dna", 1), ("pydock", 2), ("vdw", 3), ("dna", 4)):
+        rec = synth.globule(1500 + 700 * seed, 100 + seed)
+        lig = synth.duplex(4 + seed, 200 + seed)
+        cids.append(ctx.add_complex(fam, rec, lig))
+        posesets.append(synth.to_kernel_poses(synth.setup_poses(rec["coords"], 2, 8 + seed, seed)))
+    singles = [ctx.score(c, p) for c, p in zip(cids, posesets)]
+    allp = torch.tensor(np.vstack(posesets), dtype=torch.float64, device="cuda")
+    out = torch.zeros(len(allp), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    ctx.score_multi_device(cids, [len(p) for p in posesets], allp.data_ptr(), out.data_ptr())
+    lkg.lib().lkg_ctx_stream(ctx.h)
+    import ctypes
+    cudart_sync = torch.cuda.synchronize
+    # the context works on its own stream: wait for it before reading
+    assert ctypes.c_void_p(ctx.stream).value is not None
+    torch.cuda.Stream(stream_ptr=ctx.stream).synchronize()
+    cudart_sync()
+    got = out.cpu().numpy()
+    assert np.array_equal(got, np.concatenate(singles))
+
+
+def test_edge_cases(ctx):
+    rec, lig = azp_model("dna")
+    cid = ctx.add_complex("dna", rec, lig)
+    assert len(ctx.score(cid, np.zeros((0, 7)))) == 0
+    # ligand far from the receptor: no near pairs, no far field
+    far = np.array([[1, 0, 0, 0, 500.0, 0, 0]])
+    s, p = ctx.score(cid, far, parts=True)
+    assert s[0] == 0.0 and p[0, 3] == 0
+    # non-normalised quaternion is used as given (the reference never normalises)
+    q = np.array([[2.0, 0, 0, 0, 1.0, 0.5, 0.0]])
+    ref = oracle.Model("dna", rec, lig).energy_grid(q[0, 4:], q[0, :4])
+    assert rel_err(ctx.score(cid, q), [ref]).max() < FAST_TOL
+    with pytest.raises(lkg.LkgError):
+        ctx.score(999, far)
+
+
+def test_single_atom_ligand_and_tiny_receptor(ctx):
+    rec = dict(coords=np.array([[0.0, 0, 0], [4.0, 0, 0]]), ele=np.array([0.5, -0.5]), vdw=np.array([0.1, 0.2]),
+               radius=np.array([1.9, 1.7]), heavy=np.array([1, 1], np.uint8))
+    lig = dict(coords=np.array([[0.0, 0, 0]]), ele=np.array([1.0]), vdw=np.array([0.15]),
+               radius=np.array([1.8]), heavy=np.array([1], np.uint8))
+    poses = random_poses(40, [2.0, 0, 0], 9.0, 1)
+    for fam in ("dna", "pydock", "vdw"):
+        ref = oracle.Model(fam, rec, lig).batch_energy_grid(poses)
+        got = ctx.score(ctx.add_complex(fam, rec, lig), poses)
+        assert rel_err(got, ref).max() < FAST_TOL
+
+
+def test_gso_exact_ranking_matches_oracle(ctx_exact):
+    rec, lig = azp_model("dna")
+    pos = synth.setup_poses(rec["coords"], 1, 40, 324)
+    m = oracle.Model("dna", rec, lig)
+    og = oracle.GSO(m, pos, 324)
+    og.run(10)
+    cid = ctx_exact.add_complex("dna", rec, lig)
+    g = lkg.GSO(ctx_exact, [(cid, 1, 40)], pos, [324])
+    g.run(10)
+    a, b = g.state(), og.state()
+    assert np.array_equal(np.argsort(-a["scoring"], kind="stable")[:10], np.argsort(-b["scoring"], kind="stable")[:10])
+    assert np.allclose(a["translation"], b["translation"], rtol=0, atol=1e-9)
+    assert rel_err(a["scoring"], b["scoring"]).max() < 1e-9

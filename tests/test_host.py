@@ -1,0 +1,113 @@
+"""CPU-side tests of the product library: it loads, exports every symbol
+include/lkg.h declares, and its host logic (RNG, setup poses, cell-list
+packing, field geometry, SASA, synthetic inputs) behaves; no GPU calls."""
+import ctypes
+
+import numpy as np
+import pytest
+
+import oracle
+from tests.lkg_helpers import compat, header_symbols, lkg, synth
+
+
+def test_library_exports_header_symbols():
+    lib = ctypes.CDLL(lkg.LIB_PATH)
+    syms = header_symbols()
+    assert len(syms) >= 30
+    missing = [s for s in syms if not hasattr(lib, s)]
+    assert not missing, missing
+
+
+def test_status_strings_and_no_device_error():
+    L = lkg.lib()
+    assert L.lkg_status_string(0) == b"ok"
+    assert L.lkg_status_string(6) == b"device capacity exceeded"
+    if not lkg.device_available():
+        with pytest.raises(lkg.LkgError) as e:
+            lkg.Context()
+        assert e.value.status == 7
+
+
+def test_product_rng_matches_reference_kat():
+    # src/qt.rs:474-488 through the product's StdRng
+    r = lkg.Rng(324324324)
+    u1, u2, u3 = r.f64(), r.f64(), r.f64()
+    q = [np.sqrt(1 - u1) * np.sin(2 * np.pi * u2), np.sqrt(1 - u1) * np.cos(2 * np.pi * u2),
+         np.sqrt(u1) * np.sin(2 * np.pi * u3), np.sqrt(u1) * np.cos(2 * np.pi * u3)]
+    exp = [0.31924330894562036, -0.5980633213833059, 0.5444724265858514, 0.49391674399349367]
+    assert np.all(np.abs(np.array(q) - exp) < 2.3e-16)
+
+
+def test_product_rng_matches_oracle_stream():
+    a, b = lkg.Rng(42), oracle.Rng(42)
+    assert [a.f64() for _ in range(1000)] == [b.f64() for _ in range(1000)]
+
+
+def test_setup_poses_are_unit_quaternions_near_sphere():
+    c = synth.globule(800, 3)["coords"]
+    pos = synth.setup_poses(c, 3, 10, 5)
+    assert pos.shape == (30, 7)
+    assert np.allclose(np.linalg.norm(pos[:, 3:], axis=1), 1.0, atol=5e-6)
+    avg_r = np.mean(np.linalg.norm(c, axis=1))
+    r = np.linalg.norm(pos[:, :3], axis=1)
+    assert np.all(np.abs(r - (avg_r + 3.0)) < 1.8)
+    assert np.array_equal(pos, synth.setup_poses(c, 3, 10, 5))
+
+
+def test_compat_cell_list_packing_matches_oracle():
+    c = synth.globule(1500, 9)["coords"]
+    cr = compat.CudaReceptor(c, np.zeros(len(c)), np.ones(len(c)), np.ones(len(c)))
+    o = oracle.crec_build(c)
+    assert np.array_equal(cr.cell_start, o["cell_start"])
+    assert np.array_equal(cr.cell_atoms, o["cell_atoms"])
+    assert [cr.ncx, cr.ncy, cr.ncz] == list(o["nc"])
+    assert np.allclose(cr.c_o, o["origin"])
+
+
+def test_field_geometry_matches_oracle():
+    g = synth.globule(700, 4)
+    L = lkg.lib()
+    o, d, s = np.zeros(3), np.zeros(3, np.int32), ctypes.c_double()
+    c = np.ascontiguousarray(g["coords"])
+    q = np.ascontiguousarray(g["ele"])
+    assert L.lkg_field_build(lkg.ptr(c), lkg.ptr(q), len(q), lkg.ptr(o), lkg.ptr(d), ctypes.byref(s), None) == 0
+    f = oracle.Field(np.zeros((2, 3)) + c[:2], q[:2])  # geometry only depends on the bbox
+    f2 = oracle.Field(c, np.zeros(len(q)))
+    assert np.array_equal(d, f2.dims) and np.array_equal(o, f2.origin) and s.value == f2.spacing
+    del f
+
+
+def test_lr_sasa_isolated_and_buried():
+    # one isolated sphere: 4 pi (r + 1.4)^2 up to slice discretisation
+    a = lkg.lr_sasa(np.zeros((1, 3)), np.array([1.6]))
+    assert abs(a[0] - 4 * np.pi * 3.0 ** 2) / (4 * np.pi * 9.0) < 0.02
+    # a sphere inside a larger one is fully buried
+    b = lkg.lr_sasa(np.array([[0, 0, 0], [0.1, 0, 0]]), np.array([0.5, 4.0]))
+    assert b[0] == 0.0 and b[1] > 0
+
+
+def test_synthetic_config0_shape_and_charges():
+    c0 = synth.config0()
+    rec, lig = c0["rec"], c0["lig"]
+    assert len(rec["coords"]) == 12625
+    assert 1100 <= len(lig["coords"]) <= 1400
+    assert abs(rec["ele"].sum() - 10.0) < 1e-9
+    assert np.ptp(rec["ele"]) <= 1.6 and np.all(np.abs(rec["ele"]) <= 0.81)
+    assert (lig["ele"] == -1.0).sum() == 40 and np.all((lig["ele"] == 0) | (lig["ele"] == -1))
+    assert np.array_equal(rec["coords"], rec["coords"].astype(np.float32).astype(np.float64))
+    assert rec["chain_radius"] >= 30.0
+    # nonbonded spacing: atoms more than two bonds apart stay >= 3.0 A apart
+    c = rec["coords"]
+    d = np.linalg.norm(c[3:200, None, :] - c[None, :1000, :], axis=2)
+    i, j = np.nonzero(d < 2.99)
+    assert np.all(np.abs((i + 3) - j) <= 2)
+    c0b = synth.config0()
+    assert np.array_equal(c0b["rec"]["coords"], rec["coords"])
+
+
+def test_cpy_flag_matches_reference_view():
+    hyd = np.array([1, 0, 1, 1, 0, 0, 1])
+    f = compat.cpy_flag(hyd)
+    # flag(i) = i even and hyd[i // 2] != 0
+    exp = [1 if (i % 2 == 0 and hyd[i // 2] != 0) else 0 for i in range(len(hyd))]
+    assert list(f) == exp
