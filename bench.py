@@ -1,0 +1,314 @@
+#!/usr/bin/env python
+"""Benchmark: exact poses/s of the batched scorer on synthetic complexes.
+
+Workload (default): the batched exact-scorer configuration — 64 synthetic
+complexes (receptors log-uniform 2k-40k atoms, ligands 300-5k atoms; 32 dna,
+32 pydock), 20 swarms x 300 glowworms each = 384,000 poses per step, seed 11.
+One step = one scoring pass over every pose of every complex, issued as ONE
+launch group (``lkg_score_multi_device``).  ``--workload config0`` runs the
+plain dna configuration (1 x 200 poses) instead.
+
+Reported (one JSON line on rank 0):
+  value     poses/s with poses resident in HBM, CUDA events on the context's
+            stream, max over ranks (weak scaling: every rank scores its own
+            copy of the workload)
+  e2e       the same through the C ABI with host buffers (``lkg_score_multi``:
+            page-locked poses in, scores out, every step)
+  roofline  FP32 work of the dominant kernel (near pairs x FLOPs per pair
+            from the reference formulas + 30 FLOPs per charged ligand atom
+            for the far field) per launch / launch time, against the FP32
+            peak 148 SMs x 128 lanes x 2 FLOPs x max SM clock
+  cpu_baseline  the oracle (C++ restatement of the reference's CPU grid
+            path, OpenMP over poses, all host cores) on a bounded sample
+``--impl reference`` times that CPU path alone as the reference arm.
+"""
+import argparse
+import importlib
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+FLOPS_PER_PAIR = {"dna": 24, "pydock": 23, "vdw": 19, "cpydock": 25}
+FAR_FLOPS = 30
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lkg", choices=["lkg", "reference"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config0"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--tile", type=int, default=0)
+    ap.add_argument("--cell", type=float, default=0.0)
+    return ap.parse_args()
+
+
+def workload(name):
+    synth = importlib.import_module("lklight-gpu_b200.synth")
+    if name == "config0":
+        c0 = synth.config0()
+        items = [dict(rec=c0["rec"], lig=c0["lig"], family="dna", swarms=1, glowworms=200, seed=42)]
+    else:
+        items = synth.config2()
+    for it in items:
+        it["poses"] = synth.to_kernel_poses(
+            synth.setup_poses(it["rec"]["coords"], it["swarms"], it["glowworms"], it["seed"]))
+    return items
+
+
+class Clocks:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.f = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        try:
+            self.p = subprocess.Popen(["nvidia-smi", "-i", str(index), "--query-gpu=" + self.Q,
+                                       "--format=csv,noheader,nounits", "-lms", "200"],
+                                      stdout=self.f, stderr=subprocess.DEVNULL)
+        except OSError:
+            self.p = None
+
+    def stop(self):
+        if self.p is None:
+            return None
+        self.p.terminate()
+        try:
+            self.p.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.p.kill()
+        self.f.seek(0)
+        rows = [r.split(",") for r in self.f.read().strip().splitlines() if r.strip()]
+        os.unlink(self.f.name)
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx = max(mx, float(r[2]))
+                for k, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(k)
+            except (ValueError, IndexError):
+                pass
+        load = [s for s in sm if s > 0.5 * mx] or sm
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": mx or None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def cpu_sample(items, min_seconds=10.0, threads=0, max_complexes=2):
+    """Oracle poses/s on a bounded sample: the first dna and the first pydock
+    complex, poses from their setup sets, batches until min_seconds pass."""
+    import oracle
+    picks = []
+    for fam in ("dna", "pydock"):
+        for k, it in enumerate(items):
+            if it["family"] == fam:
+                picks.append(k)
+                break
+    picks = picks[:max_complexes]
+    models = [(k, oracle.Model(items[k]["family"], items[k]["rec"], items[k]["lig"])) for k in picks]
+    for _, m in models:
+        m.field()  # far field built before timing (setup, as the reference caches it)
+    done, t0, batch = 0, time.perf_counter(), 8
+    off = 0
+    while True:
+        for k, m in models:
+            p = items[k]["poses"]
+            sel = p[(off + np.arange(batch)) % len(p)]
+            m.batch_energy_grid(sel, threads=threads)
+            done += batch
+        off += batch
+        el = time.perf_counter() - t0
+        if el >= min_seconds:
+            break
+        batch = min(batch * 2, 512)
+    cores = threads if threads > 0 else os.cpu_count()
+    return done / el, cores, "poses of complexes %s (%s), %d poses, %.1f s" % (
+        picks, "/".join(items[k]["family"] for k in picks), done, el)
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    items = workload(args.workload)
+    vals = []
+    for s in range(args.warmup + args.steps):
+        v, cores, sample = cpu_sample(items, min_seconds=3.0 if s < args.warmup else 6.0)
+        if s >= args.warmup:
+            vals.append(v)
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": "exact poses/s on 1 B200 (dna); surrogate-screened at >=95% top-5 overlap",
+            "value": v, "unit": "poses/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic", "config": {"workload": args.workload, "sample": sample},
+            "cpu_baseline": {"value": v, "unit": "poses/s", "cores": cores, "kind": "port", "sample": sample},
+            "e2e": {"value": v, "unit": "poses/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference(args, rank, world)
+
+    import torch
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+    lkg = importlib.import_module("lklight-gpu_b200")
+
+    items = workload(args.workload)
+    ctx = lkg.Context(device=local, tile=args.tile, cell=args.cell)
+    stream = torch.cuda.ExternalStream(ctx.stream)
+    ids = [ctx.add_complex(it["family"], it["rec"], it["lig"]) for it in items]
+    counts = [len(it["poses"]) for it in items]
+    npose = int(sum(counts))
+    allp = np.vstack([it["poses"] for it in items])
+    d_poses = torch.tensor(allp, dtype=torch.float64, device="cuda")
+    d_scores = torch.zeros(npose, dtype=torch.float64, device="cuda")
+    d_parts = torch.zeros((npose, 4), dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+
+    # algorithmic work: near pairs counted by the exact path (equal to the
+    # oracle's count), charged ligand atoms for the far field
+    ctx.set_precision("exact")
+    ctx.score_multi_device(ids, counts, d_poses.data_ptr(), d_scores.data_ptr(), d_parts.data_ptr())
+    stream.synchronize()
+    pairs = d_parts[:, 3].cpu().numpy()
+    ctx.set_precision("fast")
+    flops, off = 0.0, 0
+    fam_pairs = {}
+    for it, n in zip(items, counts):
+        p = float(pairs[off:off + n].sum())
+        fam_pairs[it["family"]] = fam_pairs.get(it["family"], 0.0) + p
+        charged = int(np.count_nonzero(it["lig"]["ele"])) if it["family"] != "vdw" else 0
+        flops += p * FLOPS_PER_PAIR[it["family"]] + FAR_FLOPS * charged * n
+        off += n
+
+    def step():
+        ctx.score_multi_device(ids, counts, d_poses.data_ptr(), d_scores.data_ptr())
+
+    for _ in range(args.warmup):
+        step()
+    stream.synchronize()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = Clocks(local)
+    l0 = ctx.launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    for _ in range(args.steps):
+        step()
+    ev1.record(stream)
+    ev1.synchronize()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    launches = ctx.launches - l0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms_max = float(t.item())
+    value = npose * world / (ms_max / 1e3)
+
+    # e2e: host buffers through the C ABI, copies inside the timed region
+    h_poses = torch.from_numpy(allp).pin_memory()
+    h_scores = torch.zeros(npose, dtype=torch.float64).pin_memory()
+    for _ in range(max(1, args.warmup)):
+        ctx.score_multi(ids, counts, h_poses, h_scores)
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        ctx.score_multi(ids, counts, h_poses, h_scores)
+    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
+    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
+    if dist:
+        dist.all_reduce(te, op=dist.ReduceOp.MAX)
+    e2e_value = npose * world / (float(te.item()) / 1e3)
+
+    # plain single-complex scorer: one host-buffer call (one launch) per complex
+    plain = None
+    if not args.no_plain and len(items) > 1:
+        for k, cid in enumerate(ids):
+            ctx.score(cid, items[k]["poses"])
+        t0 = time.perf_counter()
+        reps = max(1, min(3, args.steps))
+        for _ in range(reps):
+            for k, cid in enumerate(ids):
+                ctx.score(cid, items[k]["poses"])
+        pms = (time.perf_counter() - t0) * 1e3 / reps
+        plain = {"value": npose / (pms / 1e3), "unit": "poses/s", "ms_per_step": pms,
+                 "what": "lkg_score per complex, host buffers, one launch and sync per complex"}
+
+    peaks = {}
+    try:
+        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+    except (OSError, ValueError):
+        pass
+    sm_max = float(peaks.get("sm_max_mhz", 1965.0))
+    fp32_peak = 148 * 128 * 2 * sm_max * 1e6 / 1e12
+    achieved = flops / (ms / 1e3) / 1e12
+
+    line = {"metric": "exact poses/s on 1 B200 (dna); surrogate-screened at >=95% top-5 overlap",
+            "value": value, "unit": "poses/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32 pair math, f64 transform and sums", "data": "synthetic",
+            "config": {"workload": args.workload, "complexes": len(items), "poses_per_step": npose,
+                       "families": sorted(set(it["family"] for it in items)),
+                       "receptor_atoms": int(sum(len(it["rec"]["coords"]) for it in items)),
+                       "ligand_atoms": int(sum(len(it["lig"]["coords"]) for it in items)),
+                       "near_pairs_per_step": float(pairs.sum()), "near_pairs_by_family": fam_pairs,
+                       "l2": "inputs larger than L2 (receptor arrays and far-field grids of all complexes)",
+                       "parallelism": "replicas" if world > 1 else "single"},
+            "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                         "frac": achieved / fp32_peak, "traffic": None,
+                         "peak_source": "148 SMs x 128 FP32 lanes x 2 x sm_max_mhz of MEASURED_PEAKS.json",
+                         "work": "near pairs x FLOPs/pair (dna 24, pydock 23, vdw 19) + 30 per charged ligand "
+                                 "atom (far field), counted per launch"},
+            "pair_rate": {"value": float(pairs.sum()) / (ms / 1e3), "unit": "near pairs/s"},
+            "e2e": {"value": e2e_value, "unit": "poses/s", "ms_per_step": float(te.item()),
+                    "h2d_bytes_per_step": npose * 7 * 8, "d2h_bytes_per_step": npose * 8,
+                    "api": "lkg_score_multi (host page-locked buffers)"},
+            "gpu_launches": int(launches), "clocks": clk}
+    if plain:
+        line["plain_single_complex"] = plain
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, cores, sample = cpu_sample(items)
+        line["cpu_baseline"] = {"value": v, "unit": "poses/s", "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

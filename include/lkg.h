@@ -174,6 +174,13 @@ int lkg_score_device(lkg_ctx* ctx, int complex_id, int n_pose, const double* d_p
 int lkg_score_multi_device(lkg_ctx* ctx, int n_items, const int* complex_ids, const int* counts,
                            const double* d_poses, double* d_scores, double* d_parts);
 
+/* Same batch with HOST buffers (synchronous): poses are copied to the
+ * device (directly by DMA when the caller's buffer is page-locked), one
+ * launch group scores every item, scores (and optional N x 4 parts) are
+ * copied back. */
+int lkg_score_multi(lkg_ctx* ctx, int n_items, const int* complex_ids, const int* counts,
+                    const double* poses, double* scores, double* parts);
+
 /* Kernel launches made by this context so far (for launch accounting). */
 int64_t lkg_ctx_launches(lkg_ctx* ctx);
 

@@ -75,6 +75,7 @@ def lib():
         "lkg_complex_add": (I, [P, I, P, P, P, P]), "lkg_complex_info": (I, [P, I, P, P, P]),
         "lkg_score": (I, [P, I, I, P, P, P]), "lkg_score_device": (I, [P, I, I, P, P, P]),
         "lkg_score_multi_device": (I, [P, I, P, P, P, P, P]),
+        "lkg_score_multi": (I, [P, I, P, P, P, P, P]),
         "lkg_field_build": (I, [P, P, I32, P, P, P, P]), "lkg_lr_sasa": (I, [P, P, I32, P]),
         "lkg_synth_chain": (I, [U64, I32, D, D, D, I32, P, P]),
         "lkg_rng_new": (P, [U64]), "lkg_rng_f64": (D, [P]), "lkg_rng_free": (None, [P]),
@@ -94,6 +95,13 @@ def lib():
         f.argtypes = args
     _lib = L
     return L
+
+
+def _addr(a):
+    """Address of a contiguous numpy array or a (CPU, possibly pinned) torch tensor."""
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
 
 
 def _check(status):
@@ -180,6 +188,19 @@ class Context:
         counts = np.ascontiguousarray(counts, np.int32)
         _check(lib().lkg_score_multi_device(self.h, len(ids), ptr(ids), ptr(counts), C.c_void_p(d_poses),
                                             C.c_void_p(d_scores), C.c_void_p(d_parts) if d_parts else None))
+
+    def score_multi(self, ids, counts, poses, scores=None, parts=None):
+        """Host-buffer batch over many complexes (one launch group); poses is
+        sum(counts) x 7.  Page-locked arrays are DMA'd without staging."""
+        ids = np.ascontiguousarray(ids, np.int32)
+        counts = np.ascontiguousarray(counts, np.int32)
+        n = int(counts.sum())
+        if scores is None:
+            scores = np.zeros(n)
+        _check(lib().lkg_score_multi(self.h, len(ids), ptr(ids), ptr(counts), C.c_void_p(_addr(poses)),
+                                     C.c_void_p(_addr(scores)), C.c_void_p(_addr(parts)) if parts is not None
+                                     else None))
+        return scores
 
     @property
     def stream(self):

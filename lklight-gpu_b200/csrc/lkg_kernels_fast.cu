@@ -8,7 +8,7 @@ cudaError_t launch_score_fast(const LaunchParams& p, int threads, int blocks, cu
     return cudaGetLastError();
 }
 
-size_t desolv_smem_bytes(int hcap, bool exact) { return (size_t)hcap * (exact ? 12 : 8); }
+size_t desolv_smem_bytes(int hcap, bool /*exact*/) { return (size_t)hcap * 12; }
 
 cudaError_t launch_desolv_fast(const LaunchParams& p, int threads, int blocks, int hcap, cudaStream_t s) {
     size_t sm = desolv_smem_bytes(hcap, false);

@@ -151,9 +151,11 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     d.ncx = nc[0]; d.ncy = nc[1]; d.ncz = nc[2];
     d.ox = o[0]; d.oy = o[1]; d.oz = o[2]; d.h = h; d.inv_h = inv_h;
     cr.n_cells = (int)ncell;
-    // desolvation hash capacity: >= 2 x receptor atoms up to 16384 slots
+    // desolvation hash capacity: >= 2 x receptor atoms up to 8192 slots
+    // (96 KB of shared memory); a pose touching more receptor atoms within
+    // 6.4 A reports LKG_ERR_CAPACITY
     int cap = 64;
-    while (cap < 2 * n && cap < 16384) cap <<= 1;
+    while (cap < 2 * n && cap < 8192) cap <<= 1;
     d.hcap = cap;
     return set_ok();
 }
@@ -627,6 +629,57 @@ int lkg_score(lkg_ctx* ctx, int id, int n, const double* poses, double* scores, 
     if ((st = check_status(ctx))) return st;
     memcpy(scores, ctx->h_out.p, ob);
     if (parts) memcpy(parts, ctx->h_out.as<char>() + ob, qb);
+    return set_ok();
+}
+
+int lkg_score_multi(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, const double* poses,
+                    double* scores, double* parts) {
+    if (!ctx || n_items < 0 || (n_items && (!ids || !counts || !poses || !scores)))
+        return set_error(LKG_ERR_ARG, "bad items");
+    size_t n = 0;
+    for (int i = 0; i < n_items; ++i) {
+        if (counts[i] < 0) return set_error(LKG_ERR_ARG, "negative pose count");
+        n += (size_t)counts[i];
+    }
+    if (n == 0) return set_ok();
+    cudaSetDevice(ctx->device);
+    const size_t pb = n * 7 * sizeof(double), ob = n * sizeof(double), qb = n * 4 * sizeof(double);
+    LKG_CK(ctx->d_poses.reserve(pb), "staging");
+    LKG_CK(ctx->d_scores.reserve(ob), "staging");
+    LKG_CK(ctx->d_parts.reserve(qb), "staging");
+    // page-locked caller buffers are DMA'd directly; pageable ones go
+    // through the context's pinned staging buffer
+    auto pinned = [](const void* p) {
+        cudaPointerAttributes a;
+        if (cudaPointerGetAttributes(&a, p) != cudaSuccess) { cudaGetLastError(); return false; }
+        return a.type == cudaMemoryTypeHost;
+    };
+    const bool pin_in = pinned(poses), pin_out = pinned(scores) && (!parts || pinned(parts));
+    const double* src = poses;
+    if (!pin_in) {
+        LKG_CK(ctx->h_poses.reserve(pb), "staging");
+        memcpy(ctx->h_poses.p, poses, pb);
+        src = ctx->h_poses.as<double>();
+    }
+    LKG_CK(cudaMemcpyAsync(ctx->d_poses.p, src, pb, cudaMemcpyHostToDevice, ctx->stream), "pose upload");
+    int st = launch_items(ctx, n_items, ids, counts, ctx->d_poses.as<double>(), ctx->d_scores.as<double>(),
+                          parts ? ctx->d_parts.as<double>() : nullptr, 0, 0, nullptr, nullptr);
+    if (st) return st;
+    double* dst_s = scores;
+    double* dst_p = parts;
+    if (!pin_out) {
+        LKG_CK(ctx->h_out.reserve(ob + qb), "staging");
+        dst_s = ctx->h_out.as<double>();
+        dst_p = parts ? (double*)(ctx->h_out.as<char>() + ob) : nullptr;
+    }
+    LKG_CK(cudaMemcpyAsync(dst_s, ctx->d_scores.p, ob, cudaMemcpyDeviceToHost, ctx->stream), "score readback");
+    if (parts) LKG_CK(cudaMemcpyAsync(dst_p, ctx->d_parts.p, qb, cudaMemcpyDeviceToHost, ctx->stream), "parts readback");
+    if ((st = wait_stream(ctx, 300.0))) return st;
+    if ((st = check_status(ctx))) return st;
+    if (!pin_out) {
+        memcpy(scores, dst_s, ob);
+        if (parts) memcpy(parts, dst_p, qb);
+    }
     return set_ok();
 }
 

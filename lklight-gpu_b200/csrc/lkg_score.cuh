@@ -213,11 +213,8 @@ __device__ __forceinline__ void pair_exact(unsigned flags, int lj_form, double q
     }
 }
 
-// g(min d^2) of the desolvation sum (cpydock.rs:648-668)
-__device__ __forceinline__ float solv_term(float d2, float asa) {
-    if (d2 <= SOLV2_F && d2 > 0.f && asa > 0.f) return fminf(-10.f * sqrtf(d2) + 65.f, asa);
-    return 0.f;
-}
+// g(min d^2) of the desolvation sum (cpydock.rs:648-668), asa > 0 atoms;
+// the constant contribution of asa < 0 atoms is added on the host side
 __device__ __forceinline__ double solv_term(double d2, double asa) {
     double sv = 0.0;
     if (d2 <= SOLV2_D && d2 > 0.0 && asa > 0.0) sv = -10.0 * sqrt(d2) + 65.0;
@@ -225,26 +222,10 @@ __device__ __forceinline__ double solv_term(double d2, double asa) {
     return sv;
 }
 
-// receptor-minimum hash in shared memory (open addressing, bounded probes)
-template <typename R> struct MinHash;
-template <> struct MinHash<float> {
-    int* keys; int* vals; int cap;
-    __device__ void init(char* smem, int cap_) {
-        cap = cap_; keys = (int*)smem; vals = keys + cap;
-        for (int s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = -1; vals[s] = 0x7f7fffff; }
-    }
-    __device__ bool insert(int k, float d2) {
-        unsigned h = ((unsigned)k * 2654435761u) & (unsigned)(cap - 1);
-        for (int probe = 0; probe < cap; ++probe) {
-            int prev = atomicCAS(keys + h, -1, k);
-            if (prev == -1 || prev == k) { atomicMin(vals + h, __float_as_int(d2)); return true; }
-            h = (h + 1) & (unsigned)(cap - 1);
-        }
-        return false;
-    }
-    __device__ float value(int s) const { return __int_as_float(vals[s]); }
-};
-template <> struct MinHash<double> {
+// receptor-minimum hash in shared memory (open addressing, bounded probes):
+// key = position-sorted receptor index, value = f64 bits of the minimum d^2
+// (non-negative doubles order like their bit patterns, so atomicMin works)
+struct MinHash {
     int* keys; unsigned long long* vals; int cap;
     __device__ void init(char* smem, int cap_) {
         cap = cap_; vals = (unsigned long long*)smem; keys = (int*)(vals + cap);
@@ -274,12 +255,17 @@ template <typename R> struct Atom;
 template <> struct Atom<float> {
     template <bool DESOLV>
     __device__ static void run(const ComplexDev& c, const Rot& rot, int j, AtomAcc& acc,
-                               float& min_l, MinHash<float>* hash, int* status,
+                               double& min_l, MinHash* hash, int* status,
                                float* out_e, float* out_v) {
         float4 b = Tr<float>::lpos(c, j);
         float4 lp = Tr<float>::lpar(c, j);
         double xd, yd, zd;
-        apply(rot, (double)b.x, (double)b.y, (double)b.z, xd, yd, zd);
+        if (DESOLV) {
+            double4 b64 = c.lpos64[j];
+            apply(rot, b64.x, b64.y, b64.z, xd, yd, zd);
+        } else {
+            apply(rot, (double)b.x, (double)b.y, (double)b.z, xd, yd, zd);
+        }
         float x = (float)xd, y = (float)yd, z = (float)zd;
         const float qj = b.w, svj = lp.x, rj = lp.y;
         const bool hj = lp.z != 0.f, lf = lp.w != 0.f;
@@ -295,9 +281,15 @@ template <> struct Atom<float> {
                 float4 pr = Tr<float>::rpar(c, k);
                 ++np;
                 pair_fast(flags, qj, svj, rj, hj, a, pr, d2, elec, vdw);
-                if (DESOLV && !lf && pr.w == 0.f) {
-                    min_l = fminf(min_l, d2);
-                    if (d2 <= SOLV2_F && !hash->insert(k, d2)) atomicOr(status, 1);
+                // desolvation minima in f64 (the g(d^2) step at 6.4 A makes
+                // f32 distances too coarse near the threshold); only pairs
+                // that can be within 6.4 A pay for it
+                if (DESOLV && !lf && pr.w == 0.f && d2 <= SOLV2_F * 1.001f) {
+                    double4 a64 = c.rpos64[k];
+                    double ex = xd - a64.x, ey = yd - a64.y, ez = zd - a64.z;
+                    double d2d = ex * ex + ey * ey + ez * ez;
+                    min_l = fmin(min_l, d2d);
+                    if (d2d <= SOLV2_D && !hash->insert(k, d2d)) atomicOr(status, 1);
                 }
             }
         });
@@ -312,7 +304,7 @@ template <> struct Atom<float> {
 template <> struct Atom<double> {
     template <bool DESOLV>
     __device__ static void run(const ComplexDev& c, const Rot& rot, int j, AtomAcc& acc,
-                               double& min_l, MinHash<double>* hash, int* status,
+                               double& min_l, MinHash* hash, int* status,
                                float* out_e, float* out_v) {
         double4 b = Tr<double>::lpos(c, j);
         double4 lp = Tr<double>::lpar(c, j);
@@ -446,7 +438,7 @@ __global__ void __launch_bounds__(256) k_score_tiles(LaunchParams p) {
         AtomAcc acc{0.0, 0.0, 0};
         if (j < c.nl && threadIdx.x < p.tile) {
             const Rot rot = pose_matrix(p.poses + 7 * g);
-            R dummy_min = (R)0;
+            double dummy_min = 0.0;
             const bool atom_out = p.atom_elec && b == 0 && pose == 0;
             Atom<R>::template run<false>(c, rot, j, acc, dummy_min, nullptr, p.status,
                                          atom_out ? p.atom_elec : nullptr, atom_out ? p.atom_vdw : nullptr);
@@ -492,7 +484,7 @@ __global__ void __launch_bounds__(512) k_score_desolv(LaunchParams p) {
         const ComplexDev& c = p.cx[__ldg(p.item_complex + b)];
         const int pose = (int)(w - __ldg(p.item_work0 + b));
         const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
-        MinHash<R> hash;
+        MinHash hash;
         hash.init(smem, c.hcap);
         __syncthreads();
         const Rot rot = pose_matrix(p.poses + 7 * g);
@@ -500,35 +492,23 @@ __global__ void __launch_bounds__(512) k_score_desolv(LaunchParams p) {
         double solv_l = 0.0;
         const bool want_pairs = !p.solv_only;
         for (int j = threadIdx.x; j < c.nl; j += blockDim.x) {
-            R min_l = (R)1e30;
+            double min_l = 1e300;
             AtomAcc a1{0.0, 0.0, 0};
             Atom<R>::template run<true>(c, rot, j, a1, min_l, &hash, p.status, nullptr, nullptr);
             if (want_pairs) { acc.elec += a1.elec; acc.vdw += a1.vdw; }
             acc.np += a1.np;
-            if (sizeof(R) == 4) {
-                float2 ls = Tr<float>::lsolv(c, j);
-                solv_l += (double)(solv_term((float)min_l, ls.y) * ls.x);
-            } else {
-                double2 ls = c.lsolv64[j];
-                solv_l += solv_term((double)min_l, ls.y) * ls.x;
-            }
+            double2 ls = c.lsolv64[j];
+            solv_l += solv_term(min_l, ls.y) * ls.x;
         }
         __syncthreads();
-        // receptor side: fixed-point sum over hash slots (slot order depends on
-        // insertion races; integer sums do not)
+        // receptor side: fixed-point (2^-40) sum over hash slots; slot order
+        // depends on insertion races, integer sums do not
         long long fix = 0;
         for (int s = threadIdx.x; s < c.hcap; s += blockDim.x) {
             int k = hash.keys[s];
             if (k < 0) continue;
-            double term;
-            if (sizeof(R) == 4) {
-                float2 rs = Tr<float>::rsolv(c, k);
-                term = (double)(solv_term((float)hash.value(s), rs.y) * rs.x);
-            } else {
-                double2 rs = c.rsolv64[k];
-                term = solv_term((double)hash.value(s), rs.y) * rs.x;
-            }
-            fix += __double2ll_rn(term * 4294967296.0);
+            double2 rs = c.rsolv64[k];
+            fix += __double2ll_rn(solv_term(hash.value(s), rs.y) * rs.x * 1099511627776.0);
         }
         fix = warp_sum(fix);
         if ((threadIdx.x & 31) == 0) s_fix[threadIdx.x >> 5] = fix;
@@ -537,7 +517,7 @@ __global__ void __launch_bounds__(512) k_score_desolv(LaunchParams p) {
         if (threadIdx.x == 0) {
             long long f = 0;
             for (int i = 0; i < (int)((blockDim.x + 31) >> 5); ++i) f += s_fix[i];
-            double solv = v[2] + (double)f * (1.0 / 4294967296.0);
+            double solv = v[2] + (double)f * (1.0 / 1099511627776.0);
             write_pose(p, c, g, v[0], v[1], solv, v[3]);
         }
         __syncthreads();
