@@ -53,6 +53,7 @@ def parse():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--cell", type=float, default=0.0)
+    ap.add_argument("--group", type=int, default=0)
     return ap.parse_args()
 
 
@@ -182,7 +183,7 @@ def main():
     lkg = importlib.import_module("lklight-gpu_b200")
 
     items = workload(args.workload)
-    ctx = lkg.Context(device=local, tile=args.tile, cell=args.cell)
+    ctx = lkg.Context(device=local, tile=args.tile, cell=args.cell, group=args.group)
     stream = torch.cuda.ExternalStream(ctx.stream)
     ids = [ctx.add_complex(it["family"], it["rec"], it["lig"]) for it in items]
     counts = [len(it["poses"]) for it in items]

@@ -146,8 +146,12 @@ typedef struct {
 int lkg_ctx_create(int device, lkg_ctx** out);
 int lkg_ctx_destroy(lkg_ctx* ctx);
 int lkg_ctx_set_precision(lkg_ctx* ctx, int precision);
-/* Tile shape for subsequent launches (0 = autotuned / default). */
+/* Tile shape: ligand atoms per work unit (64, 128 or 256) and the receptor
+ * fine-cell edge in 1/1000 A; 0 keeps the current value. */
 int lkg_ctx_set_tiles(lkg_ctx* ctx, int threads_per_block, int cell_size_milli_angstrom);
+/* Ligand atoms per candidate-search group of the warp-cooperative kernel
+ * (8, 16 or 32; default 8); fixed once complexes exist. */
+int lkg_ctx_set_group(lkg_ctx* ctx, int group);
 /* Work on this CUDA stream (cudaStream_t) instead of the context's own. */
 int lkg_ctx_set_stream(lkg_ctx* ctx, void* stream);
 void* lkg_ctx_stream(lkg_ctx* ctx);
@@ -183,6 +187,24 @@ int lkg_score_multi(lkg_ctx* ctx, int n_items, const int* complex_ids, const int
 
 /* Kernel launches made by this context so far (for launch accounting). */
 int64_t lkg_ctx_launches(lkg_ctx* ctx);
+/* Wait (bounded host poll) for the context stream and check the device
+ * status word (LKG_ERR_CAPACITY after a desolvation-hash overflow). */
+int lkg_ctx_sync(lkg_ctx* ctx);
+
+/* Plans: one batch (complexes x pose counts) prepared once — descriptors,
+ * item tables and the plan's own scratch on the device — so that a launch
+ * is kernel launches only.  lkg_plan_capture records n_launches launches
+ * on the context stream into a CUDA graph; lkg_plan_replay launches it.
+ * Adding complexes to the context afterwards invalidates the graph
+ * (replay returns LKG_ERR_STATE).  Plans of one context must not run
+ * concurrently with each other on different streams. */
+typedef struct lkg_plan lkg_plan;
+int lkg_plan_create(lkg_ctx* ctx, int n_items, const int* complex_ids, const int* counts, lkg_plan** out);
+int lkg_plan_launch(lkg_plan* plan, const double* d_poses, double* d_scores, double* d_parts);
+int lkg_plan_capture(lkg_plan* plan, const double* d_poses, double* d_scores, double* d_parts, int n_launches);
+int lkg_plan_replay(lkg_plan* plan);
+int lkg_plan_sync(lkg_plan* plan);
+int lkg_plan_destroy(lkg_plan* plan);
 
 /* ---------------------------------------------------------------------- */
 /* Setup helpers (host)                                                    */

@@ -71,11 +71,15 @@ def lib():
         "lkg_version": (C.c_char_p, []),
         "lkg_ctx_create": (I, [I, P]), "lkg_ctx_destroy": (I, [P]),
         "lkg_ctx_set_precision": (I, [P, I]), "lkg_ctx_set_tiles": (I, [P, I, I]),
-        "lkg_ctx_set_stream": (I, [P, P]), "lkg_ctx_stream": (P, [P]), "lkg_ctx_launches": (I64, [P]),
+        "lkg_ctx_set_stream": (I, [P, P]), "lkg_ctx_set_group": (I, [P, I]), "lkg_ctx_stream": (P, [P]), "lkg_ctx_launches": (I64, [P]),
         "lkg_complex_add": (I, [P, I, P, P, P, P]), "lkg_complex_info": (I, [P, I, P, P, P]),
         "lkg_score": (I, [P, I, I, P, P, P]), "lkg_score_device": (I, [P, I, I, P, P, P]),
         "lkg_score_multi_device": (I, [P, I, P, P, P, P, P]),
         "lkg_score_multi": (I, [P, I, P, P, P, P, P]),
+        "lkg_ctx_sync": (I, [P]),
+        "lkg_plan_create": (I, [P, I, P, P, P]), "lkg_plan_launch": (I, [P, P, P, P]),
+        "lkg_plan_capture": (I, [P, P, P, P, I]), "lkg_plan_replay": (I, [P]),
+        "lkg_plan_sync": (I, [P]), "lkg_plan_destroy": (I, [P]),
         "lkg_field_build": (I, [P, P, I32, P, P, P, P]), "lkg_lr_sasa": (I, [P, P, I32, P]),
         "lkg_synth_chain": (I, [U64, I32, D, D, D, I32, P, P]),
         "lkg_rng_new": (P, [U64]), "lkg_rng_f64": (D, [P]), "lkg_rng_free": (None, [P]),
@@ -137,7 +141,7 @@ def make_mol(m, keep):
 class Context:
     """A device context: resident complexes, a stream, scratch buffers."""
 
-    def __init__(self, device=0, precision="fast", tile=0, cell=0.0):
+    def __init__(self, device=0, precision="fast", tile=0, cell=0.0, group=0):
         h = C.c_void_p()
         _check(lib().lkg_ctx_create(device, C.byref(h)))
         self.h = h
@@ -146,6 +150,8 @@ class Context:
             _check(lib().lkg_ctx_set_precision(self.h, PREC_EXACT if precision == "exact" else PREC_FAST))
         if tile or cell:
             _check(lib().lkg_ctx_set_tiles(self.h, int(tile), int(round(cell * 1000))))
+        if group:
+            _check(lib().lkg_ctx_set_group(self.h, int(group)))
 
     def set_precision(self, precision):
         _check(lib().lkg_ctx_set_precision(self.h, PREC_EXACT if precision == "exact" else PREC_FAST))
@@ -202,6 +208,13 @@ class Context:
                                      else None))
         return scores
 
+    def sync(self):
+        """Bounded wait for the context stream + device status check."""
+        _check(lib().lkg_ctx_sync(self.h))
+
+    def plan(self, ids, counts):
+        return Plan(self, ids, counts)
+
     @property
     def stream(self):
         return lib().lkg_ctx_stream(self.h)
@@ -216,6 +229,43 @@ class Context:
     def close(self):
         if getattr(self, "h", None):
             lib().lkg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Plan:
+    """A batch prepared once; launches are capturable in a CUDA graph."""
+
+    def __init__(self, ctx, ids, counts):
+        self.ctx = ctx
+        ids = np.ascontiguousarray(ids, np.int32)
+        counts = np.ascontiguousarray(counts, np.int32)
+        h = C.c_void_p()
+        _check(lib().lkg_plan_create(ctx.h, len(ids), ptr(ids), ptr(counts), C.byref(h)))
+        self.h = h
+
+    def launch(self, d_poses, d_scores, d_parts=0):
+        _check(lib().lkg_plan_launch(self.h, C.c_void_p(d_poses), C.c_void_p(d_scores),
+                                     C.c_void_p(d_parts) if d_parts else None))
+
+    def capture(self, d_poses, d_scores, d_parts=0, n_launches=1):
+        _check(lib().lkg_plan_capture(self.h, C.c_void_p(d_poses), C.c_void_p(d_scores),
+                                      C.c_void_p(d_parts) if d_parts else None, n_launches))
+
+    def replay(self):
+        _check(lib().lkg_plan_replay(self.h))
+
+    def sync(self):
+        _check(lib().lkg_plan_sync(self.h))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().lkg_plan_destroy(self.h)
             self.h = None
 
     def __del__(self):

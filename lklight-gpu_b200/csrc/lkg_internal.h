@@ -2,7 +2,7 @@
 //
 // Device layout of one complex (all arrays in HBM, built once per complex):
 //   receptor atoms sorted by a fine uniform cell grid (cell edge h, default
-//   10/3 A, cells x-fastest), so that one (z, y) row of consecutive x cells
+//   2.5 A, cells x-fastest), so that one (z, y) row of consecutive x cells
 //   is one contiguous span of atoms [cell_start[row+cx0], cell_start[row+cx1+1]);
 //     rpos  float4 (x, y, z, q)              rpos64 double4 (same, f64)
 //     rpar  float4 (sqrt eps, r, heavy, excl) rpar64 double4 (sqrt eps, r, eps, heavy)
@@ -46,6 +46,8 @@ struct ComplexDev {
     const double4* lpar64;
     const double2* lsolv64;
     const int* lorig;
+    const float4* lgrp;      // per group of `group` atoms: ligand-frame centre, radius
+    int group;               // ligand atoms per candidate-search group
     int ntiles;              // ceil(nl / tile)
     // far field
     const float* phi;
@@ -67,17 +69,18 @@ struct LaunchParams {
     int n_items;
     long long total_work;
     int tile;                    // ligand atoms per work unit (non-desolv kernel)
+    int group;                   // ligand atoms per candidate-search group
     const double* poses;         // global N x 7 (w,x,y,z,tx,ty,tz)
     double* scores;              // [N] final score, or N x 2 raw (elec, vdw) when raw_pairs
     double* parts;               // [N x 4] or null: elec_raw, vdw, solv, near pairs
     int raw_pairs;               // compat: scores holds (elec_raw, vdw) pairs
     int solv_only;               // compat cuda_cpydock_solv: scores[k] = S
     // scratch (self-resetting between launches)
-    double* partials;            // [N x max_tiles x 4]
+    double* partials;            // [total_work x 4] per-unit partial sums
     int* pose_counter;           // [N]
     unsigned long long* work_counter;  // [2]: next unit, CTAs done
     int* status;                 // [4]: error flags (capacity overflow, bad index)
-    int max_tiles;
+    int max_tiles;               // unused by the kernels (kept for layout)
     // per-atom outputs (cuda_full_score): pose 0 of item 0, caller atom order
     float* atom_elec;
     float* atom_vdw;

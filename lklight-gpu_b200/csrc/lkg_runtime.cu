@@ -13,7 +13,7 @@
 
 namespace lkg {
 
-int max_blocks_score_fast(int threads);
+int max_blocks_score_fast(int threads, int group);
 int max_blocks_desolv_fast(int threads, int hcap);
 int max_blocks_score_exact(int threads);
 int max_blocks_desolv_exact(int threads, int hcap);
@@ -189,7 +189,27 @@ int build_ligand(lkg_ctx* ctx, const MolIn& L, ComplexRec& cr) {
         par64[k] = make_double4(L.svdw[i], L.rad[i], L.eps[i], L.heavy[i] ? 1.0 : 0.0);
         sol64[k] = make_double2(L.des[i], L.asa[i]);
     }
+    // bounding sphere of every group of ctx->group consecutive atoms (ligand
+    // frame), for the warp-cooperative kernel's candidate search
+    const int G = ctx->group;
+    const int ngrp = (n + G - 1) / G;
+    std::vector<float4> grp(std::max(ngrp, 1));
+    for (int gi = 0; gi < ngrp; ++gi) {
+        const int a0 = gi * G, a1 = std::min(n, a0 + G);
+        double cen[3] = {0, 0, 0};
+        for (int k = a0; k < a1; ++k)
+            for (int a = 0; a < 3; ++a) cen[a] += L.c[3 * order[k] + a];
+        for (int a = 0; a < 3; ++a) cen[a] /= (a1 - a0);
+        double r2 = 0;
+        for (int k = a0; k < a1; ++k) {
+            double dd = 0;
+            for (int a = 0; a < 3; ++a) dd += (L.c[3 * order[k] + a] - cen[a]) * (L.c[3 * order[k] + a] - cen[a]);
+            r2 = std::max(r2, dd);
+        }
+        grp[gi] = make_float4((float)cen[0], (float)cen[1], (float)cen[2], (float)(std::sqrt(r2) * (1.0 + 1e-6) + 1e-3));
+    }
     cudaStream_t s = ctx->stream;
+    LKG_CK(upload(cr.lgrp, grp, s), "upload ligand");
     LKG_CK(upload(cr.lpos, pos, s), "upload ligand");
     LKG_CK(upload(cr.lpar, par, s), "upload ligand");
     LKG_CK(upload(cr.lsolv, sol, s), "upload ligand");
@@ -202,6 +222,8 @@ int build_ligand(lkg_ctx* ctx, const MolIn& L, ComplexRec& cr) {
     d.lpos = cr.lpos.as<float4>(); d.lpar = cr.lpar.as<float4>(); d.lsolv = cr.lsolv.as<float2>();
     d.lpos64 = cr.lpos64.as<double4>(); d.lpar64 = cr.lpar64.as<double4>(); d.lsolv64 = cr.lsolv64.as<double2>();
     d.lorig = cr.lorig.as<int>();
+    d.lgrp = cr.lgrp.as<float4>();
+    d.group = G;
     d.ntiles = std::max(1, (n + ctx->tile - 1) / ctx->tile);
     return set_ok();
 }
@@ -243,41 +265,12 @@ int build_field(lkg_ctx* ctx, const MolIn& R, const lkg_field* f, bool build, Co
     return set_ok();
 }
 
-int sync_descriptors(lkg_ctx* ctx) {
-    if (!ctx->cx_dirty) return 0;
-    std::vector<ComplexDev> v;
-    for (auto& c : ctx->cx) v.push_back(c->d);
-    LKG_CK(upload(ctx->d_cx, v, ctx->stream), "descriptor upload");
-    LKG_CK(cudaStreamSynchronize(ctx->stream), "descriptor upload");
-    ctx->cx_dirty = false;
-    return 0;
-}
-
-int ensure_scratch(lkg_ctx* ctx, size_t n_poses, size_t max_tiles) {
-    if (n_poses <= ctx->cap_poses && max_tiles <= ctx->cap_tiles && ctx->status.p) return 0;
-    size_t np = std::max(n_poses, ctx->cap_poses), nt = std::max(max_tiles, ctx->cap_tiles);
-    np = std::max<size_t>(np, 1024);
-    LKG_CK(cudaStreamSynchronize(ctx->stream), "scratch");
-    LKG_CK(ctx->partials.reserve(np * nt * 4 * sizeof(double)), "scratch alloc");
-    LKG_CK(ctx->pose_counter.reserve(np * sizeof(int)), "scratch alloc");
-    LKG_CK(cudaMemset(ctx->pose_counter.p, 0, np * sizeof(int)), "scratch clear");
-    if (!ctx->work_counter.p) {
-        LKG_CK(ctx->work_counter.reserve(2 * sizeof(unsigned long long)), "scratch alloc");
-        LKG_CK(cudaMemset(ctx->work_counter.p, 0, 2 * sizeof(unsigned long long)), "scratch clear");
-        LKG_CK(ctx->status.reserve(4 * sizeof(int)), "scratch alloc");
-        LKG_CK(cudaMemset(ctx->status.p, 0, 4 * sizeof(int)), "scratch clear");
-    }
-    ctx->cap_poses = np;
-    ctx->cap_tiles = nt;
-    return 0;
-}
-
 int occupancy(lkg_ctx* ctx, bool desolv, bool exact, int threads, int hcap) {
     Occupancy& o = desolv ? ctx->occ_desolv[exact] : ctx->occ_tiles[exact];
     if (o.threads == threads && o.hcap == hcap && o.blocks > 0) return o.blocks;
     int b;
     if (desolv) b = exact ? max_blocks_desolv_exact(threads, hcap) : max_blocks_desolv_fast(threads, hcap);
-    else b = exact ? max_blocks_score_exact(threads) : max_blocks_score_fast(threads);
+    else b = exact ? max_blocks_score_exact(threads) : max_blocks_score_fast(threads, ctx->group);
     o.threads = threads; o.hcap = hcap; o.blocks = std::max(1, b);
     return o.blocks;
 }
@@ -310,97 +303,153 @@ int complex_set_ligand(lkg_ctx* ctx, int id, const MolIn& lig) {
     return st;
 }
 
-int launch_items(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, const double* d_poses,
-                 double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e,
-                 float* atom_v) {
-    if (n_items <= 0) return set_ok();
+int sync_descriptors(lkg_ctx* ctx) {
+    if (!ctx->cx_dirty) return 0;
+    std::vector<ComplexDev> v;
+    for (auto& c : ctx->cx) v.push_back(c->d);
+    LKG_CK(upload(ctx->d_cx, v, ctx->stream), "descriptor upload");
+    LKG_CK(cudaStreamSynchronize(ctx->stream), "descriptor upload");
+    ctx->cx_dirty = false;
+    return 0;
+}
+
+cudaError_t Scratch::ensure(size_t units, size_t poses, cudaStream_t s) {
+    cudaError_t e;
+    if (!status.p) {
+        if ((e = work_counter.reserve(2 * sizeof(unsigned long long))) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(work_counter.p, 0, 2 * sizeof(unsigned long long), s)) != cudaSuccess) return e;
+        if ((e = status.reserve(4 * sizeof(int))) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(status.p, 0, 4 * sizeof(int), s)) != cudaSuccess) return e;
+    }
+    if (units > cap_units) {
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+        units = std::max<size_t>(units, 4096);
+        if ((e = partials.reserve(units * 4 * sizeof(double))) != cudaSuccess) return e;
+        cap_units = units;
+    }
+    if (poses > cap_poses) {
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+        poses = std::max<size_t>(poses, 1024);
+        if ((e = pose_counter.reserve(poses * sizeof(int))) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(pose_counter.p, 0, poses * sizeof(int), s)) != cudaSuccess) return e;
+        cap_poses = poses;
+    }
+    return cudaSuccess;
+}
+
+void Group::pack(char* dst) const {
+    const size_t ni = ic.size();
+    memcpy(dst, w0.data(), (ni + 1) * sizeof(long long));
+    int* t = (int*)(dst + (ni + 1) * sizeof(long long));
+    memcpy(t, ic.data(), ni * sizeof(int));
+    memcpy(t + ni, ip0.data(), ni * sizeof(int));
+    memcpy(t + 2 * ni, inp.data(), ni * sizeof(int));
+}
+
+int build_groups(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, Group g[2], size_t* n_poses) {
     for (int i = 0; i < n_items; ++i) {
         if (ids[i] < 0 || ids[i] >= (int)ctx->cx.size()) return set_error(LKG_ERR_ARG, "bad complex id %d", ids[i]);
         if (counts[i] < 0) return set_error(LKG_ERR_ARG, "negative pose count");
     }
-    int st;
-    if ((st = sync_descriptors(ctx))) return st;
-    const bool exact = ctx->precision == LKG_PREC_EXACT;
-    size_t n_poses = 0, max_tiles = 1;
+    g[0] = Group();
+    g[1] = Group();
+    g[1].kind = 1;
+    long long pose0 = 0;
     for (int i = 0; i < n_items; ++i) {
-        n_poses += (size_t)counts[i];
-        max_tiles = std::max<size_t>(max_tiles, (size_t)ctx->cx[ids[i]]->d.ntiles);
+        const ComplexDev& d = ctx->cx[ids[i]]->d;
+        const int k = (d.flags & F_DESOLV) ? 1 : 0;
+        if (counts[i] > 0) {
+            Group& G = g[k];
+            G.ic.push_back(ids[i]);
+            G.ip0.push_back((int)pose0);
+            G.inp.push_back(counts[i]);
+            G.w0.push_back(G.w0.back() + (k ? (long long)counts[i] : (long long)counts[i] * d.ntiles));
+            G.hcap = std::max(G.hcap, d.hcap);
+        }
+        pose0 += counts[i];
     }
+    *n_poses = (size_t)pose0;
+    return set_ok();
+}
+
+int launch_group(lkg_ctx* ctx, const Group& G, const char* db, Scratch& sc, const double* d_poses,
+                 double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e, float* atom_v) {
+    const bool exact = ctx->precision == LKG_PREC_EXACT;
+    const int ni = (int)G.ic.size();
+    LaunchParams p{};
+    p.cx = ctx->d_cx.as<ComplexDev>();
+    p.item_work0 = (const long long*)db;
+    p.item_complex = (const int*)(db + (size_t)(ni + 1) * sizeof(long long));
+    p.item_pose0 = p.item_complex + ni;
+    p.item_npose = p.item_complex + 2 * ni;
+    p.n_items = ni;
+    p.total_work = G.w0.back();
+    p.tile = ctx->tile;
+    p.group = ctx->group;
+    p.poses = d_poses;
+    p.scores = d_scores;
+    p.parts = d_parts;
+    p.raw_pairs = raw_pairs;
+    p.solv_only = solv_only;
+    p.partials = sc.partials.as<double>();
+    p.pose_counter = sc.pose_counter.as<int>();
+    p.work_counter = sc.work_counter.as<unsigned long long>();
+    p.status = sc.status.as<int>();
+    p.max_tiles = 0;
+    p.atom_elec = atom_e;
+    p.atom_vdw = atom_v;
+    cudaError_t e;
+    if (G.kind == 0) {
+        int threads = ctx->tile;
+        long long blocks = (long long)ctx->sm_count * occupancy(ctx, false, exact, threads, 0);
+        blocks = std::max(1LL, std::min(blocks, p.total_work));
+        e = exact ? launch_score_exact(p, threads, (int)blocks, ctx->stream)
+                  : launch_score_fast(p, threads, (int)blocks, ctx->stream);
+    } else {
+        int threads = ctx->desolv_threads;
+        size_t smem = desolv_smem_bytes(G.hcap, exact);
+        if (smem > 227 * 1024) return set_error(LKG_ERR_CAPACITY, "desolvation hash too large");
+        long long blocks = (long long)ctx->sm_count * occupancy(ctx, true, exact, threads, G.hcap);
+        blocks = std::max(1LL, std::min(blocks, p.total_work));
+        e = exact ? launch_desolv_exact(p, threads, (int)blocks, G.hcap, ctx->stream)
+                  : launch_desolv_fast(p, threads, (int)blocks, G.hcap, ctx->stream);
+    }
+    if (e != cudaSuccess) return set_error(cuda_to_status(e), "score launch: %s", cudaGetErrorString(e));
+    ctx->launches++;
+    return set_ok();
+}
+
+int launch_items(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, const double* d_poses,
+                 double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e,
+                 float* atom_v) {
+    if (n_items <= 0) return set_ok();
+    Group g[2];
+    size_t n_poses = 0;
+    int st;
+    if ((st = build_groups(ctx, n_items, ids, counts, g, &n_poses))) return st;
     if (n_poses == 0) return set_ok();
-    if ((st = ensure_scratch(ctx, n_poses, max_tiles))) return st;
-    // two groups: tile kernel and fused-desolvation kernel
-    for (int grp = 0; grp < 2; ++grp) {
-        std::vector<int> ic, ip0, inp;
-        std::vector<long long> w0{0};
-        long long pose0 = 0;
-        int hcap = 64;
-        for (int i = 0; i < n_items; ++i) {
-            const ComplexDev& d = ctx->cx[ids[i]]->d;
-            bool des = (d.flags & F_DESOLV) != 0;
-            if (des == (grp == 1) && counts[i] > 0) {
-                ic.push_back(ids[i]);
-                ip0.push_back((int)pose0);
-                inp.push_back(counts[i]);
-                long long units = des ? (long long)counts[i] : (long long)counts[i] * d.ntiles;
-                w0.push_back(w0.back() + units);
-                hcap = std::max(hcap, d.hcap);
-            }
-            pose0 += counts[i];
-        }
-        if (ic.empty()) continue;
-        const int ni = (int)ic.size();
-        size_t bytes = (size_t)ni * 3 * sizeof(int) + (size_t)(ni + 1) * sizeof(long long) + 64;
-        LKG_CK(ctx->h_items.reserve(bytes * 2), "item staging");
-        LKG_CK(ctx->d_items.reserve(bytes * 2), "item staging");
-        // group 1 uses the second half so both tables can be in flight
-        char* hb = ctx->h_items.as<char>() + (grp ? bytes : 0);
-        char* db = ctx->d_items.as<char>() + (grp ? bytes : 0);
-        long long* hw = (long long*)hb;
-        int* hi = (int*)(hb + (size_t)(ni + 1) * sizeof(long long));
-        memcpy(hw, w0.data(), (ni + 1) * sizeof(long long));
-        memcpy(hi, ic.data(), ni * sizeof(int));
-        memcpy(hi + ni, ip0.data(), ni * sizeof(int));
-        memcpy(hi + 2 * ni, inp.data(), ni * sizeof(int));
-        LKG_CK(cudaMemcpyAsync(db, hb, bytes, cudaMemcpyHostToDevice, ctx->stream), "item upload");
-        LaunchParams p{};
-        p.cx = ctx->d_cx.as<ComplexDev>();
-        p.item_work0 = (const long long*)db;
-        p.item_complex = (const int*)(db + (size_t)(ni + 1) * sizeof(long long));
-        p.item_pose0 = p.item_complex + ni;
-        p.item_npose = p.item_complex + 2 * ni;
-        p.n_items = ni;
-        p.total_work = w0.back();
-        p.tile = ctx->tile;
-        p.poses = d_poses;
-        p.scores = d_scores;
-        p.parts = d_parts;
-        p.raw_pairs = raw_pairs;
-        p.solv_only = solv_only;
-        p.partials = ctx->partials.as<double>();
-        p.pose_counter = ctx->pose_counter.as<int>();
-        p.work_counter = ctx->work_counter.as<unsigned long long>();
-        p.status = ctx->status.as<int>();
-        p.max_tiles = (int)ctx->cap_tiles;
-        p.atom_elec = atom_e;
-        p.atom_vdw = atom_v;
-        cudaError_t e;
-        if (grp == 0) {
-            int threads = ctx->tile;
-            long long blocks = (long long)ctx->sm_count * occupancy(ctx, false, exact, threads, 0);
-            blocks = std::max(1LL, std::min(blocks, p.total_work));
-            e = exact ? launch_score_exact(p, threads, (int)blocks, ctx->stream)
-                      : launch_score_fast(p, threads, (int)blocks, ctx->stream);
-        } else {
-            int threads = ctx->desolv_threads;
-            size_t smem = desolv_smem_bytes(hcap, exact);
-            if (smem > 227 * 1024) return set_error(LKG_ERR_CAPACITY, "desolvation hash too large");
-            long long blocks = (long long)ctx->sm_count * occupancy(ctx, true, exact, threads, hcap);
-            blocks = std::max(1LL, std::min(blocks, p.total_work));
-            e = exact ? launch_desolv_exact(p, threads, (int)blocks, hcap, ctx->stream)
-                      : launch_desolv_fast(p, threads, (int)blocks, hcap, ctx->stream);
-        }
-        if (e != cudaSuccess) return set_error(cuda_to_status(e), "score launch: %s", cudaGetErrorString(e));
-        ctx->launches++;
+    if ((st = sync_descriptors(ctx))) return st;
+    const size_t units = std::max<size_t>(g[0].w0.back(), 1);
+    LKG_CK(ctx->scratch.ensure(units, n_poses, ctx->stream), "scratch");
+    const size_t b0 = (g[0].bytes() + 255) & ~(size_t)255, b1 = (g[1].bytes() + 255) & ~(size_t)255;
+    std::vector<char> packed(b0 + b1, 0);
+    g[0].pack(packed.data());
+    g[1].pack(packed.data() + b0);
+    if (packed != ctx->last_items || !ctx->d_items.p) {
+        // new tables: the previous upload may still be reading the staging buffer
+        LKG_CK(cudaStreamSynchronize(ctx->stream), "item staging");
+        LKG_CK(ctx->h_items.reserve(b0 + b1), "item staging");
+        LKG_CK(ctx->d_items.reserve(b0 + b1), "item staging");
+        memcpy(ctx->h_items.p, packed.data(), b0 + b1);
+        LKG_CK(cudaMemcpyAsync(ctx->d_items.p, ctx->h_items.p, b0 + b1, cudaMemcpyHostToDevice, ctx->stream),
+               "item upload");
+        ctx->last_items.swap(packed);
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (g[k].ic.empty()) continue;
+        st = launch_group(ctx, g[k], ctx->d_items.as<char>() + (k ? b0 : 0), ctx->scratch, d_poses, d_scores, d_parts,
+                          raw_pairs, solv_only, atom_e, atom_v);
+        if (st) return st;
     }
     return set_ok();
 }
@@ -421,15 +470,18 @@ int wait_stream(lkg_ctx* ctx, double timeout_s) {
     }
 }
 
-int check_status(lkg_ctx* ctx) {
+int check_status_word(int* d_status) {
+    if (!d_status) return set_ok();
     int h[4] = {0, 0, 0, 0};
-    LKG_CK(cudaMemcpy(h, ctx->status.p, sizeof(h), cudaMemcpyDeviceToHost), "status read");
+    LKG_CK(cudaMemcpy(h, d_status, sizeof(h), cudaMemcpyDeviceToHost), "status read");
     if (h[0] & 1) {
-        cudaMemset(ctx->status.p, 0, sizeof(h));
+        cudaMemset(d_status, 0, sizeof(h));
         return set_error(LKG_ERR_CAPACITY, "desolvation hash overflow (too many receptor atoms within 6.4 A of one pose)");
     }
     return set_ok();
 }
+
+int check_status(lkg_ctx* ctx) { return check_status_word(ctx->scratch.status.as<int>()); }
 
 }  // namespace lkg
 
@@ -500,7 +552,7 @@ int lkg_ctx_set_precision(lkg_ctx* ctx, int precision) {
 int lkg_ctx_set_tiles(lkg_ctx* ctx, int threads, int cell_milli) {
     if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
     if (threads) {
-        if (threads < 32 || threads > 256 || threads % 32) return set_error(LKG_ERR_ARG, "tile must be 32..256, multiple of 32");
+        if (threads != 64 && threads != 128 && threads != 256) return set_error(LKG_ERR_ARG, "tile must be 64, 128 or 256");
         if (!ctx->cx.empty() && threads != ctx->tile) return set_error(LKG_ERR_STATE, "tile fixed once complexes exist");
         ctx->tile = threads;
     }
@@ -509,6 +561,14 @@ int lkg_ctx_set_tiles(lkg_ctx* ctx, int threads, int cell_milli) {
         if (!ctx->cx.empty()) return set_error(LKG_ERR_STATE, "cell edge fixed once complexes exist");
         ctx->cell_h = cell_milli / 1000.0f;
     }
+    return set_ok();
+}
+
+int lkg_ctx_set_group(lkg_ctx* ctx, int group) {
+    if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
+    if (group != 8 && group != 16 && group != 32) return set_error(LKG_ERR_ARG, "group must be 8, 16 or 32");
+    if (!ctx->cx.empty() && group != ctx->group) return set_error(LKG_ERR_STATE, "group fixed once complexes exist");
+    ctx->group = group;
     return set_ok();
 }
 
@@ -703,6 +763,122 @@ int lkg_field_build(const double* coords, const double* charges, int32_t n, doub
                               d_phi.as<float>(), 0), "field build");
     LKG_CK(cudaMemcpy(phi, d_phi.p, np * sizeof(float), cudaMemcpyDeviceToHost), "field readback");
     return set_ok();
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------------------------
+// plans: a batch prepared once (descriptors, item tables, own scratch); its
+// launch is kernel launches only, so it can be captured in a CUDA graph
+// ---------------------------------------------------------------------------
+struct lkg_plan {
+    lkg_ctx* ctx = nullptr;
+    lkg::Group g[2];
+    size_t b0 = 0, n_poses = 0;
+    lkg::DBuf d_tables;
+    lkg::Scratch scratch;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    const void* captured_cx = nullptr;
+    int captured_launches = 0;
+};
+
+extern "C" {
+
+int lkg_plan_create(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, lkg_plan** out) {
+    if (!ctx || !out || n_items <= 0 || !ids || !counts) return set_error(LKG_ERR_ARG, "bad plan arguments");
+    cudaSetDevice(ctx->device);
+    auto* P = new lkg_plan();
+    P->ctx = ctx;
+    int st = build_groups(ctx, n_items, ids, counts, P->g, &P->n_poses);
+    if (!st) st = sync_descriptors(ctx);
+    if (st) { delete P; return st; }
+    const size_t b0 = (P->g[0].bytes() + 255) & ~(size_t)255, b1 = (P->g[1].bytes() + 255) & ~(size_t)255;
+    std::vector<char> packed(b0 + b1, 0);
+    P->g[0].pack(packed.data());
+    P->g[1].pack(packed.data() + b0);
+    P->b0 = b0;
+    cudaError_t e;
+    if ((e = P->d_tables.reserve(b0 + b1)) != cudaSuccess ||
+        (e = cudaMemcpy(P->d_tables.p, packed.data(), b0 + b1, cudaMemcpyHostToDevice)) != cudaSuccess ||
+        (e = P->scratch.ensure(std::max<size_t>(P->g[0].w0.back(), 1), std::max<size_t>(P->n_poses, 1), ctx->stream)) !=
+            cudaSuccess ||
+        (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) {
+        delete P;
+        return set_error(cuda_to_status(e), "plan setup: %s", cudaGetErrorString(e));
+    }
+    *out = P;
+    return set_ok();
+}
+
+int lkg_plan_launch(lkg_plan* P, const double* d_poses, double* d_scores, double* d_parts) {
+    if (!P || !d_poses || !d_scores) return set_error(LKG_ERR_ARG, "bad plan launch");
+    for (int k = 0; k < 2; ++k) {
+        if (P->g[k].ic.empty()) continue;
+        int st = launch_group(P->ctx, P->g[k], P->d_tables.as<char>() + (k ? P->b0 : 0), P->scratch, d_poses,
+                              d_scores, d_parts, 0, 0, nullptr, nullptr);
+        if (st) return st;
+    }
+    return set_ok();
+}
+
+int lkg_plan_capture(lkg_plan* P, const double* d_poses, double* d_scores, double* d_parts, int n_launches) {
+    if (!P || n_launches <= 0) return set_error(LKG_ERR_ARG, "bad capture");
+    lkg_ctx* ctx = P->ctx;
+    cudaSetDevice(ctx->device);
+    if (P->exec) { cudaGraphExecDestroy(P->exec); P->exec = nullptr; }
+    if (P->graph) { cudaGraphDestroy(P->graph); P->graph = nullptr; }
+    // occupancy queries are host-side; make them before capture
+    lkg_plan_launch(P, d_poses, d_scores, d_parts);
+    LKG_CK(cudaStreamSynchronize(ctx->stream), "pre-capture launch");
+    LKG_CK(cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal), "begin capture");
+    int st = 0;
+    for (int i = 0; i < n_launches && !st; ++i) st = lkg_plan_launch(P, d_poses, d_scores, d_parts);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+    if (st) { if (g) cudaGraphDestroy(g); return st; }
+    if (e != cudaSuccess) return set_error(cuda_to_status(e), "end capture: %s", cudaGetErrorString(e));
+    P->graph = g;
+    LKG_CK(cudaGraphInstantiate(&P->exec, g, 0), "graph instantiate");
+    P->captured_cx = ctx->d_cx.p;
+    P->captured_launches = n_launches * ((P->g[0].ic.empty() ? 0 : 1) + (P->g[1].ic.empty() ? 0 : 1));
+    return set_ok();
+}
+
+int lkg_plan_replay(lkg_plan* P) {
+    if (!P || !P->exec) return set_error(LKG_ERR_STATE, "no captured graph");
+    if (P->captured_cx != P->ctx->d_cx.p)
+        return set_error(LKG_ERR_STATE, "complexes were added after capture; capture again");
+    cudaSetDevice(P->ctx->device);
+    LKG_CK(cudaGraphLaunch(P->exec, P->ctx->stream), "graph launch");
+    P->ctx->launches += P->captured_launches;
+    return set_ok();
+}
+
+int lkg_plan_destroy(lkg_plan* P) {
+    if (!P) return set_ok();
+    cudaSetDevice(P->ctx->device);
+    cudaStreamSynchronize(P->ctx->stream);
+    if (P->exec) cudaGraphExecDestroy(P->exec);
+    if (P->graph) cudaGraphDestroy(P->graph);
+    delete P;
+    return set_ok();
+}
+
+int lkg_ctx_sync(lkg_ctx* ctx) {
+    if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
+    cudaSetDevice(ctx->device);
+    int st = wait_stream(ctx, 300.0);
+    if (st) return st;
+    return check_status(ctx);
+}
+
+int lkg_plan_sync(lkg_plan* P) {
+    if (!P) return set_error(LKG_ERR_ARG, "null plan");
+    cudaSetDevice(P->ctx->device);
+    int st = wait_stream(P->ctx, 300.0);
+    if (st) return st;
+    return check_status_word(P->scratch.status.as<int>());
 }
 
 }  // extern "C"

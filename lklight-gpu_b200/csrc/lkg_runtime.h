@@ -73,13 +73,32 @@ struct MolIn {
 struct ComplexRec {
     int family = -1;
     DBuf rpos, rpar, rsolv, rpos64, rpar64, rsolv64, rorig, cell_start;
-    DBuf lpos, lpar, lsolv, lpos64, lpar64, lsolv64, lorig;
+    DBuf lpos, lpar, lsolv, lpos64, lpar64, lsolv64, lorig, lgrp;
     DBuf phi;
     ComplexDev d{};
     int n_cells = 0;
 };
 
 struct Occupancy { int threads = 0, hcap = 0, blocks = 0; };
+
+// per-launch scratch: per-unit partial sums, per-pose counters, the work
+// counter and the status word (counters reset themselves after a launch)
+struct Scratch {
+    DBuf partials, pose_counter, work_counter, status;
+    size_t cap_units = 0, cap_poses = 0;
+    cudaError_t ensure(size_t units, size_t poses, cudaStream_t s);
+};
+
+// one launch group's item tables: (complex, first pose, pose count) per item
+// and cumulative work units; `kind` 0 = tile kernels, 1 = fused desolvation
+struct Group {
+    int kind = 0;
+    std::vector<int> ic, ip0, inp;
+    std::vector<long long> w0{0};
+    int hcap = 64;
+    size_t bytes() const { return (ic.size() + 1) * sizeof(long long) + ic.size() * 3 * sizeof(int); }
+    void pack(char* dst) const;
+};
 
 }  // namespace lkg
 
@@ -90,17 +109,17 @@ struct lkg_ctx {
     bool own_stream = false;
     int precision = LKG_PREC_FAST;
     int tile = 128;                 // ligand atoms per work unit
+    int group = 8;                  // ligand atoms per candidate-search group
     int desolv_threads = 512;
-    float cell_h = 10.0f / 3.0f;    // fine receptor cell edge (A)
+    float cell_h = 2.5f;            // fine receptor cell edge (A)
     std::vector<std::unique_ptr<lkg::ComplexRec>> cx;
     lkg::DBuf d_cx;                 // ComplexDev[] on the device
     bool cx_dirty = true;
-    // scratch (self-resetting between launches)
-    lkg::DBuf partials, pose_counter, work_counter, status;
-    size_t cap_poses = 0, cap_tiles = 0;
+    lkg::Scratch scratch;
     // item tables
     lkg::DBuf d_items;
     lkg::HBuf h_items;
+    std::vector<char> last_items;   // tables currently in d_items
     // host-buffer call staging
     lkg::DBuf d_poses, d_scores, d_parts;
     lkg::HBuf h_poses, h_out;
@@ -122,5 +141,12 @@ int launch_items(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, c
                  float* atom_v);
 int wait_stream(lkg_ctx* ctx, double timeout_s);
 int check_status(lkg_ctx* ctx);
+int check_status_word(int* d_status);
+// item tables of the two launch groups for a batch
+int build_groups(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, Group g[2], size_t* n_poses);
+int sync_descriptors(lkg_ctx* ctx);
+// launch one prepared group (kernel launches only: stream-capturable)
+int launch_group(lkg_ctx* ctx, const Group& g, const char* d_tables, Scratch& sc, const double* d_poses,
+                 double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e, float* atom_v);
 void field_geometry(const double* coords, int n, double lo[3], int dims[3], double* spacing);
 }  // namespace lkg

@@ -159,12 +159,12 @@ struct AtomAcc {
 
 __device__ __forceinline__ void pair_fast(unsigned flags, float qj, float svj, float rj, bool hj,
                                           const float4& a, const float4& pr, float d2,
-                                          float& elec, float& vdw) {
+                                          double& elec, double& vdw) {
     float ir2 = __frcp_rn(d2);
     if (flags & F_ELEC) {
         float ae = qj * a.w * ir2;
         ae = fminf(fmaxf(ae, -ES_CAP_F), ES_CAP_F);
-        elec += ae;
+        elec += (double)ae;
     }
     float sv = svj * pr.x;
     float rr = rj + pr.y;
@@ -177,7 +177,7 @@ __device__ __forceinline__ void pair_fast(unsigned flags, float qj, float svj, f
         float dmin = 0.75f * rr;
         if (d < dmin) vp += 6.f * (dmin - d);
     }
-    vdw += vp;
+    vdw += (double)vp;
 }
 
 __device__ __forceinline__ double powi6(double x) { double x2 = x * x; double x4 = x2 * x2; return x2 * x4; }
@@ -266,16 +266,20 @@ template <> struct Atom<float> {
         } else {
             apply(rot, (double)b.x, (double)b.y, (double)b.z, xd, yd, zd);
         }
+        // the f64 position as a float plus its rounding residual: x - a.x is
+        // (nearly) exact for nearby atoms, so adding the residual keeps the
+        // pair distance accurate to f32 rounding of the *difference*
         float x = (float)xd, y = (float)yd, z = (float)zd;
+        const float xl = (float)(xd - (double)x), yl = (float)(yd - (double)y), zl = (float)(zd - (double)z);
         const float qj = b.w, svj = lp.x, rj = lp.y;
         const bool hj = lp.z != 0.f, lf = lp.w != 0.f;
         const unsigned flags = c.flags;
-        float elec = 0.f, vdw = 0.f;
-        if ((flags & F_FAR) && qj != 0.f) elec += qj * sample_phi(c, x, y, z);
+        double elec = 0.0, vdw = 0.0;
+        if ((flags & F_FAR) && qj != 0.f) elec += (double)(qj * sample_phi(c, x, y, z));
         int np = 0;
         scan_rows(c, x, y, z, [&](int k) {
             float4 a = Tr<float>::rpos(c, k);
-            float dx = x - a.x, dy = y - a.y, dz = z - a.z;
+            float dx = (x - a.x) + xl, dy = (y - a.y) + yl, dz = (z - a.z) + zl;
             float d2 = dx * dx + dy * dy + dz * dz;
             if (d2 <= 100.f) {
                 float4 pr = Tr<float>::rpar(c, k);
@@ -293,10 +297,10 @@ template <> struct Atom<float> {
                 }
             }
         });
-        acc.elec += (double)elec;
-        acc.vdw += (double)vdw;
+        acc.elec += elec;
+        acc.vdw += vdw;
         acc.np += np;
-        if (out_e) { int o = c.lorig[j]; out_e[o] = elec; out_v[o] = vdw; }
+        if (out_e) { int o = c.lorig[j]; out_e[o] = (float)elec; out_v[o] = (float)vdw; }
     }
 };
 
@@ -446,14 +450,15 @@ __global__ void __launch_bounds__(256) k_score_tiles(LaunchParams p) {
         double v[3] = {acc.elec, acc.vdw, (double)acc.np};
         block_sum<3>(v, s_red);
         if (threadIdx.x == 0) {
-            double* part = p.partials + ((size_t)g * p.max_tiles + tile) * 4;
+            // partial of work unit w; the pose's units are w - tile .. w - tile + ntiles - 1
+            double* part = p.partials + (size_t)w * 4;
             part[0] = v[0]; part[1] = v[1]; part[2] = 0.0; part[3] = v[2];
             __threadfence();
             int done = atomicAdd(p.pose_counter + g, 1);
             if (done == c.ntiles - 1) {
                 __threadfence();
                 double e = 0.0, vv = 0.0, np = 0.0;
-                const double* pp = p.partials + (size_t)g * p.max_tiles * 4;
+                const double* pp = p.partials + (size_t)(w - tile) * 4;
                 for (int t = 0; t < c.ntiles; ++t) {
                     e += __ldcg(pp + 4 * t); vv += __ldcg(pp + 4 * t + 1); np += __ldcg(pp + 4 * t + 3);
                 }
