@@ -185,6 +185,21 @@ int lkg_score_multi_device(lkg_ctx* ctx, int n_items, const int* complex_ids, co
 int lkg_score_multi(lkg_ctx* ctx, int n_items, const int* complex_ids, const int* counts,
                     const double* poses, double* scores, double* parts);
 
+/* No counterpart in the reference.  lkg_score_device with no device
+ * allocation, for callers that may not allocate while scoring (a framework
+ * owning the device heap through its own pool, a latency-bound loop, code
+ * where allocation calls are not allowed).  The fast tile kernel's scratch
+ * lives in a fixed 8 MiB array inside liblkg (held on every GPU that loads
+ * the library); a batch needing more (32 B per pose and ligand tile + 4 B
+ * per pose + 64 B) fails with LKG_ERR_CAPACITY.  The first call on a device
+ * looks the array's address up (cudaGetSymbolAddress): make it before any
+ * stream capture.  Each call clears the counters it uses; calls overlapping
+ * on the GPU race on the shared array.  The complex must be resident and
+ * already scored once through a regular entry point; cpydock complexes are
+ * refused.  Asynchronous on the context stream. */
+int lkg_score_device_noalloc(lkg_ctx* ctx, int complex_id, int n_pose, const double* d_poses,
+                             double* d_scores, double* d_parts);
+
 /* Kernel launches made by this context so far (for launch accounting). */
 int64_t lkg_ctx_launches(lkg_ctx* ctx);
 /* Wait (bounded host poll) for the context stream and check the device
