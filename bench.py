@@ -48,12 +48,15 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lkg", choices=["lkg", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config2", "config0"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config0", "config3"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--cell", type=float, default=0.0)
     ap.add_argument("--group", type=int, default=0)
+    ap.add_argument("--xsub", type=int, default=0)
+    ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--gso-steps", type=int, default=200)
     return ap.parse_args()
 
 
@@ -183,7 +186,9 @@ def main():
     lkg = importlib.import_module("lklight-gpu_b200")
 
     items = workload(args.workload)
-    ctx = lkg.Context(device=local, tile=args.tile, cell=args.cell, group=args.group)
+    if args.workload == "config3":
+        return run_screened(args, lkg, torch, local, rank, world, dist)
+    ctx = lkg.Context(device=local, tile=args.tile, cell=args.cell, group=args.group, xsub=args.xsub)
     stream = torch.cuda.ExternalStream(ctx.stream)
     ids = [ctx.add_complex(it["family"], it["rec"], it["lig"]) for it in items]
     counts = [len(it["poses"]) for it in items]
@@ -210,8 +215,16 @@ def main():
         flops += p * FLOPS_PER_PAIR[it["family"]] + FAR_FLOPS * charged * n
         off += n
 
-    def step():
-        ctx.score_multi_device(ids, counts, d_poses.data_ptr(), d_scores.data_ptr())
+    # one persistent launch group per step, captured once in a CUDA graph
+    plan = lkg.Plan(ctx, ids, counts)
+    if args.no_graph:
+        def step():
+            plan.launch(d_poses.data_ptr(), d_scores.data_ptr())
+    else:
+        plan.capture(d_poses.data_ptr(), d_scores.data_ptr(), n_launches=1)
+
+        def step():
+            plan.replay()
 
     for _ in range(args.warmup):
         step()
@@ -298,12 +311,77 @@ def main():
             "e2e": {"value": e2e_value, "unit": "poses/s", "ms_per_step": float(te.item()),
                     "h2d_bytes_per_step": npose * 7 * 8, "d2h_bytes_per_step": npose * 8,
                     "api": "lkg_score_multi (host page-locked buffers)"},
-            "gpu_launches": int(launches), "clocks": clk}
+            "gpu_launches": int(launches), "clocks": clk,
+            "step": "CUDA graph replay of one persistent launch group" if not args.no_graph else "plan launch"}
     if plain:
         line["plain_single_complex"] = plain
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, cores, sample = cpu_sample(items)
         line["cpu_baseline"] = {"value": v, "unit": "poses/s", "cores": cores, "kind": "port", "sample": sample}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    plan.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def top5_overlap(tr_a, sc_a, tr_b, sc_b, tol=2.0):
+    """Share of run A's top-5 poses (engine rank order: descending scoring)
+    within tol A on every axis of some top-5 pose of run B
+    (tools/analyze_perf3.py:50-55)."""
+    ta = tr_a[np.argsort(-sc_a, kind="stable")[:5]]
+    tb = tr_b[np.argsort(-sc_b, kind="stable")[:5]]
+    return sum(1 for a in ta if any(np.all(np.abs(a - b) <= tol) for b in tb)) / 5.0
+
+
+def run_screened(args, lkg, torch, local, rank, world, dist):
+    """Surrogate-screened GSO against the plain GSO on the same complex and
+    start: the config-0 complex, 10 swarms x 1,000 glowworms, seed 3; both
+    end with an exact rescoring of the final poses.  Wall time of the whole
+    run (device scoring, surrogate training / inference, host movement)."""
+    synth = importlib.import_module("lklight-gpu_b200.synth")
+    c0 = synth.config0()
+    swarms, glow, steps = 10, 1000, args.gso_steps
+    ctx = lkg.Context(device=local, tile=args.tile, cell=args.cell, group=args.group, xsub=args.xsub)
+    cid = ctx.add_complex("dna", c0["rec"], c0["lig"])
+    pos = synth.setup_poses(c0["rec"]["coords"], swarms, glow, 3)
+    res = {}
+    for mode in ("plain", "screened", "ablation"):
+        g = lkg.GSO(ctx, [(cid, swarms, glow)], pos, [3])
+        if mode != "plain":
+            g.set_screen(candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=40,
+                         finetune_epochs=2, lr=1e-3, seed=3, random_rank=(mode == "ablation"))
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g.run(steps)
+        g.finalize()
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        st = g.state()
+        res[mode] = dict(seconds=el, scored=g.scored, predicted=g.predicted, st=st)
+        del g
+    ov = {}
+    for mode in ("screened", "ablation"):
+        o = []
+        for k in range(swarms):
+            sl = slice(k * glow, (k + 1) * glow)
+            a, b = res[mode]["st"], res["plain"]["st"]
+            o.append(top5_overlap(a["translation"][sl], a["scoring"][sl], b["translation"][sl], b["scoring"][sl]))
+        ov[mode] = float(np.mean(o))
+    best = {m: float(np.mean(res[m]["st"]["scoring"].reshape(swarms, glow).max(axis=1))) for m in res}
+    line = {"metric": "surrogate-screened GSO speedup over the plain GSO (e2e, same complex and start)",
+            "value": res["plain"]["seconds"] / res["screened"]["seconds"], "unit": "x", "n_gpus": world,
+            "higher_is_better": True, "data": "synthetic",
+            "config": {"workload": "config3", "swarms": swarms, "glowworms": glow, "steps": steps,
+                       "candidates": 4, "exact_fraction": 0.25, "rescore_every": 10, "train_steps": 20},
+            "plain": {"seconds": res["plain"]["seconds"], "exact_evals": res["plain"]["scored"],
+                      "mean_best_score": best["plain"]},
+            "screened": {"seconds": res["screened"]["seconds"], "exact_evals": res["screened"]["scored"],
+                         "surrogate_evals": res["screened"]["predicted"], "mean_best_score": best["screened"],
+                         "top5_overlap_with_plain": ov["screened"]},
+            "ablation_no_network": {"seconds": res["ablation"]["seconds"], "exact_evals": res["ablation"]["scored"],
+                                    "mean_best_score": best["ablation"], "top5_overlap_with_plain": ov["ablation"]}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -146,12 +146,17 @@ typedef struct {
 int lkg_ctx_create(int device, lkg_ctx** out);
 int lkg_ctx_destroy(lkg_ctx* ctx);
 int lkg_ctx_set_precision(lkg_ctx* ctx, int precision);
-/* Tile shape: ligand atoms per work unit (64, 128 or 256) and the receptor
- * fine-cell edge in 1/1000 A; 0 keeps the current value. */
+/* Tile shape: ligand atoms per work unit (64, 128 or 256; default 128) and
+ * the receptor cell edge in 1/1000 A (default: 4 A, 2.5 A for cpydock
+ * complexes); 0 keeps the current value. */
 int lkg_ctx_set_tiles(lkg_ctx* ctx, int threads_per_block, int cell_size_milli_angstrom);
-/* Ligand atoms per candidate-search group of the warp-cooperative kernel
- * (8, 16 or 32; default 8); fixed once complexes exist. */
+/* Ligand atoms per candidate-search group of the warp kernel (8, 16 or 32;
+ * default 8); fixed once complexes exist. */
 int lkg_ctx_set_group(lkg_ctx* ctx, int group);
+/* x sub-cells per receptor cell edge (1..8; default 8, 4 for cpydock
+ * complexes): the near scan trims each (z, y) cell row to the 10 A sphere
+ * at this finer x resolution; fixed once complexes exist. */
+int lkg_ctx_set_xsub(lkg_ctx* ctx, int xsub);
 /* Work on this CUDA stream (cudaStream_t) instead of the context's own. */
 int lkg_ctx_set_stream(lkg_ctx* ctx, void* stream);
 void* lkg_ctx_stream(lkg_ctx* ctx);
@@ -222,6 +227,33 @@ int lkg_plan_sync(lkg_plan* plan);
 int lkg_plan_destroy(lkg_plan* plan);
 
 /* ---------------------------------------------------------------------- */
+/* Learned surrogate of the pose energy (no counterpart in the reference)  */
+/* ---------------------------------------------------------------------- */
+/* 64 -> 256 -> 256 -> 256 -> 1 ReLU MLP, BF16 weights and activations with
+ * FP32 accumulation on the tensor cores, trained online on exact scores.
+ * Features: pose quaternion, translation / box scale, and at 16 ligand anchor
+ * atoms (farthest-point sampled) the far-field potential and receptor atom
+ * counts from the fine cell grid.  Target: asinh(score / s) standardised
+ * (lkg_surrogate_set_target_scale fits s, mean and spread). */
+typedef struct lkg_surrogate lkg_surrogate;
+int lkg_surrogate_create(lkg_ctx* ctx, int complex_id, uint64_t seed, lkg_surrogate** out);
+int lkg_surrogate_destroy(lkg_surrogate* s);
+int lkg_surrogate_set_target_scale(lkg_surrogate* s, int n, const double* scores);
+/* predicted scores (lkg_score units) for n device poses, device output */
+int lkg_surrogate_predict(lkg_surrogate* s, int n, const double* d_poses, double* d_pred);
+/* minibatch Adam over n device poses with their exact scores (device) */
+int lkg_surrogate_train(lkg_surrogate* s, int n, const double* d_poses, const double* d_scores, int epochs,
+                        int batch, float lr, float* loss);
+int64_t lkg_surrogate_nparams(void);
+int lkg_surrogate_get_params(lkg_surrogate* s, float* out);
+int lkg_surrogate_set_params(lkg_surrogate* s, const float* in);
+/* one forward + backward on host feature rows (bf16 bits) and standardised
+ * targets: outputs, flat FP32 gradient, loss (for gradient checks) */
+int lkg_surrogate_grad(lkg_surrogate* s, int n, const uint16_t* feats, const float* targets, float* y,
+                       float* grad, float* loss);
+int lkg_surrogate_features(lkg_surrogate* s, int n, const double* d_poses, uint16_t* out);
+
+/* ---------------------------------------------------------------------- */
 /* Setup helpers (host)                                                    */
 /* ---------------------------------------------------------------------- */
 /* Receptor far field, bit-identical to ReceptorField::build
@@ -257,6 +289,33 @@ int lkg_gso_state(lkg_gso* gso, double* trans, double* rot, double* luc, double*
                   double* vision, int32_t* nneigh);
 int64_t lkg_gso_scored(lkg_gso* gso);
 int lkg_gso_destroy(lkg_gso* gso);
+
+/* Surrogate screening of GSO moves (no counterpart in the reference; the
+ * plain run above stays the reference GSO).  The first train_steps steps run
+ * plainly and their exact energies train one surrogate per group; from then
+ * on every glowworm with neighbours draws `candidates` moves from its
+ * neighbour distribution, the surrogate ranks them, the glowworm takes the
+ * best, and per swarm the exact_fraction of moves with the largest
+ * predicted gain is scored exactly (the others carry the prediction); every
+ * rescore_every steps all glowworms are rescored exactly and the surrogate
+ * is fine-tuned on them.  random_rank = 1 is the same search without the
+ * network (seeded random ranks; unscored moves keep their previous score),
+ * for ablations. */
+typedef struct {
+    int32_t candidates;       /* moves screened per glowworm (4) */
+    double exact_fraction;    /* fraction of moves per swarm scored exactly (0.25) */
+    int32_t rescore_every;    /* full exact rescoring period in steps (10; 0 = never) */
+    int32_t train_steps;      /* plain steps whose energies train the surrogate (20) */
+    int32_t train_epochs;     /* epochs of the first training */
+    int32_t finetune_epochs;  /* epochs at every full rescoring */
+    float lr;                 /* Adam learning rate */
+    uint64_t seed;            /* surrogate initialisation, shuffles, ablation ranks */
+    int32_t random_rank;
+} lkg_screen;
+int lkg_gso_set_screen(lkg_gso* gso, const lkg_screen* cfg);
+/* exact rescoring of every glowworm (the final poses of a screened run) */
+int lkg_gso_finalize(lkg_gso* gso);
+int64_t lkg_gso_predicted(lkg_gso* gso);
 
 #ifdef __cplusplus
 }

@@ -71,12 +71,17 @@ def lib():
         "lkg_version": (C.c_char_p, []),
         "lkg_ctx_create": (I, [I, P]), "lkg_ctx_destroy": (I, [P]),
         "lkg_ctx_set_precision": (I, [P, I]), "lkg_ctx_set_tiles": (I, [P, I, I]),
-        "lkg_ctx_set_stream": (I, [P, P]), "lkg_ctx_set_group": (I, [P, I]), "lkg_ctx_stream": (P, [P]), "lkg_ctx_launches": (I64, [P]),
+        "lkg_ctx_set_stream": (I, [P, P]), "lkg_ctx_set_group": (I, [P, I]), "lkg_ctx_set_xsub": (I, [P, I]), "lkg_ctx_stream": (P, [P]), "lkg_ctx_launches": (I64, [P]),
         "lkg_complex_add": (I, [P, I, P, P, P, P]), "lkg_complex_info": (I, [P, I, P, P, P]),
         "lkg_score": (I, [P, I, I, P, P, P]), "lkg_score_device": (I, [P, I, I, P, P, P]),
         "lkg_score_multi_device": (I, [P, I, P, P, P, P, P]),
         "lkg_score_multi": (I, [P, I, P, P, P, P, P]),
         "lkg_ctx_sync": (I, [P]),
+        "lkg_surrogate_create": (I, [P, I, U64, P]), "lkg_surrogate_destroy": (I, [P]),
+        "lkg_surrogate_set_target_scale": (I, [P, I, P]), "lkg_surrogate_predict": (I, [P, I, P, P]),
+        "lkg_surrogate_train": (I, [P, I, P, P, I, I, C.c_float, P]), "lkg_surrogate_nparams": (I64, []),
+        "lkg_surrogate_get_params": (I, [P, P]), "lkg_surrogate_set_params": (I, [P, P]),
+        "lkg_surrogate_grad": (I, [P, I, P, P, P, P, P]), "lkg_surrogate_features": (I, [P, I, P, P]),
         "lkg_plan_create": (I, [P, I, P, P, P]), "lkg_plan_launch": (I, [P, P, P, P]),
         "lkg_plan_capture": (I, [P, P, P, P, I]), "lkg_plan_replay": (I, [P]),
         "lkg_plan_sync": (I, [P]), "lkg_plan_destroy": (I, [P]),
@@ -86,6 +91,7 @@ def lib():
         "lkg_gso_create": (I, [P, I, P, P, P, P, P, P]), "lkg_gso_run": (I, [P, I]),
         "lkg_gso_state": (I, [P, P, P, P, P, P, P]), "lkg_gso_scored": (I64, [P]),
         "lkg_gso_destroy": (I, [P]), "lkg_compat_cache_clear": (None, []),
+        "lkg_gso_set_screen": (I, [P, P]), "lkg_gso_finalize": (I, [P]), "lkg_gso_predicted": (I64, [P]),
         "cuda_batch_score": (I, [P, I, I, I, F, F, F, F, P, P, P, P, P, I, P, P, I, I, I, F, F, F, F,
                                  P, P, P, P, P, P, I, I, C.c_uint, P]),
         "cuda_cpydock_solv": (I, [P, P, I, P, P, I, I, I, F, F, F, F, P, P, P, P, I, I, P, P, P, P, P]),
@@ -138,10 +144,17 @@ def make_mol(m, keep):
                          for k in ("coords", "ele", "vdw", "radius", "heavy", "hyd", "des", "asa")])
 
 
+class Screen(C.Structure):
+    """``lkg_screen``: surrogate screening of GSO moves."""
+    _fields_ = [("candidates", C.c_int32), ("exact_fraction", C.c_double), ("rescore_every", C.c_int32),
+                ("train_steps", C.c_int32), ("train_epochs", C.c_int32), ("finetune_epochs", C.c_int32),
+                ("lr", C.c_float), ("seed", C.c_uint64), ("random_rank", C.c_int32)]
+
+
 class Context:
     """A device context: resident complexes, a stream, scratch buffers."""
 
-    def __init__(self, device=0, precision="fast", tile=0, cell=0.0, group=0):
+    def __init__(self, device=0, precision="fast", tile=0, cell=0.0, group=0, xsub=0):
         h = C.c_void_p()
         _check(lib().lkg_ctx_create(device, C.byref(h)))
         self.h = h
@@ -152,6 +165,8 @@ class Context:
             _check(lib().lkg_ctx_set_tiles(self.h, int(tile), int(round(cell * 1000))))
         if group:
             _check(lib().lkg_ctx_set_group(self.h, int(group)))
+        if xsub:
+            _check(lib().lkg_ctx_set_xsub(self.h, int(xsub)))
 
     def set_precision(self, precision):
         _check(lib().lkg_ctx_set_precision(self.h, PREC_EXACT if precision == "exact" else PREC_FAST))
@@ -275,6 +290,66 @@ class Plan:
             pass
 
 
+class Surrogate:
+    """BF16 tensor-core MLP surrogate of the pose energy of one complex."""
+
+    def __init__(self, ctx, cid, seed=0):
+        self.ctx = ctx
+        h = C.c_void_p()
+        _check(lib().lkg_surrogate_create(ctx.h, cid, seed, C.byref(h)))
+        self.h = h
+
+    @staticmethod
+    def nparams():
+        return lib().lkg_surrogate_nparams()
+
+    def set_target_scale(self, scores):
+        s = _arr(scores, np.float64)
+        _check(lib().lkg_surrogate_set_target_scale(self.h, len(s), ptr(s)))
+
+    def predict_device(self, n, d_poses, d_pred):
+        _check(lib().lkg_surrogate_predict(self.h, n, C.c_void_p(d_poses), C.c_void_p(d_pred)))
+
+    def train_device(self, n, d_poses, d_scores, epochs=1, batch=1024, lr=1e-3):
+        loss = C.c_float()
+        _check(lib().lkg_surrogate_train(self.h, n, C.c_void_p(d_poses), C.c_void_p(d_scores), epochs, batch,
+                                         lr, C.byref(loss)))
+        return loss.value
+
+    def params(self):
+        out = np.zeros(self.nparams(), np.float32)
+        _check(lib().lkg_surrogate_get_params(self.h, ptr(out)))
+        return out
+
+    def set_params(self, p):
+        p = _arr(p, np.float32)
+        _check(lib().lkg_surrogate_set_params(self.h, ptr(p)))
+
+    def grad(self, feats_bf16, targets):
+        f = np.ascontiguousarray(feats_bf16, np.uint16)
+        t = _arr(targets, np.float32)
+        n = len(t)
+        y, g, l = np.zeros(n, np.float32), np.zeros(self.nparams(), np.float32), C.c_float()
+        _check(lib().lkg_surrogate_grad(self.h, n, ptr(f), ptr(t), ptr(y), ptr(g), C.byref(l)))
+        return y, g, l.value
+
+    def features_device(self, n, d_poses):
+        out = np.zeros((n, 64), np.uint16)
+        _check(lib().lkg_surrogate_features(self.h, n, C.c_void_p(d_poses), ptr(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().lkg_surrogate_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class Scorer:
     """The reference ``Score`` trait for one complex (src/scoring.rs:20-81)."""
 
@@ -323,9 +398,25 @@ class GSO:
         _check(lib().lkg_gso_state(self.h, ptr(t), ptr(r), ptr(luc), ptr(sc), ptr(vis), ptr(nn)))
         return dict(translation=t, rotation=r, luciferin=luc, scoring=sc, vision=vis, neighbors=nn)
 
+    def set_screen(self, candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=40,
+                   finetune_epochs=2, lr=1e-3, seed=0, random_rank=False):
+        """Screen moves with the surrogate (random_rank: the same search with
+        random candidate ranks instead of the network, for ablations)."""
+        cfg = Screen(candidates, exact_fraction, rescore_every, train_steps, train_epochs, finetune_epochs, lr, seed,
+                     1 if random_rank else 0)
+        _check(lib().lkg_gso_set_screen(self.h, C.byref(cfg)))
+
+    def finalize(self):
+        """Exact rescoring of every glowworm."""
+        _check(lib().lkg_gso_finalize(self.h))
+
     @property
     def scored(self):
         return lib().lkg_gso_scored(self.h)
+
+    @property
+    def predicted(self):
+        return lib().lkg_gso_predicted(self.h)
 
     def __del__(self):
         if getattr(self, "h", None):

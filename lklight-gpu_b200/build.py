@@ -20,7 +20,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fopenmp", "-I" + INCLUDE]
 NO_FMAD = {"lkg_kernels_exact.cu", "lkg_field.cu"}
-HEADERS = ["lkg_internal.h", "lkg_runtime.h", "lkg_score.cuh", "lkg_score_v2.cuh", "lkg_rng.h"]
+HEADERS = ["lkg_internal.h", "lkg_runtime.h", "lkg_score.cuh", "lkg_score_warp.cuh", "lkg_rng.h"]
 
 
 def _nvcc():

@@ -50,6 +50,8 @@ struct Glow {
     Quat r;
     double luciferin = 5.0, vision = 0.2, scoring = 0.0;   // glowworm.rs:45-51
     bool moved = false;
+    bool exact_next = false;      // screened run: score this move exactly
+    double pred = 0.0;            // screened run: surrogate score of the move
     uint32_t step = 0;
     std::vector<uint32_t> nb;
     std::vector<double> prob;
@@ -100,9 +102,10 @@ struct Swarm {
         }
     }
 
-    void movement() {  // swarm.rs:105-174
+    // neighbour lists and selection probabilities (swarm.rs:105-128,
+    // glowworm.rs:114-128) of every glowworm from the current state
+    void prepare() {
         const size_t n = g.size();
-        if (!n) return;
         pos.resize(3 * n);
         rot.resize(n);
         luc.resize(n);
@@ -112,7 +115,7 @@ struct Swarm {
             luc[i] = g[i].luciferin;
         }
         neighbours();
-        for (size_t i = 0; i < n; ++i) {  // glowworm.rs:114-128
+        for (size_t i = 0; i < n; ++i) {
             Glow& gw = g[i];
             gw.prob.clear();
             double total = 0.0;
@@ -123,30 +126,76 @@ struct Swarm {
             }
             for (auto& p : gw.prob) p /= total;
         }
+    }
+
+    // the neighbour a uniform draw selects (glowworm.rs:130-142)
+    uint32_t select(const Glow& gw, uint32_t self, double u) const {
+        if (gw.nb.empty()) return self;
+        double sum = 0.0;
+        size_t k = 0;
+        while (sum < u && k < gw.prob.size()) { sum += gw.prob[k]; ++k; }
+        return gw.nb[k == 0 ? 0 : k - 1];
+    }
+
+    // pose after a move towards neighbour nid (glowworm.rs:144-166)
+    void moved_pose(const Glow& gw, uint32_t nid, double t[3], Quat& r) const {
+        double dx = pos[3 * nid] - gw.t[0], dy = pos[3 * nid + 1] - gw.t[1], dz = pos[3 * nid + 2] - gw.t[2];
+        double norm = std::sqrt(dx * dx + dy * dy + dz * dz);
+        double coef = 0.5 / norm;
+        t[0] = gw.t[0] + dx * coef;
+        t[1] = gw.t[1] + dy * coef;
+        t[2] = gw.t[2] + dz * coef;
+        r = q_slerp(gw.r, rot[nid], 0.5);
+        q_normalize(r);
+    }
+
+    void update_vision(Glow& gw) {
+        double v = gw.vision + BETA * (double)(MAX_NEIGHBORS - (int)gw.nb.size());
+        gw.vision = std::fmin(MAX_VISION, std::fmax(0.0, v));
+    }
+
+    void movement() {  // swarm.rs:105-174
+        const size_t n = g.size();
+        if (!n) return;
+        prepare();
         std::vector<double> rnd(n);
         for (size_t i = 0; i < n; ++i) rnd[i] = rng.gen_f64();
         for (size_t i = 0; i < n; ++i) {
             Glow& gw = g[i];
-            uint32_t nid = (uint32_t)i;
-            if (!gw.nb.empty()) {  // glowworm.rs:130-142
-                double sum = 0.0;
-                size_t k = 0;
-                while (sum < rnd[i] && k < gw.prob.size()) { sum += gw.prob[k]; ++k; }
-                nid = gw.nb[k == 0 ? 0 : k - 1];
+            const uint32_t nid = select(gw, (uint32_t)i, rnd[i]);
+            gw.moved = nid != (uint32_t)i;
+            if (gw.moved) moved_pose(gw, nid, gw.t, gw.r);
+            update_vision(gw);
+        }
+    }
+
+    // screened movement, part 1: K draws per glowworm (serially, glowworm
+    // by glowworm), the candidate poses of those with neighbours
+    // (kernel layout w, x, y, z, tx, ty, tz), vision update
+    void propose(int K, std::vector<double>& cand, std::vector<uint32_t>& owner) {
+        const size_t n = g.size();
+        cand.clear();
+        owner.clear();
+        if (!n) return;
+        prepare();
+        std::vector<double> rnd(n * (size_t)K);
+        for (auto& u : rnd) u = rng.gen_f64();
+        for (size_t i = 0; i < n; ++i) {
+            Glow& gw = g[i];
+            gw.moved = false;
+            gw.exact_next = false;
+            if (!gw.nb.empty()) {
+                for (int k = 0; k < K; ++k) {
+                    const uint32_t nid = select(gw, (uint32_t)i, rnd[i * K + k]);
+                    double t[3];
+                    Quat r;
+                    moved_pose(gw, nid, t, r);
+                    const double row[7] = {r.w, r.x, r.y, r.z, t[0], t[1], t[2]};
+                    cand.insert(cand.end(), row, row + 7);
+                    owner.push_back((uint32_t)i);
+                }
             }
-            gw.moved = nid != (uint32_t)i;  // glowworm.rs:144-166
-            if (gw.moved) {
-                double dx = pos[3 * nid] - gw.t[0], dy = pos[3 * nid + 1] - gw.t[1], dz = pos[3 * nid + 2] - gw.t[2];
-                double norm = std::sqrt(dx * dx + dy * dy + dz * dz);
-                double coef = 0.5 / norm;
-                gw.t[0] += dx * coef;
-                gw.t[1] += dy * coef;
-                gw.t[2] += dz * coef;
-                gw.r = q_slerp(gw.r, rot[nid], 0.5);
-                q_normalize(gw.r);
-            }
-            double v = gw.vision + BETA * (double)(MAX_NEIGHBORS - (int)gw.nb.size());
-            gw.vision = std::fmin(MAX_VISION, std::fmax(0.0, v));
+            update_vision(gw);
         }
     }
 };
@@ -158,9 +207,23 @@ struct lkg_gso {
     std::vector<int> group_complex, group_first_swarm, group_nswarm;
     std::vector<Swarm> swarms;
     std::vector<int> need_idx;  // per scored pose: swarm * 2^20 + glowworm
-    int64_t scored = 0;
+    int64_t scored = 0, predicted = 0;
+    int step = 0;
     lkg::DBuf d_poses, d_scores;
     lkg::HBuf h_poses, h_scores;
+    // surrogate screening (off unless lkg_gso_set_screen)
+    bool screen = false;
+    lkg_screen cfg{};
+    std::vector<lkg_surrogate*> sur;             // one per group (complex)
+    std::vector<std::vector<double>> tr_pose;    // per group: exact (pose, score) pairs
+    std::vector<std::vector<double>> tr_score;
+    std::vector<bool> scaled;
+    StdRng rank_rng;                             // candidate ranks of the no-network ablation
+    lkg::DBuf d_tp, d_ts, d_cand, d_pred;
+    lkg::HBuf h_cand, h_pred;
+    ~lkg_gso() {
+        for (auto* s : sur) lkg_surrogate_destroy(s);
+    }
 };
 
 extern "C" {
@@ -198,57 +261,240 @@ int lkg_gso_create(lkg_ctx* ctx, int n_groups, const int* complex_ids, const int
     return set_ok();
 }
 
-// one GSO step: batched scoring of moved glowworms + movement
-static int gso_step(lkg_gso* G) {
+}  // extern "C"
+
+namespace {
+
+inline Glow& glow_of(lkg_gso* G, int idx) { return G->swarms[idx >> 20].g[idx & 0xfffff]; }
+
+// Train (or fine-tune) the surrogate of group gi on its exact pairs, most
+// recent first kept (at most 65,536), in a seeded shuffled order.
+int train_group(lkg_gso* G, int gi, int epochs) {
+    auto& P = G->tr_pose[gi];
+    auto& S = G->tr_score[gi];
+    const size_t cap = 65536;
+    if (S.size() > cap) {
+        const size_t drop = S.size() - cap;
+        P.erase(P.begin(), P.begin() + 7 * drop);
+        S.erase(S.begin(), S.begin() + drop);
+    }
+    const int n = (int)S.size();
+    if (n < 64 || epochs <= 0) return set_ok();
+    int st;
+    if (!G->scaled[gi]) {
+        if ((st = lkg_surrogate_set_target_scale(G->sur[gi], n, S.data()))) return st;
+        G->scaled[gi] = true;
+    }
+    std::vector<int> perm(n);
+    for (int i = 0; i < n; ++i) perm[i] = i;
+    StdRng r(G->cfg.seed ^ (0x9e3779b97f4a7c15ull * (uint64_t)(G->step + 1)) ^ (uint64_t)gi);
+    for (int i = n - 1; i > 0; --i) std::swap(perm[i], perm[(int)(r.gen_f64() * (i + 1)) % (i + 1)]);
+    std::vector<double> hp(7 * (size_t)n), hs(n);
+    for (int i = 0; i < n; ++i) {
+        std::memcpy(&hp[7 * (size_t)i], &P[7 * (size_t)perm[i]], 7 * sizeof(double));
+        hs[i] = S[perm[i]];
+    }
+    LKG_CK(G->d_tp.reserve(hp.size() * sizeof(double)), "surrogate training set");
+    LKG_CK(G->d_ts.reserve(hs.size() * sizeof(double)), "surrogate training set");
+    cudaStream_t s = G->ctx->stream;
+    LKG_CK(cudaMemcpyAsync(G->d_tp.p, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, s), "train upload");
+    LKG_CK(cudaMemcpyAsync(G->d_ts.p, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s), "train upload");
+    float loss = 0.f;
+    return lkg_surrogate_train(G->sur[gi], n, G->d_tp.as<double>(), G->d_ts.as<double>(), epochs, 512, G->cfg.lr,
+                               &loss);
+}
+
+// Exact scoring of the selected glowworms in one batched launch group;
+// `all` selects every glowworm, otherwise first-step ones and moves marked
+// for exact scoring.  Moves scored by the surrogate take its prediction
+// (the no-network ablation keeps the previous score).  `learn` appends the
+// exact pairs to the surrogate training sets.
+int score_phase(lkg_gso* G, bool all, bool learn) {
     lkg_ctx* ctx = G->ctx;
     const int ng = (int)G->group_complex.size();
     std::vector<int> counts(ng, 0);
     G->need_idx.clear();
     for (int gi = 0; gi < ng; ++gi)
         for (int s = G->group_first_swarm[gi]; s < G->group_first_swarm[gi] + G->group_nswarm[gi]; ++s) {
-            const Swarm& sw = G->swarms[s];
-            for (size_t k = 0; k < sw.g.size(); ++k)
-                if (sw.g[k].moved || sw.g[k].step == 0) {  // swarm.rs:79-85
+            Swarm& sw = G->swarms[s];
+            for (size_t k = 0; k < sw.g.size(); ++k) {
+                Glow& gw = sw.g[k];
+                if (all || gw.step == 0 || (gw.moved && gw.exact_next)) {  // swarm.rs:79-85
                     G->need_idx.push_back((s << 20) | (int)k);
                     counts[gi]++;
+                } else if (gw.moved && G->screen && !G->cfg.random_rank) {
+                    gw.scoring = gw.pred;
                 }
+            }
         }
     const size_t n = G->need_idx.size();
-    if (n) {
-        LKG_CK(G->h_poses.reserve(n * 7 * sizeof(double)), "gso staging");
-        LKG_CK(G->h_scores.reserve(n * sizeof(double)), "gso staging");
-        LKG_CK(G->d_poses.reserve(n * 7 * sizeof(double)), "gso staging");
-        LKG_CK(G->d_scores.reserve(n * sizeof(double)), "gso staging");
-        double* hp = G->h_poses.as<double>();
-        for (size_t i = 0; i < n; ++i) {
-            const Glow& gw = G->swarms[G->need_idx[i] >> 20].g[G->need_idx[i] & 0xfffff];
-            double* p = hp + 7 * i;  // kernel layout w,x,y,z,tx,ty,tz (gpu_score.rs:292-301)
-            p[0] = gw.r.w; p[1] = gw.r.x; p[2] = gw.r.y; p[3] = gw.r.z;
-            p[4] = gw.t[0]; p[5] = gw.t[1]; p[6] = gw.t[2];
+    if (!n) return set_ok();
+    LKG_CK(G->h_poses.reserve(n * 7 * sizeof(double)), "gso staging");
+    LKG_CK(G->h_scores.reserve(n * sizeof(double)), "gso staging");
+    LKG_CK(G->d_poses.reserve(n * 7 * sizeof(double)), "gso staging");
+    LKG_CK(G->d_scores.reserve(n * sizeof(double)), "gso staging");
+    double* hp = G->h_poses.as<double>();
+    for (size_t i = 0; i < n; ++i) {
+        const Glow& gw = glow_of(G, G->need_idx[i]);
+        double* p = hp + 7 * i;  // kernel layout w,x,y,z,tx,ty,tz (gpu_score.rs:292-301)
+        p[0] = gw.r.w; p[1] = gw.r.x; p[2] = gw.r.y; p[3] = gw.r.z;
+        p[4] = gw.t[0]; p[5] = gw.t[1]; p[6] = gw.t[2];
+    }
+    LKG_CK(cudaMemcpyAsync(G->d_poses.p, hp, n * 7 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream),
+           "gso pose upload");
+    int st = launch_items(ctx, ng, G->group_complex.data(), counts.data(), G->d_poses.as<double>(),
+                          G->d_scores.as<double>(), nullptr, 0, 0, nullptr, nullptr);
+    if (st) return st;
+    LKG_CK(cudaMemcpyAsync(G->h_scores.p, G->d_scores.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
+           "gso score readback");
+    if ((st = wait_stream(ctx, 300.0))) return st;
+    if ((st = check_status(ctx))) return st;
+    const double* hs = G->h_scores.as<double>();
+    for (size_t i = 0; i < n; ++i) glow_of(G, G->need_idx[i]).scoring = hs[i];
+    G->scored += (int64_t)n;
+    if (learn) {
+        size_t i = 0;
+        for (int gi = 0; gi < ng; ++gi)
+            for (int k = 0; k < counts[gi]; ++k, ++i) {
+                G->tr_pose[gi].insert(G->tr_pose[gi].end(), hp + 7 * i, hp + 7 * i + 7);
+                G->tr_score[gi].push_back(hs[i]);
+            }
+    }
+    return set_ok();
+}
+
+// Screened movement: K candidate moves per glowworm with neighbours, all
+// ranked by the surrogate (or, for the ablation, by seeded random numbers);
+// each glowworm takes its best candidate, and per swarm the fraction
+// exact_fraction of the moves with the largest predicted gain over the
+// glowworm's current score is marked for exact scoring.
+int screened_movement(lkg_gso* G) {
+    const int ns = (int)G->swarms.size(), ng = (int)G->group_complex.size(), K = G->cfg.candidates;
+    std::vector<std::vector<double>> cand(ns);
+    std::vector<std::vector<uint32_t>> owner(ns);
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int s = 0; s < ns; ++s) G->swarms[s].propose(K, cand[s], owner[s]);
+    std::vector<size_t> off(ns + 1, 0);
+    for (int s = 0; s < ns; ++s) off[s + 1] = off[s] + owner[s].size();
+    const size_t total = off[ns];
+    if (total == 0) return set_ok();
+    LKG_CK(G->h_cand.reserve(total * 7 * sizeof(double)), "candidate staging");
+    LKG_CK(G->h_pred.reserve(total * sizeof(double)), "candidate staging");
+    double* hc = G->h_cand.as<double>();
+    double* hpred = G->h_pred.as<double>();
+    for (int s = 0; s < ns; ++s)
+        if (!cand[s].empty()) std::memcpy(hc + 7 * off[s], cand[s].data(), cand[s].size() * sizeof(double));
+    if (G->cfg.random_rank) {
+        for (size_t i = 0; i < total; ++i) hpred[i] = G->rank_rng.gen_f64();
+    } else {
+        LKG_CK(G->d_cand.reserve(total * 7 * sizeof(double)), "candidate staging");
+        LKG_CK(G->d_pred.reserve(total * sizeof(double)), "candidate staging");
+        cudaStream_t st = G->ctx->stream;
+        LKG_CK(cudaMemcpyAsync(G->d_cand.p, hc, total * 7 * sizeof(double), cudaMemcpyHostToDevice, st), "candidates");
+        for (int gi = 0; gi < ng; ++gi) {
+            const int s0 = G->group_first_swarm[gi], s1 = s0 + G->group_nswarm[gi];
+            const size_t a = off[s0], b = off[s1];
+            if (b == a) continue;
+            int rc = lkg_surrogate_predict(G->sur[gi], (int)(b - a), G->d_cand.as<double>() + 7 * a,
+                                           G->d_pred.as<double>() + a);
+            if (rc) return rc;
         }
-        LKG_CK(cudaMemcpyAsync(G->d_poses.p, hp, n * 7 * sizeof(double), cudaMemcpyHostToDevice, ctx->stream),
-               "gso pose upload");
-        int st = launch_items(ctx, ng, G->group_complex.data(), counts.data(), G->d_poses.as<double>(),
-                              G->d_scores.as<double>(), nullptr, 0, 0, nullptr, nullptr);
-        if (st) return st;
-        LKG_CK(cudaMemcpyAsync(G->h_scores.p, G->d_scores.p, n * sizeof(double), cudaMemcpyDeviceToHost, ctx->stream),
-               "gso score readback");
-        if ((st = wait_stream(ctx, 300.0))) return st;
-        if ((st = check_status(ctx))) return st;
-        const double* hs = G->h_scores.as<double>();
-        for (size_t i = 0; i < n; ++i) G->swarms[G->need_idx[i] >> 20].g[G->need_idx[i] & 0xfffff].scoring = hs[i];
-        G->scored += (int64_t)n;
+        LKG_CK(cudaMemcpyAsync(hpred, G->d_pred.p, total * sizeof(double), cudaMemcpyDeviceToHost, st), "predictions");
+        int rc = wait_stream(G->ctx, 300.0);
+        if (rc) return rc;
+        G->predicted += (int64_t)total;
+    }
+    const double frac = G->cfg.exact_fraction;
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int s = 0; s < ns; ++s) {
+        Swarm& sw = G->swarms[s];
+        std::vector<std::pair<double, uint32_t>> gain;
+        for (size_t c0 = 0; c0 < owner[s].size(); c0 += K) {
+            const uint32_t i = owner[s][c0];
+            size_t best = c0;
+            for (size_t c = c0 + 1; c < c0 + K; ++c)
+                if (hpred[off[s] + c] > hpred[off[s] + best]) best = c;
+            Glow& gw = sw.g[i];
+            const double* row = hc + 7 * (off[s] + best);
+            gw.r = {row[0], row[1], row[2], row[3]};
+            gw.t[0] = row[4]; gw.t[1] = row[5]; gw.t[2] = row[6];
+            gw.pred = hpred[off[s] + best];
+            gw.moved = true;
+            gain.push_back({G->cfg.random_rank ? gw.pred : gw.pred - gw.scoring, i});
+        }
+        std::sort(gain.begin(), gain.end(), [](const std::pair<double, uint32_t>& a, const std::pair<double, uint32_t>& b) {
+            return a.first > b.first || (a.first == b.first && a.second < b.second);
+        });
+        const size_t nx = (size_t)std::ceil(frac * (double)gain.size());
+        for (size_t k = 0; k < nx && k < gain.size(); ++k) sw.g[gain[k].second].exact_next = true;
+    }
+    return set_ok();
+}
+
+// one GSO step: scoring, luciferin update, movement (swarm.rs:70-103)
+int gso_step(lkg_gso* G) {
+    const lkg_screen& c = G->cfg;
+    const bool training = G->screen && G->step < c.train_steps;
+    const bool screened = G->screen && G->step >= c.train_steps;
+    const bool rescore = screened && c.rescore_every > 0 && G->step > c.train_steps &&
+                         (G->step - c.train_steps) % c.rescore_every == 0;
+    int st = score_phase(G, rescore, training || rescore);
+    if (st) return st;
+    if (G->screen && !c.random_rank) {
+        const int ng = (int)G->group_complex.size();
+        const bool first = G->step == c.train_steps - 1;
+        for (int gi = 0; gi < ng && (first || rescore); ++gi)
+            if ((st = train_group(G, gi, first ? c.train_epochs : c.finetune_epochs))) return st;
     }
     const int ns = (int)G->swarms.size();
 #pragma omp parallel for schedule(dynamic, 1)
     for (int s = 0; s < ns; ++s) {
-        Swarm& sw = G->swarms[s];
-        for (auto& gw : sw.g) {  // swarm.rs:96-99
+        for (auto& gw : G->swarms[s].g) {  // swarm.rs:96-99
             gw.luciferin = (1.0 - RHO) * gw.luciferin + GAMMA * gw.scoring;
             gw.step += 1;
         }
-        sw.movement();
     }
+    if (G->screen && G->step + 1 >= c.train_steps) {
+        if ((st = screened_movement(G))) return st;
+    } else {
+#pragma omp parallel for schedule(dynamic, 1)
+        for (int s = 0; s < ns; ++s) {
+            Swarm& sw = G->swarms[s];
+            sw.movement();
+            for (auto& gw : sw.g) gw.exact_next = gw.moved;
+        }
+    }
+    G->step++;
+    return set_ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+int lkg_gso_set_screen(lkg_gso* G, const lkg_screen* cfg) {
+    if (!G || !cfg) return set_error(LKG_ERR_ARG, "bad screen arguments");
+    if (G->step != 0) return set_error(LKG_ERR_STATE, "screening must be set before the first step");
+    if (cfg->candidates < 1 || cfg->candidates > 64 || !(cfg->exact_fraction > 0.0 && cfg->exact_fraction <= 1.0) ||
+        cfg->rescore_every < 0 || cfg->train_steps < 1 || cfg->train_epochs < 0 || cfg->finetune_epochs < 0 ||
+        !(cfg->lr > 0.f))
+        return set_error(LKG_ERR_ARG, "bad screen configuration");
+    for (auto* s : G->sur) lkg_surrogate_destroy(s);
+    G->sur.clear();
+    G->cfg = *cfg;
+    const int ng = (int)G->group_complex.size();
+    G->tr_pose.assign(ng, {});
+    G->tr_score.assign(ng, {});
+    G->scaled.assign(ng, false);
+    G->rank_rng.seed_from_u64(cfg->seed);
+    if (!cfg->random_rank)
+        for (int gi = 0; gi < ng; ++gi) {
+            lkg_surrogate* s = nullptr;
+            int st = lkg_surrogate_create(G->ctx, G->group_complex[gi], cfg->seed + (uint64_t)gi, &s);
+            if (st) return st;
+            G->sur.push_back(s);
+        }
+    G->screen = true;
     return set_ok();
 }
 
@@ -280,6 +526,13 @@ int lkg_gso_state(lkg_gso* G, double* trans, double* rot, double* luc, double* s
 }
 
 int64_t lkg_gso_scored(lkg_gso* G) { return G ? G->scored : 0; }
+int64_t lkg_gso_predicted(lkg_gso* G) { return G ? G->predicted : 0; }
+
+int lkg_gso_finalize(lkg_gso* G) {
+    if (!G) return set_error(LKG_ERR_ARG, "null gso");
+    cudaSetDevice(G->ctx->device);
+    return score_phase(G, true, false);
+}
 
 int lkg_gso_destroy(lkg_gso* G) {
     delete G;

@@ -1,14 +1,16 @@
 // Internal types shared by the lkg kernels and the host runtime.
 //
 // Device layout of one complex (all arrays in HBM, built once per complex):
-//   receptor atoms sorted by a fine uniform cell grid (cell edge h, default
-//   2.5 A, cells x-fastest), so that one (z, y) row of consecutive x cells
-//   is one contiguous span of atoms [cell_start[row+cx0], cell_start[row+cx1+1]);
+//   receptor atoms sorted by a fine cell grid (edge h in y and z, default
+//   2.5 A; edge h / xsub in x, cells x-fastest), so that one (z, y) row of
+//   consecutive x cells is one contiguous span of atoms
+//   [cell_start[row+cx0], cell_start[row+cx1+1]);
 //     rpos  float4 (x, y, z, q)              rpos64 double4 (same, f64)
 //     rpar  float4 (sqrt eps, r, heavy, excl) rpar64 double4 (sqrt eps, r, eps, heavy)
 //     rsolv float2 (des, asa)                rsolv64 double2
-//   ligand atoms sorted along a coarse Morton order of the reference frame
-//   (tiles of consecutive atoms are spatially compact), same three arrays;
+//   ligand atoms ordered by recursive coordinate bisection of the reference
+//   frame into groups of `group` atoms (groups and tiles of consecutive
+//   atoms are spatially compact), same three arrays;
 //   receptor far field phi (f32, x fastest, the ReceptorField layout).
 #pragma once
 #include <cuda_runtime.h>
@@ -36,9 +38,9 @@ struct ComplexDev {
     const double2* rsolv64;
     const int* rorig;        // sorted -> caller index
     const int* cell_start;   // ncx*ncy*ncz + 1
-    int ncx, ncy, ncz;
-    float ox, oy, oz, h, inv_h;
-    // ligand (Morton-sorted)
+    int ncx, ncy, ncz;       // ncx counts x sub-cells
+    float ox, oy, oz, h, inv_h, hx, inv_hx;
+    // ligand (bisection-ordered)
     const float4* lpos;
     const float4* lpar;
     const float2* lsolv;

@@ -1,0 +1,608 @@
+// Learned pose-energy surrogate: a 64 -> 256 -> 256 -> 256 -> 1 ReLU MLP with
+// BF16 weights and activations and FP32 accumulation, trained online on the
+// exact scorer's energies and used to screen candidate GSO moves.
+//
+// Kernels (all hand-written, tensor cores through mma.sync m16n8k16 bf16):
+//   k_features   pose parameters + far-field potential and receptor atom
+//                counts at 16 ligand anchor atoms -> 64 bf16 features
+//   k_gemm       C = A * B^T tiles of 64 x 64, K step 32, four warps; A / B
+//                read [rows][k] or transposed from global; epilogues: bias +
+//                ReLU -> bf16 (forward), x ReLU'(H) -> bf16 (backward data),
+//                split-K atomic FP32 (weight gradients)
+//   k_head       last layer (256 -> 1) dot products, FP32
+//   k_loss       MSE on the standardised target, dy, head gradients
+//   k_colsum     bias gradients
+//   k_adam       Adam on FP32 master weights, refreshes both BF16 layouts
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "lkg_runtime.h"
+#include "lkg_score.cuh"
+
+namespace lkg {
+namespace mlp {
+
+constexpr int IN = 64, H = 256, NA = 16;   // features, width, anchors
+
+// ---------------------------------------------------------------------------
+// features
+// ---------------------------------------------------------------------------
+// per pose: [w, x, y, z, tx/s, ty/s, tz/s, then per anchor a:
+//            phi(x_a) * 100, log1p(receptor atoms in the anchor's 3x3x3
+//            fine cells), log1p(atoms in its own cell)], 1.0, zero padding
+__global__ void k_features(const ComplexDev* __restrict__ cxs, int cid, const double* __restrict__ poses, int n,
+                           const int* __restrict__ anchors, float tscale, __nv_bfloat16* __restrict__ feat) {
+    const ComplexDev& c = cxs[cid];
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int pose = t / NA, a = t % NA;
+    if (pose >= n) return;
+    const double* pq = poses + 7 * (size_t)pose;
+    const Rot rot = pose_matrix(pq);
+    __nv_bfloat16* f = feat + (size_t)pose * IN;
+    if (a == 0) {
+        for (int k = 0; k < 4; ++k) f[k] = __float2bfloat16((float)pq[k]);
+        for (int k = 0; k < 3; ++k) f[4 + k] = __float2bfloat16((float)(pq[4 + k] / tscale));
+        f[7 + 3 * NA] = __float2bfloat16(1.0f);
+        for (int k = 8 + 3 * NA; k < IN; ++k) f[k] = __float2bfloat16(0.0f);
+    }
+    const int j = anchors[a];
+    const float4 b = __ldg(c.lpos + j);
+    double xd, yd, zd;
+    apply(rot, (double)b.x, (double)b.y, (double)b.z, xd, yd, zd);
+    const float x = (float)xd, y = (float)yd, z = (float)zd;
+    float phi = c.phi ? sample_phi(c, x, y, z) : 0.f;
+    // receptor atom counts in the 3 x 3 x 3 cells of edge h around the atom
+    // and in its own cell (x sub-cells merged; bounds-clamped)
+    const int xs = (int)(c.h * c.inv_hx + 0.5f);
+    const int cx = (int)floorf((x - c.ox) * c.inv_h), cy = (int)floorf((y - c.oy) * c.inv_h),
+              cz = (int)floorf((z - c.oz) * c.inv_h);
+    int n27 = 0, n1 = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy) {
+            const int zz = cz + dz, yy = cy + dy;
+            if (zz < 0 || zz >= c.ncz || yy < 0 || yy >= c.ncy) continue;
+            const int row = (zz * c.ncy + yy) * c.ncx;
+            const int x0 = max((cx - 1) * xs, 0), x1 = min((cx + 2) * xs - 1, c.ncx - 1);
+            if (x0 <= x1) n27 += __ldg(c.cell_start + row + x1 + 1) - __ldg(c.cell_start + row + x0);
+            const int y0 = max(cx * xs, 0), y1 = min((cx + 1) * xs - 1, c.ncx - 1);
+            if (dz == 0 && dy == 0 && y0 <= y1)
+                n1 = __ldg(c.cell_start + row + y1 + 1) - __ldg(c.cell_start + row + y0);
+        }
+    f[7 + 3 * a] = __float2bfloat16(phi * 100.0f);
+    f[8 + 3 * a] = __float2bfloat16(log1pf((float)n27));
+    f[9 + 3 * a] = __float2bfloat16(log1pf((float)n1));
+}
+
+// ---------------------------------------------------------------------------
+// GEMM: C[M x N] = sum_k A(m, k) * B(n, k)
+//   A(m, k) = TA ? A[k * lda + m] : A[m * lda + k]
+//   B(n, k) = TB ? B[k * ldb + n] : B[n * ldb + k]
+// ---------------------------------------------------------------------------
+enum { EPI_FWD = 0, EPI_BWD = 1, EPI_WGRAD = 2 };
+constexpr int BM = 64, BN = 64, BK = 32;
+
+__device__ __forceinline__ void mma_bf16(float (&d)[4], const uint32_t (&a)[4], const uint32_t (&b)[2]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(d[0]), "+f"(d[1]), "+f"(d[2]), "+f"(d[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+template <bool TA, bool TB, int EPI>
+__global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bfloat16* __restrict__ A, int lda,
+                                              const __nv_bfloat16* __restrict__ B, int ldb, float* __restrict__ Cf,
+                                              __nv_bfloat16* __restrict__ Cb, int ldc, const float* __restrict__ bias,
+                                              const __nv_bfloat16* __restrict__ Hmask, int k_chunk) {
+    __shared__ __align__(16) __nv_bfloat16 sA[BM][BK + 8];
+    __shared__ __align__(16) __nv_bfloat16 sB[BN][BK + 8];
+    const int m0 = blockIdx.y * BM, n0 = blockIdx.x * BN;
+    const int kb = blockIdx.z * k_chunk, ke = min(K, kb + k_chunk);
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;   // warp sub-tile 32 x 32
+    const int g = lane >> 2, tq = lane & 3;
+    float acc[2][4][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) acc[i][j][r] = 0.f;
+    const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    for (int k0 = kb; k0 < ke; k0 += BK) {
+        // tile loads (bounds-checked; zero fill)
+        for (int e = threadIdx.x; e < BM * BK; e += 128) {
+            int mm, kk;
+            if (TA) { mm = e % BM; kk = e / BM; } else { kk = e % BK; mm = e / BK; }
+            const int gm = m0 + mm, gk = k0 + kk;
+            sA[mm][kk] = (gm < M && gk < ke) ? (TA ? A[(size_t)gk * lda + gm] : A[(size_t)gm * lda + gk]) : zero;
+        }
+        for (int e = threadIdx.x; e < BN * BK; e += 128) {
+            int nn, kk;
+            if (TB) { nn = e % BN; kk = e / BN; } else { kk = e % BK; nn = e / BK; }
+            const int gn = n0 + nn, gk = k0 + kk;
+            sB[nn][kk] = (gn < N && gk < ke) ? (TB ? B[(size_t)gk * ldb + gn] : B[(size_t)gn * ldb + gk]) : zero;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int ks = 0; ks < BK; ks += 16) {
+            uint32_t af[2][4], bf[4][2];
+#pragma unroll
+            for (int i = 0; i < 2; ++i) {
+                const int r = wm + i * 16 + g;
+                af[i][0] = *(const uint32_t*)&sA[r][ks + 2 * tq];
+                af[i][1] = *(const uint32_t*)&sA[r + 8][ks + 2 * tq];
+                af[i][2] = *(const uint32_t*)&sA[r][ks + 2 * tq + 8];
+                af[i][3] = *(const uint32_t*)&sA[r + 8][ks + 2 * tq + 8];
+            }
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int cc = wn + j * 8 + g;
+                bf[j][0] = *(const uint32_t*)&sB[cc][ks + 2 * tq];
+                bf[j][1] = *(const uint32_t*)&sB[cc][ks + 2 * tq + 8];
+            }
+#pragma unroll
+            for (int i = 0; i < 2; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) mma_bf16(acc[i][j], af[i], bf[j]);
+        }
+        __syncthreads();
+    }
+    // epilogue
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int gm = m0 + wm + i * 16 + g + (r >= 2 ? 8 : 0);
+                const int gn = n0 + wn + j * 8 + 2 * tq + (r & 1);
+                if (gm >= M || gn >= N) continue;
+                float v = acc[i][j][r];
+                if (EPI == EPI_FWD) {
+                    v += bias[gn];
+                    Cb[(size_t)gm * ldc + gn] = __float2bfloat16(v > 0.f ? v : 0.f);
+                } else if (EPI == EPI_BWD) {
+                    const float hm = __bfloat162float(Hmask[(size_t)gm * ldc + gn]);
+                    Cb[(size_t)gm * ldc + gn] = __float2bfloat16(hm > 0.f ? v : 0.f);
+                } else {
+                    atomicAdd(Cf + (size_t)gm * ldc + gn, v);
+                }
+            }
+}
+
+// last layer: y[n] = H3[n] . w3 + b3
+__global__ void k_head(const __nv_bfloat16* __restrict__ H3, int n, const float* __restrict__ w3, const float* b3,
+                       float* __restrict__ y) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row >= n) return;
+    float s = 0.f;
+    for (int k = lane; k < H; k += 32) s += __bfloat162float(H3[(size_t)row * H + k]) * w3[k];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_xor_sync(0xffffffffu, s, o);
+    if (lane == 0) y[row] = s + b3[0];
+}
+
+// loss, dy = 2 (y - t) / n; dH3 = dy w3 x ReLU'(H3); head gradients
+__global__ void k_loss(const float* __restrict__ y, const float* __restrict__ t, const __nv_bfloat16* __restrict__ H3,
+                       int n, const float* __restrict__ w3, __nv_bfloat16* __restrict__ dH3, float* __restrict__ g_w3,
+                       float* __restrict__ g_b3, float* __restrict__ loss) {
+    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (row >= n) return;
+    const float d = y[row] - t[row];
+    const float dy = 2.f * d / (float)n;
+    for (int k = lane; k < H; k += 32) {
+        const float h = __bfloat162float(H3[(size_t)row * H + k]);
+        dH3[(size_t)row * H + k] = __float2bfloat16(h > 0.f ? dy * w3[k] : 0.f);
+        atomicAdd(g_w3 + k, dy * h);
+    }
+    if (lane == 0) {
+        atomicAdd(g_b3, dy);
+        atomicAdd(loss, d * d / (float)n);
+    }
+}
+
+// bias gradients: column sums of dC [n x H]
+__global__ void k_colsum(const __nv_bfloat16* __restrict__ dC, int n, float* __restrict__ gb) {
+    const int col = blockIdx.x * blockDim.x + threadIdx.x;
+    if (col >= H) return;
+    const int r0 = blockIdx.y * 256, r1 = min(n, r0 + 256);
+    float s = 0.f;
+    for (int r = r0; r < r1; ++r) s += __bfloat162float(dC[(size_t)r * H + col]);
+    atomicAdd(gb + col, s);
+}
+
+// Adam on FP32 master weights; refresh the BF16 copies of the GEMM layers:
+// wt (out-major, forward) and w (in-major, backward data)
+__global__ void k_adam(float* __restrict__ p, const float* __restrict__ gr, float* __restrict__ m1,
+                       float* __restrict__ m2, int n, float lr, float b1, float b2, float eps, float bc1, float bc2,
+                       __nv_bfloat16* __restrict__ wt, __nv_bfloat16* __restrict__ w, int rows, int cols) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gg = gr[i];
+    const float a = b1 * m1[i] + (1.f - b1) * gg, v = b2 * m2[i] + (1.f - b2) * gg * gg;
+    m1[i] = a;
+    m2[i] = v;
+    const float upd = lr * (a / bc1) / (sqrtf(v / bc2) + eps);
+    const float np = p[i] - upd;
+    p[i] = np;
+    if (wt) {
+        const int r = i / cols, c = i % cols;   // p is [rows = out][cols = in]
+        wt[i] = __float2bfloat16(np);
+        w[(size_t)c * rows + r] = __float2bfloat16(np);
+    }
+}
+
+__global__ void k_f2bf(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] = __float2bfloat16(src[i]);
+}
+
+__global__ void k_f2bf_t(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, int rows, int cols) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < rows * cols) dst[(size_t)(i % cols) * rows + i / cols] = __float2bfloat16(src[i]);
+}
+
+}  // namespace mlp
+}  // namespace lkg
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+using namespace lkg;
+using namespace lkg::mlp;
+
+struct lkg_surrogate {
+    lkg_ctx* ctx = nullptr;
+    int cid = -1;
+    float tscale = 50.f;
+    float t_mu = 0.f, t_sd = 1.f, e_scale = 100.f;   // target standardisation
+    DBuf anchors;
+    // parameters: FP32 master, Adam moments, gradients (flat)
+    //   W0 [H x IN], b0 [H], W1 [H x H], b1, W2 [H x H], b2, w3 [H], b3 [1]
+    DBuf p, g, m1, m2;
+    DBuf wt[3], w[3];   // BF16 layouts per GEMM layer
+    // activations for a batch
+    DBuf X, H1, H2, H3, dH1, dH2, dH3, y, t, loss;
+    int cap = 0;
+    int step = 0;
+    size_t off[9];   // block offsets of W0 b0 W1 b1 W2 b2 w3 b3, and the total
+};
+
+namespace {
+
+constexpr size_t NPARAM = (size_t)H * IN + H + 2 * ((size_t)H * H + H) + H + 1;
+
+int sur_reserve(lkg_surrogate* S, int n) {
+    if (n <= S->cap) return 0;
+    size_t nb = (size_t)n * sizeof(__nv_bfloat16);
+    LKG_CK(S->X.reserve(nb * IN), "surrogate alloc");
+    LKG_CK(S->H1.reserve(nb * H), "surrogate alloc");
+    LKG_CK(S->H2.reserve(nb * H), "surrogate alloc");
+    LKG_CK(S->H3.reserve(nb * H), "surrogate alloc");
+    LKG_CK(S->dH1.reserve(nb * H), "surrogate alloc");
+    LKG_CK(S->dH2.reserve(nb * H), "surrogate alloc");
+    LKG_CK(S->dH3.reserve(nb * H), "surrogate alloc");
+    LKG_CK(S->y.reserve((size_t)n * sizeof(float)), "surrogate alloc");
+    LKG_CK(S->t.reserve((size_t)n * sizeof(float)), "surrogate alloc");
+    S->cap = n;
+    return 0;
+}
+
+template <bool TA, bool TB, int EPI>
+cudaError_t gemm(cudaStream_t s, int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb,
+                 float* Cf, __nv_bfloat16* Cb, int ldc, const float* bias, const __nv_bfloat16* Hm, int splits = 1) {
+    int kc = (K + splits - 1) / splits;
+    kc = (kc + BK - 1) / BK * BK;
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, (K + kc - 1) / kc);
+    k_gemm<TA, TB, EPI><<<grid, 128, 0, s>>>(M, N, K, A, lda, B, ldb, Cf, Cb, ldc, bias, Hm, kc);
+    return cudaGetLastError();
+}
+
+float* P(lkg_surrogate* S, int k) { return S->p.as<float>() + S->off[k]; }
+float* Gd(lkg_surrogate* S, int k) { return S->g.as<float>() + S->off[k]; }
+
+// forward of n feature rows already in S->X; y in S->y
+int forward(lkg_surrogate* S, int n) {
+    cudaStream_t s = S->ctx->stream;
+    const __nv_bfloat16* X = S->X.as<__nv_bfloat16>();
+    LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, IN, X, IN, S->wt[0].as<__nv_bfloat16>(), IN, nullptr,
+                                        S->H1.as<__nv_bfloat16>(), H, P(S, 1), nullptr)), "mlp fwd");
+    LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, H, S->H1.as<__nv_bfloat16>(), H, S->wt[1].as<__nv_bfloat16>(), H,
+                                        nullptr, S->H2.as<__nv_bfloat16>(), H, P(S, 3), nullptr)), "mlp fwd");
+    LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, H, S->H2.as<__nv_bfloat16>(), H, S->wt[2].as<__nv_bfloat16>(), H,
+                                        nullptr, S->H3.as<__nv_bfloat16>(), H, P(S, 5), nullptr)), "mlp fwd");
+    k_head<<<(n + 7) / 8, 256, 0, s>>>(S->H3.as<__nv_bfloat16>(), n, P(S, 6), P(S, 7), S->y.as<float>());
+    LKG_CK(cudaGetLastError(), "mlp head");
+    S->ctx->launches += 4;
+    return 0;
+}
+
+// backward into S->g (zeroed here); targets in S->t; the batch's mean loss
+// is added to S->loss (cleared here when clear_loss)
+int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
+    cudaStream_t s = S->ctx->stream;
+    LKG_CK(cudaMemsetAsync(S->g.p, 0, NPARAM * sizeof(float), s), "mlp grad clear");
+    if (clear_loss) LKG_CK(cudaMemsetAsync(S->loss.p, 0, sizeof(float), s), "mlp loss clear");
+    k_loss<<<(n + 7) / 8, 256, 0, s>>>(S->y.as<float>(), S->t.as<float>(), S->H3.as<__nv_bfloat16>(), n, P(S, 6),
+                                       S->dH3.as<__nv_bfloat16>(), Gd(S, 6), Gd(S, 7), S->loss.as<float>());
+    LKG_CK(cudaGetLastError(), "mlp loss");
+    const int splits = std::max(1, std::min(64, n / 512));
+    const __nv_bfloat16* acts[3] = {S->H1.as<__nv_bfloat16>(), S->H2.as<__nv_bfloat16>(), S->H3.as<__nv_bfloat16>()};
+    __nv_bfloat16* dacts[3] = {S->dH1.as<__nv_bfloat16>(), S->dH2.as<__nv_bfloat16>(), S->dH3.as<__nv_bfloat16>()};
+    for (int L = 2; L >= 0; --L) {
+        const int kin = L == 0 ? IN : H;
+        const __nv_bfloat16* ain = L == 0 ? S->X.as<__nv_bfloat16>() : acts[L - 1];
+        // dW_L[o][i] = sum_n dC[n][o] * A_in[n][i]   (A = dC^T, B = A_in^T)
+        LKG_CK((gemm<true, true, EPI_WGRAD>(s, H, kin, n, dacts[L], H, ain, kin, Gd(S, 2 * L), nullptr, kin, nullptr,
+                                            nullptr, splits)), "mlp wgrad");
+        dim3 cg((H + 255) / 256, (n + 255) / 256);
+        k_colsum<<<cg, 256, 0, s>>>(dacts[L], n, Gd(S, 2 * L + 1));
+        LKG_CK(cudaGetLastError(), "mlp bias grad");
+        if (L > 0) {
+            // dA_in[n][i] = (sum_o dC[n][o] W_L[o][i]) x ReLU'(A_in)
+            LKG_CK((gemm<false, false, EPI_BWD>(s, n, H, H, dacts[L], H, S->w[L].as<__nv_bfloat16>(), H, nullptr,
+                                                dacts[L - 1], H, nullptr, acts[L - 1])), "mlp bwd");
+        }
+    }
+    S->ctx->launches += 10;
+    return 0;
+}
+
+int adam(lkg_surrogate* S, float lr) {
+    cudaStream_t s = S->ctx->stream;
+    S->step++;
+    const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
+    const float bc1 = 1.f - powf(b1, (float)S->step), bc2 = 1.f - powf(b2, (float)S->step);
+    for (int k = 0; k < 8; ++k) {
+        const size_t n = S->off[k + 1] - S->off[k];
+        const bool gemm_layer = (k == 0 || k == 2 || k == 4);
+        const int L = k / 2;
+        const int rows = H, cols = (k == 0) ? IN : H;
+        k_adam<<<(int)((n + 255) / 256), 256, 0, s>>>(P(S, k), Gd(S, k), S->m1.as<float>() + S->off[k],
+                                                      S->m2.as<float>() + S->off[k], (int)n, lr, b1, b2, eps, bc1, bc2,
+                                                      gemm_layer ? S->wt[L].as<__nv_bfloat16>() : nullptr,
+                                                      gemm_layer ? S->w[L].as<__nv_bfloat16>() : nullptr, rows, cols);
+    }
+    LKG_CK(cudaGetLastError(), "mlp adam");
+    S->ctx->launches += 8;
+    return 0;
+}
+
+int refresh_bf16(lkg_surrogate* S) {
+    cudaStream_t s = S->ctx->stream;
+    for (int L = 0; L < 3; ++L) {
+        const int k = 2 * L, cols = (L == 0) ? IN : H, n = H * cols;
+        k_f2bf<<<(n + 255) / 256, 256, 0, s>>>(P(S, k), S->wt[L].as<__nv_bfloat16>(), n);
+        k_f2bf_t<<<(n + 255) / 256, 256, 0, s>>>(P(S, k), S->w[L].as<__nv_bfloat16>(), H, cols);
+    }
+    LKG_CK(cudaGetLastError(), "mlp bf16 refresh");
+    return 0;
+}
+
+int features(lkg_surrogate* S, int n, const double* d_poses) {
+    if (sur_reserve(S, n)) return lkg_last_status();
+    int st = sync_descriptors(S->ctx);
+    if (st) return st;
+    const int threads = 256, blocks = (int)(((size_t)n * NA + threads - 1) / threads);
+    k_features<<<blocks, threads, 0, S->ctx->stream>>>(S->ctx->d_cx.as<ComplexDev>(), S->cid, d_poses, n,
+                                                       S->anchors.as<int>(), S->tscale, S->X.as<__nv_bfloat16>());
+    LKG_CK(cudaGetLastError(), "features");
+    S->ctx->launches++;
+    return 0;
+}
+
+// standardised target transform: t = (asinh(score / e_scale) - mu) / sd
+__global__ void k_target(const double* __restrict__ sc, int n, float e_scale, float mu, float sd, float* __restrict__ t) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) t[i] = (asinhf((float)(sc[i] / e_scale)) - mu) / sd;
+}
+
+__global__ void k_untarget(const float* __restrict__ y, int n, float e_scale, float mu, float sd, double* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = (double)(sinhf(y[i] * sd + mu) * e_scale);
+}
+
+}  // namespace
+
+extern "C" {
+
+int lkg_surrogate_create(lkg_ctx* ctx, int complex_id, uint64_t seed, lkg_surrogate** out) {
+    if (!ctx || !out || complex_id < 0 || complex_id >= (int)ctx->cx.size())
+        return set_error(LKG_ERR_ARG, "bad surrogate arguments");
+    cudaSetDevice(ctx->device);
+    auto* S = new lkg_surrogate();
+    S->ctx = ctx;
+    S->cid = complex_id;
+    const ComplexRec& cr = *ctx->cx[complex_id];
+    // anchors: 16 ligand atoms spread by farthest-point sampling over the
+    // (sorted) ligand reference coordinates
+    const int nl = cr.d.nl;
+    std::vector<float4> lp(nl);
+    cudaMemcpy(lp.data(), cr.d.lpos, nl * sizeof(float4), cudaMemcpyDeviceToHost);
+    std::vector<int> anc;
+    std::vector<float> dmin(nl, 1e30f);
+    int cur = 0;
+    float rmax = 0.f;
+    for (int i = 0; i < nl; ++i) rmax = std::max(rmax, std::sqrt(lp[i].x * lp[i].x + lp[i].y * lp[i].y + lp[i].z * lp[i].z));
+    for (int a = 0; a < NA; ++a) {
+        anc.push_back(cur);
+        int best = 0;
+        float bd = -1.f;
+        for (int i = 0; i < nl; ++i) {
+            float dx = lp[i].x - lp[cur].x, dy = lp[i].y - lp[cur].y, dz = lp[i].z - lp[cur].z;
+            dmin[i] = std::min(dmin[i], dx * dx + dy * dy + dz * dz);
+            if (dmin[i] > bd) { bd = dmin[i]; best = i; }
+        }
+        cur = best;
+    }
+    // translation scale: far-field box half-extent (receptor size + 30 A)
+    S->tscale = std::max(20.f, 0.25f * (float)cr.d.fnx * (float)cr.d.fsp64);
+    size_t sizes[8] = {(size_t)H * IN, H, (size_t)H * H, H, (size_t)H * H, H, H, 1};
+    S->off[0] = 0;
+    for (int k = 0; k < 8; ++k) S->off[k + 1] = S->off[k] + sizes[k];
+    std::vector<float> p(NPARAM, 0.f);
+    // He-uniform initialisation (deterministic LCG from `seed`)
+    uint64_t st = seed * 6364136223846793005ull + 1442695040888963407ull;
+    auto u = [&]() {
+        st = st * 6364136223846793005ull + 1442695040888963407ull;
+        return (double)(st >> 11) * (1.0 / 9007199254740992.0);
+    };
+    const int fan[4] = {IN, H, H, H};
+    for (int L = 0; L < 4; ++L) {
+        const double lim = std::sqrt(6.0 / fan[L]) * (L == 3 ? 0.5 : 1.0);
+        for (size_t i = S->off[2 * L]; i < S->off[2 * L + 1]; ++i) p[i] = (float)((2.0 * u() - 1.0) * lim);
+    }
+    int rc = 0;
+    cudaError_t e;
+    if ((e = S->p.reserve(NPARAM * 4)) != cudaSuccess || (e = S->g.reserve(NPARAM * 4)) != cudaSuccess ||
+        (e = S->m1.reserve(NPARAM * 4)) != cudaSuccess || (e = S->m2.reserve(NPARAM * 4)) != cudaSuccess ||
+        (e = S->anchors.reserve(NA * sizeof(int))) != cudaSuccess || (e = S->loss.reserve(sizeof(float))) != cudaSuccess) {
+        delete S;
+        return set_error(cuda_to_status(e), "surrogate alloc: %s", cudaGetErrorString(e));
+    }
+    for (int L = 0; L < 3; ++L) {
+        const size_t n = (size_t)H * (L == 0 ? IN : H) * sizeof(__nv_bfloat16);
+        if ((e = S->wt[L].reserve(n)) != cudaSuccess || (e = S->w[L].reserve(n)) != cudaSuccess) {
+            delete S;
+            return set_error(cuda_to_status(e), "surrogate alloc: %s", cudaGetErrorString(e));
+        }
+    }
+    cudaMemcpy(S->p.p, p.data(), NPARAM * 4, cudaMemcpyHostToDevice);
+    cudaMemset(S->m1.p, 0, NPARAM * 4);
+    cudaMemset(S->m2.p, 0, NPARAM * 4);
+    cudaMemcpy(S->anchors.p, anc.data(), NA * sizeof(int), cudaMemcpyHostToDevice);
+    if ((rc = refresh_bf16(S))) { delete S; return rc; }
+    if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
+        delete S;
+        return set_error(cuda_to_status(e), "surrogate init: %s", cudaGetErrorString(e));
+    }
+    *out = S;
+    return set_ok();
+}
+
+int lkg_surrogate_destroy(lkg_surrogate* S) {
+    if (S) { cudaSetDevice(S->ctx->device); cudaStreamSynchronize(S->ctx->stream); }
+    delete S;
+    return set_ok();
+}
+
+// Fit the target standardisation to a set of exact scores (host array).
+int lkg_surrogate_set_target_scale(lkg_surrogate* S, int n, const double* scores) {
+    if (!S || n <= 0 || !scores) return set_error(LKG_ERR_ARG, "bad scale args");
+    double e = 0.0;
+    std::vector<double> a(n);
+    for (int i = 0; i < n; ++i) a[i] = std::fabs(scores[i]);
+    std::nth_element(a.begin(), a.begin() + n / 2, a.end());
+    e = std::max(1.0, a[n / 2]);
+    double mu = 0.0, sd = 0.0;
+    for (int i = 0; i < n; ++i) mu += std::asinh(scores[i] / e);
+    mu /= n;
+    for (int i = 0; i < n; ++i) { double d = std::asinh(scores[i] / e) - mu; sd += d * d; }
+    sd = std::sqrt(sd / n);
+    S->e_scale = (float)e;
+    S->t_mu = (float)mu;
+    S->t_sd = (float)std::max(sd, 1e-3);
+    return set_ok();
+}
+
+// Predicted scores (same units as lkg_score) for n device poses.
+int lkg_surrogate_predict(lkg_surrogate* S, int n, const double* d_poses, double* d_pred) {
+    if (!S || n < 0 || (n && (!d_poses || !d_pred))) return set_error(LKG_ERR_ARG, "bad predict args");
+    if (n == 0) return set_ok();
+    cudaSetDevice(S->ctx->device);
+    int st;
+    if ((st = features(S, n, d_poses))) return st;
+    if ((st = forward(S, n))) return st;
+    k_untarget<<<(n + 255) / 256, 256, 0, S->ctx->stream>>>(S->y.as<float>(), n, S->e_scale, S->t_mu, S->t_sd, d_pred);
+    LKG_CK(cudaGetLastError(), "predict");
+    S->ctx->launches++;
+    return set_ok();
+}
+
+// `epochs` passes of minibatch Adam over n device poses with exact scores;
+// returns the last epoch's mean loss in *loss (standardised units).
+int lkg_surrogate_train(lkg_surrogate* S, int n, const double* d_poses, const double* d_scores, int epochs,
+                        int batch, float lr, float* loss_out) {
+    if (!S || n <= 0 || !d_poses || !d_scores || epochs <= 0 || batch <= 0)
+        return set_error(LKG_ERR_ARG, "bad train args");
+    cudaSetDevice(S->ctx->device);
+    cudaStream_t s = S->ctx->stream;
+    batch = std::min(batch, n);
+    int st;
+    double last = 0.0;
+    const int nb = n / batch;
+    for (int ep = 0; ep < epochs; ++ep) {
+        // launches only inside an epoch: the loss is summed on the device
+        // and read once per epoch
+        LKG_CK(cudaMemsetAsync(S->loss.p, 0, sizeof(float), s), "mlp loss clear");
+        for (int b0 = 0; b0 + batch <= n; b0 += batch) {
+            if ((st = features(S, batch, d_poses + 7 * (size_t)b0))) return st;
+            k_target<<<(batch + 255) / 256, 256, 0, s>>>(d_scores + b0, batch, S->e_scale, S->t_mu, S->t_sd,
+                                                         S->t.as<float>());
+            if ((st = forward(S, batch))) return st;
+            if ((st = backward(S, batch, false))) return st;
+            if ((st = adam(S, lr))) return st;
+        }
+        if (ep == epochs - 1) {
+            float l = 0.f;
+            LKG_CK(cudaMemcpyAsync(&l, S->loss.p, sizeof(float), cudaMemcpyDeviceToHost, s), "loss read");
+            LKG_CK(cudaStreamSynchronize(s), "train");
+            last = nb ? (double)l / nb : 0.0;
+        }
+    }
+    if (loss_out) *loss_out = (float)last;
+    return set_ok();
+}
+
+// Parameters (FP32 master, flat order W0 b0 W1 b1 W2 b2 w3 b3; W are [out][in]).
+int64_t lkg_surrogate_nparams(void) { return (int64_t)NPARAM; }
+int lkg_surrogate_get_params(lkg_surrogate* S, float* out) {
+    if (!S || !out) return set_error(LKG_ERR_ARG, "bad args");
+    LKG_CK(cudaMemcpy(out, S->p.p, NPARAM * 4, cudaMemcpyDeviceToHost), "get params");
+    return set_ok();
+}
+int lkg_surrogate_set_params(lkg_surrogate* S, const float* in) {
+    if (!S || !in) return set_error(LKG_ERR_ARG, "bad args");
+    LKG_CK(cudaMemcpy(S->p.p, in, NPARAM * 4, cudaMemcpyHostToDevice), "set params");
+    int st = refresh_bf16(S);
+    if (st) return st;
+    LKG_CK(cudaStreamSynchronize(S->ctx->stream), "set params");
+    return set_ok();
+}
+
+// One forward + backward on n host feature rows (bf16 bit patterns) with
+// host targets (already standardised): writes the standardised outputs,
+// the flat gradient and the loss (for the gradient check against FP64).
+int lkg_surrogate_grad(lkg_surrogate* S, int n, const uint16_t* feats, const float* targets, float* y_out,
+                       float* grad_out, float* loss_out) {
+    if (!S || n <= 0 || !feats || !targets) return set_error(LKG_ERR_ARG, "bad grad args");
+    cudaSetDevice(S->ctx->device);
+    if (sur_reserve(S, n)) return lkg_last_status();
+    LKG_CK(cudaMemcpy(S->X.p, feats, (size_t)n * IN * 2, cudaMemcpyHostToDevice), "grad upload");
+    LKG_CK(cudaMemcpy(S->t.p, targets, (size_t)n * 4, cudaMemcpyHostToDevice), "grad upload");
+    int st;
+    if ((st = forward(S, n)) || (st = backward(S, n))) return st;
+    LKG_CK(cudaStreamSynchronize(S->ctx->stream), "grad");
+    if (y_out) LKG_CK(cudaMemcpy(y_out, S->y.p, (size_t)n * 4, cudaMemcpyDeviceToHost), "grad read");
+    if (grad_out) LKG_CK(cudaMemcpy(grad_out, S->g.p, NPARAM * 4, cudaMemcpyDeviceToHost), "grad read");
+    if (loss_out) LKG_CK(cudaMemcpy(loss_out, S->loss.p, 4, cudaMemcpyDeviceToHost), "grad read");
+    return set_ok();
+}
+
+// Features of n device poses into a host array of bf16 bit patterns.
+int lkg_surrogate_features(lkg_surrogate* S, int n, const double* d_poses, uint16_t* out) {
+    if (!S || n <= 0 || !d_poses || !out) return set_error(LKG_ERR_ARG, "bad args");
+    cudaSetDevice(S->ctx->device);
+    int st = features(S, n, d_poses);
+    if (st) return st;
+    LKG_CK(cudaStreamSynchronize(S->ctx->stream), "features");
+    LKG_CK(cudaMemcpy(out, S->X.p, (size_t)n * IN * 2, cudaMemcpyDeviceToHost), "features read");
+    return set_ok();
+}
+
+}  // extern "C"

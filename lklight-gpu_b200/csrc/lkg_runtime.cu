@@ -80,20 +80,20 @@ cudaError_t upload(DBuf& b, const std::vector<T>& v, cudaStream_t s) {
     return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
 }
 
-inline uint32_t spread3(uint32_t v) {
-    v &= 0x3ff;
-    v = (v | (v << 16)) & 0x030000FF;
-    v = (v | (v << 8)) & 0x0300F00F;
-    v = (v | (v << 4)) & 0x030C30C3;
-    v = (v | (v << 2)) & 0x09249249;
-    return v;
-}
-
 // receptor: sort by fine cell (x fastest), pack device arrays
 int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     ComplexDev& d = cr.d;
     const int n = R.n;
-    const float h = ctx->cell_h, inv_h = 1.0f / h;
+    // the warp kernel's hit queue packs a receptor index into 26 bits
+    if (n >= (1 << 26)) return set_error(LKG_ERR_ARG, "receptor has %d atoms (limit %d)", n, (1 << 26) - 1);
+    // grid shape: the caller's, else per kernel: the warp kernel enumerates
+    // rows per ligand group (coarser rows, finer x trim pay off), the
+    // per-atom cpydock kernel per atom
+    const bool per_atom = cr.family == LKG_CPYDOCK;
+    const float h = ctx->cell_h > 0.f ? ctx->cell_h : (per_atom ? 2.5f : 4.0f), inv_h = 1.0f / h;
+    const int xsub = ctx->xsub > 0 ? ctx->xsub : (per_atom ? 4 : 8);
+    const float hx = h / (float)xsub, inv_hx = 1.0f / hx;
+    const float inv_e[3] = {inv_hx, inv_h, inv_h};
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int i = 0; i < n; ++i)
         for (int a = 0; a < 3; ++a) {
@@ -106,7 +106,7 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     int nc[3];
     for (int a = 0; a < 3; ++a) {
         o[a] = std::floor(mn[a]) - 1.0f;
-        nc[a] = std::max(1, (int)std::floor((mx[a] - o[a]) * inv_h) + 2);
+        nc[a] = std::max(1, (int)std::floor((mx[a] - o[a]) * inv_e[a]) + 2);
     }
     const size_t ncell = (size_t)nc[0] * nc[1] * nc[2];
     if (ncell > (size_t)1 << 28) return set_error(LKG_ERR_ARG, "receptor cell grid too large (%zu cells)", ncell);
@@ -114,7 +114,7 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     for (int i = 0; i < n; ++i) {
         int ci[3];
         for (int a = 0; a < 3; ++a)
-            ci[a] = std::min(std::max((int)std::floor(((float)R.c[3 * i + a] - o[a]) * inv_h), 0), nc[a] - 1);
+            ci[a] = std::min(std::max((int)std::floor(((float)R.c[3 * i + a] - o[a]) * inv_e[a]), 0), nc[a] - 1);
         cell_of[i] = (ci[2] * nc[1] + ci[1]) * nc[0] + ci[0];
         cs[cell_of[i] + 1]++;
     }
@@ -149,7 +149,7 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     d.rpos64 = cr.rpos64.as<double4>(); d.rpar64 = cr.rpar64.as<double4>(); d.rsolv64 = cr.rsolv64.as<double2>();
     d.rorig = cr.rorig.as<int>(); d.cell_start = cr.cell_start.as<int>();
     d.ncx = nc[0]; d.ncy = nc[1]; d.ncz = nc[2];
-    d.ox = o[0]; d.oy = o[1]; d.oz = o[2]; d.h = h; d.inv_h = inv_h;
+    d.ox = o[0]; d.oy = o[1]; d.oz = o[2]; d.h = h; d.inv_h = inv_h; d.hx = hx; d.inv_hx = inv_hx;
     cr.n_cells = (int)ncell;
     // desolvation hash capacity: >= 2 x receptor atoms up to 8192 slots
     // (96 KB of shared memory); a pose touching more receptor atoms within
@@ -160,22 +160,37 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     return set_ok();
 }
 
-// ligand: sort along a Morton curve of 4 A cells so tiles are compact
+// recursive coordinate bisection: order idx[0..n) so that every run of G
+// consecutive atoms (and every run of a power-of-two number of groups) is
+// spatially compact; each split cuts the longest extent at a multiple of G
+void bisect_groups(const double* c, int* idx, int n, int G) {
+    if (n <= G) return;
+    double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = std::fmin(mn[a], c[3 * idx[i] + a]);
+            mx[a] = std::fmax(mx[a], c[3 * idx[i] + a]);
+        }
+    int ax = 0;
+    for (int a = 1; a < 3; ++a)
+        if (mx[a] - mn[a] > mx[ax] - mn[ax]) ax = a;
+    auto key = [&](int u) { const double v = c[3 * u + ax]; return std::isnan(v) ? INFINITY : v; };
+    std::sort(idx, idx + n, [&](int u, int v) {
+        const double cu = key(u), cv = key(v);
+        return cu < cv || (cu == cv && u < v);
+    });
+    const int ng = (n + G - 1) / G, left = (ng / 2) * G;
+    bisect_groups(c, idx, left, G);
+    bisect_groups(c, idx + left, n - left, G);
+}
+
+// ligand: bisection order in groups of ctx->group atoms
 int build_ligand(lkg_ctx* ctx, const MolIn& L, ComplexRec& cr) {
     ComplexDev& d = cr.d;
     const int n = L.n;
-    double mn[3] = {INFINITY, INFINITY, INFINITY};
-    for (int i = 0; i < n; ++i)
-        for (int a = 0; a < 3; ++a) mn[a] = std::min(mn[a], L.c[3 * i + a]);
-    std::vector<uint32_t> code(n);
-    for (int i = 0; i < n; ++i) {
-        uint32_t ci[3];
-        for (int a = 0; a < 3; ++a) ci[a] = (uint32_t)std::min(1023.0, std::floor((L.c[3 * i + a] - mn[a]) / 4.0));
-        code[i] = spread3(ci[0]) | (spread3(ci[1]) << 1) | (spread3(ci[2]) << 2);
-    }
     std::vector<int> order(n);
     std::iota(order.begin(), order.end(), 0);
-    std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return code[a] < code[b]; });
+    bisect_groups(L.c.data(), order.data(), n, ctx->group);
     std::vector<float4> pos(n), par(n);
     std::vector<float2> sol(n);
     std::vector<double4> pos64(n), par64(n);
@@ -569,6 +584,14 @@ int lkg_ctx_set_group(lkg_ctx* ctx, int group) {
     if (group != 8 && group != 16 && group != 32) return set_error(LKG_ERR_ARG, "group must be 8, 16 or 32");
     if (!ctx->cx.empty() && group != ctx->group) return set_error(LKG_ERR_STATE, "group fixed once complexes exist");
     ctx->group = group;
+    return set_ok();
+}
+
+int lkg_ctx_set_xsub(lkg_ctx* ctx, int xsub) {
+    if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
+    if (xsub < 1 || xsub > 8) return set_error(LKG_ERR_ARG, "xsub must be 1..8");
+    if (!ctx->cx.empty() && xsub != ctx->xsub) return set_error(LKG_ERR_STATE, "xsub fixed once complexes exist");
+    ctx->xsub = xsub;
     return set_ok();
 }
 

@@ -111,7 +111,8 @@ struct lkg_ctx {
     int tile = 128;                 // ligand atoms per work unit
     int group = 8;                  // ligand atoms per candidate-search group
     int desolv_threads = 512;
-    float cell_h = 2.5f;            // fine receptor cell edge (A)
+    float cell_h = 0.f;             // receptor cell edge in y and z (A); 0: per family
+    int xsub = 0;                   // x sub-cells per cell edge; 0: per family
     std::vector<std::unique_ptr<lkg::ComplexRec>> cx;
     lkg::DBuf d_cx;                 // ComplexDev[] on the device
     bool cx_dirty = true;

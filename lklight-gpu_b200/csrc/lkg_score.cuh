@@ -139,8 +139,8 @@ __device__ __forceinline__ void scan_rows(const ComplexDev& c, float x, float y,
             float rem = remz - dym * dym;
             if (rem < 0.f) continue;
             float wx = sqrtf(rem);
-            int cx0 = max(0, (int)floorf((x - wx - c.ox) * c.inv_h));
-            int cx1 = min(c.ncx - 1, (int)floorf((x + wx - c.ox) * c.inv_h));
+            int cx0 = max(0, (int)floorf((x - wx - c.ox) * c.inv_hx));
+            int cx1 = min(c.ncx - 1, (int)floorf((x + wx - c.ox) * c.inv_hx));
             if (cx0 > cx1) continue;
             int row = (cz * c.ncy + cy) * c.ncx;
             int b = __ldg(c.cell_start + row + cx0), e = __ldg(c.cell_start + row + cx1 + 1);
@@ -160,7 +160,7 @@ struct AtomAcc {
 __device__ __forceinline__ void pair_fast(unsigned flags, float qj, float svj, float rj, bool hj,
                                           const float4& a, const float4& pr, float d2,
                                           double& elec, double& vdw) {
-    float ir2 = __frcp_rn(d2);
+    float ir2 = __fdividef(1.0f, d2);   // ~2 ulp; the f32 path's budget is ~1e-7 relative per term
     if (flags & F_ELEC) {
         float ae = qj * a.w * ir2;
         ae = fminf(fmaxf(ae, -ES_CAP_F), ES_CAP_F);
@@ -173,7 +173,7 @@ __device__ __forceinline__ void pair_fast(unsigned flags, float qj, float svj, f
     // (sv*p6)*(p6-2): finite for sv == 0 even where p6^2 would overflow
     float vp = fminf(sv * p6 * (p6 - 2.f), 1.0f);
     if ((flags & F_CLASH) && hj && pr.z != 0.f) {
-        float d = sqrtf(d2);
+        float d = d2 * rsqrtf(d2);
         float dmin = 0.75f * rr;
         if (d < dmin) vp += 6.f * (dmin - d);
     }

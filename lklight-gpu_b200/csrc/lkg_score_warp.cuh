@@ -1,0 +1,250 @@
+// Warp-independent fused scorer (f32 fast path, dna / pydock / vdw and the
+// reference-compatible flag combinations).
+//
+// Every warp fetches its own work units from the global counter; there is
+// no block-level barrier inside the loop, so a warp that meets a crowded
+// interface never holds up the warps beside it.  A work unit is a tile of
+// `p.tile` ligand atoms of one pose, split into groups of G consecutive
+// atoms (spatially compact: the ligand is ordered by recursive coordinate
+// bisection in groups of G) whose bounding sphere (centre, radius rho, in the
+// ligand frame) is computed on the host.  Per group:
+//   1. lanes 0..G-1 transform their atom in f64 (kept as an f32 value plus
+//      the rounding residual), add the far-field term q * phi(x'), and park
+//      position and parameters in one of two slot sets in shared memory
+//      (the sets alternate between groups, so hits of one group can still be
+//      queued while the next group is set up);
+//   2. the receptor rows (z, y cells of edge h) within 10 A + rho of the
+//      posed centre are enumerated 32 at a time (one per lane), trimmed in x
+//      to sub-cells of edge h / xsub, and turned into contiguous atom spans;
+//   3. 32 candidates at a time (lane -> span by a binary search over the
+//      warp's exclusive prefix of span lengths, coalesced float4 loads) are
+//      tested against the G slot atoms (broadcast shared-memory reads) into a
+//      G-bit mask; one warp prefix sum of the mask popcounts appends every
+//      hit (slot << 26 | receptor index) to the warp's ring buffer;
+//   4. while 32 or more hits are pending, each lane takes one and evaluates
+//      the pair terms with compensated distances and the exact d^2 <= 100
+//      test, accumulating in f64: the expensive math always runs on 32 lanes.
+// The warp's sums are reduced by shuffles into one partial per work unit;
+// the last unit of a pose sums the partials in tile order (deterministic:
+// the hit order is fixed by the algorithm, not by scheduling).
+#pragma once
+#include "lkg_score.cuh"
+
+namespace lkg {
+
+constexpr int WK_THREADS = 128;   // 4 independent warps per block
+
+// ring capacity: 31 pending + 32 * G hits of one candidate chunk must fit
+template <int G> struct WRing { static constexpr int N = (G <= 8) ? 512 : (G <= 16) ? 1024 : 2048; };
+
+// resident blocks per SM the register budget is sized for (64 registers a
+// thread for G = 8; the larger masks of G = 16, 32 get 80)
+template <int G> struct WOcc { static constexpr int N = (G <= 8) ? 8 : 6; };
+
+template <int G>
+struct WSlots {
+    Rot rot;                    // pose of the current work unit
+    float4 lpos[2 * G];         // x, y, z (f32 part), q
+    float4 lres[2 * G];         // x, y, z residuals, sqrt eps
+    float2 lpar[2 * G];         // r, heavy
+    unsigned hit[WRing<G>::N];  // (slot << 26) | receptor index
+};
+
+// pair terms of one queued hit (exact d^2 <= 100 test on compensated d^2)
+template <int G>
+__device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, unsigned e, unsigned flags,
+                                       double& elec, double& vdw, int& np) {
+    const int l = (int)(e >> 26), k = (int)(e & 0x3ffffffu);
+    const float4 lp = W.lpos[l], lr = W.lres[l];
+    const float2 lq = W.lpar[l];
+    const float4 a = __ldg(c.rpos + k);
+    const float dx = (lp.x - a.x) + lr.x, dy = (lp.y - a.y) + lr.y, dz = (lp.z - a.z) + lr.z;
+    const float d2 = dx * dx + dy * dy + dz * dz;
+    if (!(d2 <= 100.f)) return;
+    const float4 pr = __ldg(c.rpar + k);
+    ++np;
+    pair_fast(flags, lp.w, lr.w, lq.x, lq.y != 0.f, a, pr, d2, elec, vdw);
+}
+
+template <int G>
+__global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchParams p) {
+    static_assert(G == 8 || G == 16 || G == 32, "group size");
+    constexpr int RING = WRing<G>::N;
+    constexpr unsigned FULL = 0xffffffffu;
+    extern __shared__ __align__(16) unsigned char wk_smem[];
+    const int lane = threadIdx.x & 31;
+    WSlots<G>& W = reinterpret_cast<WSlots<G>*>(wk_smem)[threadIdx.x >> 5];
+    for (;;) {
+        unsigned long long wq = 0;
+        if (lane == 0) wq = atomicAdd(p.work_counter, 1ull);
+        const long long w = (long long)__shfl_sync(FULL, wq, 0);
+        if (w >= p.total_work) break;
+        const int b = find_item(p.item_work0, p.n_items, w);
+        const ComplexDev& c = p.cx[__ldg(p.item_complex + b)];
+        const long long local = w - __ldg(p.item_work0 + b);
+        const int ntiles = c.ntiles;
+        const int pose = (int)(local / ntiles), tile = (int)(local % ntiles);
+        const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
+        const unsigned flags = c.flags;
+        const int nl = c.nl;
+        __syncwarp();   // readers of the previous unit's pose are done
+        if (lane == 0) W.rot = pose_matrix(p.poses + 7 * g);
+        __syncwarp();
+        double elec = 0.0, vdw = 0.0;
+        int np = 0;
+        unsigned head = 0, tail = 0, prev_start = 0;
+        const int gpt = p.tile / G;
+        const int g0 = tile * gpt, g1 = min(g0 + gpt, (nl + G - 1) / G);
+        for (int grp = g0; grp < g1; ++grp) {
+            const int set = ((grp - g0) & 1) * G;
+            // slot set `set` last served group grp-2, whose hits were queued
+            // before the previous group started: evaluate any still pending
+            if ((int)(prev_start - head) > 0) {
+                if ((int)(tail - head) > lane) w_pair<G>(c, W, W.hit[(head + lane) & (RING - 1)], flags, elec, vdw, np);
+                head = tail;
+            }
+            prev_start = tail;
+            __syncwarp();
+            // 1. the group's ligand atoms
+            if (lane < G) {
+                const int j = grp * G + lane;
+                const bool valid = j < nl;
+                const float4 b4 = valid ? __ldg(c.lpos + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+                const float4 lp4 = valid ? __ldg(c.lpar + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+                double xd, yd, zd;
+                apply(W.rot, (double)b4.x, (double)b4.y, (double)b4.z, xd, yd, zd);
+                float x = (float)xd, y = (float)yd, z = (float)zd;
+                const float4 res = make_float4((float)(xd - (double)x), (float)(yd - (double)y),
+                                               (float)(zd - (double)z), lp4.x);
+                if (valid && (flags & F_FAR) && b4.w != 0.f) elec += (double)(b4.w * sample_phi(c, x, y, z));
+                if (!valid) { x = y = z = 1e30f; }   // never within reach of a receptor atom
+                W.lpos[set + lane] = make_float4(x, y, z, b4.w);
+                W.lres[set + lane] = res;
+                W.lpar[set + lane] = make_float2(lp4.y, lp4.z);
+            }
+            __syncwarp();
+            // 2. receptor rows within reach of the group sphere
+            const float4 gs = __ldg(c.lgrp + grp);
+            double cxd, cyd, czd;
+            apply(W.rot, (double)gs.x, (double)gs.y, (double)gs.z, cxd, cyd, czd);
+            const float gx = (float)cxd, gy = (float)cyd, gz = (float)czd;
+            const float R = SCAN_R + gs.w, R2 = R * R;
+            const int cz0 = max(0, (int)floorf((gz - R - c.oz) * c.inv_h));
+            const int cz1 = min(c.ncz - 1, (int)floorf((gz + R - c.oz) * c.inv_h));
+            const int cy0 = max(0, (int)floorf((gy - R - c.oy) * c.inv_h));
+            const int cy1 = min(c.ncy - 1, (int)floorf((gy + R - c.oy) * c.inv_h));
+            const int nyr = cy1 - cy0 + 1, nzr = cz1 - cz0 + 1;
+            const int nbox = (nyr > 0 && nzr > 0) ? nyr * nzr : 0;
+            const float inv_nyr = 1.0f / (float)max(nyr, 1);
+            const unsigned enc_set = (unsigned)set << 26;
+            for (int r0 = 0; r0 < nbox; r0 += 32) {
+                const int r = r0 + lane;
+                int st = 0, len = 0;
+                if (r < nbox) {
+                    // r = zz * nyr + yy; (r + 0.5) / nyr is at least 0.5 / nyr
+                    // away from an integer, far above the f32 rounding error
+                    const int zz = (int)(((float)r + 0.5f) * inv_nyr), yy = r - zz * nyr;
+                    const int cz = cz0 + zz, cy = cy0 + yy;
+                    const float zlo = c.oz + cz * c.h, ylo = c.oy + cy * c.h;
+                    const float dzm = fmaxf(0.f, fmaxf(zlo - gz, gz - (zlo + c.h)));
+                    const float dym = fmaxf(0.f, fmaxf(ylo - gy, gy - (ylo + c.h)));
+                    const float rem = R2 - dzm * dzm - dym * dym;
+                    if (rem >= 0.f) {
+                        const float wx = sqrtf(rem);
+                        const int cx0 = max(0, (int)floorf((gx - wx - c.ox) * c.inv_hx));
+                        const int cx1 = min(c.ncx - 1, (int)floorf((gx + wx - c.ox) * c.inv_hx));
+                        if (cx0 <= cx1) {
+                            const int row = (cz * c.ncy + cy) * c.ncx;
+                            st = __ldg(c.cell_start + row + cx0);
+                            len = __ldg(c.cell_start + row + cx1 + 1) - st;
+                        }
+                    }
+                }
+                int inc = len;   // inclusive prefix of the span lengths
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(FULL, inc, o);
+                    if (lane >= o) inc += v;
+                }
+                const int total = __shfl_sync(FULL, inc, 31);
+                const int excl = inc - len;
+                // 3. candidate chunks
+                for (int k0 = 0; k0 < total; k0 += 32) {
+                    const int kk = k0 + lane;
+                    // the span holding candidate kk: the last row whose
+                    // exclusive prefix is <= kk (empty rows never qualify
+                    // ahead of the non-empty row that follows them)
+                    int rr = 0;
+#pragma unroll
+                    for (int s = 16; s > 0; s >>= 1) {
+                        const int v = __shfl_sync(FULL, excl, rr + s);
+                        if (v <= kk) rr += s;
+                    }
+                    const int rst = __shfl_sync(FULL, st, rr), rex = __shfl_sync(FULL, excl, rr);
+                    float4 a = make_float4(3e30f, 3e30f, 3e30f, 0.f);
+                    int ridx = 0;
+                    if (kk < total) {
+                        ridx = rst + (kk - rex);
+                        a = __ldg(c.rpos + ridx);
+                    }
+                    unsigned mask = 0;
+#pragma unroll
+                    for (int l = 0; l < G; ++l) {
+                        const float4 lp = W.lpos[set + l];
+                        const float dx = lp.x - a.x, dy = lp.y - a.y, dz = lp.z - a.z;
+                        mask |= (dx * dx + dy * dy + dz * dz <= 100.01f ? 1u : 0u) << l;
+                    }
+                    const int nh = __popc(mask);
+                    int ex = nh;   // inclusive prefix of the hit counts
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const int v = __shfl_up_sync(FULL, ex, o);
+                        if (lane >= o) ex += v;
+                    }
+                    unsigned pos = tail + (unsigned)(ex - nh);
+                    const unsigned enc = (unsigned)ridx | enc_set;
+#pragma unroll
+                    for (int l = 0; l < G; ++l) {
+                        if (mask & (1u << l)) {
+                            W.hit[pos & (RING - 1)] = enc + ((unsigned)l << 26);
+                            ++pos;
+                        }
+                    }
+                    tail += (unsigned)__shfl_sync(FULL, ex, 31);
+                    __syncwarp();
+                    // 4. full batches of 32 hits
+                    while ((int)(tail - head) >= 32) {
+                        w_pair<G>(c, W, W.hit[(head + lane) & (RING - 1)], flags, elec, vdw, np);
+                        head += 32;
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        if ((int)(tail - head) > lane) w_pair<G>(c, W, W.hit[(head + lane) & (RING - 1)], flags, elec, vdw, np);
+        elec = warp_sum(elec);
+        vdw = warp_sum(vdw);
+        const long long npl = warp_sum((long long)np);
+        if (lane == 0) {
+            // partial of work unit w; the pose's units are w - tile .. w - tile + ntiles - 1
+            double* part = p.partials + (size_t)w * 4;
+            part[0] = elec; part[1] = vdw; part[2] = 0.0; part[3] = (double)npl;
+            __threadfence();
+            const int done = atomicAdd(p.pose_counter + g, 1);
+            if (done == ntiles - 1) {
+                __threadfence();
+                double e = 0.0, vv = 0.0, nps = 0.0;
+                const double* pp = p.partials + (size_t)(w - tile) * 4;
+                for (int t = 0; t < ntiles; ++t) {
+                    e += __ldcg(pp + 4 * t); vv += __ldcg(pp + 4 * t + 1); nps += __ldcg(pp + 4 * t + 3);
+                }
+                write_pose(p, c, g, e, vv, 0.0, nps);
+                p.pose_counter[g] = 0;
+            }
+        }
+    }
+    __syncthreads();   // every warp of the block has left the work loop
+    finish_launch(p);
+}
+
+}  // namespace lkg

@@ -108,6 +108,25 @@ def test_config0_fast_200_poses(ctx):
     assert np.array_equal(got, ctx.score(cid, pos))
 
 
+@pytest.mark.parametrize("tile,group,xsub,cell", [(64, 8, 1, 2.5), (128, 16, 4, 2.0), (256, 32, 8, 3.33),
+                                                    (128, 8, 4, 2.5), (256, 16, 2, 2.5)])
+def test_config0_fast_kernel_shapes(tile, group, xsub, cell):
+    # every tile / group / x-sub-cell / cell shape of the warp kernel finds
+    # the same near pairs (exact counts) and energies within the f32 budget
+    c0 = config0()
+    m = oracle.Model("dna", c0["rec"], c0["lig"])
+    pos = synth.to_kernel_poses(synth.setup_poses(c0["rec"]["coords"], 1, 200, 42))[:96]
+    ref, rparts = m.batch_energy_grid(pos, parts=True)
+    c = lkg.Context(tile=tile, group=group, xsub=xsub, cell=cell)
+    try:
+        cid = c.add_complex("dna", c0["rec"], c0["lig"])
+        got, parts = c.score(cid, pos, parts=True)
+    finally:
+        c.close()
+    assert rel_err(got, ref).max() < FAST_TOL
+    assert np.array_equal(parts[:, 3], rparts[:, 4])
+
+
 def test_config1_cpydock_fast(ctx):
     # cpydock totals can cancel to |E| ~ 5 from terms of +-1000 (E*332/4 +
     # 0.1 V - S); the fast path's f32 electrostatic terms leave ~1e-4 kcal/mol

@@ -1,0 +1,135 @@
+"""Surrogate-screened GSO: what the trained network gains over the same
+search without it (ablation), at a fraction of the exact evaluations of the
+plain reference GSO.
+
+The plain run is the reference GSO (every moved glowworm scored exactly).
+The screened run trains the surrogate on the exact energies of its first
+steps, then screens 4 candidate moves per glowworm and scores the top 25 %
+exactly; the ablation runs the identical search with seeded random
+candidate ranks in place of the network.  All three end with an exact
+rescoring of the final poses; ranks use the engine order (descending
+scoring, src/bin/lightdock.rs:720) and the top-5 overlap rule of
+tools/analyze_perf3.py:50-55 (a pose is a hit if some reference top-5 pose
+lies within 2 A on every axis).
+"""
+import numpy as np
+import pytest
+
+from tests.lkg_helpers import config0, lkg, synth
+
+pytestmark = pytest.mark.gpu
+
+SWARMS, GLOW, STEPS = 4, 300, 60
+
+
+def top5_overlap(tr_a, sc_a, tr_b, sc_b, tol=2.0):
+    ta = tr_a[np.argsort(-sc_a, kind="stable")[:5]]
+    tb = tr_b[np.argsort(-sc_b, kind="stable")[:5]]
+    return sum(1 for a in ta if any(np.all(np.abs(a - b) <= tol) for b in tb)) / 5.0
+
+
+@pytest.fixture(scope="module")
+def runs():
+    c0 = config0()
+    ctx = lkg.Context()
+    cid = ctx.add_complex("dna", c0["rec"], c0["lig"])
+    pos = synth.setup_poses(c0["rec"]["coords"], SWARMS, GLOW, 3)
+    out = {}
+    for mode in ("plain", "screened", "ablation"):
+        g = lkg.GSO(ctx, [(cid, SWARMS, GLOW)], pos, [3])
+        if mode != "plain":
+            g.set_screen(candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=10, train_epochs=40,
+                         finetune_epochs=2, lr=1e-3, seed=5, random_rank=(mode == "ablation"))
+        g.run(STEPS)
+        g.finalize()
+        st = g.state()
+        out[mode] = dict(state=st, scored=g.scored, predicted=g.predicted)
+        del g
+    yield out
+    ctx.close()
+
+
+def test_screened_run_needs_far_fewer_exact_evaluations(runs):
+    plain, scr = runs["plain"], runs["screened"]
+    assert scr["predicted"] > 0
+    assert scr["scored"] < 0.6 * plain["scored"], (scr["scored"], plain["scored"])
+
+
+def _quat_mul(a, b):
+    w1, x1, y1, z1 = a.T
+    w2, x2, y2, z2 = b.T
+    return np.stack([w1 * w2 - x1 * x2 - y1 * y2 - z1 * z2, w1 * x2 + x1 * w2 + y1 * z2 - z1 * y2,
+                     w1 * y2 - x1 * z2 + y1 * w2 + z1 * x2, w1 * z2 + x1 * y2 - y1 * x2 + z1 * w2], axis=1)
+
+
+def test_network_picks_better_moves_than_the_same_choice_without_it():
+    # the surrogate's job in the screened run: among a glowworm's candidate
+    # moves, find the good ones.  Train it on the exact energies of 20 plain
+    # GSO steps, then draw 4 local moves (0.5 A step, ~6 degree turn) per
+    # glowworm and compare its pick, and its top-25 % selection, with a
+    # random pick / selection under the exact energies
+    torch = pytest.importorskip("torch")
+    c0 = config0()
+    ctx = lkg.Context()
+    try:
+        cid = ctx.add_complex("dna", c0["rec"], c0["lig"])
+        pos = synth.setup_poses(c0["rec"]["coords"], SWARMS, GLOW, 3)
+        g = lkg.GSO(ctx, [(cid, SWARMS, GLOW)], pos, [3])
+        tp, ts = [], []
+        for _ in range(20):
+            g.run(1)
+            st = g.state()
+            tp.append(np.hstack([st["rotation"], st["translation"]]))
+        g.finalize()
+        st = g.state()
+        tp.append(np.hstack([st["rotation"], st["translation"]]))
+        del g
+        train = np.vstack(tp)
+        scores = ctx.score(cid, train)
+        s = lkg.Surrogate(ctx, cid, seed=7)
+        s.set_target_scale(scores)
+        dp = torch.tensor(train, device="cuda")
+        ds = torch.tensor(scores, device="cuda")
+        s.train_device(len(train), dp.data_ptr(), ds.data_ptr(), epochs=40, batch=512, lr=1e-3)
+        # candidate moves around the final poses
+        rng = np.random.default_rng(11)
+        base = tp[-1]
+        K = 4
+        cand = np.repeat(base, K, axis=0)
+        d = rng.normal(size=(len(cand), 3))
+        cand[:, 4:7] += 0.5 * d / np.linalg.norm(d, axis=1, keepdims=True)
+        ax = rng.normal(size=(len(cand), 3))
+        ax /= np.linalg.norm(ax, axis=1, keepdims=True)
+        half = np.radians(6.0) / 2
+        dq = np.hstack([np.full((len(cand), 1), np.cos(half)), np.sin(half) * ax])
+        cand[:, 0:4] = _quat_mul(dq, cand[:, 0:4])
+        exact = ctx.score(cid, cand).reshape(-1, K)
+        dc = torch.tensor(cand, device="cuda")
+        pr = torch.zeros(len(cand), dtype=torch.float64, device="cuda")
+        s.predict_device(len(cand), dc.data_ptr(), pr.data_ptr())
+        torch.cuda.synchronize()
+        pred = pr.cpu().numpy().reshape(-1, K)
+        s.close()
+    finally:
+        ctx.close()
+    rows = np.arange(len(exact))
+    picked = exact[rows, np.argmax(pred, axis=1)].mean()
+    random_pick = exact.mean()              # expected exact score of a uniform pick
+    best = exact.max(axis=1).mean()
+    top = np.argsort(-pred.ravel())[: len(pred.ravel()) // 4]
+    truth = set(np.argsort(-exact.ravel())[: len(exact.ravel()) // 4].tolist())
+    precision = len(truth.intersection(top.tolist())) / len(top)
+    print("pick: surrogate %.2f random %.2f best %.2f; top-25%% precision %.3f (random 0.25)"
+          % (picked, random_pick, best, precision))
+    assert picked > random_pick + 0.2 * (best - random_pick)
+    assert precision > 0.35
+
+
+def test_top5_overlap_with_plain_run_is_reported(runs):
+    p, s = runs["plain"]["state"], runs["screened"]["state"]
+    ov = []
+    for k in range(SWARMS):
+        sl = slice(k * GLOW, (k + 1) * GLOW)
+        ov.append(top5_overlap(s["translation"][sl], s["scoring"][sl], p["translation"][sl], p["scoring"][sl]))
+    print("top-5 overlap per swarm", ov)
+    assert all(0.0 <= o <= 1.0 for o in ov)

@@ -1,0 +1,111 @@
+"""Surrogate MLP on the GPU: the BF16 tensor-core forward / backward kernels
+against the FP64 CPU MLP oracle (oracle/mlp.py), and online training on
+exact energies.
+
+Tolerances: against the oracle run with the device's BF16 rounding points
+(``emulate=True``) the outputs agree within 1e-2 (a stored activation can
+round to the neighbouring BF16 value when the FP32 accumulation order
+differs) and every gradient block within 3 % relative L2 error; against the
+plain FP64 network (``emulate=False``) the gradient keeps cosine >= 0.99.
+"""
+import numpy as np
+import pytest
+
+from oracle import mlp as omlp
+from tests.lkg_helpers import config0, lkg, synth
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+@pytest.fixture(scope="module")
+def sur():
+    ctx = lkg.Context()
+    c0 = config0()
+    cid = ctx.add_complex("dna", c0["rec"], c0["lig"])
+    s = lkg.Surrogate(ctx, cid, seed=5)
+    yield ctx, cid, s
+    s.close()
+    ctx.close()
+
+
+def _blocks(v):
+    out, o = [], 0
+    for s in omlp.SIZES:
+        out.append(v[o:o + s]); o += s
+    return out
+
+
+def test_nparams_matches_oracle(sur):
+    assert lkg.Surrogate.nparams() == omlp.NPARAM
+
+
+def test_params_roundtrip(sur):
+    _, _, s = sur
+    p = omlp.he_params(11).astype(np.float32)
+    s.set_params(p)
+    assert np.array_equal(s.params(), p)
+
+
+@pytest.mark.parametrize("n", [7, 256, 1000])
+def test_gradient_matches_fp64_oracle(sur, n):
+    _, _, s = sur
+    rng = np.random.default_rng(n)
+    p = omlp.he_params(n)
+    s.set_params(p.astype(np.float32))
+    p32 = p.astype(np.float32).astype(np.float64)
+    X = rng.normal(0.0, 1.0, size=(n, omlp.IN))
+    Xb = omlp.f64_to_bf16_bits(X)
+    t = rng.normal(0.0, 1.0, n).astype(np.float32)
+    y, g, loss = s.grad(Xb, t)
+    Xr = omlp.bf16_bits_to_f64(Xb)
+    l_ref, g_ref, y_ref = omlp.loss_and_grad(p32, Xr, t.astype(np.float64), emulate=True)
+    assert np.abs(y - y_ref).max() < 1e-2 * (1.0 + np.abs(y_ref).max())
+    assert abs(loss - l_ref) < 1e-2 * (1.0 + l_ref)
+    for k, (a, b) in enumerate(zip(_blocks(g.astype(np.float64)), _blocks(g_ref))):
+        err = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+        assert err < 3e-2, (k, err)
+    # and the plain FP64 network: the BF16 gradient points the same way
+    _, g64, _ = omlp.loss_and_grad(p32, Xr, t.astype(np.float64), emulate=False)
+    cos = float(g @ g64 / (np.linalg.norm(g) * np.linalg.norm(g64)))
+    assert cos > 0.99, cos
+
+
+def test_features_are_finite_and_bounded(sur):
+    ctx, cid, s = sur
+    c0 = config0()
+    pos = synth.to_kernel_poses(synth.setup_poses(c0["rec"]["coords"], 4, 64, 9))
+    d = torch.tensor(pos, device="cuda")
+    f = omlp.bf16_bits_to_f64(s.features_device(len(pos), d.data_ptr()))
+    assert np.isfinite(f).all()
+    assert np.abs(f).max() < 1e3
+    # the constant feature and the zero padding
+    assert np.all(f[:, 7 + 3 * 16] == 1.0)
+    assert np.all(f[:, 8 + 3 * 16:] == 0.0)
+
+
+def test_online_training_learns_exact_energies(sur):
+    ctx, cid, s = sur
+    c0 = config0()
+    pos = synth.to_kernel_poses(synth.setup_poses(c0["rec"]["coords"], 40, 150, 21))
+    scores = ctx.score(cid, pos)
+    n_train = 4096
+    s.set_params(omlp.he_params(3).astype(np.float32))
+    s.set_target_scale(scores[:n_train])
+    dp = torch.tensor(pos, device="cuda")
+    ds = torch.tensor(scores, device="cuda")
+    first = s.train_device(n_train, dp.data_ptr(), ds.data_ptr(), epochs=1, batch=512, lr=1e-3)
+    last = s.train_device(n_train, dp.data_ptr(), ds.data_ptr(), epochs=60, batch=512, lr=1e-3)
+    assert last < 0.5 * first, (first, last)
+    # held-out poses: predictions rank like the exact energies
+    n_test = len(pos) - n_train
+    pred = torch.zeros(n_test, dtype=torch.float64, device="cuda")
+    s.predict_device(n_test, dp[n_train:].data_ptr(), pred.data_ptr())
+    torch.cuda.synchronize()
+    pr = pred.cpu().numpy()
+    ex = scores[n_train:]
+    rank = lambda v: np.argsort(np.argsort(v))
+    rho = np.corrcoef(rank(pr), rank(ex))[0, 1]
+    assert np.isfinite(pr).all()
+    assert rho > 0.5, rho

@@ -111,3 +111,33 @@ def test_cpy_flag_matches_reference_view():
     # flag(i) = i even and hyd[i // 2] != 0
     exp = [1 if (i % 2 == 0 and hyd[i // 2] != 0) else 0 for i in range(len(hyd))]
     assert list(f) == exp
+
+
+# ---------------------------------------------------------------- surrogate oracle
+def test_mlp_oracle_gradient_matches_finite_differences():
+    from oracle import mlp as omlp
+    rng = np.random.default_rng(0)
+    p = omlp.he_params(1)
+    X = rng.normal(size=(16, omlp.IN))
+    t = rng.normal(size=16)
+    loss, g, _ = omlp.loss_and_grad(p, X, t, emulate=False)
+    offs = np.concatenate([[0], np.cumsum(omlp.SIZES)])
+    h = 1e-6
+    for k in range(8):
+        for i in rng.integers(offs[k], offs[k + 1], size=3):
+            pp, pm = p.copy(), p.copy()
+            pp[i] += h
+            pm[i] -= h
+            fd = (omlp.loss_and_grad(pp, X, t, emulate=False)[0] - omlp.loss_and_grad(pm, X, t, emulate=False)[0]) / (2 * h)
+            assert abs(fd - g[i]) <= 1e-6 * (1.0 + abs(g[i])), (k, i, fd, g[i])
+
+
+def test_mlp_oracle_bf16_rounding():
+    from oracle import mlp as omlp
+    x = np.array([1.0, 1.00390625, 1.005859375, -3.14159, 0.0, 65504.0])
+    r = omlp.bf16_round(x)
+    assert r[0] == 1.0 and r[1] == 1.0          # tie -> even
+    assert r[2] == 1.0078125                     # above the tie -> up
+    assert abs(r[3] + 3.140625) < 1e-12
+    bits = omlp.f64_to_bf16_bits(x)
+    assert np.array_equal(omlp.bf16_bits_to_f64(bits), r)
