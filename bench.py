@@ -57,6 +57,8 @@ def parse():
     ap.add_argument("--xsub", type=int, default=0)
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--gso-steps", type=int, default=200)
+    ap.add_argument("--complexes", type=int, default=0,
+                    help="score only the first K complexes of the workload (profiling-size cases)")
     return ap.parse_args()
 
 
@@ -185,9 +187,11 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     lkg = importlib.import_module("lklight-gpu_b200")
 
-    items = workload(args.workload)
     if args.workload == "config3":
         return run_screened(args, lkg, torch, local, rank, world, dist)
+    items = workload(args.workload)
+    if args.complexes:
+        items = items[:args.complexes]
     ctx = lkg.Context(device=local, tile=args.tile, cell=args.cell, group=args.group, xsub=args.xsub)
     stream = torch.cuda.ExternalStream(ctx.stream)
     ids = [ctx.add_complex(it["family"], it["rec"], it["lig"]) for it in items]
