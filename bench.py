@@ -363,7 +363,7 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
         st = g.state()
-        res[mode] = dict(seconds=el, scored=g.scored, predicted=g.predicted, st=st)
+        res[mode] = dict(seconds=el, scored=g.scored, predicted=g.predicted, st=st, phases=g.timing())
         del g
     ov = {}
     for mode in ("screened", "ablation"):
@@ -380,12 +380,13 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
             "config": {"workload": "config3", "swarms": swarms, "glowworms": glow, "steps": steps,
                        "candidates": 4, "exact_fraction": 0.25, "rescore_every": 10, "train_steps": 20},
             "plain": {"seconds": res["plain"]["seconds"], "exact_evals": res["plain"]["scored"],
-                      "mean_best_score": best["plain"]},
+                      "mean_best_score": best["plain"], "phases_s": res["plain"]["phases"]},
             "screened": {"seconds": res["screened"]["seconds"], "exact_evals": res["screened"]["scored"],
                          "surrogate_evals": res["screened"]["predicted"], "mean_best_score": best["screened"],
-                         "top5_overlap_with_plain": ov["screened"]},
+                         "top5_overlap_with_plain": ov["screened"], "phases_s": res["screened"]["phases"]},
             "ablation_no_network": {"seconds": res["ablation"]["seconds"], "exact_evals": res["ablation"]["scored"],
-                                    "mean_best_score": best["ablation"], "top5_overlap_with_plain": ov["ablation"]}}
+                                    "mean_best_score": best["ablation"], "top5_overlap_with_plain": ov["ablation"],
+                                    "phases_s": res["ablation"]["phases"]}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

@@ -316,6 +316,9 @@ int lkg_gso_set_screen(lkg_gso* gso, const lkg_screen* cfg);
 /* exact rescoring of every glowworm (the final poses of a screened run) */
 int lkg_gso_finalize(lkg_gso* gso);
 int64_t lkg_gso_predicted(lkg_gso* gso);
+/* wall seconds so far in: out[0] exact scoring (launch, copies, wait),
+ * out[1] host movement, out[2] surrogate inference, out[3] training */
+int lkg_gso_timing(lkg_gso* gso, double* out);
 
 #ifdef __cplusplus
 }

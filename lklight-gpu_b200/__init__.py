@@ -91,7 +91,7 @@ def lib():
         "lkg_gso_create": (I, [P, I, P, P, P, P, P, P]), "lkg_gso_run": (I, [P, I]),
         "lkg_gso_state": (I, [P, P, P, P, P, P, P]), "lkg_gso_scored": (I64, [P]),
         "lkg_gso_destroy": (I, [P]), "lkg_compat_cache_clear": (None, []),
-        "lkg_gso_set_screen": (I, [P, P]), "lkg_gso_finalize": (I, [P]), "lkg_gso_predicted": (I64, [P]),
+        "lkg_gso_set_screen": (I, [P, P]), "lkg_gso_finalize": (I, [P]), "lkg_gso_predicted": (I64, [P]), "lkg_gso_timing": (I, [P, P]),
         "cuda_batch_score": (I, [P, I, I, I, F, F, F, F, P, P, P, P, P, I, P, P, I, I, I, F, F, F, F,
                                  P, P, P, P, P, P, I, I, C.c_uint, P]),
         "cuda_cpydock_solv": (I, [P, P, I, P, P, I, I, I, F, F, F, F, P, P, P, P, I, I, P, P, P, P, P]),
@@ -417,6 +417,13 @@ class GSO:
     @property
     def predicted(self):
         return lib().lkg_gso_predicted(self.h)
+
+    def timing(self):
+        """Wall seconds in exact scoring, host movement, surrogate inference
+        and surrogate training."""
+        t = np.zeros(4)
+        _check(lib().lkg_gso_timing(self.h, ptr(t)))
+        return dict(exact=t[0], movement=t[1], inference=t[2], training=t[3])
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -10,6 +10,7 @@
 // vision-range update).  Every swarm of a complex is seeded with the same
 // seed, as every `LKlight run` of a setup is (simulator.rs:184, lib.rs:58).
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
 #include <unordered_map>
@@ -67,24 +68,37 @@ struct Swarm {
     std::vector<Quat> rot;
     std::vector<double> luc;
 
-    // neighbour lists: uniform hash with cell = max vision range, candidates
-    // re-sorted by id (swarm.rs:181-230), identical to the all-pairs scan
+    // neighbour lists: uniform hash with cell = the largest vision range in
+    // the swarm (so the 27 cells around a glowworm hold every glowworm it
+    // can see), candidates re-sorted by id (swarm.rs:181-230): identical to
+    // the all-pairs scan
     void neighbours() {
         const size_t n = g.size();
-        const double cell = MAX_VISION;
+        double vmax = 0.0;
+        for (size_t i = 0; i < n; ++i) vmax = std::fmax(vmax, g[i].vision);
+        if (!(vmax > 0.0)) {   // nobody sees anybody (d^2 < 0 never holds)
+            for (size_t i = 0; i < n; ++i) g[i].nb.clear();
+            return;
+        }
+        // any cell edge >= vmax is exact; the floor keeps indices small
+        const double cell = std::fmin(std::fmax(vmax, 0.05), MAX_VISION);
         std::unordered_map<int64_t, std::vector<uint32_t>> cells;
         cells.reserve(n * 2);
         auto key = [](int64_t x, int64_t y, int64_t z) {
             return ((x & 0x1fffff) << 42) | ((y & 0x1fffff) << 21) | (z & 0x1fffff);
         };
+        // cell index, clamped before the integer conversion (NaN -> 0); a
+        // clamped or aliased key only adds candidates, never drops one
+        auto idx = [cell](double v) {
+            const double f = std::floor(v / cell);
+            return (int64_t)(f > 1e15 ? 1e15 : (f < -1e15 ? -1e15 : (f == f ? f : 0.0)));
+        };
         for (size_t i = 0; i < n; ++i)
-            cells[key((int64_t)std::floor(g[i].t[0] / cell), (int64_t)std::floor(g[i].t[1] / cell),
-                      (int64_t)std::floor(g[i].t[2] / cell))].push_back((uint32_t)i);
+            cells[key(idx(g[i].t[0]), idx(g[i].t[1]), idx(g[i].t[2]))].push_back((uint32_t)i);
         for (size_t i = 0; i < n; ++i) {
             Glow& g1 = g[i];
             double vr2 = g1.vision * g1.vision;
-            int64_t cx = (int64_t)std::floor(g1.t[0] / cell), cy = (int64_t)std::floor(g1.t[1] / cell),
-                    cz = (int64_t)std::floor(g1.t[2] / cell);
+            int64_t cx = idx(g1.t[0]), cy = idx(g1.t[1]), cz = idx(g1.t[2]);
             g1.nb.clear();
             for (int64_t dz = -1; dz <= 1; ++dz)
                 for (int64_t dy = -1; dy <= 1; ++dy)
@@ -170,8 +184,8 @@ struct Swarm {
     }
 
     // screened movement, part 1: K draws per glowworm (serially, glowworm
-    // by glowworm), the candidate poses of those with neighbours
-    // (kernel layout w, x, y, z, tx, ty, tz), vision update
+    // by glowworm); for those with neighbours the current pose and the K
+    // candidate poses (kernel layout w, x, y, z, tx, ty, tz); vision update
     void propose(int K, std::vector<double>& cand, std::vector<uint32_t>& owner) {
         const size_t n = g.size();
         cand.clear();
@@ -185,6 +199,11 @@ struct Swarm {
             gw.moved = false;
             gw.exact_next = false;
             if (!gw.nb.empty()) {
+                // candidate 0 is the glowworm's current pose: the surrogate's
+                // gain estimate is relative to its own value there
+                const double cur[7] = {gw.r.w, gw.r.x, gw.r.y, gw.r.z, gw.t[0], gw.t[1], gw.t[2]};
+                cand.insert(cand.end(), cur, cur + 7);
+                owner.push_back((uint32_t)i);
                 for (int k = 0; k < K; ++k) {
                     const uint32_t nid = select(gw, (uint32_t)i, rnd[i * K + k]);
                     double t[3];
@@ -209,6 +228,10 @@ struct lkg_gso {
     std::vector<int> need_idx;  // per scored pose: swarm * 2^20 + glowworm
     int64_t scored = 0, predicted = 0;
     int step = 0;
+    // wall seconds per phase: exact scoring, host movement, surrogate
+    // inference, surrogate training
+    double t_exact = 0.0, t_move = 0.0, t_infer = 0.0, t_train = 0.0;
+    std::vector<int> last_counts;   // exact scorings per group in the last scoring phase
     lkg::DBuf d_poses, d_scores;
     lkg::HBuf h_poses, h_scores;
     // surrogate screening (off unless lkg_gso_set_screen)
@@ -267,22 +290,31 @@ namespace {
 
 inline Glow& glow_of(lkg_gso* G, int idx) { return G->swarms[idx >> 20].g[idx & 0xfffff]; }
 
-// Train (or fine-tune) the surrogate of group gi on its exact pairs, most
-// recent first kept (at most 65,536), in a seeded shuffled order.
-int train_group(lkg_gso* G, int gi, int epochs) {
+inline double now_s() {
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+// Train (or fine-tune) the surrogate of group gi on its exact pairs (the
+// last `recent` of them when recent > 0; at most 65,536 are kept), in a
+// seeded shuffled order.
+int train_group(lkg_gso* G, int gi, int epochs, size_t recent) {
     auto& P = G->tr_pose[gi];
-    auto& S = G->tr_score[gi];
+    auto& S0 = G->tr_score[gi];
     const size_t cap = 65536;
-    if (S.size() > cap) {
-        const size_t drop = S.size() - cap;
+    if (S0.size() > cap) {
+        const size_t drop = S0.size() - cap;
         P.erase(P.begin(), P.begin() + 7 * drop);
-        S.erase(S.begin(), S.begin() + drop);
+        S0.erase(S0.begin(), S0.begin() + drop);
     }
-    const int n = (int)S.size();
+    const size_t first = (recent > 0 && recent < S0.size()) ? S0.size() - recent : 0;
+    const int n = (int)(S0.size() - first);
     if (n < 64 || epochs <= 0) return set_ok();
+    const double t0 = now_s();
+    const double* S = S0.data() + first;
+    const double* PP = P.data() + 7 * first;
     int st;
     if (!G->scaled[gi]) {
-        if ((st = lkg_surrogate_set_target_scale(G->sur[gi], n, S.data()))) return st;
+        if ((st = lkg_surrogate_set_target_scale(G->sur[gi], n, S))) return st;
         G->scaled[gi] = true;
     }
     std::vector<int> perm(n);
@@ -291,7 +323,7 @@ int train_group(lkg_gso* G, int gi, int epochs) {
     for (int i = n - 1; i > 0; --i) std::swap(perm[i], perm[(int)(r.gen_f64() * (i + 1)) % (i + 1)]);
     std::vector<double> hp(7 * (size_t)n), hs(n);
     for (int i = 0; i < n; ++i) {
-        std::memcpy(&hp[7 * (size_t)i], &P[7 * (size_t)perm[i]], 7 * sizeof(double));
+        std::memcpy(&hp[7 * (size_t)i], PP + 7 * (size_t)perm[i], 7 * sizeof(double));
         hs[i] = S[perm[i]];
     }
     LKG_CK(G->d_tp.reserve(hp.size() * sizeof(double)), "surrogate training set");
@@ -300,8 +332,10 @@ int train_group(lkg_gso* G, int gi, int epochs) {
     LKG_CK(cudaMemcpyAsync(G->d_tp.p, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, s), "train upload");
     LKG_CK(cudaMemcpyAsync(G->d_ts.p, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s), "train upload");
     float loss = 0.f;
-    return lkg_surrogate_train(G->sur[gi], n, G->d_tp.as<double>(), G->d_ts.as<double>(), epochs, 512, G->cfg.lr,
-                               &loss);
+    st = lkg_surrogate_train(G->sur[gi], n, G->d_tp.as<double>(), G->d_ts.as<double>(), epochs, 512, G->cfg.lr,
+                             &loss);
+    G->t_train += now_s() - t0;
+    return st;
 }
 
 // Exact scoring of the selected glowworms in one batched launch group;
@@ -310,6 +344,7 @@ int train_group(lkg_gso* G, int gi, int epochs) {
 // (the no-network ablation keeps the previous score).  `learn` appends the
 // exact pairs to the surrogate training sets.
 int score_phase(lkg_gso* G, bool all, bool learn) {
+    struct Acc { double& t; double t0; ~Acc() { t += now_s() - t0; } } acc{G->t_exact, now_s()};
     lkg_ctx* ctx = G->ctx;
     const int ng = (int)G->group_complex.size();
     std::vector<int> counts(ng, 0);
@@ -327,6 +362,7 @@ int score_phase(lkg_gso* G, bool all, bool learn) {
                 }
             }
         }
+    G->last_counts = counts;
     const size_t n = G->need_idx.size();
     if (!n) return set_ok();
     LKG_CK(G->h_poses.reserve(n * 7 * sizeof(double)), "gso staging");
@@ -366,9 +402,11 @@ int score_phase(lkg_gso* G, bool all, bool learn) {
 // Screened movement: K candidate moves per glowworm with neighbours, all
 // ranked by the surrogate (or, for the ablation, by seeded random numbers);
 // each glowworm takes its best candidate, and per swarm the fraction
-// exact_fraction of the moves with the largest predicted gain over the
-// glowworm's current score is marked for exact scoring.
+// exact_fraction of the moves with the largest predicted gain (surrogate at
+// the move minus surrogate at the current pose) is marked for exact
+// scoring; the others carry current score + predicted gain.
 int screened_movement(lkg_gso* G) {
+    double t0 = now_s();
     const int ns = (int)G->swarms.size(), ng = (int)G->group_complex.size(), K = G->cfg.candidates;
     std::vector<std::vector<double>> cand(ns);
     std::vector<std::vector<uint32_t>> owner(ns);
@@ -384,6 +422,8 @@ int screened_movement(lkg_gso* G) {
     double* hpred = G->h_pred.as<double>();
     for (int s = 0; s < ns; ++s)
         if (!cand[s].empty()) std::memcpy(hc + 7 * off[s], cand[s].data(), cand[s].size() * sizeof(double));
+    G->t_move += now_s() - t0;
+    t0 = now_s();
     if (G->cfg.random_rank) {
         for (size_t i = 0; i < total; ++i) hpred[i] = G->rank_rng.gen_f64();
     } else {
@@ -404,23 +444,27 @@ int screened_movement(lkg_gso* G) {
         if (rc) return rc;
         G->predicted += (int64_t)total;
     }
+    G->t_infer += now_s() - t0;
+    t0 = now_s();
     const double frac = G->cfg.exact_fraction;
 #pragma omp parallel for schedule(dynamic, 1)
     for (int s = 0; s < ns; ++s) {
         Swarm& sw = G->swarms[s];
         std::vector<std::pair<double, uint32_t>> gain;
-        for (size_t c0 = 0; c0 < owner[s].size(); c0 += K) {
+        for (size_t c0 = 0; c0 < owner[s].size(); c0 += K + 1) {
             const uint32_t i = owner[s][c0];
-            size_t best = c0;
-            for (size_t c = c0 + 1; c < c0 + K; ++c)
+            size_t best = c0 + 1;
+            for (size_t c = c0 + 2; c <= c0 + K; ++c)
                 if (hpred[off[s] + c] > hpred[off[s] + best]) best = c;
             Glow& gw = sw.g[i];
             const double* row = hc + 7 * (off[s] + best);
             gw.r = {row[0], row[1], row[2], row[3]};
             gw.t[0] = row[4]; gw.t[1] = row[5]; gw.t[2] = row[6];
-            gw.pred = hpred[off[s] + best];
+            // predicted change from the current pose, applied to its score
+            const double g = hpred[off[s] + best] - hpred[off[s] + c0];
+            gw.pred = gw.scoring + g;
             gw.moved = true;
-            gain.push_back({G->cfg.random_rank ? gw.pred : gw.pred - gw.scoring, i});
+            gain.push_back({g, i});
         }
         std::sort(gain.begin(), gain.end(), [](const std::pair<double, uint32_t>& a, const std::pair<double, uint32_t>& b) {
             return a.first > b.first || (a.first == b.first && a.second < b.second);
@@ -428,6 +472,7 @@ int screened_movement(lkg_gso* G) {
         const size_t nx = (size_t)std::ceil(frac * (double)gain.size());
         for (size_t k = 0; k < nx && k < gain.size(); ++k) sw.g[gain[k].second].exact_next = true;
     }
+    G->t_move += now_s() - t0;
     return set_ok();
 }
 
@@ -443,8 +488,12 @@ int gso_step(lkg_gso* G) {
     if (G->screen && !c.random_rank) {
         const int ng = (int)G->group_complex.size();
         const bool first = G->step == c.train_steps - 1;
+        // first training: every exact pair so far; fine-tuning: the pairs of
+        // this full rescoring
         for (int gi = 0; gi < ng && (first || rescore); ++gi)
-            if ((st = train_group(G, gi, first ? c.train_epochs : c.finetune_epochs))) return st;
+            if ((st = train_group(G, gi, first ? c.train_epochs : c.finetune_epochs,
+                                  first ? 0 : (size_t)G->last_counts[gi])))
+                return st;
     }
     const int ns = (int)G->swarms.size();
 #pragma omp parallel for schedule(dynamic, 1)
@@ -457,12 +506,14 @@ int gso_step(lkg_gso* G) {
     if (G->screen && G->step + 1 >= c.train_steps) {
         if ((st = screened_movement(G))) return st;
     } else {
+        const double t0 = now_s();
 #pragma omp parallel for schedule(dynamic, 1)
         for (int s = 0; s < ns; ++s) {
             Swarm& sw = G->swarms[s];
             sw.movement();
             for (auto& gw : sw.g) gw.exact_next = gw.moved;
         }
+        G->t_move += now_s() - t0;
     }
     G->step++;
     return set_ok();
@@ -527,6 +578,12 @@ int lkg_gso_state(lkg_gso* G, double* trans, double* rot, double* luc, double* s
 
 int64_t lkg_gso_scored(lkg_gso* G) { return G ? G->scored : 0; }
 int64_t lkg_gso_predicted(lkg_gso* G) { return G ? G->predicted : 0; }
+
+int lkg_gso_timing(lkg_gso* G, double* out) {
+    if (!G || !out) return set_error(LKG_ERR_ARG, "bad timing arguments");
+    out[0] = G->t_exact; out[1] = G->t_move; out[2] = G->t_infer; out[3] = G->t_train;
+    return set_ok();
+}
 
 int lkg_gso_finalize(lkg_gso* G) {
     if (!G) return set_error(LKG_ERR_ARG, "null gso");

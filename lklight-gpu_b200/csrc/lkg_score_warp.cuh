@@ -46,24 +46,57 @@ struct WSlots {
     Rot rot;                    // pose of the current work unit
     float4 lpos[2 * G];         // x, y, z (f32 part), q
     float4 lres[2 * G];         // x, y, z residuals, sqrt eps
+    float4 ltest[2 * G];        // candidate test: -2 l', |l'|^2 - 100.01 (l' = l - group centre)
     float2 lpar[2 * G];         // r, heavy
     unsigned hit[WRing<G>::N];  // (slot << 26) | receptor index
 };
 
-// pair terms of one queued hit (exact d^2 <= 100 test on compensated d^2)
+// pair terms of one queued hit: the exact d^2 <= 100 test on the
+// compensated d^2, then the reference formulas (those of pair_fast) with
+// the clash term selected instead of branched on
 template <int G>
 __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, unsigned e, unsigned flags,
                                        double& elec, double& vdw, int& np) {
     const int l = (int)(e >> 26), k = (int)(e & 0x3ffffffu);
+    const float4 a = __ldg(c.rpos + k);
+    const float4 pr = __ldg(c.rpar + k);
     const float4 lp = W.lpos[l], lr = W.lres[l];
     const float2 lq = W.lpar[l];
-    const float4 a = __ldg(c.rpos + k);
     const float dx = (lp.x - a.x) + lr.x, dy = (lp.y - a.y) + lr.y, dz = (lp.z - a.z) + lr.z;
     const float d2 = dx * dx + dy * dy + dz * dz;
     if (!(d2 <= 100.f)) return;
-    const float4 pr = __ldg(c.rpar + k);
     ++np;
-    pair_fast(flags, lp.w, lr.w, lq.x, lq.y != 0.f, a, pr, d2, elec, vdw);
+    const float ir2 = __fdividef(1.0f, d2);
+    if (flags & F_ELEC) {
+        float ae = lp.w * a.w * ir2;
+        ae = fminf(fmaxf(ae, -ES_CAP_F), ES_CAP_F);
+        elec += (double)ae;
+    }
+    const float sv = lr.w * pr.x;
+    const float rr = lq.x + pr.y;
+    const float rr2 = rr * rr;
+    const float p6 = rr2 * rr2 * rr2 * (ir2 * ir2 * ir2);
+    float vp = fminf(sv * p6 * (p6 - 2.f), 1.0f);
+    const float d = d2 * rsqrtf(d2), dmin = 0.75f * rr;
+    const bool clash = (flags & F_CLASH) && lq.y != 0.f && pr.z != 0.f && d < dmin;
+    vp = clash ? vp + 6.f * (dmin - d) : vp;
+    vdw += (double)vp;
+}
+
+// receptor atom of candidate kk of the current rows: the span is the last
+// row whose exclusive prefix is <= kk (empty rows never qualify ahead of the
+// non-empty row that follows them); far away when kk is past the end
+__device__ __forceinline__ void w_fetch(const ComplexDev& c, int st, int excl, int total, int kk, float4& a,
+                                        int& ridx) {
+    int rr = 0;
+#pragma unroll
+    for (int s = 16; s > 0; s >>= 1) {
+        const int v = __shfl_sync(0xffffffffu, excl, rr + s);
+        if (v <= kk) rr += s;
+    }
+    const int rst = __shfl_sync(0xffffffffu, st, rr), rex = __shfl_sync(0xffffffffu, excl, rr);
+    ridx = rst + (kk - rex);
+    a = kk < total ? __ldg(c.rpos + ridx) : make_float4(3e30f, 3e30f, 3e30f, 0.f);
 }
 
 template <int G>
@@ -122,12 +155,23 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
                 W.lres[set + lane] = res;
                 W.lpar[set + lane] = make_float2(lp4.y, lp4.z);
             }
-            __syncwarp();
             // 2. receptor rows within reach of the group sphere
             const float4 gs = __ldg(c.lgrp + grp);
             double cxd, cyd, czd;
             apply(W.rot, (double)gs.x, (double)gs.y, (double)gs.z, cxd, cyd, czd);
             const float gx = (float)cxd, gy = (float)cyd, gz = (float)czd;
+            if (lane < G) {
+                // candidate test |a' - l'|^2 <= 100.01 as |a'|^2 - 2 a'.l' +
+                // |l'|^2 in the group frame (|a'| <= ~20 A: rounding ~1e-4,
+                // far inside the 0.01 margin); invalid slots never pass
+                const float4 lp = W.lpos[set + lane];
+                const float lx = lp.x - gx, ly = lp.y - gy, lz = lp.z - gz;
+                const bool far_slot = !(lp.x < 1e29f);
+                W.ltest[set + lane] = far_slot ? make_float4(0.f, 0.f, 0.f, 3e30f)
+                                               : make_float4(-2.f * lx, -2.f * ly, -2.f * lz,
+                                                             lx * lx + ly * ly + lz * lz - 100.01f);
+            }
+            __syncwarp();
             const float R = SCAN_R + gs.w, R2 = R * R;
             const int cz0 = max(0, (int)floorf((gz - R - c.oz) * c.inv_h));
             const int cz1 = min(c.ncz - 1, (int)floorf((gz + R - c.oz) * c.inv_h));
@@ -168,31 +212,23 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
                 }
                 const int total = __shfl_sync(FULL, inc, 31);
                 const int excl = inc - len;
-                // 3. candidate chunks
+                // 3. candidate chunks; the next chunk's receptor atoms are
+                //    fetched while the current one is tested
+                float4 an = make_float4(3e30f, 3e30f, 3e30f, 0.f);
+                int rn = 0;
+                if (total > 0) w_fetch(c, st, excl, total, lane, an, rn);
                 for (int k0 = 0; k0 < total; k0 += 32) {
-                    const int kk = k0 + lane;
-                    // the span holding candidate kk: the last row whose
-                    // exclusive prefix is <= kk (empty rows never qualify
-                    // ahead of the non-empty row that follows them)
-                    int rr = 0;
-#pragma unroll
-                    for (int s = 16; s > 0; s >>= 1) {
-                        const int v = __shfl_sync(FULL, excl, rr + s);
-                        if (v <= kk) rr += s;
-                    }
-                    const int rst = __shfl_sync(FULL, st, rr), rex = __shfl_sync(FULL, excl, rr);
-                    float4 a = make_float4(3e30f, 3e30f, 3e30f, 0.f);
-                    int ridx = 0;
-                    if (kk < total) {
-                        ridx = rst + (kk - rex);
-                        a = __ldg(c.rpos + ridx);
-                    }
+                    const float4 a = an;
+                    const int ridx = rn;
+                    if (k0 + 32 < total) w_fetch(c, st, excl, total, k0 + 32 + lane, an, rn);
+                    const float ax = a.x - gx, ay = a.y - gy, az = a.z - gz;
+                    const float aa = ax * ax + ay * ay + az * az;
                     unsigned mask = 0;
 #pragma unroll
                     for (int l = 0; l < G; ++l) {
-                        const float4 lp = W.lpos[set + l];
-                        const float dx = lp.x - a.x, dy = lp.y - a.y, dz = lp.z - a.z;
-                        mask |= (dx * dx + dy * dy + dz * dz <= 100.01f ? 1u : 0u) << l;
+                        const float4 t = W.ltest[set + l];
+                        const float q = fmaf(ax, t.x, fmaf(ay, t.y, fmaf(az, t.z, aa + t.w)));
+                        mask |= (q <= 0.f ? 1u : 0u) << l;
                     }
                     const int nh = __popc(mask);
                     int ex = nh;   // inclusive prefix of the hit counts
