@@ -361,8 +361,8 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
     for mode in ("plain", "screened", "ablation"):
         g = lkg.GSO(ctx, [(cid, swarms, glow)], pos, [3])
         if mode != "plain":
-            g.set_screen(candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=40,
-                         finetune_epochs=2, lr=1e-3, seed=3, random_rank=(mode == "ablation"))
+            g.set_screen(candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=20,
+                         finetune_epochs=2, lr=1e-3, seed=3, random_rank=(mode == "ablation"), batch=1024)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g.run(steps)

@@ -311,6 +311,7 @@ typedef struct {
     float lr;                 /* Adam learning rate */
     uint64_t seed;            /* surrogate initialisation, shuffles, ablation ranks */
     int32_t random_rank;
+    int32_t batch;            /* training minibatch (1024; 0 = 1024) */
 } lkg_screen;
 int lkg_gso_set_screen(lkg_gso* gso, const lkg_screen* cfg);
 /* exact rescoring of every glowworm (the final poses of a screened run) */

@@ -148,7 +148,7 @@ class Screen(C.Structure):
     """``lkg_screen``: surrogate screening of GSO moves."""
     _fields_ = [("candidates", C.c_int32), ("exact_fraction", C.c_double), ("rescore_every", C.c_int32),
                 ("train_steps", C.c_int32), ("train_epochs", C.c_int32), ("finetune_epochs", C.c_int32),
-                ("lr", C.c_float), ("seed", C.c_uint64), ("random_rank", C.c_int32)]
+                ("lr", C.c_float), ("seed", C.c_uint64), ("random_rank", C.c_int32), ("batch", C.c_int32)]
 
 
 class Context:
@@ -398,12 +398,12 @@ class GSO:
         _check(lib().lkg_gso_state(self.h, ptr(t), ptr(r), ptr(luc), ptr(sc), ptr(vis), ptr(nn)))
         return dict(translation=t, rotation=r, luciferin=luc, scoring=sc, vision=vis, neighbors=nn)
 
-    def set_screen(self, candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=40,
-                   finetune_epochs=2, lr=1e-3, seed=0, random_rank=False):
+    def set_screen(self, candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=20,
+                   finetune_epochs=2, lr=1e-3, seed=0, random_rank=False, batch=1024):
         """Screen moves with the surrogate (random_rank: the same search with
         random candidate ranks instead of the network, for ablations)."""
         cfg = Screen(candidates, exact_fraction, rescore_every, train_steps, train_epochs, finetune_epochs, lr, seed,
-                     1 if random_rank else 0)
+                     1 if random_rank else 0, batch)
         _check(lib().lkg_gso_set_screen(self.h, C.byref(cfg)))
 
     def finalize(self):

@@ -68,50 +68,76 @@ struct Swarm {
     std::vector<Quat> rot;
     std::vector<double> luc;
 
-    // neighbour lists: uniform hash with cell = the largest vision range in
-    // the swarm (so the 27 cells around a glowworm hold every glowworm it
-    // can see), candidates re-sorted by id (swarm.rs:181-230): identical to
-    // the all-pairs scan
+    // neighbour lists (swarm.rs:181-230), identical to the all-pairs scan:
+    // the neighbours of glowworm i are the glowworms brighter than i within
+    // its vision range, in id order.  Two orders of the swarm are built
+    // once per step: by x and by luciferin.  Each glowworm scans the shorter
+    // of (a) its x-window [x - v, x + v] and (b) the glowworms brighter than
+    // itself, testing every candidate exactly.  (a) is short for the dim,
+    // short-sighted majority, (b) for the brightest glowworms, whose vision
+    // grows to the 5 A maximum because nobody outshines them.
+    std::vector<uint32_t> xorder, lorder, lrank;
+    std::vector<double> xs, ys, zs, ls, bx, by, bz, bl;   // sorted copies (contiguous scans)
+    std::vector<uint32_t> tmp;
     void neighbours() {
         const size_t n = g.size();
-        double vmax = 0.0;
-        for (size_t i = 0; i < n; ++i) vmax = std::fmax(vmax, g[i].vision);
-        if (!(vmax > 0.0)) {   // nobody sees anybody (d^2 < 0 never holds)
-            for (size_t i = 0; i < n; ++i) g[i].nb.clear();
-            return;
+        // NaN coordinates / luciferin sort last and never pass a test
+        auto kx = [this](uint32_t i) { const double v = g[i].t[0]; return v == v ? v : INFINITY; };
+        auto kl = [this](uint32_t i) { const double v = g[i].luciferin; return v == v ? v : INFINITY; };
+        xorder.resize(n);
+        lorder.resize(n);
+        for (size_t i = 0; i < n; ++i) xorder[i] = lorder[i] = (uint32_t)i;
+        std::sort(xorder.begin(), xorder.end(), [&](uint32_t a, uint32_t b) {
+            const double xa = kx(a), xb = kx(b);
+            return xa < xb || (xa == xb && a < b);
+        });
+        std::sort(lorder.begin(), lorder.end(), [&](uint32_t a, uint32_t b) {
+            const double la = kl(a), lb = kl(b);
+            return la < lb || (la == lb && a < b);
+        });
+        lrank.resize(n);
+        xs.resize(n); ys.resize(n); zs.resize(n); ls.resize(n);
+        bx.resize(n); by.resize(n); bz.resize(n); bl.resize(n);
+        for (size_t k = 0; k < n; ++k) {
+            const Glow& q = g[xorder[k]];
+            xs[k] = kx(xorder[k]); ys[k] = q.t[1]; zs[k] = q.t[2]; ls[k] = q.luciferin;
+            const Glow& b = g[lorder[k]];
+            bx[k] = b.t[0]; by[k] = b.t[1]; bz[k] = b.t[2]; bl[k] = b.luciferin;
+            lrank[lorder[k]] = (uint32_t)k;
         }
-        // any cell edge >= vmax is exact; the floor keeps indices small
-        const double cell = std::fmin(std::fmax(vmax, 0.05), MAX_VISION);
-        std::unordered_map<int64_t, std::vector<uint32_t>> cells;
-        cells.reserve(n * 2);
-        auto key = [](int64_t x, int64_t y, int64_t z) {
-            return ((x & 0x1fffff) << 42) | ((y & 0x1fffff) << 21) | (z & 0x1fffff);
-        };
-        // cell index, clamped before the integer conversion (NaN -> 0); a
-        // clamped or aliased key only adds candidates, never drops one
-        auto idx = [cell](double v) {
-            const double f = std::floor(v / cell);
-            return (int64_t)(f > 1e15 ? 1e15 : (f < -1e15 ? -1e15 : (f == f ? f : 0.0)));
-        };
-        for (size_t i = 0; i < n; ++i)
-            cells[key(idx(g[i].t[0]), idx(g[i].t[1]), idx(g[i].t[2]))].push_back((uint32_t)i);
         for (size_t i = 0; i < n; ++i) {
             Glow& g1 = g[i];
-            double vr2 = g1.vision * g1.vision;
-            int64_t cx = idx(g1.t[0]), cy = idx(g1.t[1]), cz = idx(g1.t[2]);
             g1.nb.clear();
-            for (int64_t dz = -1; dz <= 1; ++dz)
-                for (int64_t dy = -1; dy <= 1; ++dy)
-                    for (int64_t dx = -1; dx <= 1; ++dx) {
-                        auto it = cells.find(key(cx + dx, cy + dy, cz + dz));
-                        if (it == cells.end()) continue;
-                        for (uint32_t id : it->second) {
-                            const Glow& g2 = g[id];
-                            if (id == i || !(g1.luciferin < g2.luciferin)) continue;
-                            double ddx = g1.t[0] - g2.t[0], ddy = g1.t[1] - g2.t[1], ddz = g1.t[2] - g2.t[2];
-                            if (ddx * ddx + ddy * ddy + ddz * ddz < vr2) g1.nb.push_back(id);
-                        }
-                    }
+            const double v = g1.vision, vr2 = v * v;
+            if (!(v > 0.0)) continue;   // d^2 < 0 never holds
+            const double x = g1.t[0], y = g1.t[1], z = g1.t[2], l1 = g1.luciferin;
+            // the window is widened past the rounding of x +- v: extra
+            // candidates are harmless, each is tested exactly
+            const double w = v * (1.0 + 1e-9) + 1e-12;
+            const size_t k0 = (size_t)(std::lower_bound(xs.begin(), xs.end(), x - w) - xs.begin());
+            const size_t k1 = (size_t)(std::upper_bound(xs.begin() + k0, xs.end(), x + w) - xs.begin());
+            const size_t r = lrank[i];
+            // branch-free appends: the brighter / in-range tests are coin
+            // flips for the branch predictor
+            size_t cnt = 0;
+            if (k1 - k0 <= n - 1 - r) {
+                if (tmp.size() < k1 - k0) tmp.resize(k1 - k0);
+                for (size_t k = k0; k < k1; ++k) {
+                    const double ddx = x - xs[k], ddy = y - ys[k], ddz = z - zs[k];
+                    tmp[cnt] = xorder[k];
+                    // l1 < l1 is false: i itself never passes
+                    cnt += (size_t)((l1 < ls[k]) & (ddx * ddx + ddy * ddy + ddz * ddz < vr2));
+                }
+            } else {
+                if (tmp.size() < n - 1 - r) tmp.resize(n - 1 - r);
+                for (size_t k = r + 1; k < n; ++k) {
+                    const double ddx = x - bx[k], ddy = y - by[k], ddz = z - bz[k];
+                    tmp[cnt] = lorder[k];
+                    // equal luciferin does not count
+                    cnt += (size_t)((l1 < bl[k]) & (ddx * ddx + ddy * ddy + ddz * ddz < vr2));
+                }
+            }
+            g1.nb.assign(tmp.begin(), tmp.begin() + cnt);
             std::sort(g1.nb.begin(), g1.nb.end());
         }
     }
@@ -332,8 +358,8 @@ int train_group(lkg_gso* G, int gi, int epochs, size_t recent) {
     LKG_CK(cudaMemcpyAsync(G->d_tp.p, hp.data(), hp.size() * sizeof(double), cudaMemcpyHostToDevice, s), "train upload");
     LKG_CK(cudaMemcpyAsync(G->d_ts.p, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice, s), "train upload");
     float loss = 0.f;
-    st = lkg_surrogate_train(G->sur[gi], n, G->d_tp.as<double>(), G->d_ts.as<double>(), epochs, 512, G->cfg.lr,
-                             &loss);
+    st = lkg_surrogate_train(G->sur[gi], n, G->d_tp.as<double>(), G->d_ts.as<double>(), epochs,
+                             G->cfg.batch > 0 ? G->cfg.batch : 1024, G->cfg.lr, &loss);
     G->t_train += now_s() - t0;
     return st;
 }

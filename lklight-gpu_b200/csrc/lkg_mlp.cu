@@ -12,7 +12,8 @@
 //   k_head       last layer (256 -> 1) dot products, FP32
 //   k_loss       MSE on the standardised target, dy, head gradients
 //   k_colsum     bias gradients
-//   k_adam       Adam on FP32 master weights, refreshes both BF16 layouts
+//   k_adam_all   Adam on the FP32 master weights (one launch), refreshes both
+//                BF16 layouts of the GEMM weights
 #include <cuda_bf16.h>
 
 #include <algorithm>
@@ -216,24 +217,34 @@ __global__ void k_colsum(const __nv_bfloat16* __restrict__ dC, int n, float* __r
     atomicAdd(gb + col, s);
 }
 
-// Adam on FP32 master weights; refresh the BF16 copies of the GEMM layers:
-// wt (out-major, forward) and w (in-major, backward data)
-__global__ void k_adam(float* __restrict__ p, const float* __restrict__ gr, float* __restrict__ m1,
-                       float* __restrict__ m2, int n, float lr, float b1, float b2, float eps, float bc1, float bc2,
-                       __nv_bfloat16* __restrict__ wt, __nv_bfloat16* __restrict__ w, int rows, int cols) {
+// the three GEMM layers inside the flat parameter vector
+struct AdamLayers {
+    int off[3], cols[3];
+    __nv_bfloat16* wt[3];
+    __nv_bfloat16* w[3];
+};
+
+// Adam over the whole flat parameter vector in one launch; GEMM-layer
+// entries also refresh both BF16 layouts
+__global__ void k_adam_all(float* __restrict__ p, const float* __restrict__ gr, float* __restrict__ m1,
+                           float* __restrict__ m2, int n, float lr, float b1, float b2, float eps, float bc1,
+                           float bc2, AdamLayers L) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float gg = gr[i];
     const float a = b1 * m1[i] + (1.f - b1) * gg, v = b2 * m2[i] + (1.f - b2) * gg * gg;
     m1[i] = a;
     m2[i] = v;
-    const float upd = lr * (a / bc1) / (sqrtf(v / bc2) + eps);
-    const float np = p[i] - upd;
+    const float np = p[i] - lr * (a / bc1) / (sqrtf(v / bc2) + eps);
     p[i] = np;
-    if (wt) {
-        const int r = i / cols, c = i % cols;   // p is [rows = out][cols = in]
-        wt[i] = __float2bfloat16(np);
-        w[(size_t)c * rows + r] = __float2bfloat16(np);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int j = i - L.off[k];
+        if (j >= 0 && j < H * L.cols[k]) {
+            const int r = j / L.cols[k], c = j % L.cols[k];   // [rows = out][cols = in]
+            L.wt[k][j] = __float2bfloat16(np);
+            L.w[k][(size_t)c * H + r] = __float2bfloat16(np);
+        }
     }
 }
 
@@ -358,18 +369,18 @@ int adam(lkg_surrogate* S, float lr) {
     S->step++;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     const float bc1 = 1.f - powf(b1, (float)S->step), bc2 = 1.f - powf(b2, (float)S->step);
-    for (int k = 0; k < 8; ++k) {
-        const size_t n = S->off[k + 1] - S->off[k];
-        const bool gemm_layer = (k == 0 || k == 2 || k == 4);
-        const int L = k / 2;
-        const int rows = H, cols = (k == 0) ? IN : H;
-        k_adam<<<(int)((n + 255) / 256), 256, 0, s>>>(P(S, k), Gd(S, k), S->m1.as<float>() + S->off[k],
-                                                      S->m2.as<float>() + S->off[k], (int)n, lr, b1, b2, eps, bc1, bc2,
-                                                      gemm_layer ? S->wt[L].as<__nv_bfloat16>() : nullptr,
-                                                      gemm_layer ? S->w[L].as<__nv_bfloat16>() : nullptr, rows, cols);
+    AdamLayers L;
+    for (int k = 0; k < 3; ++k) {
+        L.off[k] = (int)S->off[2 * k];
+        L.cols[k] = k == 0 ? IN : H;
+        L.wt[k] = S->wt[k].as<__nv_bfloat16>();
+        L.w[k] = S->w[k].as<__nv_bfloat16>();
     }
+    const int n = (int)NPARAM;
+    k_adam_all<<<(n + 255) / 256, 256, 0, s>>>(S->p.as<float>(), S->g.as<float>(), S->m1.as<float>(),
+                                               S->m2.as<float>(), n, lr, b1, b2, eps, bc1, bc2, L);
     LKG_CK(cudaGetLastError(), "mlp adam");
-    S->ctx->launches += 8;
+    S->ctx->launches += 1;
     return 0;
 }
 
