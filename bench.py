@@ -59,6 +59,7 @@ def parse():
     ap.add_argument("--group", type=int, default=0)
     ap.add_argument("--xsub", type=int, default=0)
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--gso-steps", type=int, default=200)
     ap.add_argument("--complexes", type=int, default=0,
                     help="score only the first K complexes of the workload (profiling-size cases)")
@@ -195,7 +196,13 @@ def main():
     items = workload(args.workload)
     if args.complexes:
         items = items[:args.complexes]
-    ctx = lkg.Context(device=local, tile=args.tile, cell=args.cell, group=args.group, xsub=args.xsub)
+    shape = dict(tile=args.tile, group=args.group, cell=args.cell, xsub=args.xsub, source="command line")
+    if not (args.tile or args.group or args.cell or args.xsub) and not args.no_autotune and len(items) > 1:
+        # tile shapes picked by the autotuner (a sample of the batch, CUDA-graph
+        # replays per candidate shape; cached per device and batch signature)
+        autotune = importlib.import_module("lklight-gpu_b200.autotune")
+        shape = autotune.autotune(items, device=local)
+    ctx = lkg.Context(device=local, tile=shape["tile"], cell=shape["cell"], group=shape["group"], xsub=shape["xsub"])
     stream = torch.cuda.ExternalStream(ctx.stream)
     ids = [ctx.add_complex(it["family"], it["rec"], it["lig"]) for it in items]
     counts = [len(it["poses"]) for it in items]
@@ -308,7 +315,8 @@ def main():
                        "ligand_atoms": int(sum(len(it["lig"]["coords"]) for it in items)),
                        "near_pairs_per_step": float(pairs.sum()), "near_pairs_by_family": fam_pairs,
                        "l2": "inputs larger than L2 (receptor arrays and far-field grids of all complexes)",
-                       "parallelism": "replicas" if world > 1 else "single"},
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "tile_shape": {k: shape.get(k) for k in ("tile", "group", "cell", "xsub", "source")}},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak,
                          "traffic": TRAFFIC_PER_POSE * npose if args.workload == "config2" else None,

@@ -162,9 +162,11 @@ __device__ __forceinline__ void pair_fast(unsigned flags, float qj, float svj, f
                                           double& elec, double& vdw) {
     float ir2 = __fdividef(1.0f, d2);   // ~2 ulp; the f32 path's budget is ~1e-7 relative per term
     if (flags & F_ELEC) {
-        float ae = qj * a.w * ir2;
-        ae = fminf(fmaxf(ae, -ES_CAP_F), ES_CAP_F);
-        elec += (double)ae;
+        // a clamped term is the exact f64 cap, as in the reference: its f32
+        // rounding would otherwise add up over the many clamped pairs of a
+        // clashing pose
+        const float ae = qj * a.w * ir2;
+        elec += ae >= ES_CAP_F ? ES_CAP_D : (ae <= -ES_CAP_F ? -ES_CAP_D : (double)ae);
     }
     float sv = svj * pr.x;
     float rr = rj + pr.y;

@@ -17,10 +17,11 @@
 //      posed centre are enumerated 32 at a time (one per lane), trimmed in x
 //      to sub-cells of edge h / xsub, and turned into contiguous atom spans;
 //   3. 32 candidates at a time (lane -> span by a binary search over the
-//      warp's exclusive prefix of span lengths, coalesced float4 loads) are
-//      tested against the G slot atoms (broadcast shared-memory reads) into a
-//      G-bit mask; one warp prefix sum of the mask popcounts appends every
-//      hit (slot << 26 | receptor index) to the warp's ring buffer;
+//      warp's exclusive prefix of span lengths, coalesced float4 loads, the
+//      next chunk loaded while this one is tested) are tested against the G
+//      slot atoms (broadcast shared-memory reads), slot by slot; a ballot
+//      per slot appends that slot's hits (slot << 26 | receptor index) to
+//      the warp's ring buffer in lane order;
 //   4. while 32 or more hits are pending, each lane takes one and evaluates
 //      the pair terms with compensated distances and the exact d^2 <= 100
 //      test, accumulating in f64: the expensive math always runs on 32 lanes.
@@ -52,8 +53,9 @@ struct WSlots {
 };
 
 // pair terms of one queued hit: the exact d^2 <= 100 test on the
-// compensated d^2, then the reference formulas (those of pair_fast) with
-// the clash term selected instead of branched on
+// compensated d^2, then the reference formulas (those of pair_fast); the
+// rare queued pair beyond 10 A and the clash term are selected, not
+// branched on
 template <int G>
 __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, unsigned e, unsigned flags,
                                        double& elec, double& vdw, int& np) {
@@ -64,13 +66,14 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
     const float2 lq = W.lpar[l];
     const float dx = (lp.x - a.x) + lr.x, dy = (lp.y - a.y) + lr.y, dz = (lp.z - a.z) + lr.z;
     const float d2 = dx * dx + dy * dy + dz * dz;
-    if (!(d2 <= 100.f)) return;
-    ++np;
+    const bool in = d2 <= 100.f;
+    np += in ? 1 : 0;
     const float ir2 = __fdividef(1.0f, d2);
     if (flags & F_ELEC) {
-        float ae = lp.w * a.w * ir2;
-        ae = fminf(fmaxf(ae, -ES_CAP_F), ES_CAP_F);
-        elec += (double)ae;
+        // a clamped term is the exact f64 cap (see pair_fast)
+        const float ae = lp.w * a.w * ir2;
+        const double ed = ae >= ES_CAP_F ? ES_CAP_D : (ae <= -ES_CAP_F ? -ES_CAP_D : (double)ae);
+        elec += in ? ed : 0.0;
     }
     const float sv = lr.w * pr.x;
     const float rr = lq.x + pr.y;
@@ -80,7 +83,7 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
     const float d = d2 * rsqrtf(d2), dmin = 0.75f * rr;
     const bool clash = (flags & F_CLASH) && lq.y != 0.f && pr.z != 0.f && d < dmin;
     vp = clash ? vp + 6.f * (dmin - d) : vp;
-    vdw += (double)vp;
+    vdw += in ? (double)vp : 0.0;
 }
 
 // receptor atom of candidate kk of the current rows: the span is the last
@@ -106,6 +109,7 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char wk_smem[];
     const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
     WSlots<G>& W = reinterpret_cast<WSlots<G>*>(wk_smem)[threadIdx.x >> 5];
     for (;;) {
         unsigned long long wq = 0;
@@ -223,30 +227,19 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
                     if (k0 + 32 < total) w_fetch(c, st, excl, total, k0 + 32 + lane, an, rn);
                     const float ax = a.x - gx, ay = a.y - gy, az = a.z - gz;
                     const float aa = ax * ax + ay * ay + az * az;
-                    unsigned mask = 0;
+                    // test slot by slot; one ballot per slot appends that
+                    // slot's hits to the ring in lane order (consecutive
+                    // words: no bank conflicts, no prefix scan)
+                    const unsigned enc = (unsigned)ridx | enc_set;
 #pragma unroll
                     for (int l = 0; l < G; ++l) {
                         const float4 t = W.ltest[set + l];
                         const float q = fmaf(ax, t.x, fmaf(ay, t.y, fmaf(az, t.z, aa + t.w)));
-                        mask |= (q <= 0.f ? 1u : 0u) << l;
+                        const bool h = q <= 0.f;
+                        const unsigned b = __ballot_sync(FULL, h);
+                        if (h) W.hit[(tail + __popc(b & lt_mask)) & (RING - 1)] = enc + ((unsigned)l << 26);
+                        tail += (unsigned)__popc(b);
                     }
-                    const int nh = __popc(mask);
-                    int ex = nh;   // inclusive prefix of the hit counts
-#pragma unroll
-                    for (int o = 1; o < 32; o <<= 1) {
-                        const int v = __shfl_up_sync(FULL, ex, o);
-                        if (lane >= o) ex += v;
-                    }
-                    unsigned pos = tail + (unsigned)(ex - nh);
-                    const unsigned enc = (unsigned)ridx | enc_set;
-#pragma unroll
-                    for (int l = 0; l < G; ++l) {
-                        if (mask & (1u << l)) {
-                            W.hit[pos & (RING - 1)] = enc + ((unsigned)l << 26);
-                            ++pos;
-                        }
-                    }
-                    tail += (unsigned)__shfl_sync(FULL, ex, 31);
                     __syncwarp();
                     // 4. full batches of 32 hits
                     while ((int)(tail - head) >= 32) {
