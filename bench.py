@@ -155,6 +155,21 @@ def cpu_sample(items, min_seconds=10.0, threads=0, max_complexes=2):
         picks, "/".join(items[k]["family"] for k in picks), done, el)
 
 
+def max_over_ranks(v, dist, device):
+    """The slowest rank's value: every multi-rank time is the max over ranks."""
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_rate(units_per_rank, world, ms_max):
+    """Whole-job throughput: every rank processes units_per_rank (replicas,
+    weak scaling), the job takes the slowest rank's time."""
+    return units_per_rank * world / (ms_max / 1e3)
+
+
 def run_reference(args, rank, world):
     if rank != 0:
         return
@@ -260,11 +275,8 @@ def main():
     clk = clocks.stop()
     launches = ctx.launches - l0
     ms = ev0.elapsed_time(ev1) / args.steps
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_max = float(t.item())
-    value = npose * world / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, dist, "cuda")
+    value = job_rate(npose, world, ms_max)
 
     # e2e: host buffers through the C ABI, copies inside the timed region
     h_poses = torch.from_numpy(allp).pin_memory()
@@ -273,14 +285,17 @@ def main():
         ctx.score_multi(ids, counts, h_poses, h_scores)
     if dist:
         dist.barrier()
-    t0 = time.perf_counter()
+    # device-timed on the context stream: the events bracket every call's
+    # H2D of poses, the launch group and the D2H of scores (and any host
+    # gap between calls)
+    ev2, ev3 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev2.record(stream)
     for _ in range(args.steps):
         ctx.score_multi(ids, counts, h_poses, h_scores)
-    e2e_ms = (time.perf_counter() - t0) * 1e3 / args.steps
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device="cuda")
-    if dist:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = npose * world / (float(te.item()) / 1e3)
+    ev3.record(stream)
+    ev3.synchronize()
+    e2e_ms_max = max_over_ranks(ev2.elapsed_time(ev3) / args.steps, dist, "cuda")
+    e2e_value = job_rate(npose, world, e2e_ms_max)
 
     # plain single-complex scorer: one host-buffer call (one launch) per complex
     plain = None
@@ -327,7 +342,7 @@ def main():
                          "work": "near pairs x FLOPs/pair (dna 24, pydock 23, vdw 19) + 30 per charged ligand "
                                  "atom (far field), counted per launch"},
             "pair_rate": {"value": float(pairs.sum()) / (ms / 1e3), "unit": "near pairs/s"},
-            "e2e": {"value": e2e_value, "unit": "poses/s", "ms_per_step": float(te.item()),
+            "e2e": {"value": e2e_value, "unit": "poses/s", "ms_per_step": e2e_ms_max,
                     "h2d_bytes_per_step": npose * 7 * 8, "d2h_bytes_per_step": npose * 8,
                     "api": "lkg_score_multi (host page-locked buffers)"},
             "gpu_launches": int(launches), "clocks": clk,
