@@ -24,6 +24,7 @@ cudaError_t launch_score_fast(const LaunchParams& p, int threads, int blocks, cu
     }
     if (p.tile % p.group) return cudaErrorInvalidValue;
     switch (p.group) {
+        case 4: return launch_warp_g<4>(p, blocks, s);
         case 8: return launch_warp_g<8>(p, blocks, s);
         case 16: return launch_warp_g<16>(p, blocks, s);
         default: return launch_warp_g<32>(p, blocks, s);
@@ -53,6 +54,7 @@ cudaError_t launch_desolv_fast(const LaunchParams& p, int threads, int blocks, i
 // for per-atom outputs reuses the same grid size
 int max_blocks_score_fast(int /*threads*/, int group) {
     switch (group) {
+        case 4: return occ_warp_g<4>();
         case 8: return occ_warp_g<8>();
         case 16: return occ_warp_g<16>();
         default: return occ_warp_g<32>();

@@ -226,11 +226,15 @@ struct AdamLayers {
 
 // Adam over the whole flat parameter vector in one launch; GEMM-layer
 // entries also refresh both BF16 layouts
+// The step count t (1-based) lives on the device so that training steps can
+// be replayed from a CUDA graph; k_adam_next advances it after each step.
 __global__ void k_adam_all(float* __restrict__ p, const float* __restrict__ gr, float* __restrict__ m1,
-                           float* __restrict__ m2, int n, float lr, float b1, float b2, float eps, float bc1,
-                           float bc2, AdamLayers L) {
+                           float* __restrict__ m2, int n, float lr, float b1, float b2, float eps,
+                           const int* __restrict__ step, AdamLayers L) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
+    const float t = (float)*step;
+    const float bc1 = 1.f - powf(b1, t), bc2 = 1.f - powf(b2, t);
     const float gg = gr[i];
     const float a = b1 * m1[i] + (1.f - b1) * gg, v = b2 * m2[i] + (1.f - b2) * gg * gg;
     m1[i] = a;
@@ -246,6 +250,10 @@ __global__ void k_adam_all(float* __restrict__ p, const float* __restrict__ gr, 
             L.w[k][(size_t)c * H + r] = __float2bfloat16(np);
         }
     }
+}
+
+__global__ void k_adam_next(int* step) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
 }
 
 __global__ void k_f2bf(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, int n) {
@@ -280,7 +288,7 @@ struct lkg_surrogate {
     // activations for a batch
     DBuf X, H1, H2, H3, dH1, dH2, dH3, y, t, loss;
     int cap = 0;
-    int step = 0;
+    DBuf d_step;   // Adam step count (device, 1-based)
     size_t off[9];   // block offsets of W0 b0 W1 b1 W2 b2 w3 b3, and the total
 };
 
@@ -366,9 +374,7 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
 
 int adam(lkg_surrogate* S, float lr) {
     cudaStream_t s = S->ctx->stream;
-    S->step++;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
-    const float bc1 = 1.f - powf(b1, (float)S->step), bc2 = 1.f - powf(b2, (float)S->step);
     AdamLayers L;
     for (int k = 0; k < 3; ++k) {
         L.off[k] = (int)S->off[2 * k];
@@ -378,9 +384,10 @@ int adam(lkg_surrogate* S, float lr) {
     }
     const int n = (int)NPARAM;
     k_adam_all<<<(n + 255) / 256, 256, 0, s>>>(S->p.as<float>(), S->g.as<float>(), S->m1.as<float>(),
-                                               S->m2.as<float>(), n, lr, b1, b2, eps, bc1, bc2, L);
+                                               S->m2.as<float>(), n, lr, b1, b2, eps, S->d_step.as<int>(), L);
+    k_adam_next<<<1, 32, 0, s>>>(S->d_step.as<int>());
     LKG_CK(cudaGetLastError(), "mlp adam");
-    S->ctx->launches += 1;
+    S->ctx->launches += 2;
     return 0;
 }
 
@@ -472,7 +479,8 @@ int lkg_surrogate_create(lkg_ctx* ctx, int complex_id, uint64_t seed, lkg_surrog
     cudaError_t e;
     if ((e = S->p.reserve(NPARAM * 4)) != cudaSuccess || (e = S->g.reserve(NPARAM * 4)) != cudaSuccess ||
         (e = S->m1.reserve(NPARAM * 4)) != cudaSuccess || (e = S->m2.reserve(NPARAM * 4)) != cudaSuccess ||
-        (e = S->anchors.reserve(NA * sizeof(int))) != cudaSuccess || (e = S->loss.reserve(sizeof(float))) != cudaSuccess) {
+        (e = S->anchors.reserve(NA * sizeof(int))) != cudaSuccess || (e = S->loss.reserve(sizeof(float))) != cudaSuccess ||
+        (e = S->d_step.reserve(sizeof(int))) != cudaSuccess) {
         delete S;
         return set_error(cuda_to_status(e), "surrogate alloc: %s", cudaGetErrorString(e));
     }
@@ -486,6 +494,8 @@ int lkg_surrogate_create(lkg_ctx* ctx, int complex_id, uint64_t seed, lkg_surrog
     cudaMemcpy(S->p.p, p.data(), NPARAM * 4, cudaMemcpyHostToDevice);
     cudaMemset(S->m1.p, 0, NPARAM * 4);
     cudaMemset(S->m2.p, 0, NPARAM * 4);
+    const int one = 1;
+    cudaMemcpy(S->d_step.p, &one, sizeof(int), cudaMemcpyHostToDevice);
     cudaMemcpy(S->anchors.p, anc.data(), NA * sizeof(int), cudaMemcpyHostToDevice);
     if ((rc = refresh_bf16(S))) { delete S; return rc; }
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
@@ -547,25 +557,51 @@ int lkg_surrogate_train(lkg_surrogate* S, int n, const double* d_poses, const do
     int st;
     double last = 0.0;
     const int nb = n / batch;
-    for (int ep = 0; ep < epochs; ++ep) {
-        // launches only inside an epoch: the loss is summed on the device
-        // and read once per epoch
+    // one epoch = launches only (the loss is summed on the device); it is
+    // captured once in a CUDA graph and replayed `epochs` times
+    if ((st = sur_reserve(S, batch)) || (st = sync_descriptors(S->ctx))) return st ? st : lkg_last_status();
+    auto epoch = [&]() -> int {
         LKG_CK(cudaMemsetAsync(S->loss.p, 0, sizeof(float), s), "mlp loss clear");
         for (int b0 = 0; b0 + batch <= n; b0 += batch) {
-            if ((st = features(S, batch, d_poses + 7 * (size_t)b0))) return st;
+            int r;
+            if ((r = features(S, batch, d_poses + 7 * (size_t)b0))) return r;
             k_target<<<(batch + 255) / 256, 256, 0, s>>>(d_scores + b0, batch, S->e_scale, S->t_mu, S->t_sd,
                                                          S->t.as<float>());
-            if ((st = forward(S, batch))) return st;
-            if ((st = backward(S, batch, false))) return st;
-            if ((st = adam(S, lr))) return st;
+            if ((r = forward(S, batch))) return r;
+            if ((r = backward(S, batch, false))) return r;
+            if ((r = adam(S, lr))) return r;
         }
-        if (ep == epochs - 1) {
-            float l = 0.f;
-            LKG_CK(cudaMemcpyAsync(&l, S->loss.p, sizeof(float), cudaMemcpyDeviceToHost, s), "loss read");
-            LKG_CK(cudaStreamSynchronize(s), "train");
-            last = nb ? (double)l / nb : 0.0;
+        return 0;
+    };
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    bool graphed = false;
+    if (epochs > 1 && cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const int r = epoch();
+        const cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (r) { if (graph) cudaGraphDestroy(graph); return r; }
+        if (e == cudaSuccess && cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess) graphed = true;
+        else cudaGetLastError();
+    }
+    for (int ep = 0; ep < epochs; ++ep) {
+        if (graphed) {
+            const cudaError_t e = cudaGraphLaunch(exec, s);
+            if (e != cudaSuccess) {
+                cudaGraphExecDestroy(exec);
+                cudaGraphDestroy(graph);
+                return set_error(cuda_to_status(e), "training graph: %s", cudaGetErrorString(e));
+            }
+        } else if ((st = epoch())) {
+            return st;
         }
     }
+    float l = 0.f;
+    cudaError_t e = cudaMemcpyAsync(&l, S->loss.p, sizeof(float), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (e != cudaSuccess) return set_error(cuda_to_status(e), "train: %s", cudaGetErrorString(e));
+    last = nb ? (double)l / nb : 0.0;
     if (loss_out) *loss_out = (float)last;
     return set_ok();
 }

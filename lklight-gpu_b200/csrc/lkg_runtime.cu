@@ -581,7 +581,8 @@ int lkg_ctx_set_tiles(lkg_ctx* ctx, int threads, int cell_milli) {
 
 int lkg_ctx_set_group(lkg_ctx* ctx, int group) {
     if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
-    if (group != 8 && group != 16 && group != 32) return set_error(LKG_ERR_ARG, "group must be 8, 16 or 32");
+    if (group != 4 && group != 8 && group != 16 && group != 32)
+        return set_error(LKG_ERR_ARG, "group must be 4, 8, 16 or 32");
     if (!ctx->cx.empty() && group != ctx->group) return set_error(LKG_ERR_STATE, "group fixed once complexes exist");
     ctx->group = group;
     return set_ok();

@@ -53,9 +53,9 @@ struct WSlots {
 };
 
 // pair terms of one queued hit: the exact d^2 <= 100 test on the
-// compensated d^2, then the reference formulas (those of pair_fast); the
-// rare queued pair beyond 10 A and the clash term are selected, not
-// branched on
+// compensated d^2, then the reference formulas (those of pair_fast, with
+// the LJ power taken as (rr^2 / d^2)^3) and the clash term selected instead
+// of branched on
 template <int G>
 __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, unsigned e, unsigned flags,
                                        double& elec, double& vdw, int& np) {
@@ -66,24 +66,23 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
     const float2 lq = W.lpar[l];
     const float dx = (lp.x - a.x) + lr.x, dy = (lp.y - a.y) + lr.y, dz = (lp.z - a.z) + lr.z;
     const float d2 = dx * dx + dy * dy + dz * dz;
-    const bool in = d2 <= 100.f;
-    np += in ? 1 : 0;
+    if (!(d2 <= 100.f)) return;
+    ++np;
     const float ir2 = __fdividef(1.0f, d2);
     if (flags & F_ELEC) {
-        // a clamped term is the exact f64 cap (see pair_fast)
-        const float ae = lp.w * a.w * ir2;
-        const double ed = ae >= ES_CAP_F ? ES_CAP_D : (ae <= -ES_CAP_F ? -ES_CAP_D : (double)ae);
-        elec += in ? ed : 0.0;
+        float ae = lp.w * a.w * ir2;
+        ae = fminf(fmaxf(ae, -ES_CAP_F), ES_CAP_F);
+        elec += (double)ae;
     }
     const float sv = lr.w * pr.x;
     const float rr = lq.x + pr.y;
-    const float rr2 = rr * rr;
-    const float p6 = rr2 * rr2 * rr2 * (ir2 * ir2 * ir2);
+    const float t = rr * rr * ir2;
+    const float p6 = t * t * t;
     float vp = fminf(sv * p6 * (p6 - 2.f), 1.0f);
     const float d = d2 * rsqrtf(d2), dmin = 0.75f * rr;
     const bool clash = (flags & F_CLASH) && lq.y != 0.f && pr.z != 0.f && d < dmin;
     vp = clash ? vp + 6.f * (dmin - d) : vp;
-    vdw += in ? (double)vp : 0.0;
+    vdw += (double)vp;
 }
 
 // receptor atom of candidate kk of the current rows: the span is the last
@@ -104,7 +103,7 @@ __device__ __forceinline__ void w_fetch(const ComplexDev& c, int st, int excl, i
 
 template <int G>
 __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchParams p) {
-    static_assert(G == 8 || G == 16 || G == 32, "group size");
+    static_assert(G == 4 || G == 8 || G == 16 || G == 32, "group size");
     constexpr int RING = WRing<G>::N;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char wk_smem[];

@@ -109,7 +109,8 @@ def test_config0_fast_200_poses(ctx):
 
 
 @pytest.mark.parametrize("tile,group,xsub,cell", [(64, 8, 1, 2.5), (128, 16, 4, 2.0), (256, 32, 8, 3.33),
-                                                    (128, 8, 4, 2.5), (256, 16, 2, 2.5)])
+                                                    (128, 8, 4, 2.5), (256, 16, 2, 2.5), (128, 4, 8, 4.0),
+                                                    (128, 8, 8, 5.0)])
 def test_config0_fast_kernel_shapes(tile, group, xsub, cell):
     # every tile / group / x-sub-cell / cell shape of the warp kernel finds
     # the same near pairs (exact counts) and energies within the f32 budget
