@@ -147,15 +147,15 @@ int lkg_ctx_create(int device, lkg_ctx** out);
 int lkg_ctx_destroy(lkg_ctx* ctx);
 int lkg_ctx_set_precision(lkg_ctx* ctx, int precision);
 /* Tile shape: ligand atoms per work unit (64, 128 or 256; default 128) and
- * the receptor cell edge in 1/1000 A (default: 4 A, 2.5 A for cpydock
- * complexes); 0 keeps the current value. */
+ * the receptor cell edge in 1/1000 A (default: 4 A; 2.5 A for cpydock
+ * complexes with groups of 32); 0 keeps the current value. */
 int lkg_ctx_set_tiles(lkg_ctx* ctx, int threads_per_block, int cell_size_milli_angstrom);
 /* Ligand atoms per candidate-search group of the warp kernel (4, 8, 16 or
  * 32; default 8); fixed once complexes exist. */
 int lkg_ctx_set_group(lkg_ctx* ctx, int group);
 /* x sub-cells per receptor cell edge (1..8; default 8, 4 for cpydock
- * complexes): the near scan trims each (z, y) cell row to the 10 A sphere
- * at this finer x resolution; fixed once complexes exist. */
+ * complexes with groups of 32): the near scan trims each (z, y) cell row to
+ * the 10 A sphere at this finer x resolution; fixed once complexes exist. */
 int lkg_ctx_set_xsub(lkg_ctx* ctx, int xsub);
 /* Work on this CUDA stream (cudaStream_t) instead of the context's own. */
 int lkg_ctx_set_stream(lkg_ctx* ctx, void* stream);

@@ -42,12 +42,38 @@ static int occ_warp_g() {
 
 size_t desolv_smem_bytes(int hcap, bool /*exact*/) { return (size_t)hcap * 12; }
 
+// cpydock: the warp kernel for group sizes up to 16 (its per-warp slots and
+// the block's minimum hash fit in shared memory), the per-atom kernel above
+template <int G>
+static cudaError_t launch_warp_desolv_g(const LaunchParams& p, int blocks, int hcap, cudaStream_t s) {
+    const size_t sm = wd_smem<G>(hcap);
+    cudaError_t e = cudaFuncSetAttribute(k_score_warp_desolv<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_score_warp_desolv<G><<<blocks, WD_THREADS, sm, s>>>(p);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_desolv_fast(const LaunchParams& p, int threads, int blocks, int hcap, cudaStream_t s) {
+    switch (p.group) {
+        case 4: return launch_warp_desolv_g<4>(p, blocks, hcap, s);
+        case 8: return launch_warp_desolv_g<8>(p, blocks, hcap, s);
+        case 16: return launch_warp_desolv_g<16>(p, blocks, hcap, s);
+        default: break;
+    }
     size_t sm = desolv_smem_bytes(hcap, false);
     cudaError_t e = cudaFuncSetAttribute(k_score_desolv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     k_score_desolv<float><<<blocks, threads, sm, s>>>(p);
     return cudaGetLastError();
+}
+
+template <int G>
+static int occ_warp_desolv_g(int hcap) {
+    int n = 0;
+    const size_t sm = wd_smem<G>(hcap);
+    cudaFuncSetAttribute(k_score_warp_desolv<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_score_warp_desolv<G>, WD_THREADS, sm);
+    return n;
 }
 
 // persistent grid of the warp kernel (blocks per SM); the per-thread kernel
@@ -60,7 +86,13 @@ int max_blocks_score_fast(int /*threads*/, int group) {
         default: return occ_warp_g<32>();
     }
 }
-int max_blocks_desolv_fast(int threads, int hcap) {
+int max_blocks_desolv_fast(int threads, int hcap, int group) {
+    switch (group) {
+        case 4: return occ_warp_desolv_g<4>(hcap);
+        case 8: return occ_warp_desolv_g<8>(hcap);
+        case 16: return occ_warp_desolv_g<16>(hcap);
+        default: break;
+    }
     int n = 0;
     size_t sm = desolv_smem_bytes(hcap, false);
     cudaFuncSetAttribute(k_score_desolv<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

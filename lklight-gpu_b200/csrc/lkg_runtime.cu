@@ -14,7 +14,7 @@
 namespace lkg {
 
 int max_blocks_score_fast(int threads, int group);
-int max_blocks_desolv_fast(int threads, int hcap);
+int max_blocks_desolv_fast(int threads, int hcap, int group);
 int max_blocks_score_exact(int threads);
 int max_blocks_desolv_exact(int threads, int hcap);
 
@@ -86,10 +86,10 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     const int n = R.n;
     // the warp kernel's hit queue packs a receptor index into 26 bits
     if (n >= (1 << 26)) return set_error(LKG_ERR_ARG, "receptor has %d atoms (limit %d)", n, (1 << 26) - 1);
-    // grid shape: the caller's, else per kernel: the warp kernel enumerates
-    // rows per ligand group (coarser rows, finer x trim pay off), the
-    // per-atom cpydock kernel per atom
-    const bool per_atom = cr.family == LKG_CPYDOCK;
+    // grid shape: the caller's, else per kernel: the warp kernels enumerate
+    // rows per ligand group (coarser rows, finer x trim pay off); cpydock
+    // with groups of 32 runs the per-atom kernel, which scans rows per atom
+    const bool per_atom = cr.family == LKG_CPYDOCK && ctx->group > 16;
     const float h = ctx->cell_h > 0.f ? ctx->cell_h : (per_atom ? 2.5f : 4.0f), inv_h = 1.0f / h;
     const int xsub = ctx->xsub > 0 ? ctx->xsub : (per_atom ? 4 : 8);
     const float hx = h / (float)xsub, inv_hx = 1.0f / hx;
@@ -284,7 +284,7 @@ int occupancy(lkg_ctx* ctx, bool desolv, bool exact, int threads, int hcap) {
     Occupancy& o = desolv ? ctx->occ_desolv[exact] : ctx->occ_tiles[exact];
     if (o.threads == threads && o.hcap == hcap && o.blocks > 0) return o.blocks;
     int b;
-    if (desolv) b = exact ? max_blocks_desolv_exact(threads, hcap) : max_blocks_desolv_fast(threads, hcap);
+    if (desolv) b = exact ? max_blocks_desolv_exact(threads, hcap) : max_blocks_desolv_fast(threads, hcap, ctx->group);
     else b = exact ? max_blocks_score_exact(threads) : max_blocks_score_fast(threads, ctx->group);
     o.threads = threads; o.hcap = hcap; o.blocks = std::max(1, b);
     return o.blocks;

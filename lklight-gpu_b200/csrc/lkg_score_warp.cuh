@@ -42,6 +42,17 @@ template <int G> struct WRing { static constexpr int N = (G <= 8) ? 512 : (G <= 
 // thread for G = 8; the larger masks of G = 16, 32 get 80)
 template <int G> struct WOcc { static constexpr int N = (G <= 8) ? 8 : 6; };
 
+// per-warp desolvation state of the two slot sets (cpydock): the slot
+// atoms' f64 positions, their running minimum d^2 to non-excluded receptor
+// atoms (f64 bits; non-negative doubles order like their bit patterns) and
+// whether the ligand atom itself is excluded
+template <int G>
+struct WDes {
+    double lx[2 * G], ly[2 * G], lz[2 * G];
+    unsigned long long lmin[2 * G];
+    int lf[2 * G];
+};
+
 template <int G>
 struct WSlots {
     Rot rot;                    // pose of the current work unit
@@ -55,10 +66,12 @@ struct WSlots {
 // pair terms of one queued hit: the exact d^2 <= 100 test on the
 // compensated d^2, then the reference formulas (those of pair_fast, with
 // the LJ power taken as (rr^2 / d^2)^3) and the clash term selected instead
-// of branched on
-template <int G>
-__device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, unsigned e, unsigned flags,
-                                       double& elec, double& vdw, int& np) {
+// of branched on.  DESOLV: pairs that can lie within 6.4 A also update both
+// atoms' minimum distance in f64 (cpydock.rs:615-668), the ligand atom's in
+// its slot, the receptor atom's in the block's hash.
+template <int G, bool DESOLV>
+__device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, WDes<G>* D, MinHash* hash,
+                                       int* status, unsigned e, unsigned flags, double& elec, double& vdw, int& np) {
     const int l = (int)(e >> 26), k = (int)(e & 0x3ffffffu);
     const float4 a = __ldg(c.rpos + k);
     const float4 pr = __ldg(c.rpar + k);
@@ -83,6 +96,13 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
     const bool clash = (flags & F_CLASH) && lq.y != 0.f && pr.z != 0.f && d < dmin;
     vp = clash ? vp + 6.f * (dmin - d) : vp;
     vdw += (double)vp;
+    if (DESOLV && !D->lf[l] && pr.w == 0.f && d2 <= SOLV2_F * 1.001f) {
+        const double4 a64 = c.rpos64[k];
+        const double ex = D->lx[l] - a64.x, ey = D->ly[l] - a64.y, ez = D->lz[l] - a64.z;
+        const double d2d = ex * ex + ey * ey + ez * ez;
+        atomicMin(&D->lmin[l], (unsigned long long)__double_as_longlong(d2d));
+        if (d2d <= SOLV2_D && !hash->insert(k, d2d)) atomicOr(status, 1);
+    }
 }
 
 // receptor atom of candidate kk of the current rows: the span is the last
@@ -101,14 +121,183 @@ __device__ __forceinline__ void w_fetch(const ComplexDev& c, int st, int excl, i
     a = kk < total ? __ldg(c.rpos + ridx) : make_float4(3e30f, 3e30f, 3e30f, 0.f);
 }
 
+constexpr unsigned long long W_NOMIN = 0x7fefffffffffffffull;   // largest finite double
+
+// The warp's sums over its groups.
+struct WAcc {
+    double elec = 0.0, vdw = 0.0, solv = 0.0;
+    int np = 0;
+};
+
+// Scores groups g_first, g_first + g_step, ... (< g_end) of one pose whose
+// rotation is in W.rot, into acc (per lane).  DESOLV also adds each slot
+// atom's g(min d^2) * des to acc.solv once its hits are all evaluated.
+template <int G, bool DESOLV>
+__device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes<G>* D, MinHash* hash, int* status,
+                                         int g_first, int g_end, int g_step, WAcc& acc) {
+    constexpr int RING = WRing<G>::N;
+    constexpr unsigned FULL = 0xffffffffu;
+    const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
+    const unsigned flags = c.flags;
+    const int nl = c.nl;
+    unsigned head = 0, tail = 0, prev_start = 0;
+    int jdes0 = -1, jdes1 = -1;   // DESOLV: this lane's slot atom in set 0 / set 1
+    auto drain_partial = [&]() {
+        if ((int)(tail - head) > lane)
+            w_pair<G, DESOLV>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, acc.elec, acc.vdw, acc.np);
+        head = tail;
+    };
+    auto finalize = [&](int set) {   // DESOLV: the slot set's minima are final
+        const int j = set ? jdes1 : jdes0;
+        if (DESOLV && lane < G && j >= 0) {
+            const double2 ls = c.lsolv64[j];
+            acc.solv += solv_term(__longlong_as_double((long long)D->lmin[set + lane]), ls.y) * ls.x;
+        }
+        if (set) jdes1 = -1; else jdes0 = -1;
+    };
+    int it = 0;
+    for (int grp = g_first; grp < g_end; grp += g_step, ++it) {
+        const int set = (it & 1) * G;
+        // slot set `set` last served the group before the previous one, whose
+        // hits were queued before the previous group started: evaluate any
+        // still pending
+        if ((int)(prev_start - head) > 0) drain_partial();
+        prev_start = tail;
+        __syncwarp();
+        finalize(set);
+        // 1. the group's ligand atoms
+        if (lane < G) {
+            const int j = grp * G + lane;
+            const bool valid = j < nl;
+            const float4 b4 = valid ? __ldg(c.lpos + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 lp4 = valid ? __ldg(c.lpar + j) : make_float4(0.f, 0.f, 0.f, 0.f);
+            double xd, yd, zd;
+            if (DESOLV) {   // the cpydock kernels transform the f64 coordinates
+                const double4 b64 = valid ? c.lpos64[j] : make_double4(0.0, 0.0, 0.0, 0.0);
+                apply(W.rot, b64.x, b64.y, b64.z, xd, yd, zd);
+            } else {
+                apply(W.rot, (double)b4.x, (double)b4.y, (double)b4.z, xd, yd, zd);
+            }
+            float x = (float)xd, y = (float)yd, z = (float)zd;
+            const float4 res = make_float4((float)(xd - (double)x), (float)(yd - (double)y),
+                                           (float)(zd - (double)z), lp4.x);
+            if (valid && (flags & F_FAR) && b4.w != 0.f) acc.elec += (double)(b4.w * sample_phi(c, x, y, z));
+            if (!valid) { x = y = z = 1e30f; }   // never within reach of a receptor atom
+            W.lpos[set + lane] = make_float4(x, y, z, b4.w);
+            W.lres[set + lane] = res;
+            W.lpar[set + lane] = make_float2(lp4.y, lp4.z);
+            if (DESOLV) {
+                D->lx[set + lane] = xd; D->ly[set + lane] = yd; D->lz[set + lane] = zd;
+                D->lmin[set + lane] = W_NOMIN;
+                D->lf[set + lane] = lp4.w != 0.f;
+                if (set) jdes1 = valid ? j : -1; else jdes0 = valid ? j : -1;
+            }
+        }
+        // 2. receptor rows within reach of the group sphere
+        const float4 gs = __ldg(c.lgrp + grp);
+        double cxd, cyd, czd;
+        apply(W.rot, (double)gs.x, (double)gs.y, (double)gs.z, cxd, cyd, czd);
+        const float gx = (float)cxd, gy = (float)cyd, gz = (float)czd;
+        if (lane < G) {
+            // candidate test |a' - l'|^2 <= 100.01 as |a'|^2 - 2 a'.l' +
+            // |l'|^2 in the group frame (|a'| <= ~20 A: rounding ~1e-4,
+            // far inside the 0.01 margin); invalid slots never pass
+            const float4 lp = W.lpos[set + lane];
+            const float lx = lp.x - gx, ly = lp.y - gy, lz = lp.z - gz;
+            const bool far_slot = !(lp.x < 1e29f);
+            W.ltest[set + lane] = far_slot ? make_float4(0.f, 0.f, 0.f, 3e30f)
+                                           : make_float4(-2.f * lx, -2.f * ly, -2.f * lz,
+                                                         lx * lx + ly * ly + lz * lz - 100.01f);
+        }
+        __syncwarp();
+        const float R = SCAN_R + gs.w, R2 = R * R;
+        const int cz0 = max(0, (int)floorf((gz - R - c.oz) * c.inv_h));
+        const int cz1 = min(c.ncz - 1, (int)floorf((gz + R - c.oz) * c.inv_h));
+        const int cy0 = max(0, (int)floorf((gy - R - c.oy) * c.inv_h));
+        const int cy1 = min(c.ncy - 1, (int)floorf((gy + R - c.oy) * c.inv_h));
+        const int nyr = cy1 - cy0 + 1, nzr = cz1 - cz0 + 1;
+        const int nbox = (nyr > 0 && nzr > 0) ? nyr * nzr : 0;
+        const float inv_nyr = 1.0f / (float)max(nyr, 1);
+        const unsigned enc_set = (unsigned)set << 26;
+        for (int r0 = 0; r0 < nbox; r0 += 32) {
+            const int r = r0 + lane;
+            int st = 0, len = 0;
+            if (r < nbox) {
+                // r = zz * nyr + yy; (r + 0.5) / nyr is at least 0.5 / nyr
+                // away from an integer, far above the f32 rounding error
+                const int zz = (int)(((float)r + 0.5f) * inv_nyr), yy = r - zz * nyr;
+                const int cz = cz0 + zz, cy = cy0 + yy;
+                const float zlo = c.oz + cz * c.h, ylo = c.oy + cy * c.h;
+                const float dzm = fmaxf(0.f, fmaxf(zlo - gz, gz - (zlo + c.h)));
+                const float dym = fmaxf(0.f, fmaxf(ylo - gy, gy - (ylo + c.h)));
+                const float rem = R2 - dzm * dzm - dym * dym;
+                if (rem >= 0.f) {
+                    const float wx = sqrtf(rem);
+                    const int cx0 = max(0, (int)floorf((gx - wx - c.ox) * c.inv_hx));
+                    const int cx1 = min(c.ncx - 1, (int)floorf((gx + wx - c.ox) * c.inv_hx));
+                    if (cx0 <= cx1) {
+                        const int row = (cz * c.ncy + cy) * c.ncx;
+                        st = __ldg(c.cell_start + row + cx0);
+                        len = __ldg(c.cell_start + row + cx1 + 1) - st;
+                    }
+                }
+            }
+            int inc = len;   // inclusive prefix of the span lengths
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(FULL, inc, o);
+                if (lane >= o) inc += v;
+            }
+            const int total = __shfl_sync(FULL, inc, 31);
+            const int excl = inc - len;
+            // 3. candidate chunks; the next chunk's receptor atoms are
+            //    fetched while the current one is tested
+            float4 an = make_float4(3e30f, 3e30f, 3e30f, 0.f);
+            int rn = 0;
+            if (total > 0) w_fetch(c, st, excl, total, lane, an, rn);
+            for (int k0 = 0; k0 < total; k0 += 32) {
+                const float4 a = an;
+                const int ridx = rn;
+                if (k0 + 32 < total) w_fetch(c, st, excl, total, k0 + 32 + lane, an, rn);
+                const float ax = a.x - gx, ay = a.y - gy, az = a.z - gz;
+                const float aa = ax * ax + ay * ay + az * az;
+                // test slot by slot; one ballot per slot appends that slot's
+                // hits to the ring in lane order (consecutive words: no bank
+                // conflicts, no prefix scan)
+                const unsigned enc = (unsigned)ridx | enc_set;
+#pragma unroll
+                for (int l = 0; l < G; ++l) {
+                    const float4 t = W.ltest[set + l];
+                    const float q = fmaf(ax, t.x, fmaf(ay, t.y, fmaf(az, t.z, aa + t.w)));
+                    const bool h = q <= 0.f;
+                    const unsigned b = __ballot_sync(FULL, h);
+                    if (h) W.hit[(tail + __popc(b & lt_mask)) & (RING - 1)] = enc + ((unsigned)l << 26);
+                    tail += (unsigned)__popc(b);
+                }
+                __syncwarp();
+                // 4. full batches of 32 hits
+                while ((int)(tail - head) >= 32) {
+                    w_pair<G, DESOLV>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, acc.elec,
+                                      acc.vdw, acc.np);
+                    head += 32;
+                }
+            }
+        }
+    }
+    __syncwarp();
+    drain_partial();
+    __syncwarp();
+    finalize(0);
+    finalize(G);
+}
+
 template <int G>
 __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchParams p) {
     static_assert(G == 4 || G == 8 || G == 16 || G == 32, "group size");
-    constexpr int RING = WRing<G>::N;
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char wk_smem[];
     const int lane = threadIdx.x & 31;
-    const unsigned lt_mask = (1u << lane) - 1u;
     WSlots<G>& W = reinterpret_cast<WSlots<G>*>(wk_smem)[threadIdx.x >> 5];
     for (;;) {
         unsigned long long wq = 0;
@@ -121,138 +310,15 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
         const int ntiles = c.ntiles;
         const int pose = (int)(local / ntiles), tile = (int)(local % ntiles);
         const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
-        const unsigned flags = c.flags;
-        const int nl = c.nl;
         __syncwarp();   // readers of the previous unit's pose are done
         if (lane == 0) W.rot = pose_matrix(p.poses + 7 * g);
         __syncwarp();
-        double elec = 0.0, vdw = 0.0;
-        int np = 0;
-        unsigned head = 0, tail = 0, prev_start = 0;
         const int gpt = p.tile / G;
-        const int g0 = tile * gpt, g1 = min(g0 + gpt, (nl + G - 1) / G);
-        for (int grp = g0; grp < g1; ++grp) {
-            const int set = ((grp - g0) & 1) * G;
-            // slot set `set` last served group grp-2, whose hits were queued
-            // before the previous group started: evaluate any still pending
-            if ((int)(prev_start - head) > 0) {
-                if ((int)(tail - head) > lane) w_pair<G>(c, W, W.hit[(head + lane) & (RING - 1)], flags, elec, vdw, np);
-                head = tail;
-            }
-            prev_start = tail;
-            __syncwarp();
-            // 1. the group's ligand atoms
-            if (lane < G) {
-                const int j = grp * G + lane;
-                const bool valid = j < nl;
-                const float4 b4 = valid ? __ldg(c.lpos + j) : make_float4(0.f, 0.f, 0.f, 0.f);
-                const float4 lp4 = valid ? __ldg(c.lpar + j) : make_float4(0.f, 0.f, 0.f, 0.f);
-                double xd, yd, zd;
-                apply(W.rot, (double)b4.x, (double)b4.y, (double)b4.z, xd, yd, zd);
-                float x = (float)xd, y = (float)yd, z = (float)zd;
-                const float4 res = make_float4((float)(xd - (double)x), (float)(yd - (double)y),
-                                               (float)(zd - (double)z), lp4.x);
-                if (valid && (flags & F_FAR) && b4.w != 0.f) elec += (double)(b4.w * sample_phi(c, x, y, z));
-                if (!valid) { x = y = z = 1e30f; }   // never within reach of a receptor atom
-                W.lpos[set + lane] = make_float4(x, y, z, b4.w);
-                W.lres[set + lane] = res;
-                W.lpar[set + lane] = make_float2(lp4.y, lp4.z);
-            }
-            // 2. receptor rows within reach of the group sphere
-            const float4 gs = __ldg(c.lgrp + grp);
-            double cxd, cyd, czd;
-            apply(W.rot, (double)gs.x, (double)gs.y, (double)gs.z, cxd, cyd, czd);
-            const float gx = (float)cxd, gy = (float)cyd, gz = (float)czd;
-            if (lane < G) {
-                // candidate test |a' - l'|^2 <= 100.01 as |a'|^2 - 2 a'.l' +
-                // |l'|^2 in the group frame (|a'| <= ~20 A: rounding ~1e-4,
-                // far inside the 0.01 margin); invalid slots never pass
-                const float4 lp = W.lpos[set + lane];
-                const float lx = lp.x - gx, ly = lp.y - gy, lz = lp.z - gz;
-                const bool far_slot = !(lp.x < 1e29f);
-                W.ltest[set + lane] = far_slot ? make_float4(0.f, 0.f, 0.f, 3e30f)
-                                               : make_float4(-2.f * lx, -2.f * ly, -2.f * lz,
-                                                             lx * lx + ly * ly + lz * lz - 100.01f);
-            }
-            __syncwarp();
-            const float R = SCAN_R + gs.w, R2 = R * R;
-            const int cz0 = max(0, (int)floorf((gz - R - c.oz) * c.inv_h));
-            const int cz1 = min(c.ncz - 1, (int)floorf((gz + R - c.oz) * c.inv_h));
-            const int cy0 = max(0, (int)floorf((gy - R - c.oy) * c.inv_h));
-            const int cy1 = min(c.ncy - 1, (int)floorf((gy + R - c.oy) * c.inv_h));
-            const int nyr = cy1 - cy0 + 1, nzr = cz1 - cz0 + 1;
-            const int nbox = (nyr > 0 && nzr > 0) ? nyr * nzr : 0;
-            const float inv_nyr = 1.0f / (float)max(nyr, 1);
-            const unsigned enc_set = (unsigned)set << 26;
-            for (int r0 = 0; r0 < nbox; r0 += 32) {
-                const int r = r0 + lane;
-                int st = 0, len = 0;
-                if (r < nbox) {
-                    // r = zz * nyr + yy; (r + 0.5) / nyr is at least 0.5 / nyr
-                    // away from an integer, far above the f32 rounding error
-                    const int zz = (int)(((float)r + 0.5f) * inv_nyr), yy = r - zz * nyr;
-                    const int cz = cz0 + zz, cy = cy0 + yy;
-                    const float zlo = c.oz + cz * c.h, ylo = c.oy + cy * c.h;
-                    const float dzm = fmaxf(0.f, fmaxf(zlo - gz, gz - (zlo + c.h)));
-                    const float dym = fmaxf(0.f, fmaxf(ylo - gy, gy - (ylo + c.h)));
-                    const float rem = R2 - dzm * dzm - dym * dym;
-                    if (rem >= 0.f) {
-                        const float wx = sqrtf(rem);
-                        const int cx0 = max(0, (int)floorf((gx - wx - c.ox) * c.inv_hx));
-                        const int cx1 = min(c.ncx - 1, (int)floorf((gx + wx - c.ox) * c.inv_hx));
-                        if (cx0 <= cx1) {
-                            const int row = (cz * c.ncy + cy) * c.ncx;
-                            st = __ldg(c.cell_start + row + cx0);
-                            len = __ldg(c.cell_start + row + cx1 + 1) - st;
-                        }
-                    }
-                }
-                int inc = len;   // inclusive prefix of the span lengths
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int v = __shfl_up_sync(FULL, inc, o);
-                    if (lane >= o) inc += v;
-                }
-                const int total = __shfl_sync(FULL, inc, 31);
-                const int excl = inc - len;
-                // 3. candidate chunks; the next chunk's receptor atoms are
-                //    fetched while the current one is tested
-                float4 an = make_float4(3e30f, 3e30f, 3e30f, 0.f);
-                int rn = 0;
-                if (total > 0) w_fetch(c, st, excl, total, lane, an, rn);
-                for (int k0 = 0; k0 < total; k0 += 32) {
-                    const float4 a = an;
-                    const int ridx = rn;
-                    if (k0 + 32 < total) w_fetch(c, st, excl, total, k0 + 32 + lane, an, rn);
-                    const float ax = a.x - gx, ay = a.y - gy, az = a.z - gz;
-                    const float aa = ax * ax + ay * ay + az * az;
-                    // test slot by slot; one ballot per slot appends that
-                    // slot's hits to the ring in lane order (consecutive
-                    // words: no bank conflicts, no prefix scan)
-                    const unsigned enc = (unsigned)ridx | enc_set;
-#pragma unroll
-                    for (int l = 0; l < G; ++l) {
-                        const float4 t = W.ltest[set + l];
-                        const float q = fmaf(ax, t.x, fmaf(ay, t.y, fmaf(az, t.z, aa + t.w)));
-                        const bool h = q <= 0.f;
-                        const unsigned b = __ballot_sync(FULL, h);
-                        if (h) W.hit[(tail + __popc(b & lt_mask)) & (RING - 1)] = enc + ((unsigned)l << 26);
-                        tail += (unsigned)__popc(b);
-                    }
-                    __syncwarp();
-                    // 4. full batches of 32 hits
-                    while ((int)(tail - head) >= 32) {
-                        w_pair<G>(c, W, W.hit[(head + lane) & (RING - 1)], flags, elec, vdw, np);
-                        head += 32;
-                    }
-                }
-            }
-        }
-        __syncwarp();
-        if ((int)(tail - head) > lane) w_pair<G>(c, W, W.hit[(head + lane) & (RING - 1)], flags, elec, vdw, np);
-        elec = warp_sum(elec);
-        vdw = warp_sum(vdw);
-        const long long npl = warp_sum((long long)np);
+        const int g0 = tile * gpt, g1 = min(g0 + gpt, (c.nl + G - 1) / G);
+        WAcc acc;
+        w_groups<G, false>(c, W, nullptr, nullptr, nullptr, g0, g1, 1, acc);
+        const double elec = warp_sum(acc.elec), vdw = warp_sum(acc.vdw);
+        const long long npl = warp_sum((long long)acc.np);
         if (lane == 0) {
             // partial of work unit w; the pose's units are w - tile .. w - tile + ntiles - 1
             double* part = p.partials + (size_t)w * 4;
@@ -272,6 +338,69 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
         }
     }
     __syncthreads();   // every warp of the block has left the work loop
+    finish_launch(p);
+}
+
+// cpydock: one block per pose (the receptor-side minima live in the block's
+// shared-memory hash); warp k takes the pose's groups k, k + NW, ... (a fixed
+// assignment: the sums do not depend on scheduling).  Block layout of the
+// dynamic shared memory: hash (hcap x 12 B), then NW x WSlots, NW x WDes.
+constexpr int WD_THREADS = 512;
+
+template <int G>
+__host__ __device__ constexpr size_t wd_smem(int hcap) {
+    return (size_t)hcap * 12 + (size_t)(WD_THREADS / 32) * (sizeof(WSlots<G>) + sizeof(WDes<G>));
+}
+
+template <int G>
+__global__ void __launch_bounds__(WD_THREADS, 1) k_score_warp_desolv(LaunchParams p) {
+    constexpr int NW = WD_THREADS / 32;
+    extern __shared__ __align__(16) unsigned char wd_smem_raw[];
+    __shared__ long long s_work;
+    __shared__ double s_red[4][32];
+    __shared__ long long s_fix[32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (;;) {
+        if (threadIdx.x == 0) s_work = (long long)atomicAdd(p.work_counter, 1ull);
+        __syncthreads();
+        const long long w = s_work;
+        __syncthreads();
+        if (w >= p.total_work) break;
+        const int b = find_item(p.item_work0, p.n_items, w);
+        const ComplexDev& c = p.cx[__ldg(p.item_complex + b)];
+        const int pose = (int)(w - __ldg(p.item_work0 + b));
+        const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
+        MinHash hash;
+        hash.init(reinterpret_cast<char*>(wd_smem_raw), c.hcap);
+        unsigned char* base = wd_smem_raw + (size_t)c.hcap * 12;
+        WSlots<G>& W = reinterpret_cast<WSlots<G>*>(base)[wid];
+        WDes<G>* D = reinterpret_cast<WDes<G>*>(base + (size_t)NW * sizeof(WSlots<G>)) + wid;
+        if (lane == 0) W.rot = pose_matrix(p.poses + 7 * g);
+        __syncthreads();   // hash cleared, poses set
+        WAcc acc;
+        w_groups<G, true>(c, W, D, &hash, p.status, wid, (c.nl + G - 1) / G, NW, acc);
+        __syncthreads();   // every pair has updated the hash
+        // receptor side: fixed-point (2^-40) sum over hash slots; slot order
+        // depends on insertion races, integer sums do not
+        long long fix = 0;
+        for (int s = threadIdx.x; s < c.hcap; s += blockDim.x) {
+            const int k = hash.keys[s];
+            if (k < 0) continue;
+            const double2 rs = c.rsolv64[k];
+            fix += __double2ll_rn(solv_term(hash.value(s), rs.y) * rs.x * 1099511627776.0);
+        }
+        fix = warp_sum(fix);
+        if (lane == 0) s_fix[wid] = fix;
+        double v[4] = {acc.elec, acc.vdw, acc.solv, (double)acc.np};
+        block_sum<4>(v, s_red);   // contains __syncthreads: s_fix is complete
+        if (threadIdx.x == 0) {
+            long long f = 0;
+            for (int i = 0; i < NW; ++i) f += s_fix[i];
+            write_pose(p, c, g, p.solv_only ? 0.0 : v[0], p.solv_only ? 0.0 : v[1],
+                       v[2] + (double)f * (1.0 / 1099511627776.0), v[3]);
+        }
+        __syncthreads();
+    }
     finish_launch(p);
 }
 
