@@ -277,7 +277,8 @@ template <> struct Atom<float> {
         const bool hj = lp.z != 0.f, lf = lp.w != 0.f;
         const unsigned flags = c.flags;
         double elec = 0.0, vdw = 0.0;
-        if ((flags & F_FAR) && qj != 0.f) elec += (double)(qj * sample_phi(c, x, y, z));
+        // far field with the reference's f64 interpolation (per atom, cheap)
+        if ((flags & F_FAR) && qj != 0.f) elec += c.lpos64[j].w * sample_phi(c, xd, yd, zd);
         int np = 0;
         scan_rows(c, x, y, z, [&](int k) {
             float4 a = Tr<float>::rpos(c, k);

@@ -182,7 +182,9 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
             float x = (float)xd, y = (float)yd, z = (float)zd;
             const float4 res = make_float4((float)(xd - (double)x), (float)(yd - (double)y),
                                            (float)(zd - (double)z), lp4.x);
-            if (valid && (flags & F_FAR) && b4.w != 0.f) acc.elec += (double)(b4.w * sample_phi(c, x, y, z));
+            // far field with the reference's f64 interpolation (a per-atom
+            // cost; f32 here would add up over thousands of charged atoms)
+            if (valid && (flags & F_FAR) && b4.w != 0.f) acc.elec += c.lpos64[j].w * sample_phi(c, xd, yd, zd);
             if (!valid) { x = y = z = 1e30f; }   // never within reach of a receptor atom
             W.lpos[set + lane] = make_float4(x, y, z, b4.w);
             W.lres[set + lane] = res;
