@@ -313,7 +313,8 @@ def main():
 
     peaks = {}
     try:
-        peaks = json.load(open(os.path.join(REPO, "MEASURED_PEAKS.json")))
+        with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
     except (OSError, ValueError):
         pass
     sm_max = float(peaks.get("sm_max_mhz", 1965.0))

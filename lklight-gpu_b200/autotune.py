@@ -52,7 +52,8 @@ def autotune(items, device=0, candidates=CANDIDATES, sample=8, poses_per_complex
     cache = {}
     if cache_path and os.path.exists(cache_path):
         try:
-            cache = json.load(open(cache_path))
+            with open(cache_path) as f:
+                cache = json.load(f)
         except (OSError, ValueError):
             cache = {}
     if key in cache:

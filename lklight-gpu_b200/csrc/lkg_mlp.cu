@@ -298,6 +298,7 @@ constexpr size_t NPARAM = (size_t)H * IN + H + 2 * ((size_t)H * H + H) + H + 1;
 
 int sur_reserve(lkg_surrogate* S, int n) {
     if (n <= S->cap) return 0;
+    if (S->cap > 0) n = std::max(n, S->cap + S->cap / 2);   // grow geometrically
     size_t nb = (size_t)n * sizeof(__nv_bfloat16);
     LKG_CK(S->X.reserve(nb * IN), "surrogate alloc");
     LKG_CK(S->H1.reserve(nb * H), "surrogate alloc");

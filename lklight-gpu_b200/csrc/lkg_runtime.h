@@ -2,6 +2,7 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 #include <memory>
 #include <string>
@@ -32,11 +33,16 @@ struct DBuf {
     DBuf& operator=(const DBuf&) = delete;
     ~DBuf() { release(); }
     void release() { if (p) cudaFree(p); p = nullptr; bytes = 0; }
-    cudaError_t reserve(size_t n) {  // grow-only, contents not kept
+    // grow-only, contents not kept; a buffer that has to grow again grows
+    // by at least half its size, so slowly rising demands (the candidate
+    // counts of successive GSO steps) do not reallocate every time (each
+    // cudaFree synchronises the device)
+    cudaError_t reserve(size_t n) {
         if (n <= bytes && p) return cudaSuccess;
+        const size_t want = p ? std::max(n, bytes + bytes / 2) : n;
         release();
-        cudaError_t e = cudaMalloc(&p, n ? n : 16);
-        if (e == cudaSuccess) bytes = n ? n : 16;
+        cudaError_t e = cudaMalloc(&p, want ? want : 16);
+        if (e == cudaSuccess) bytes = want ? want : 16;
         else p = nullptr;
         return e;
     }
@@ -51,12 +57,13 @@ struct HBuf {
     HBuf(const HBuf&) = delete;
     HBuf& operator=(const HBuf&) = delete;
     ~HBuf() { if (p) cudaFreeHost(p); }
-    cudaError_t reserve(size_t n) {
+    cudaError_t reserve(size_t n) {   // grow-only, geometric like DBuf
         if (n <= bytes && p) return cudaSuccess;
+        const size_t want = p ? std::max(n, bytes + bytes / 2) : n;
         if (p) cudaFreeHost(p);
         p = nullptr; bytes = 0;
-        cudaError_t e = cudaMallocHost(&p, n ? n : 16);
-        if (e == cudaSuccess) bytes = n ? n : 16;
+        cudaError_t e = cudaMallocHost(&p, want ? want : 16);
+        if (e == cudaSuccess) bytes = want ? want : 16;
         return e;
     }
     template <class T> T* as() const { return (T*)p; }

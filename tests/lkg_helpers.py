@@ -22,7 +22,8 @@ def rel_err(a, b):
 
 def header_symbols():
     """Every function declared in include/lkg.h."""
-    src = open(os.path.join(REPO, "include", "lkg.h")).read()
+    with open(os.path.join(REPO, "include", "lkg.h")) as f:
+        src = f.read()
     src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
     return sorted(set(re.findall(r"\b((?:cuda|lkg)_\w+)\s*\(", src)))
 
