@@ -91,7 +91,7 @@ def lib():
         "lkg_gso_create": (I, [P, I, P, P, P, P, P, P]), "lkg_gso_run": (I, [P, I]),
         "lkg_gso_state": (I, [P, P, P, P, P, P, P]), "lkg_gso_scored": (I64, [P]),
         "lkg_gso_destroy": (I, [P]), "lkg_compat_cache_clear": (None, []),
-        "lkg_gso_set_screen": (I, [P, P]), "lkg_gso_finalize": (I, [P]), "lkg_gso_predicted": (I64, [P]), "lkg_gso_timing": (I, [P, P]),
+        "lkg_gso_set_screen": (I, [P, P]), "lkg_gso_finalize": (I, [P]), "lkg_gso_predicted": (I64, [P]), "lkg_gso_timing": (I, [P, P]), "lkg_gso_run_device": (I, [P, I]),
         "cuda_batch_score": (I, [P, I, I, I, F, F, F, F, P, P, P, P, P, I, P, P, I, I, I, F, F, F, F,
                                  P, P, P, P, P, P, I, I, C.c_uint, P]),
         "cuda_cpydock_solv": (I, [P, P, I, P, P, I, I, I, F, F, F, F, P, P, P, P, I, I, P, P, P, P, P]),
@@ -388,8 +388,10 @@ class GSO:
                                     C.byref(h)))
         self.h = h
 
-    def run(self, steps):
-        _check(lib().lkg_gso_run(self.h, steps))
+    def run(self, steps, device=False):
+        """steps of the plain GSO; device=True runs whole steps on the GPU
+        (graph-replayed; not bitwise equal to the host GSO, see lkg.h)."""
+        _check((lib().lkg_gso_run_device if device else lib().lkg_gso_run)(self.h, steps))
 
     def state(self):
         n = self.n

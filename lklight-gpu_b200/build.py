@@ -19,8 +19,8 @@ INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_FLAGS = ["-O3", "-std=c++17", "-lineinfo", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fopenmp", "-I" + INCLUDE]
-NO_FMAD = {"lkg_kernels_exact.cu", "lkg_field.cu"}
-HEADERS = ["lkg_internal.h", "lkg_runtime.h", "lkg_score.cuh", "lkg_score_warp.cuh", "lkg_rng.h"]
+NO_FMAD = {"lkg_kernels_exact.cu", "lkg_field.cu", "lkg_gso_dev.cu"}
+HEADERS = ["lkg_internal.h", "lkg_runtime.h", "lkg_score.cuh", "lkg_score_warp.cuh", "lkg_rng.h", "lkg_gso_dev.h"]
 
 
 def _nvcc():

@@ -16,6 +16,7 @@
 #include <unordered_map>
 #include <vector>
 
+#include "lkg_gso_dev.h"
 #include "lkg_rng.h"
 #include "lkg_runtime.h"
 
@@ -270,8 +271,15 @@ struct lkg_gso {
     StdRng rank_rng;                             // candidate ranks of the no-network ablation
     lkg::DBuf d_tp, d_ts, d_cand, d_pred;
     lkg::HBuf h_cand, h_pred;
+    // device-resident plain GSO (lkg_gso_run_device)
+    lkg_plan* dplan = nullptr;
+    cudaGraphExec_t dexec = nullptr;
+    lkg::GsoDevState ds{}, ds_captured{};
+    lkg::DBuf dbuf[24];
     ~lkg_gso() {
         for (auto* s : sur) lkg_surrogate_destroy(s);
+        if (dexec) cudaGraphExecDestroy(dexec);
+        if (dplan) lkg_plan_destroy(dplan);
     }
 };
 
@@ -604,6 +612,139 @@ int lkg_gso_state(lkg_gso* G, double* trans, double* rot, double* luc, double* s
 
 int64_t lkg_gso_scored(lkg_gso* G) { return G ? G->scored : 0; }
 int64_t lkg_gso_predicted(lkg_gso* G) { return G ? G->predicted : 0; }
+
+// Plain GSO steps on the device: the state goes up once, every step (score
+// all glowworms, luciferin, select, move) runs as kernel launches replayed
+// from one CUDA graph, and the state comes back at the end.  Unmoved
+// glowworms are rescored with the same pose, which gives the same score.
+int lkg_gso_run_device(lkg_gso* G, int steps) {
+    if (!G || steps < 0) return set_error(LKG_ERR_ARG, "bad gso run");
+    if (G->screen) return set_error(LKG_ERR_STATE, "the device GSO runs the plain GSO only");
+    if (steps == 0) return set_ok();
+    lkg_ctx* ctx = G->ctx;
+    cudaSetDevice(ctx->device);
+    const double t0 = now_s();
+    const int ns = (int)G->swarms.size(), ng = (int)G->group_complex.size();
+    std::vector<int> first(ns), cnt(ns), of, counts(ng, 0);
+    int n = 0, maxs = 0;
+    for (int s = 0; s < ns; ++s) {
+        first[s] = n;
+        cnt[s] = (int)G->swarms[s].g.size();
+        maxs = std::max(maxs, cnt[s]);
+        for (int k = 0; k < cnt[s]; ++k) of.push_back(s);
+        n += cnt[s];
+    }
+    for (int gi = 0; gi < ng; ++gi)
+        for (int s = G->group_first_swarm[gi]; s < G->group_first_swarm[gi] + G->group_nswarm[gi]; ++s)
+            counts[gi] += cnt[s];
+    if (n == 0) return set_ok();
+    // host state -> device
+    std::vector<double> a[10];
+    for (auto& v : a) v.resize(n);
+    std::vector<double> pose(7 * (size_t)n);
+    std::vector<uint32_t> keys(8 * (size_t)ns);
+    std::vector<unsigned long long> draws(ns);
+    for (int s = 0, i = 0; s < ns; ++s) {
+        const Swarm& sw = G->swarms[s];
+        for (int k = 0; k < 8; ++k) keys[8 * s + k] = sw.rng.key()[k];
+        draws[s] = sw.rng.words_used() / 2;
+        for (const Glow& gw : sw.g) {
+            a[0][i] = gw.t[0]; a[1][i] = gw.t[1]; a[2][i] = gw.t[2];
+            a[3][i] = gw.r.w; a[4][i] = gw.r.x; a[5][i] = gw.r.y; a[6][i] = gw.r.z;
+            a[7][i] = gw.luciferin; a[8][i] = gw.vision; a[9][i] = gw.scoring;
+            const double row[7] = {gw.r.w, gw.r.x, gw.r.y, gw.r.z, gw.t[0], gw.t[1], gw.t[2]};
+            std::memcpy(&pose[7 * (size_t)i], row, sizeof(row));
+            ++i;
+        }
+    }
+    cudaStream_t st = ctx->stream;
+    lkg::DBuf* b = G->dbuf;
+    for (int k = 0; k < 10; ++k) LKG_CK(b[k].reserve(n * sizeof(double)), "device gso");
+    for (int k = 10; k < 18; ++k) LKG_CK(b[k].reserve(n * sizeof(double)), "device gso");
+    LKG_CK(b[18].reserve(7 * (size_t)n * sizeof(double)), "device gso");
+    LKG_CK(b[19].reserve(2 * (size_t)n * sizeof(int)), "device gso");
+    LKG_CK(b[20].reserve((2 * (size_t)ns + n) * sizeof(int)), "device gso");
+    LKG_CK(b[21].reserve(keys.size() * sizeof(uint32_t)), "device gso");
+    LKG_CK(b[22].reserve(ns * sizeof(unsigned long long)), "device gso");
+    for (int k = 0; k < 10; ++k)
+        LKG_CK(cudaMemcpyAsync(b[k].p, a[k].data(), n * sizeof(double), cudaMemcpyHostToDevice, st), "device gso");
+    LKG_CK(cudaMemcpyAsync(b[18].p, pose.data(), pose.size() * sizeof(double), cudaMemcpyHostToDevice, st), "device gso");
+    std::vector<int> meta;
+    meta.insert(meta.end(), first.begin(), first.end());
+    meta.insert(meta.end(), cnt.begin(), cnt.end());
+    meta.insert(meta.end(), of.begin(), of.end());
+    LKG_CK(cudaMemcpyAsync(b[20].p, meta.data(), meta.size() * sizeof(int), cudaMemcpyHostToDevice, st), "device gso");
+    LKG_CK(cudaMemcpyAsync(b[21].p, keys.data(), keys.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, st),
+           "device gso");
+    LKG_CK(cudaMemcpyAsync(b[22].p, draws.data(), ns * sizeof(unsigned long long), cudaMemcpyHostToDevice, st),
+           "device gso");
+    lkg::GsoDevState& S = G->ds;
+    S.n = n; S.n_swarms = ns; S.max_swarm = maxs;
+    double* d[18];
+    for (int k = 0; k < 18; ++k) d[k] = b[k].as<double>();
+    S.tx = d[0]; S.ty = d[1]; S.tz = d[2]; S.qw = d[3]; S.qx = d[4]; S.qy = d[5]; S.qz = d[6];
+    S.luc = d[7]; S.vis = d[8]; S.score = d[9];
+    S.ntx = d[10]; S.nty = d[11]; S.ntz = d[12]; S.nqw = d[13]; S.nqx = d[14]; S.nqy = d[15]; S.nqz = d[16];
+    S.nvis = d[17];
+    S.poses = b[18].as<double>();
+    S.nid = b[19].as<int>(); S.nnb = S.nid + n;
+    S.swarm_first = b[20].as<int>(); S.swarm_n = S.swarm_first + ns; S.swarm_of = S.swarm_n + ns;
+    S.keys = b[21].as<uint32_t>();
+    S.draws = b[22].as<unsigned long long>();
+    int rc;
+    if (!G->dplan && (rc = lkg_plan_create(ctx, ng, G->group_complex.data(), counts.data(), &G->dplan))) return rc;
+    // first step eagerly (it also makes the plan's host-side queries)
+    if ((rc = lkg_plan_launch(G->dplan, S.poses, S.score, nullptr))) return rc;
+    LKG_CK(lkg::gso_dev_after_scoring(S, st), "device gso step");
+    if (steps > 1) {
+        if (G->dexec && std::memcmp(&G->ds_captured, &S, sizeof(S)) != 0) {
+            cudaGraphExecDestroy(G->dexec);
+            G->dexec = nullptr;
+        }
+        if (!G->dexec) {
+            LKG_CK(cudaStreamSynchronize(st), "device gso");
+            LKG_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "device gso capture");
+            rc = lkg_plan_launch(G->dplan, S.poses, S.score, nullptr);
+            const cudaError_t e1 = rc ? cudaSuccess : lkg::gso_dev_after_scoring(S, st);
+            cudaGraph_t graph = nullptr;
+            const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+            if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+            if (e1 != cudaSuccess || e2 != cudaSuccess) {
+                if (graph) cudaGraphDestroy(graph);
+                return set_error(cuda_to_status(e1 != cudaSuccess ? e1 : e2), "device gso capture failed");
+            }
+            const cudaError_t e3 = cudaGraphInstantiate(&G->dexec, graph, 0);
+            cudaGraphDestroy(graph);
+            if (e3 != cudaSuccess) return set_error(cuda_to_status(e3), "device gso graph: %s", cudaGetErrorString(e3));
+            G->ds_captured = S;
+        }
+        for (int k = 1; k < steps; ++k) LKG_CK(cudaGraphLaunch(G->dexec, st), "device gso step");
+    }
+    if ((rc = wait_stream(ctx, 300.0)) || (rc = check_status(ctx))) return rc;
+    // device -> host state
+    for (int k = 0; k < 10; ++k)
+        LKG_CK(cudaMemcpy(a[k].data(), b[k].p, n * sizeof(double), cudaMemcpyDeviceToHost), "device gso");
+    std::vector<int> nid(2 * (size_t)n);
+    LKG_CK(cudaMemcpy(nid.data(), b[19].p, nid.size() * sizeof(int), cudaMemcpyDeviceToHost), "device gso");
+    for (int s = 0, i = 0; s < ns; ++s) {
+        Swarm& sw = G->swarms[s];
+        for (size_t k = 0; k < sw.g.size(); ++k, ++i) {
+            Glow& gw = sw.g[k];
+            gw.t[0] = a[0][i]; gw.t[1] = a[1][i]; gw.t[2] = a[2][i];
+            gw.r = {a[3][i], a[4][i], a[5][i], a[6][i]};
+            gw.luciferin = a[7][i]; gw.vision = a[8][i]; gw.scoring = a[9][i];
+            gw.moved = nid[i] != (int)k;
+            gw.exact_next = gw.moved;
+            gw.nb.assign((size_t)nid[n + i], 0u);   // the count only (state reports it)
+            gw.step += (uint32_t)steps;
+        }
+        sw.rng.set_words_used(2 * (draws[s] + (unsigned long long)steps * sw.g.size()));
+    }
+    G->scored += (int64_t)steps * n;
+    G->step += steps;
+    G->t_exact += now_s() - t0;
+    return set_ok();
+}
 
 int lkg_gso_timing(lkg_gso* G, double* out) {
     if (!G || !out) return set_error(LKG_ERR_ARG, "bad timing arguments");

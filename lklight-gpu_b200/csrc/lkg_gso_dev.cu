@@ -1,0 +1,196 @@
+// Device-resident GSO step (plain GSO only): luciferin update, neighbour
+// selection and movement of every glowworm of every swarm on the GPU, so
+// that one whole GSO step (score, luciferin, select, move) is a sequence of
+// kernel launches that a CUDA graph replays.
+//
+// The arithmetic follows the host GSO (swarm.rs:96-174, glowworm.rs:84-166)
+// operation by operation and this file is compiled without FMA contraction,
+// so every f64 result matches the host's except the slerp: its acos / sin
+// come from the device math library instead of glibc, which can differ in
+// the last place; trajectories therefore agree closely for a few steps and
+// then drift apart as chaotic runs do.  The host GSO stays the parity mode.
+//
+// Random numbers: the swarm's StdRng stream (ChaCha20, 64-bit counter) is
+// counter-based, so draw i of swarm s is computed directly from block i / 8
+// of the swarm's keystream (words 2i, 2i + 1: every GSO draw is a 64-bit
+// draw, so draws never straddle a word pair).
+#include <algorithm>
+#include <cstdint>
+
+#include "lkg_gso_dev.h"
+
+namespace lkg {
+namespace {
+
+constexpr double RHO = 0.5, GAMMA = 0.4, BETA = 0.08, MAX_VISION = 5.0;
+constexpr int MAX_NEIGHBORS = 5;
+
+__device__ __forceinline__ uint32_t rotl32(uint32_t v, int c) { return (v << c) | (v >> (32 - c)); }
+
+// draw `i` of the stream with key k (gen::<f64>: top 53 bits of the u64
+// whose low word comes first)
+__device__ double chacha_f64(const uint32_t* __restrict__ k, unsigned long long i) {
+    const unsigned long long blk = i >> 3;
+    uint32_t s[16] = {0x61707865u, 0x3320646eu, 0x79622d32u, 0x6b206574u, k[0], k[1], k[2], k[3],
+                      k[4], k[5], k[6], k[7], (uint32_t)blk, (uint32_t)(blk >> 32), 0u, 0u};
+    uint32_t x[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) x[j] = s[j];
+#define QR(a, b, c, d)                              \
+    x[a] += x[b]; x[d] = rotl32(x[d] ^ x[a], 16);   \
+    x[c] += x[d]; x[b] = rotl32(x[b] ^ x[c], 12);   \
+    x[a] += x[b]; x[d] = rotl32(x[d] ^ x[a], 8);    \
+    x[c] += x[d]; x[b] = rotl32(x[b] ^ x[c], 7);
+    for (int r = 0; r < 10; ++r) {
+        QR(0, 4, 8, 12) QR(1, 5, 9, 13) QR(2, 6, 10, 14) QR(3, 7, 11, 15)
+        QR(0, 5, 10, 15) QR(1, 6, 11, 12) QR(2, 7, 8, 13) QR(3, 4, 9, 14)
+    }
+#undef QR
+    const int w = (int)(i & 7) * 2;
+    uint32_t lo = 0, hi = 0;
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        if (j == w) lo = x[j] + s[j];
+        if (j == w + 1) hi = x[j] + s[j];
+    }
+    const unsigned long long v = ((unsigned long long)hi << 32) | lo;
+    return (double)(v >> 11) * (1.0 / 9007199254740992.0);
+}
+
+// luciferin update with this step's scores (swarm.rs:96-99)
+__global__ void k_gso_luciferin(GsoDevState S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n) return;
+    S.luc[i] = (1.0 - RHO) * S.luc[i] + GAMMA * S.score[i];
+}
+
+// neighbours (brighter, within the vision range, in id order) and the
+// roulette selection with the glowworm's draw (glowworm.rs:114-142); grid:
+// (swarms, ceil(max swarm size / blockDim))
+__global__ void k_gso_select(GsoDevState S) {
+    __shared__ double sx[256], sy[256], sz[256], sl[256];
+    const int sw = blockIdx.x;
+    const int first = S.swarm_first[sw], n = S.swarm_n[sw];
+    const int li = blockIdx.y * blockDim.x + threadIdx.x;
+    const bool act = li < n;
+    const int i = first + (act ? li : 0);
+    const double x = S.tx[i], y = S.ty[i], z = S.tz[i], l1 = S.luc[i], v = S.vis[i];
+    const double vr2 = v * v;
+    int cnt = 0;
+    double total = 0.0;
+    // pass 1: count and total of the luciferin differences, id order
+    for (int j0 = 0; j0 < n; j0 += blockDim.x) {
+        __syncthreads();
+        if (j0 + (int)threadIdx.x < n) {
+            const int j = first + j0 + threadIdx.x;
+            sx[threadIdx.x] = S.tx[j]; sy[threadIdx.x] = S.ty[j]; sz[threadIdx.x] = S.tz[j]; sl[threadIdx.x] = S.luc[j];
+        }
+        __syncthreads();
+        const int m = min((int)blockDim.x, n - j0);
+        for (int jj = 0; jj < m; ++jj) {
+            const double dx = x - sx[jj], dy = y - sy[jj], dz = z - sz[jj];
+            if (act && j0 + jj != li && l1 < sl[jj] && dx * dx + dy * dy + dz * dz < vr2) {
+                ++cnt;
+                total += sl[jj] - l1;
+            }
+        }
+    }
+    // pass 2: roulette over prob_k = (l_k - l_i) / total in id order
+    const double u = act ? chacha_f64(S.keys + 8 * sw, S.draws[sw] + (unsigned long long)li) : 0.0;
+    double sum = 0.0;
+    int sel = -1, firstnb = -1;
+    bool stop = false;
+    for (int j0 = 0; j0 < n; j0 += blockDim.x) {   // block-uniform bounds: barriers inside
+        __syncthreads();
+        if (j0 + (int)threadIdx.x < n) {
+            const int j = first + j0 + threadIdx.x;
+            sx[threadIdx.x] = S.tx[j]; sy[threadIdx.x] = S.ty[j]; sz[threadIdx.x] = S.tz[j]; sl[threadIdx.x] = S.luc[j];
+        }
+        __syncthreads();
+        const int m = min((int)blockDim.x, n - j0);
+        for (int jj = 0; jj < m; ++jj) {
+            const double dx = x - sx[jj], dy = y - sy[jj], dz = z - sz[jj];
+            if (act && j0 + jj != li && l1 < sl[jj] && dx * dx + dy * dy + dz * dz < vr2) {
+                if (firstnb < 0) firstnb = j0 + jj;
+                if (!stop) {
+                    if (sum < u) { sum += (sl[jj] - l1) / total; sel = j0 + jj; }
+                    else stop = true;
+                }
+            }
+        }
+    }
+    if (act) {
+        S.nid[i] = cnt == 0 ? li : (sel >= 0 ? sel : firstnb);
+        S.nnb[i] = cnt;
+    }
+}
+
+__device__ __forceinline__ void qnorm(double& w, double& x, double& y, double& z) {   // qt.rs:36-46
+    const double n = sqrt(w * w + x * x + y * y + z * z);
+    w /= n; x /= n; y /= n; z /= n;
+}
+
+// movement towards the selected neighbour and vision update
+// (glowworm.rs:144-166, qt.rs:80-104); reads the step's starting state,
+// writes the new one into the second buffer
+__global__ void k_gso_move(GsoDevState S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n) return;
+    const int sw = S.swarm_of[i];
+    const int nid = S.swarm_first[sw] + S.nid[i];
+    double tx = S.tx[i], ty = S.ty[i], tz = S.tz[i];
+    double w = S.qw[i], x = S.qx[i], y = S.qy[i], z = S.qz[i];
+    if (nid != i) {
+        const double dx = S.tx[nid] - tx, dy = S.ty[nid] - ty, dz = S.tz[nid] - tz;
+        const double norm = sqrt(dx * dx + dy * dy + dz * dz);
+        const double coef = 0.5 / norm;
+        tx += dx * coef; ty += dy * coef; tz += dz * coef;
+        double w2 = S.qw[nid], x2 = S.qx[nid], y2 = S.qy[nid], z2 = S.qz[nid];
+        qnorm(w, x, y, z);
+        qnorm(w2, x2, y2, z2);
+        double dot = w * w2 + x * x2 + y * y2 + z * z2;
+        if (dot < 0.0) { w = -w; x = -x; y = -y; z = -z; dot *= -1.0; }
+        if (dot > 0.9995) {
+            w = w + (w2 - w) * 0.5; x = x + (x2 - x) * 0.5; y = y + (y2 - y) * 0.5; z = z + (z2 - z) * 0.5;
+            qnorm(w, x, y, z);
+        } else {
+            dot = fmax(fmin(dot, 1.0), -1.0);
+            const double omega = acos(dot), so = sin(omega);
+            const double a = sin((1.0 - 0.5) * omega) / so, b = sin(0.5 * omega) / so;
+            w = w * a + w2 * b; x = x * a + x2 * b; y = y * a + y2 * b; z = z * a + z2 * b;
+        }
+        qnorm(w, x, y, z);
+    }
+    const double v = S.vis[i] + BETA * (double)(MAX_NEIGHBORS - S.nnb[i]);
+    S.ntx[i] = tx; S.nty[i] = ty; S.ntz[i] = tz;
+    S.nqw[i] = w; S.nqx[i] = x; S.nqy[i] = y; S.nqz[i] = z;
+    S.nvis[i] = fmin(MAX_VISION, fmax(0.0, v));
+}
+
+// the new state becomes current; scorer poses (w, x, y, z, tx, ty, tz);
+// each swarm's draw counter advances by its size
+__global__ void k_gso_commit(GsoDevState S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < S.n_swarms) S.draws[i] += (unsigned long long)S.swarm_n[i];
+    if (i >= S.n) return;
+    S.tx[i] = S.ntx[i]; S.ty[i] = S.nty[i]; S.tz[i] = S.ntz[i];
+    S.qw[i] = S.nqw[i]; S.qx[i] = S.nqx[i]; S.qy[i] = S.nqy[i]; S.qz[i] = S.nqz[i];
+    S.vis[i] = S.nvis[i];
+    double* p = S.poses + 7 * (size_t)i;
+    p[0] = S.qw[i]; p[1] = S.qx[i]; p[2] = S.qy[i]; p[3] = S.qz[i];
+    p[4] = S.tx[i]; p[5] = S.ty[i]; p[6] = S.tz[i];
+}
+
+}  // namespace
+
+cudaError_t gso_dev_after_scoring(const GsoDevState& S, cudaStream_t s) {
+    const int t = 256, b = (S.n + t - 1) / t;
+    k_gso_luciferin<<<b, t, 0, s>>>(S);
+    dim3 g(S.n_swarms, (S.max_swarm + 255) / 256);
+    k_gso_select<<<g, 256, 0, s>>>(S);
+    k_gso_move<<<b, t, 0, s>>>(S);
+    k_gso_commit<<<(std::max(S.n, S.n_swarms) + t - 1) / t, t, 0, s>>>(S);
+    return cudaGetLastError();
+}
+
+}  // namespace lkg

@@ -42,6 +42,21 @@ class StdRng {
 
     double gen_f64() { return (double)(next_u64() >> 11) * (1.0 / 9007199254740992.0); }
 
+    // position in the keystream, in 32-bit words consumed since seeding
+    // (the device GSO draws word pairs 2i, 2i + 1 for draw i directly)
+    uint64_t words_used() const { return idx_ >= 64 ? ctr_ * 16 : (ctr_ - 4) * 16 + (uint64_t)idx_; }
+    void set_words_used(uint64_t w) {
+        if (w % 64 == 0) {
+            ctr_ = w / 16;
+            idx_ = 64;
+        } else {
+            ctr_ = (w / 64) * 4;
+            refill();
+            idx_ = (int)(w % 64);
+        }
+    }
+    const uint32_t* key() const { return key_; }
+
   private:
     static uint32_t rotl(uint32_t v, int c) { return (v << c) | (v >> (32 - c)); }
 
