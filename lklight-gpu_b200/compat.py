@@ -65,8 +65,10 @@ def pack_poses(translations, rotations):
     return np.ascontiguousarray(np.hstack([q, t]))
 
 
-def batch_raw(field, rec, lig, poses, flags):
-    """cuda_batch_score: returns N x 2 (raw electrostatics, LJ[+clash])."""
+def batch_raw(field, rec, lig, poses, flags, library=None):
+    """cuda_batch_score: returns N x 2 (raw electrostatics, LJ[+clash]).
+    ``library``: another ctypes library exporting the same symbol (the
+    reference's own kernels, in tests); liblkg by default."""
     poses = np.ascontiguousarray(poses, np.float64).reshape(-1, 7)
     n = len(poses)
     out = np.zeros(2 * n)
@@ -78,13 +80,16 @@ def batch_raw(field, rec, lig, poses, flags):
         sp = float(field["spacing"])
     else:
         phi, nx, ny, nz, ox, oy, oz, sp = dummy, 0, 0, 0, 0.0, 0.0, 0.0, 0.0
-    r = lib().cuda_batch_score(ptr(phi), nx, ny, nz, ox, oy, oz, sp,
+    L = library if library is not None else lib()
+    r = L.cuda_batch_score(ptr(phi), nx, ny, nz, ox, oy, oz, sp,
                                ptr(rec.r_coords), ptr(rec.r_ele), ptr(rec.r_svdw), ptr(rec.r_vdwr),
                                ptr(rec.r_heavy), rec.nr, ptr(rec.cell_start), ptr(rec.cell_atoms),
                                rec.ncx, rec.ncy, rec.ncz, rec.c_o[0], rec.c_o[1], rec.c_o[2], rec.c_sp,
                                ptr(lig.base), ptr(poses), ptr(lig.ele), ptr(lig.svdw), ptr(lig.vdw),
                                ptr(lig.heavy), lig.nl, n, flags, ptr(out))
     if r != 0:
+        if library is not None:
+            raise RuntimeError("cuda_batch_score returned %d" % r)
         raise LkgError(lib().lkg_last_status(), lib().lkg_last_error().decode())
     return out.reshape(n, 2)
 

@@ -1,0 +1,65 @@
+"""The reference's own CUDA scorer (src/cuda/full_score.cu, compiled
+unmodified for sm_100a into oracle/_ref by oracle/Makefile) against liblkg's
+compatible entry point, on the same packed inputs.
+
+Both compute the pair terms in f32 and sum differently, so they agree within
+the 1e-5 relative budget of the fast path, not bit for bit; the near-pair
+work is the same.  The test also times both for the record (printed).
+Calls keep N constant: the reference caches its output buffer at the size of
+its first call.
+"""
+import ctypes as C
+import os
+import time
+
+import numpy as np
+import pytest
+
+from tests.lkg_helpers import compat, config0, lkg, rel_err, synth
+
+pytestmark = pytest.mark.gpu
+
+REF = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "libref_cuda.so")
+
+
+@pytest.fixture(scope="module")
+def reflib():
+    if not os.path.exists(REF):
+        pytest.skip("reference kernels not built (oracle/Makefile ref needs the reference tree)")
+    L = C.CDLL(REF)
+    ours = lkg.lib().cuda_batch_score
+    L.cuda_batch_score.argtypes = ours.argtypes
+    L.cuda_batch_score.restype = ours.restype
+    return L
+
+
+def test_reference_kernel_and_liblkg_agree_on_config0(reflib):
+    c0 = config0()
+    rec, lig = c0["rec"], c0["lig"]
+    crec = compat.CudaReceptor(rec["coords"], rec["ele"], np.sqrt(rec["vdw"]), rec["radius"], rec["heavy"])
+    clig = compat.CudaLigand(lig["coords"], lig["ele"], np.sqrt(lig["vdw"]), lig["radius"], lig["heavy"])
+    field = lkg.field_build(rec["coords"], rec["ele"])
+    pos = synth.to_kernel_poses(synth.setup_poses(rec["coords"], 20, 300, 42))   # 6000 poses
+    flags = 7
+    raw_ref = compat.batch_raw(field, crec, clig, pos, flags, library=reflib)
+    raw_lkg = compat.batch_raw(field, crec, clig, pos, flags)
+    s_ref = -(raw_ref[:, 0] * 83.0 + raw_ref[:, 1])
+    s_lkg = -(raw_lkg[:, 0] * 83.0 + raw_lkg[:, 1])
+    assert rel_err(s_lkg, s_ref).max() < 1e-5
+    # and both against the oracle (the reference's CPU grid path)
+    import oracle
+    ora = oracle.Model("dna", rec, lig).batch_energy_grid(pos[:200])
+    print("max rel vs oracle: reference kernel %.2e, liblkg %.2e" % (rel_err(s_ref[:200], ora).max(),
+                                                                      rel_err(s_lkg[:200], ora).max()))
+    assert rel_err(s_lkg[:200], ora).max() < 1e-5
+    t = {}
+    for name, L in (("reference", reflib), ("liblkg", None)):
+        compat.batch_raw(field, crec, clig, pos, flags, library=L)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            compat.batch_raw(field, crec, clig, pos, flags, library=L)
+        t[name] = (time.perf_counter() - t0) / 3
+    print("cuda_batch_score, 6000 poses of the config-0 complex (host buffers, per call): reference %.2f ms "
+          "(%.0f poses/s), liblkg %.2f ms (%.0f poses/s), ratio %.1fx" % (
+              t["reference"] * 1e3, len(pos) / t["reference"], t["liblkg"] * 1e3, len(pos) / t["liblkg"],
+              t["reference"] / t["liblkg"]))
