@@ -644,6 +644,7 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
     std::vector<double> pose(7 * (size_t)n);
     std::vector<uint32_t> keys(8 * (size_t)ns);
     std::vector<unsigned long long> draws(ns);
+    std::vector<unsigned char> mask(n + 64, 0);   // the counter after the mask starts at zero
     for (int s = 0, i = 0; s < ns; ++s) {
         const Swarm& sw = G->swarms[s];
         for (int k = 0; k < 8; ++k) keys[8 * s + k] = sw.rng.key()[k];
@@ -654,6 +655,7 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
             a[7][i] = gw.luciferin; a[8][i] = gw.vision; a[9][i] = gw.scoring;
             const double row[7] = {gw.r.w, gw.r.x, gw.r.y, gw.r.z, gw.t[0], gw.t[1], gw.t[2]};
             std::memcpy(&pose[7 * (size_t)i], row, sizeof(row));
+            mask[i] = (gw.moved || gw.step == 0) ? 1 : 0;   // swarm.rs:79-85
             ++i;
         }
     }
@@ -666,6 +668,7 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
     LKG_CK(b[20].reserve((2 * (size_t)ns + n) * sizeof(int)), "device gso");
     LKG_CK(b[21].reserve(keys.size() * sizeof(uint32_t)), "device gso");
     LKG_CK(b[22].reserve(ns * sizeof(unsigned long long)), "device gso");
+    LKG_CK(b[23].reserve(n + 64), "device gso");   // mask bytes, then the scored counter (8-aligned)
     for (int k = 0; k < 10; ++k)
         LKG_CK(cudaMemcpyAsync(b[k].p, a[k].data(), n * sizeof(double), cudaMemcpyHostToDevice, st), "device gso");
     LKG_CK(cudaMemcpyAsync(b[18].p, pose.data(), pose.size() * sizeof(double), cudaMemcpyHostToDevice, st), "device gso");
@@ -678,6 +681,7 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
            "device gso");
     LKG_CK(cudaMemcpyAsync(b[22].p, draws.data(), ns * sizeof(unsigned long long), cudaMemcpyHostToDevice, st),
            "device gso");
+    LKG_CK(cudaMemcpyAsync(b[23].p, mask.data(), mask.size(), cudaMemcpyHostToDevice, st), "device gso");
     lkg::GsoDevState& S = G->ds;
     S.n = n; S.n_swarms = ns; S.max_swarm = maxs;
     double* d[18];
@@ -691,10 +695,12 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
     S.swarm_first = b[20].as<int>(); S.swarm_n = S.swarm_first + ns; S.swarm_of = S.swarm_n + ns;
     S.keys = b[21].as<uint32_t>();
     S.draws = b[22].as<unsigned long long>();
+    S.mask = b[23].as<unsigned char>();
+    S.nscored = reinterpret_cast<unsigned long long*>(b[23].as<unsigned char>() + ((n + 7) & ~7));
     int rc;
     if (!G->dplan && (rc = lkg_plan_create(ctx, ng, G->group_complex.data(), counts.data(), &G->dplan))) return rc;
     // first step eagerly (it also makes the plan's host-side queries)
-    if ((rc = lkg_plan_launch(G->dplan, S.poses, S.score, nullptr))) return rc;
+    if ((rc = lkg::plan_launch_masked(G->dplan, S.poses, S.score, S.mask))) return rc;
     LKG_CK(lkg::gso_dev_after_scoring(S, st), "device gso step");
     if (steps > 1) {
         if (G->dexec && std::memcmp(&G->ds_captured, &S, sizeof(S)) != 0) {
@@ -704,7 +710,7 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
         if (!G->dexec) {
             LKG_CK(cudaStreamSynchronize(st), "device gso");
             LKG_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "device gso capture");
-            rc = lkg_plan_launch(G->dplan, S.poses, S.score, nullptr);
+            rc = lkg::plan_launch_masked(G->dplan, S.poses, S.score, S.mask);
             const cudaError_t e1 = rc ? cudaSuccess : lkg::gso_dev_after_scoring(S, st);
             cudaGraph_t graph = nullptr;
             const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
@@ -740,7 +746,9 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
         }
         sw.rng.set_words_used(2 * (draws[s] + (unsigned long long)steps * sw.g.size()));
     }
-    G->scored += (int64_t)steps * n;
+    unsigned long long nsc = 0;
+    LKG_CK(cudaMemcpy(&nsc, S.nscored, sizeof(nsc), cudaMemcpyDeviceToHost), "device gso");
+    G->scored += (int64_t)nsc;
     G->step += steps;
     G->t_exact += now_s() - t0;
     return set_ok();

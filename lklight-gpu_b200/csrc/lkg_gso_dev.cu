@@ -57,9 +57,13 @@ __device__ double chacha_f64(const uint32_t* __restrict__ k, unsigned long long 
     return (double)(v >> 11) * (1.0 / 9007199254740992.0);
 }
 
-// luciferin update with this step's scores (swarm.rs:96-99)
+// luciferin update with this step's scores (swarm.rs:96-99); unmoved
+// glowworms were not rescored and keep their score (swarm.rs:79-85)
 __global__ void k_gso_luciferin(GsoDevState S) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool scored = i < S.n && S.mask[i];
+    const unsigned b = __ballot_sync(0xffffffffu, scored);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(S.nscored, (unsigned long long)__popc(b));
     if (i >= S.n) return;
     S.luc[i] = (1.0 - RHO) * S.luc[i] + GAMMA * S.score[i];
 }
@@ -165,6 +169,7 @@ __global__ void k_gso_move(GsoDevState S) {
     S.ntx[i] = tx; S.nty[i] = ty; S.ntz[i] = tz;
     S.nqw[i] = w; S.nqx[i] = x; S.nqy[i] = y; S.nqz[i] = z;
     S.nvis[i] = fmin(MAX_VISION, fmax(0.0, v));
+    S.mask[i] = nid != i;   // the next step scores the moved glowworms
 }
 
 // the new state becomes current; scorer poses (w, x, y, z, tx, ty, tz);
@@ -184,7 +189,7 @@ __global__ void k_gso_commit(GsoDevState S) {
 }  // namespace
 
 cudaError_t gso_dev_after_scoring(const GsoDevState& S, cudaStream_t s) {
-    const int t = 256, b = (S.n + t - 1) / t;
+    const int t = 256, b = (S.n + t - 1) / t;   // full warps: the ballot in k_gso_luciferin
     k_gso_luciferin<<<b, t, 0, s>>>(S);
     dim3 g(S.n_swarms, (S.max_swarm + 255) / 256);
     k_gso_select<<<g, 256, 0, s>>>(S);

@@ -16,6 +16,8 @@ struct GsoDevState {
     const int *swarm_first, *swarm_n, *swarm_of;
     const uint32_t* keys;          // 8 ChaCha key words per swarm
     unsigned long long* draws;     // 64-bit draws consumed per swarm
+    unsigned char* mask;           // 1: pose to score this step (moved, or never scored)
+    unsigned long long* nscored;   // poses scored so far
 };
 
 // luciferin update, selection, movement and commit of one step, given the

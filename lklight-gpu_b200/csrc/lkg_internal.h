@@ -86,6 +86,9 @@ struct LaunchParams {
     // per-atom outputs (cuda_full_score): pose 0 of item 0, caller atom order
     float* atom_elec;
     float* atom_vdw;
+    // optional [N]: poses whose byte is 0 are skipped (their score and parts
+    // keep their previous values: the device GSO's unmoved glowworms)
+    const unsigned char* pose_mask;
 };
 
 constexpr double FACTOR = 332.0;

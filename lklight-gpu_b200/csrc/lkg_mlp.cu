@@ -211,7 +211,7 @@ __global__ void k_loss(const float* __restrict__ y, const float* __restrict__ t,
 __global__ void k_colsum(const __nv_bfloat16* __restrict__ dC, int n, float* __restrict__ gb) {
     const int col = blockIdx.x * blockDim.x + threadIdx.x;
     if (col >= H) return;
-    const int r0 = blockIdx.y * 256, r1 = min(n, r0 + 256);
+    const int r0 = blockIdx.y * 32, r1 = min(n, r0 + 32);
     float s = 0.f;
     for (int r = r0; r < r1; ++r) s += __bfloat162float(dC[(size_t)r * H + col]);
     atomicAdd(gb + col, s);
@@ -351,7 +351,10 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
     k_loss<<<(n + 7) / 8, 256, 0, s>>>(S->y.as<float>(), S->t.as<float>(), S->H3.as<__nv_bfloat16>(), n, P(S, 6),
                                        S->dH3.as<__nv_bfloat16>(), Gd(S, 6), Gd(S, 7), S->loss.as<float>());
     LKG_CK(cudaGetLastError(), "mlp loss");
-    const int splits = std::max(1, std::min(64, n / 512));
+    // weight gradients reduce over the batch: split it so that the 16 output
+    // tiles of a layer still fill the GPU (split-K partial sums meet in FP32
+    // atomics)
+    const int splits = std::max(1, std::min(64, n / 64));
     const __nv_bfloat16* acts[3] = {S->H1.as<__nv_bfloat16>(), S->H2.as<__nv_bfloat16>(), S->H3.as<__nv_bfloat16>()};
     __nv_bfloat16* dacts[3] = {S->dH1.as<__nv_bfloat16>(), S->dH2.as<__nv_bfloat16>(), S->dH3.as<__nv_bfloat16>()};
     for (int L = 2; L >= 0; --L) {
@@ -360,7 +363,7 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
         // dW_L[o][i] = sum_n dC[n][o] * A_in[n][i]   (A = dC^T, B = A_in^T)
         LKG_CK((gemm<true, true, EPI_WGRAD>(s, H, kin, n, dacts[L], H, ain, kin, Gd(S, 2 * L), nullptr, kin, nullptr,
                                             nullptr, splits)), "mlp wgrad");
-        dim3 cg((H + 255) / 256, (n + 255) / 256);
+        dim3 cg((H + 255) / 256, (n + 31) / 32);
         k_colsum<<<cg, 256, 0, s>>>(dacts[L], n, Gd(S, 2 * L + 1));
         LKG_CK(cudaGetLastError(), "mlp bias grad");
         if (L > 0) {

@@ -388,7 +388,8 @@ int build_groups(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, G
 }
 
 int launch_group(lkg_ctx* ctx, const Group& G, const char* db, Scratch& sc, const double* d_poses,
-                 double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e, float* atom_v) {
+                 double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e, float* atom_v,
+                 const unsigned char* pose_mask) {
     const bool exact = ctx->precision == LKG_PREC_EXACT;
     const int ni = (int)G.ic.size();
     LaunchParams p{};
@@ -413,6 +414,7 @@ int launch_group(lkg_ctx* ctx, const Group& G, const char* db, Scratch& sc, cons
     p.max_tiles = 0;
     p.atom_elec = atom_e;
     p.atom_vdw = atom_v;
+    p.pose_mask = pose_mask;
     cudaError_t e;
     if (G.kind == 0) {
         int threads = ctx->tile;
@@ -845,6 +847,23 @@ int lkg_plan_launch(lkg_plan* P, const double* d_poses, double* d_scores, double
     }
     return set_ok();
 }
+
+}  // extern "C"
+
+namespace lkg {
+int plan_launch_masked(lkg_plan* P, const double* d_poses, double* d_scores, const unsigned char* d_mask) {
+    if (!P || !d_poses || !d_scores) return set_error(LKG_ERR_ARG, "bad plan launch");
+    for (int k = 0; k < 2; ++k) {
+        if (P->g[k].ic.empty()) continue;
+        int st = launch_group(P->ctx, P->g[k], P->d_tables.as<char>() + (k ? P->b0 : 0), P->scratch, d_poses,
+                              d_scores, nullptr, 0, 0, nullptr, nullptr, d_mask);
+        if (st) return st;
+    }
+    return set_ok();
+}
+}  // namespace lkg
+
+extern "C" {
 
 int lkg_plan_capture(lkg_plan* P, const double* d_poses, double* d_scores, double* d_parts, int n_launches) {
     if (!P || n_launches <= 0) return set_error(LKG_ERR_ARG, "bad capture");

@@ -155,6 +155,9 @@ int build_groups(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, G
 int sync_descriptors(lkg_ctx* ctx);
 // launch one prepared group (kernel launches only: stream-capturable)
 int launch_group(lkg_ctx* ctx, const Group& g, const char* d_tables, Scratch& sc, const double* d_poses,
-                 double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e, float* atom_v);
+                 double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e, float* atom_v,
+                 const unsigned char* pose_mask = nullptr);
+// a plan's launch group(s) scoring only the poses whose mask byte is set
+int plan_launch_masked(lkg_plan* plan, const double* d_poses, double* d_scores, const unsigned char* d_mask);
 void field_geometry(const double* coords, int n, double lo[3], int dims[3], double* spacing);
 }  // namespace lkg

@@ -441,6 +441,7 @@ __global__ void __launch_bounds__(256) k_score_tiles(LaunchParams p) {
         const long long local = w - __ldg(p.item_work0 + b);
         const int pose = (int)(local / c.ntiles), tile = (int)(local % c.ntiles);
         const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
+        if (p.pose_mask && !p.pose_mask[g]) continue;   // block-uniform: pose skipped
         const int j = tile * p.tile + threadIdx.x;
         AtomAcc acc{0.0, 0.0, 0};
         if (j < c.nl && threadIdx.x < p.tile) {
@@ -492,6 +493,7 @@ __global__ void __launch_bounds__(512) k_score_desolv(LaunchParams p) {
         const ComplexDev& c = p.cx[__ldg(p.item_complex + b)];
         const int pose = (int)(w - __ldg(p.item_work0 + b));
         const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
+        if (p.pose_mask && !p.pose_mask[g]) continue;   // block-uniform: pose skipped
         MinHash hash;
         hash.init(smem, c.hcap);
         __syncthreads();

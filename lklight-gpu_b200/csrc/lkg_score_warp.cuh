@@ -312,6 +312,7 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
         const int ntiles = c.ntiles;
         const int pose = (int)(local / ntiles), tile = (int)(local % ntiles);
         const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
+        if (p.pose_mask && !p.pose_mask[g]) continue;   // pose skipped: keeps its score
         __syncwarp();   // readers of the previous unit's pose are done
         if (lane == 0) W.rot = pose_matrix(p.poses + 7 * g);
         __syncwarp();
@@ -372,6 +373,7 @@ __global__ void __launch_bounds__(WD_THREADS, 1) k_score_warp_desolv(LaunchParam
         const ComplexDev& c = p.cx[__ldg(p.item_complex + b)];
         const int pose = (int)(w - __ldg(p.item_work0 + b));
         const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
+        if (p.pose_mask && !p.pose_mask[g]) continue;   // block-uniform: pose skipped
         MinHash hash;
         hash.init(reinterpret_cast<char*>(wd_smem_raw), c.hcap);
         unsigned char* base = wd_smem_raw + (size_t)c.hcap * 12;
