@@ -2,9 +2,10 @@
 unmodified for sm_100a into oracle/_ref by oracle/Makefile) against liblkg's
 compatible entry point, on the same packed inputs.
 
-Both compute the pair terms in f32 and sum differently, so they agree within
-the 1e-5 relative budget of the fast path, not bit for bit; the near-pair
-work is the same.  The test also times both for the record (printed).
+Both compute the pair terms in f32; liblkg sums in f64 and stays within the
+1e-5 relative budget of the oracle, the reference kernel's f32 block sums
+drift further (both errors are printed).  The test also times both for the
+record (printed).
 Calls keep N constant: the reference caches its output buffer at the size of
 its first call.
 """
@@ -45,13 +46,18 @@ def test_reference_kernel_and_liblkg_agree_on_config0(reflib):
     raw_lkg = compat.batch_raw(field, crec, clig, pos, flags)
     s_ref = -(raw_ref[:, 0] * 83.0 + raw_ref[:, 1])
     s_lkg = -(raw_lkg[:, 0] * 83.0 + raw_lkg[:, 1])
-    assert rel_err(s_lkg, s_ref).max() < 1e-5
-    # and both against the oracle (the reference's CPU grid path)
+    # the reference kernel sums in f32 per thread and block (full_score.cu
+    # :296-335): it drifts from the exact energy further than liblkg does.
+    # Judge both against the oracle (the reference's CPU grid path) on the
+    # poses where they disagree most, plus a plain sample
     import oracle
-    ora = oracle.Model("dna", rec, lig).batch_energy_grid(pos[:200])
-    print("max rel vs oracle: reference kernel %.2e, liblkg %.2e" % (rel_err(s_ref[:200], ora).max(),
-                                                                      rel_err(s_lkg[:200], ora).max()))
-    assert rel_err(s_lkg[:200], ora).max() < 1e-5
+    worst = np.argsort(-rel_err(s_lkg, s_ref))[:100]
+    pick = np.unique(np.concatenate([worst, np.arange(0, len(pos), 60)]))
+    ora = oracle.Model("dna", rec, lig).batch_energy_grid(pos[pick])
+    e_ref, e_lkg = rel_err(s_ref[pick], ora).max(), rel_err(s_lkg[pick], ora).max()
+    print("max rel vs oracle on %d poses: reference kernel %.2e, liblkg %.2e" % (len(pick), e_ref, e_lkg))
+    assert e_lkg < 1e-5
+    assert e_lkg <= e_ref
     t = {}
     for name, L in (("reference", reflib), ("liblkg", None)):
         compat.batch_raw(field, crec, clig, pos, flags, library=L)
