@@ -382,14 +382,14 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
     cid = ctx.add_complex("dna", c0["rec"], c0["lig"])
     pos = synth.setup_poses(c0["rec"]["coords"], swarms, glow, 3)
     res = {}
-    for mode in ("plain", "screened", "ablation"):
+    for mode in ("plain", "device", "screened", "ablation"):
         g = lkg.GSO(ctx, [(cid, swarms, glow)], pos, [3])
-        if mode != "plain":
+        if mode in ("screened", "ablation"):
             g.set_screen(candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=20,
                          finetune_epochs=2, lr=1e-3, seed=3, random_rank=(mode == "ablation"), batch=1024)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        g.run(steps)
+        g.run(steps, device=(mode == "device"))
         g.finalize()
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
@@ -412,6 +412,10 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
                        "candidates": 4, "exact_fraction": 0.25, "rescore_every": 10, "train_steps": 20},
             "plain": {"seconds": res["plain"]["seconds"], "exact_evals": res["plain"]["scored"],
                       "mean_best_score": best["plain"], "phases_s": res["plain"]["phases"]},
+            "plain_device_gso": {"seconds": res["device"]["seconds"], "exact_evals": res["device"]["scored"],
+                                 "mean_best_score": best["device"], "speedup_over_host_gso":
+                                 res["plain"]["seconds"] / res["device"]["seconds"],
+                                 "what": "the plain GSO with whole steps on the device (graph replays)"},
             "screened": {"seconds": res["screened"]["seconds"], "exact_evals": res["screened"]["scored"],
                          "surrogate_evals": res["screened"]["predicted"], "mean_best_score": best["screened"],
                          "top5_overlap_with_plain": ov["screened"], "phases_s": res["screened"]["phases"]},
