@@ -91,7 +91,7 @@ def lib():
         "lkg_gso_create": (I, [P, I, P, P, P, P, P, P]), "lkg_gso_run": (I, [P, I]),
         "lkg_gso_state": (I, [P, P, P, P, P, P, P]), "lkg_gso_scored": (I64, [P]),
         "lkg_gso_destroy": (I, [P]), "lkg_compat_cache_clear": (None, []),
-        "lkg_gso_set_screen": (I, [P, P]), "lkg_gso_finalize": (I, [P]), "lkg_gso_predicted": (I64, [P]), "lkg_gso_timing": (I, [P, P]), "lkg_gso_run_device": (I, [P, I]),
+        "lkg_gso_set_screen": (I, [P, P]), "lkg_gso_finalize": (I, [P]), "lkg_gso_predicted": (I64, [P]), "lkg_gso_timing": (I, [P, P]), "lkg_surrogate_set_backend": (I, [P, I]), "lkg_surrogate_status": (I, [P, P]), "lkg_gso_run_device": (I, [P, I]),
         "cuda_batch_score": (I, [P, I, I, I, F, F, F, F, P, P, P, P, P, I, P, P, I, I, I, F, F, F, F,
                                  P, P, P, P, P, P, I, I, C.c_uint, P]),
         "cuda_cpydock_solv": (I, [P, P, I, P, P, I, I, I, F, F, F, F, P, P, P, P, I, I, P, P, P, P, P]),
@@ -332,6 +332,15 @@ class Surrogate:
         y, g, l = np.zeros(n, np.float32), np.zeros(self.nparams(), np.float32), C.c_float()
         _check(lib().lkg_surrogate_grad(self.h, n, ptr(f), ptr(t), ptr(y), ptr(g), C.byref(l)))
         return y, g, l.value
+
+    def set_backend(self, tcgen05):
+        """Forward layers on tcgen05 (True) or mma.sync (False)."""
+        _check(lib().lkg_surrogate_set_backend(self.h, 1 if tcgen05 else 0))
+
+    def status(self):
+        b = C.c_int()
+        _check(lib().lkg_surrogate_status(self.h, C.byref(b)))
+        return b.value
 
     def features_device(self, n, d_poses):
         out = np.zeros((n, 64), np.uint16)

@@ -177,6 +177,146 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
             }
 }
 
+// ---------------------------------------------------------------------------
+// Forward layer on the 5th-generation tensor cores (tcgen05, sm_100a):
+//   Y[M x 256] = ReLU(X[M x K] W^T + b) -> bf16, W [256 x K] (K = 64 or 256)
+// One CTA (4 warps) per 128-row tile and the full width N = 256: the A tile
+// and all of W are staged in shared memory in the canonical K-major layout
+// without swizzle (8-row x 16-byte core matrices, core matrices along K
+// 128 B apart, 8-row groups (K / 8) * 128 B apart); one elected thread issues
+// K / 16 tcgen05.mma (M = 128, N = 256, K = 16, BF16 in, FP32 accumulate)
+// into a 128-lane x 256-column TMEM accumulator and commits them to an
+// mbarrier; each warp then reads its 32 TMEM lanes (32 rows) back with
+// tcgen05.ld, adds the bias, applies ReLU and stores bf16.  The mbarrier
+// wait is bounded: a wait that runs out sets status bit 2 and the CTA skips
+// the epilogue (the accumulator is freed after the commit has been waited
+// for with the same bound).
+// ---------------------------------------------------------------------------
+constexpr int TC_BM = 128, TC_N = 256, TC_KMAX = 256;
+constexpr size_t TC_SMEM = (size_t)(TC_BM + TC_N) * TC_KMAX * 2 + 128;   // A, B tiles + barrier / TMEM address
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// K-major, no swizzle: LBO = 128 B (next 8 elements of K), SBO = (K / 8) * 128 B
+// (next 8 rows); version 1 (bits 46-47); layout type 0
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, int K) {
+    const uint64_t start = (saddr >> 4) & 0x3fff;
+    const uint64_t lbo = (128 >> 4) & 0x3fff;
+    const uint64_t sbo = (((uint64_t)K / 8) * 128 >> 4) & 0x3fff;
+    return start | (lbo << 16) | (sbo << 32) | (1ull << 46);
+}
+
+__global__ void __launch_bounds__(128, 1)
+k_gemm_tc(int M, int K, const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ W,
+          const float* __restrict__ bias, __nv_bfloat16* __restrict__ Y, int* __restrict__ status) {
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(tc_smem);
+    __nv_bfloat16* sB = sA + (size_t)TC_BM * K;
+    unsigned long long* bar = reinterpret_cast<unsigned long long*>(tc_smem + (size_t)(TC_BM + TC_N) * TC_KMAX * 2);
+    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * TC_BM;
+    const int kc = K / 8;   // 16-byte chunks per row
+    // 1. TMEM: 256 columns (the FP32 accumulator); mbarrier
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(tmem_slot)), "r"(TC_N));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    // 2. operand tiles, 16-byte chunks in the canonical core-matrix layout
+    for (int e = tid; e < TC_BM * kc; e += 128) {
+        const int r = e / kc, c = e % kc, gm = m0 + r;
+        uint4 v = make_uint4(0u, 0u, 0u, 0u);
+        if (gm < M) v = *reinterpret_cast<const uint4*>(X + (size_t)gm * K + 8 * c);
+        *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(sA) + (size_t)(r >> 3) * kc * 128 + c * 128 +
+                                  (r & 7) * 16) = v;
+    }
+    for (int e = tid; e < TC_N * kc; e += 128) {
+        const int r = e / kc, c = e % kc;
+        const uint4 v = *reinterpret_cast<const uint4*>(W + (size_t)r * K + 8 * c);
+        *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(sB) + (size_t)(r >> 3) * kc * 128 + c * 128 +
+                                  (r & 7) * 16) = v;
+    }
+    // generic-proxy stores -> visible to the tensor core's async proxy
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = *tmem_slot;
+    // 3. one thread issues the MMAs and commits them to the barrier
+    if (tid == 0) {
+        // kind::f16 descriptor: D f32 (bits 4-5 = 1), A bf16 (7-9 = 1), B bf16
+        // (10-12 = 1), both K-major, N >> 3 at 17-22, M >> 4 at 24-28
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                               ((uint32_t)(TC_BM >> 4) << 24);
+        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
+        for (int ks = 0; ks < K / 16; ++ks) {
+            const uint64_t ad = tc_desc(a0 + ks * 256, K), bd = tc_desc(b0 + ks * 256, K);
+            const uint32_t acc = ks > 0 ? 1u : 0u;
+            asm volatile(
+                "{\n\t.reg .pred p;\n\t"
+                "setp.ne.b32 p, %4, 0;\n\t"
+                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+        }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(smem_u32(bar)) : "memory");
+    }
+    // 4. bounded wait for the accumulator (phase 0)
+    bool done = false;
+    for (int it = 0; it < (1 << 22) && !done; ++it) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred P1;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                     : "=r"(ok) : "r"(smem_u32(bar)), "r"(0u) : "memory");
+        done = ok != 0;
+    }
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!done) {
+        if (lane == 0) atomicOr(status, 4);
+    } else {
+        // 5. epilogue: warp w holds rows 32w .. 32w + 31 (TMEM lanes)
+        const int row = m0 + warp * 32 + lane;
+        for (int c0 = 0; c0 < TC_N; c0 += 32) {
+            uint32_t r[32];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                         "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                         "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                           "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+                           "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+                           "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (row < M) {
+                __align__(16) __nv_bfloat16 o[32];
+#pragma unroll
+                for (int j = 0; j < 32; ++j) {
+                    const float v = __uint_as_float(r[j]) + bias[c0 + j];
+                    o[j] = __float2bfloat16(v > 0.f ? v : 0.f);
+                }
+                uint4* dst = reinterpret_cast<uint4*>(Y + (size_t)row * TC_N + c0);
+#pragma unroll
+                for (int q = 0; q < 4; ++q) dst[q] = reinterpret_cast<const uint4*>(o)[q];
+            }
+        }
+    }
+    // 6. free the accumulator
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TC_N));
+    }
+}
+
 // last layer: y[n] = H3[n] . w3 + b3
 __global__ void k_head(const __nv_bfloat16* __restrict__ H3, int n, const float* __restrict__ w3, const float* b3,
                        float* __restrict__ y) {
@@ -289,6 +429,8 @@ struct lkg_surrogate {
     DBuf X, H1, H2, H3, dH1, dH2, dH3, y, t, loss;
     int cap = 0;
     DBuf d_step;   // Adam step count (device, 1-based)
+    int tc = 0;    // forward layers on tcgen05 (1) or mma.sync (0)
+    DBuf d_status; // tcgen05 wait time-outs (bit 2)
     size_t off[9];   // block offsets of W0 b0 W1 b1 W2 b2 w3 b3, and the total
 };
 
@@ -327,9 +469,28 @@ float* P(lkg_surrogate* S, int k) { return S->p.as<float>() + S->off[k]; }
 float* Gd(lkg_surrogate* S, int k) { return S->g.as<float>() + S->off[k]; }
 
 // forward of n feature rows already in S->X; y in S->y
+cudaError_t gemm_tc(lkg_surrogate* S, int n, int K, const __nv_bfloat16* X, const __nv_bfloat16* W, const float* b,
+                    __nv_bfloat16* Y) {
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+    if (e != cudaSuccess) return e;
+    k_gemm_tc<<<(n + TC_BM - 1) / TC_BM, 128, TC_SMEM, S->ctx->stream>>>(n, K, X, W, b, Y, S->d_status.as<int>());
+    return cudaGetLastError();
+}
+
 int forward(lkg_surrogate* S, int n) {
     cudaStream_t s = S->ctx->stream;
     const __nv_bfloat16* X = S->X.as<__nv_bfloat16>();
+    if (S->tc) {
+        LKG_CK(gemm_tc(S, n, IN, X, S->wt[0].as<__nv_bfloat16>(), P(S, 1), S->H1.as<__nv_bfloat16>()), "mlp fwd tc");
+        LKG_CK(gemm_tc(S, n, H, S->H1.as<__nv_bfloat16>(), S->wt[1].as<__nv_bfloat16>(), P(S, 3),
+                       S->H2.as<__nv_bfloat16>()), "mlp fwd tc");
+        LKG_CK(gemm_tc(S, n, H, S->H2.as<__nv_bfloat16>(), S->wt[2].as<__nv_bfloat16>(), P(S, 5),
+                       S->H3.as<__nv_bfloat16>()), "mlp fwd tc");
+        k_head<<<(n + 7) / 8, 256, 0, s>>>(S->H3.as<__nv_bfloat16>(), n, P(S, 6), P(S, 7), S->y.as<float>());
+        LKG_CK(cudaGetLastError(), "mlp head");
+        S->ctx->launches += 4;
+        return 0;
+    }
     LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, IN, X, IN, S->wt[0].as<__nv_bfloat16>(), IN, nullptr,
                                         S->H1.as<__nv_bfloat16>(), H, P(S, 1), nullptr)), "mlp fwd");
     LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, H, S->H1.as<__nv_bfloat16>(), H, S->wt[1].as<__nv_bfloat16>(), H,
@@ -484,7 +645,7 @@ int lkg_surrogate_create(lkg_ctx* ctx, int complex_id, uint64_t seed, lkg_surrog
     if ((e = S->p.reserve(NPARAM * 4)) != cudaSuccess || (e = S->g.reserve(NPARAM * 4)) != cudaSuccess ||
         (e = S->m1.reserve(NPARAM * 4)) != cudaSuccess || (e = S->m2.reserve(NPARAM * 4)) != cudaSuccess ||
         (e = S->anchors.reserve(NA * sizeof(int))) != cudaSuccess || (e = S->loss.reserve(sizeof(float))) != cudaSuccess ||
-        (e = S->d_step.reserve(sizeof(int))) != cudaSuccess) {
+        (e = S->d_step.reserve(sizeof(int))) != cudaSuccess || (e = S->d_status.reserve(sizeof(int))) != cudaSuccess) {
         delete S;
         return set_error(cuda_to_status(e), "surrogate alloc: %s", cudaGetErrorString(e));
     }
@@ -500,6 +661,7 @@ int lkg_surrogate_create(lkg_ctx* ctx, int complex_id, uint64_t seed, lkg_surrog
     cudaMemset(S->m2.p, 0, NPARAM * 4);
     const int one = 1;
     cudaMemcpy(S->d_step.p, &one, sizeof(int), cudaMemcpyHostToDevice);
+    cudaMemset(S->d_status.p, 0, sizeof(int));
     cudaMemcpy(S->anchors.p, anc.data(), NA * sizeof(int), cudaMemcpyHostToDevice);
     if ((rc = refresh_bf16(S))) { delete S; return rc; }
     if ((e = cudaDeviceSynchronize()) != cudaSuccess) {
@@ -607,6 +769,24 @@ int lkg_surrogate_train(lkg_surrogate* S, int n, const double* d_poses, const do
     if (e != cudaSuccess) return set_error(cuda_to_status(e), "train: %s", cudaGetErrorString(e));
     last = nb ? (double)l / nb : 0.0;
     if (loss_out) *loss_out = (float)last;
+    return set_ok();
+}
+
+// Forward layers on tcgen05 (1) or on the mma.sync kernel (0, default).
+int lkg_surrogate_set_backend(lkg_surrogate* S, int tcgen05) {
+    if (!S) return set_error(LKG_ERR_ARG, "null surrogate");
+    S->tc = tcgen05 ? 1 : 0;
+    return set_ok();
+}
+
+// Kernel status bits since the last call (4: a tcgen05 accumulator wait ran
+// out); cleared by the call.
+int lkg_surrogate_status(lkg_surrogate* S, int* bits) {
+    if (!S || !bits) return set_error(LKG_ERR_ARG, "bad status args");
+    cudaSetDevice(S->ctx->device);
+    LKG_CK(cudaStreamSynchronize(S->ctx->stream), "surrogate status");
+    LKG_CK(cudaMemcpy(bits, S->d_status.p, sizeof(int), cudaMemcpyDeviceToHost), "surrogate status");
+    LKG_CK(cudaMemset(S->d_status.p, 0, sizeof(int)), "surrogate status");
     return set_ok();
 }
 

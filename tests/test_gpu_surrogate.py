@@ -109,3 +109,58 @@ def test_online_training_learns_exact_energies(sur):
     rho = np.corrcoef(rank(pr), rank(ex))[0, 1]
     assert np.isfinite(pr).all()
     assert rho > 0.5, rho
+
+
+@pytest.mark.parametrize("n", [100, 1000, 4096])
+def test_tcgen05_forward_matches_mma_sync_and_the_oracle(sur, n):
+    # the forward layers on tcgen05 (TMEM accumulators) against the mma.sync
+    # kernel and the FP64 oracle; the backward pass reuses their activations
+    _, _, s = sur
+    rng = np.random.default_rng(100 + n)
+    p = omlp.he_params(7 + n)
+    s.set_params(p.astype(np.float32))
+    X = rng.normal(0.0, 1.0, size=(n, omlp.IN))
+    Xb = omlp.f64_to_bf16_bits(X)
+    t = rng.normal(0.0, 1.0, n).astype(np.float32)
+    s.set_backend(False)
+    y0, g0, l0 = s.grad(Xb, t)
+    s.set_backend(True)
+    try:
+        y1, g1, l1 = s.grad(Xb, t)
+        assert s.status() == 0
+    finally:
+        s.set_backend(False)
+    scale = 1.0 + np.abs(y0).max()
+    assert np.abs(y1 - y0).max() < 1e-2 * scale
+    p32 = p.astype(np.float32).astype(np.float64)
+    _, g_ref, y_ref = omlp.loss_and_grad(p32, omlp.bf16_bits_to_f64(Xb), t.astype(np.float64), emulate=True)
+    assert np.abs(y1 - y_ref).max() < 1e-2 * (1.0 + np.abs(y_ref).max())
+    cos = float(g1 @ g_ref / (np.linalg.norm(g1) * np.linalg.norm(g_ref)))
+    assert cos > 0.999, cos
+
+
+def test_tcgen05_predict_throughput_is_reported(sur):
+    import time
+    ctx, cid, s = sur
+    n = 32768
+    c0 = config0()
+    pos = synth.to_kernel_poses(synth.setup_poses(c0["rec"]["coords"], 16, n // 16, 4))
+    d = torch.tensor(pos, device="cuda")
+    out = {}
+    for tc in (False, True):
+        s.set_backend(tc)
+        pr = torch.zeros(n, dtype=torch.float64, device="cuda")
+        s.predict_device(n, d.data_ptr(), pr.data_ptr())
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(20):
+            s.predict_device(n, d.data_ptr(), pr.data_ptr())
+        torch.cuda.synchronize()
+        out[tc] = ((time.perf_counter() - t0) / 20, pr.cpu().numpy())
+    s.set_backend(False)
+    assert s.status() == 0
+    flop = 2.0 * n * (64 * 256 + 2 * 256 * 256 + 256)
+    print("surrogate predict, %d poses: mma.sync %.3f ms (%.1f TFLOP/s), tcgen05 %.3f ms (%.1f TFLOP/s)" % (
+        n, out[False][0] * 1e3, flop / out[False][0] / 1e12, out[True][0] * 1e3, flop / out[True][0] / 1e12))
+    a, b = out[False][1], out[True][1]
+    assert np.abs(a - b).max() < 1e-2 * (1.0 + np.abs(a).max())
