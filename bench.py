@@ -51,7 +51,7 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lkg", choices=["lkg", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config2", "config0", "config3", "config4"])
+    ap.add_argument("--workload", default="config2", choices=["config2", "config0", "config1", "config3", "config4"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--tile", type=int, default=0)
@@ -71,6 +71,12 @@ def workload(name):
     if name == "config0":
         c0 = synth.config0()
         items = [dict(rec=c0["rec"], lig=c0["lig"], family="dna", swarms=1, glowworms=200, seed=42)]
+    elif name == "config1":
+        base = synth.config0()
+        items = []
+        for fam in ("vdw", "pydock", "cpydock"):
+            c1 = synth.config1(fam, base=base)
+            items.append(dict(rec=c1["rec"], lig=c1["lig"], family=fam, swarms=6, glowworms=300, seed=7))
     elif name == "config4":
         c4 = synth.config4()
         items = [dict(rec=c4["rec"], lig=c4["lig"], family="cpydock", swarms=50, glowworms=500, seed=19)]
@@ -358,6 +364,9 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "config4":
         v, cores, sample = cpu_sample(items)
         line["cpu_baseline"] = {"value": v, "unit": "poses/s", "cores": cores, "kind": "port", "sample": sample}
+        v1, _, sample1 = cpu_sample(items, min_seconds=5.0, threads=1)
+        line["cpu_baseline_single_thread"] = {"value": v1, "unit": "poses/s", "cores": 1, "kind": "port",
+                                              "sample": sample1}
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()
