@@ -252,8 +252,8 @@ int lkg_surrogate_set_params(lkg_surrogate* s, const float* in);
 int lkg_surrogate_grad(lkg_surrogate* s, int n, const uint16_t* feats, const float* targets, float* y,
                        float* grad, float* loss);
 int lkg_surrogate_features(lkg_surrogate* s, int n, const double* d_poses, uint16_t* out);
-/* forward layers on the tcgen05 tensor cores (TMEM accumulators; 1) or on
- * the mma.sync kernel (0, default) */
+/* forward layers on the tcgen05 tensor cores (TMEM accumulators; 1,
+ * default) or on the mma.sync kernel (0) */
 int lkg_surrogate_set_backend(lkg_surrogate* s, int tcgen05);
 /* kernel status bits since the last call (4: a tcgen05 accumulator wait ran
  * out and that tile was skipped); cleared by the call */

@@ -429,7 +429,7 @@ struct lkg_surrogate {
     DBuf X, H1, H2, H3, dH1, dH2, dH3, y, t, loss;
     int cap = 0;
     DBuf d_step;   // Adam step count (device, 1-based)
-    int tc = 0;    // forward layers on tcgen05 (1) or mma.sync (0)
+    int tc = 1;    // forward layers on tcgen05 (1, default) or mma.sync (0)
     DBuf d_status; // tcgen05 wait time-outs (bit 2)
     size_t off[9];   // block offsets of W0 b0 W1 b1 W2 b2 w3 b3, and the total
 };
@@ -772,7 +772,7 @@ int lkg_surrogate_train(lkg_surrogate* S, int n, const double* d_poses, const do
     return set_ok();
 }
 
-// Forward layers on tcgen05 (1) or on the mma.sync kernel (0, default).
+// Forward layers on tcgen05 (1, default) or on the mma.sync kernel (0).
 int lkg_surrogate_set_backend(lkg_surrogate* S, int tcgen05) {
     if (!S) return set_error(LKG_ERR_ARG, "null surrogate");
     S->tc = tcgen05 ? 1 : 0;
