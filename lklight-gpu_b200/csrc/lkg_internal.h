@@ -56,6 +56,7 @@ struct ComplexDev {
     int fnx, fny, fnz;
     float fox, foy, foz, fsp;
     double fox64, foy64, foz64, fsp64;
+    double finv64;           // 1 / spacing when the spacing is a power of two (then x * finv64 == x / spacing), else 0
     // desolvation
     int hcap;                // receptor-minimum hash capacity (power of two)
     double solv_const;       // sum over asa<0 atoms of asa*des (CPU-grid semantics)

@@ -277,6 +277,11 @@ int build_field(lkg_ctx* ctx, const MolIn& R, const lkg_field* f, bool build, Co
     LKG_CK(cudaStreamSynchronize(s), "field upload");
     d.phi = cr.phi.as<float>();
     d.fox = (float)d.fox64; d.foy = (float)d.foy64; d.foz = (float)d.foz64; d.fsp = (float)d.fsp64;
+    {
+        int ex = 0;
+        const double m = std::frexp(d.fsp64, &ex);
+        d.finv64 = (m == 0.5 && d.fsp64 > 0.0) ? 1.0 / d.fsp64 : 0.0;   // exact reciprocal of 2^k
+    }
     return set_ok();
 }
 

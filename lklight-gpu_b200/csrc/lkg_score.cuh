@@ -96,7 +96,12 @@ __device__ __forceinline__ float sample_phi(const ComplexDev& c, float x, float 
 __device__ __forceinline__ double sample_phi(const ComplexDev& c, double x, double y, double z) {
     // grid_dna.rs:159-197 including the `tx as f32` weights
     double s = c.fsp64;
-    double fx = (x - c.fox64) / s, fy = (y - c.foy64) / s, fz = (z - c.foz64) / s;
+    double fx, fy, fz;
+    if (c.finv64 != 0.0) {   // power-of-two spacing (0.5 A): the same quotient, no divisions
+        fx = (x - c.fox64) * c.finv64; fy = (y - c.foy64) * c.finv64; fz = (z - c.foz64) * c.finv64;
+    } else {
+        fx = (x - c.fox64) / s; fy = (y - c.foy64) / s; fz = (z - c.foz64) / s;
+    }
     double ix = floor(fx), iy = floor(fy), iz = floor(fz);
     if (ix < 0.0 || iy < 0.0 || iz < 0.0) return 0.0;
     if (!(ix < (double)(c.fnx - 1) && iy < (double)(c.fny - 1) && iz < (double)(c.fnz - 1))) return 0.0;
