@@ -9,6 +9,7 @@ namespace lkg {
 
 struct GsoDevState {
     int n, n_swarms, max_swarm;
+    int reserved;                  // keeps the struct free of padding (it is compared bytewise)
     double *tx, *ty, *tz, *qw, *qx, *qy, *qz, *luc, *vis, *score;   // current state
     double *ntx, *nty, *ntz, *nqw, *nqx, *nqy, *nqz, *nvis;          // after the move
     double* poses;                 // scorer input, n x 7 (w, x, y, z, tx, ty, tz)

@@ -92,9 +92,11 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
     const float t = rr * rr * ir2;
     const float p6 = t * t * t;
     float vp = fminf(sv * p6 * (p6 - 2.f), 1.0f);
-    const float d = d2 * rsqrtf(d2), dmin = 0.75f * rr;
-    const bool clash = (flags & F_CLASH) && lq.y != 0.f && pr.z != 0.f && d < dmin;
-    vp = clash ? vp + 6.f * (dmin - d) : vp;
+    if (flags & F_CLASH) {   // uniform per complex: the other families skip the distance
+        const float d = d2 * rsqrtf(d2), dmin = 0.75f * rr;
+        const bool clash = lq.y != 0.f && pr.z != 0.f && d < dmin;
+        vp = clash ? vp + 6.f * (dmin - d) : vp;
+    }
     vdw += (double)vp;
     if (DESOLV && !D->lf[l] && pr.w == 0.f && d2 <= SOLV2_F * 1.001f) {
         const double4 a64 = c.rpos64[k];
