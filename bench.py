@@ -51,7 +51,8 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lkg", choices=["lkg", "reference"])
-    ap.add_argument("--workload", default="config2", choices=["config2", "config0", "config1", "config3", "config4"])
+    ap.add_argument("--workload", default="config2",
+                    choices=["config2", "config0", "config1", "config3", "config4", "config4-gso"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--tile", type=int, default=0)
@@ -215,7 +216,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     lkg = importlib.import_module("lklight-gpu_b200")
 
-    if args.workload == "config3":
+    if args.workload in ("config3", "config4-gso"):
         return run_screened(args, lkg, torch, local, rank, world, dist)
     items = workload(args.workload)
     if args.complexes:
@@ -386,21 +387,27 @@ def top5_overlap(tr_a, sc_a, tr_b, sc_b, tol=2.0):
 
 def run_screened(args, lkg, torch, local, rank, world, dist):
     """Surrogate-screened GSO against the plain GSO on the same complex and
-    start: the config-0 complex, 10 swarms x 1,000 glowworms, seed 3; both
-    end with an exact rescoring of the final poses.  Wall time of the whole
-    run (device scoring, surrogate training / inference, host movement)."""
+    start, both ending with an exact rescoring of the final poses; wall time
+    of the whole run (device scoring, surrogate training / inference, host
+    movement).  config3: the config-0 complex (dna), 10 swarms x 1,000
+    glowworms, seed 3.  config4-gso: the config-4 complex (cpydock, 101k-atom
+    receptor, 12k-atom ligand), 50 x 500, seed 19, 100 steps."""
     synth = importlib.import_module("lklight-gpu_b200.synth")
-    c0 = synth.config0()
-    swarms, glow, steps = 10, 1000, args.gso_steps
+    if args.workload == "config4-gso":
+        c = synth.config4()
+        family, swarms, glow, steps, seed = "cpydock", 50, 500, min(args.gso_steps, 100), 19
+    else:
+        c = synth.config0()
+        family, swarms, glow, steps, seed = "dna", 10, 1000, args.gso_steps, 3
     ctx = lkg.Context(device=local, tile=args.tile, cell=args.cell, group=args.group, xsub=args.xsub)
-    cid = ctx.add_complex("dna", c0["rec"], c0["lig"])
-    pos = synth.setup_poses(c0["rec"]["coords"], swarms, glow, 3)
+    cid = ctx.add_complex(family, c["rec"], c["lig"])
+    pos = synth.setup_poses(c["rec"]["coords"], swarms, glow, seed)
     res = {}
     for mode in ("plain", "device", "screened", "ablation"):
-        g = lkg.GSO(ctx, [(cid, swarms, glow)], pos, [3])
+        g = lkg.GSO(ctx, [(cid, swarms, glow)], pos, [seed])
         if mode in ("screened", "ablation"):
             g.set_screen(candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=20,
-                         finetune_epochs=2, lr=1e-3, seed=3, random_rank=(mode == "ablation"), batch=1024)
+                         finetune_epochs=2, lr=1e-3, seed=seed, random_rank=(mode == "ablation"), batch=1024)
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g.run(steps, device=(mode == "device"))
@@ -422,7 +429,7 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
     line = {"metric": "surrogate-screened GSO speedup over the plain GSO (e2e, same complex and start)",
             "value": res["plain"]["seconds"] / res["screened"]["seconds"], "unit": "x", "n_gpus": world,
             "higher_is_better": True, "data": "synthetic",
-            "config": {"workload": "config3", "swarms": swarms, "glowworms": glow, "steps": steps,
+            "config": {"workload": args.workload, "family": family, "swarms": swarms, "glowworms": glow, "steps": steps,
                        "candidates": 4, "exact_fraction": 0.25, "rescore_every": 10, "train_steps": 20},
             "plain": {"seconds": res["plain"]["seconds"], "exact_evals": res["plain"]["scored"],
                       "mean_best_score": best["plain"], "phases_s": res["plain"]["phases"]},
