@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lkg", choices=["lkg", "reference"])
     ap.add_argument("--workload", default="config2",
-                    choices=["config2", "config0", "config1", "config3", "config4", "config4-gso"])
+                    choices=["config2", "config0", "config1", "config3", "config4", "config4-gso",
+                             "restraints"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--tile", type=int, default=0)
@@ -81,11 +82,20 @@ def workload(name):
     elif name == "config4":
         c4 = synth.config4()
         items = [dict(rec=c4["rec"], lig=c4["lig"], family="cpydock", swarms=50, glowworms=500, seed=19)]
+    elif name == "restraints":
+        # the config-0 complex (dna) at the config-3 swarm layout, with active
+        # restraints and a membrane: runs the reference scores on its CPU path only
+        c0 = synth.config0()
+        items = [dict(rec=c0["rec"], lig=c0["lig"], family="dna", swarms=10, glowworms=1000, seed=3)]
     else:
         items = synth.config2()
     for it in items:
         it["poses"] = synth.to_kernel_poses(
             synth.setup_poses(it["rec"]["coords"], it["swarms"], it["glowworms"], it["seed"]))
+    if name == "restraints":
+        it = items[0]
+        centres = it["poses"][::it["glowworms"], 4:7]
+        it["restraints"] = synth.restraints(it["rec"]["coords"], len(it["lig"]["coords"]), centres, 23)
     return items
 
 
@@ -145,8 +155,11 @@ def cpu_sample(items, min_seconds=10.0, threads=0, max_complexes=2):
                 break
     picks = picks[:max_complexes]
     models = [(k, oracle.Model(items[k]["family"], items[k]["rec"], items[k]["lig"])) for k in picks]
-    for _, m in models:
+    for k, m in models:
         m.field()  # far field built before timing (setup, as the reference caches it)
+        if "restraints" in items[k]:
+            rr, lr, mem = items[k]["restraints"]
+            m.set_restraints(rr, int(rr.max()) + 1, lr, int(lr.max()) + 1, mem)
     done, t0, batch = 0, time.perf_counter(), 8
     off = 0
     while True:
@@ -230,6 +243,9 @@ def main():
     ctx = lkg.Context(device=local, tile=shape["tile"], cell=shape["cell"], group=shape["group"], xsub=shape["xsub"])
     stream = torch.cuda.ExternalStream(ctx.stream)
     ids = [ctx.add_complex(it["family"], it["rec"], it["lig"]) for it in items]
+    for cid, it in zip(ids, items):
+        if "restraints" in it:
+            ctx.set_restraints(cid, *it["restraints"])
     counts = [len(it["poses"]) for it in items]
     npose = int(sum(counts))
     allp = np.vstack([it["poses"] for it in items])
@@ -360,6 +376,32 @@ def main():
             "step": "CUDA graph replay of one persistent launch group" if not args.no_graph else "plan launch"}
     if plain:
         line["plain_single_complex"] = plain
+    if any("restraints" in it for it in items):
+        # the same poses without restraints / membrane: the cost of the
+        # interface bits; and the fractions seen, to show they were exercised
+        h_iface = ctx.score_interface(ids[0], items[0]["poses"])[1]
+        rr, lr, mem = items[0]["restraints"]
+        line["config"]["restraints"] = {
+            "receptor_residues": int(rr.max()) + 1, "ligand_residues": int(lr.max()) + 1, "membrane_beads": len(mem),
+            "poses_with": {k: int((h_iface[:, i] > 0).sum()) for i, k in enumerate(("rec", "lig", "membrane"))}}
+        plan.close()
+        for cid in ids:
+            ctx.set_restraints(cid)
+        plan = lkg.Plan(ctx, ids, counts)
+        plan.capture(d_poses.data_ptr(), d_scores.data_ptr(), n_launches=1)
+        for _ in range(args.warmup):
+            plan.replay()
+        e4, e5 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e4.record(stream)
+        for _ in range(args.steps):
+            plan.replay()
+        e5.record(stream)
+        e5.synchronize()
+        pms = e4.elapsed_time(e5) / args.steps
+        line["without_restraints"] = {"value": npose / (pms / 1e3), "unit": "poses/s", "ms_per_step": pms,
+                                      "restraint_overhead": ms / pms - 1.0}
+        for cid, it in zip(ids, items):
+            ctx.set_restraints(cid, *it["restraints"])
     # (the oracle's CPU far-field build for the 101k-atom cpydock receptor
     # alone takes minutes: no CPU sample for that workload)
     if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "config4":

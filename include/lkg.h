@@ -167,11 +167,38 @@ int lkg_complex_add(lkg_ctx* ctx, int family, const lkg_mol* receptor, const lkg
 /* Receptor / ligand atom counts and near-cell geometry of a complex. */
 int lkg_complex_info(lkg_ctx* ctx, int complex_id, int* nr, int* nl, int* n_cells);
 
+/* Active restraints and membrane of a complex, scored in the batch kernels
+ * (the reference sends such runs to its CPU path: dna.rs:885-897,1047-1056,
+ * pydock.rs:461-470, vdw.rs:262-272, cpydock.rs:690-700).
+ *   rec_residue[i]: for receptor atom i (caller order), the index
+ *     0..n_rec_res-1 of its active-restraint residue, or -1.  One index per
+ *     key of the reference's `active_restraints` map (every index must have
+ *     at least one atom, as the map's keys do); lig_residue likewise.
+ *   membrane: receptor atom indices of the membrane beads (MMB.BJ,
+ *     pydock.rs:77-80), each at most once.
+ * A pair within INTERFACE_CUTOFF (3.9 A) marks both atoms as interface
+ * atoms; per pose pr / pl = satisfied restraint residues / all (receptor /
+ * ligand) and m = membrane beads at the interface / all (scoring.rs:83-108);
+ * the score s becomes s + pr*s + pl*s - (m > 0 ? 999 m : 0) in the family's
+ * operation order (dna.rs:989-995; vdw: no membrane term, vdw.rs:146-149).
+ * The reference's passive restraints and ligand membrane do not enter the
+ * score and are not taken.  All counts 0 clears the complex's restraints.
+ * Plans made before the call must be made again. */
+int lkg_complex_set_restraints(lkg_ctx* ctx, int complex_id, const int32_t* rec_residue, int n_rec_res,
+                               const int32_t* lig_residue, int n_lig_res, const int32_t* membrane,
+                               int n_membrane);
+
 /* Score::batch_energy for one complex, host buffers: poses N x 7 -> scores.
  * parts (optional, N x 4): raw near+far electrostatics, LJ (+clash),
  * desolvation sum, near pairs (d <= 10 A) counted by the kernel. */
 int lkg_score(lkg_ctx* ctx, int complex_id, int n_pose, const double* poses,
               double* scores, double* parts);
+
+/* lkg_score plus the interface terms of every pose, host buffers:
+ * iface N x 3 = (pr, pl, m) as above (zeros for a complex without
+ * restraints or membrane). */
+int lkg_score_interface(lkg_ctx* ctx, int complex_id, int n_pose, const double* poses, double* scores,
+                        double* iface);
 
 /* Device-pointer variant, asynchronous on the context stream. */
 int lkg_score_device(lkg_ctx* ctx, int complex_id, int n_pose, const double* d_poses,
@@ -241,6 +268,10 @@ int lkg_surrogate_destroy(lkg_surrogate* s);
 int lkg_surrogate_set_target_scale(lkg_surrogate* s, int n, const double* scores);
 /* predicted scores (lkg_score units) for n device poses, device output */
 int lkg_surrogate_predict(lkg_surrogate* s, int n, const double* d_poses, double* d_pred);
+/* Allocate the activation buffers for predictions of up to n_predict poses
+ * per call and training batches of train_batch rows now (growing them
+ * later reallocates, which synchronises the device). */
+int lkg_surrogate_reserve(lkg_surrogate* s, int n_predict, int train_batch);
 /* minibatch Adam over n device poses with their exact scores (device) */
 int lkg_surrogate_train(lkg_surrogate* s, int n, const double* d_poses, const double* d_scores, int epochs,
                         int batch, float lr, float* loss);
@@ -301,6 +332,10 @@ int lkg_gso_run_device(lkg_gso* gso, int steps);
 int lkg_gso_state(lkg_gso* gso, double* trans, double* rot, double* luc, double* scoring,
                   double* vision, int32_t* nneigh);
 int64_t lkg_gso_scored(lkg_gso* gso);
+/* Swarm::save (swarm.rs:232-271): write swarm `swarm` (index over all
+ * groups, in creation order) as <directory>/gso_<step>.out in the
+ * reference's format (what `lklight rank` and `generate` read). */
+int lkg_gso_save(lkg_gso* gso, int swarm, int step, const char* directory);
 int lkg_gso_destroy(lkg_gso* gso);
 
 /* Surrogate screening of GSO moves (no counterpart in the reference; the

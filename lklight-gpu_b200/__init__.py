@@ -74,6 +74,9 @@ def lib():
         "lkg_ctx_set_stream": (I, [P, P]), "lkg_ctx_set_group": (I, [P, I]), "lkg_ctx_set_xsub": (I, [P, I]), "lkg_ctx_stream": (P, [P]), "lkg_ctx_launches": (I64, [P]),
         "lkg_complex_add": (I, [P, I, P, P, P, P]), "lkg_complex_info": (I, [P, I, P, P, P]),
         "lkg_score": (I, [P, I, I, P, P, P]), "lkg_score_device": (I, [P, I, I, P, P, P]),
+        "lkg_score_interface": (I, [P, I, I, P, P, P]),
+        "lkg_complex_set_restraints": (I, [P, I, P, I, P, I, P, I]),
+        "lkg_surrogate_reserve": (I, [P, I, I]),
         "lkg_score_multi_device": (I, [P, I, P, P, P, P, P]),
         "lkg_score_multi": (I, [P, I, P, P, P, P, P]),
         "lkg_ctx_sync": (I, [P]),
@@ -90,6 +93,7 @@ def lib():
         "lkg_rng_new": (P, [U64]), "lkg_rng_f64": (D, [P]), "lkg_rng_free": (None, [P]),
         "lkg_gso_create": (I, [P, I, P, P, P, P, P, P]), "lkg_gso_run": (I, [P, I]),
         "lkg_gso_state": (I, [P, P, P, P, P, P, P]), "lkg_gso_scored": (I64, [P]),
+        "lkg_gso_save": (I, [P, I, I, C.c_char_p]),
         "lkg_gso_destroy": (I, [P]), "lkg_compat_cache_clear": (None, []),
         "lkg_gso_set_screen": (I, [P, P]), "lkg_gso_finalize": (I, [P]), "lkg_gso_predicted": (I64, [P]), "lkg_gso_timing": (I, [P, P]), "lkg_surrogate_set_backend": (I, [P, I]), "lkg_surrogate_status": (I, [P, P]), "lkg_gso_run_device": (I, [P, I]),
         "cuda_batch_score": (I, [P, I, I, I, F, F, F, F, P, P, P, P, P, I, P, P, I, I, I, F, F, F, F,
@@ -199,6 +203,33 @@ class Context:
         pa = np.zeros((len(p), 4)) if parts else None
         _check(lib().lkg_score(self.h, cid, len(p), ptr(p), ptr(out), ptr(pa)))
         return (out, pa) if parts else out
+
+    def set_restraints(self, cid, rec_residue=None, lig_residue=None, membrane=None):
+        """Active restraints and membrane of complex cid: rec_residue /
+        lig_residue give each atom's restraint residue index (-1 = none;
+        the count is max + 1), membrane the receptor atom indices of the
+        membrane beads.  No arguments clears them."""
+        def res(a):
+            if a is None:
+                return None, 0
+            a = np.ascontiguousarray(a, np.int32)
+            return a, (int(a.max()) + 1 if len(a) and a.max() >= 0 else 0)
+        rr, nr = res(rec_residue)
+        lr, nl = res(lig_residue)
+        mm = None if membrane is None else np.ascontiguousarray(membrane, np.int32)
+        nm = 0 if mm is None else len(mm)
+        _check(lib().lkg_complex_set_restraints(self.h, cid, ptr(rr) if nr else None, nr, ptr(lr) if nl else None,
+                                                nl, ptr(mm) if nm else None, nm))
+
+    def score_interface(self, cid, poses):
+        """Scores with the restraint / membrane terms, and per pose the
+        receptor and ligand restraint fractions and the membrane
+        intersection (N x 3)."""
+        p = _arr(poses, np.float64).reshape(-1, 7)
+        out = np.zeros(len(p))
+        f = np.zeros((len(p), 3))
+        _check(lib().lkg_score_interface(self.h, cid, len(p), ptr(p), ptr(out), ptr(f)))
+        return out, f
 
     def score_device(self, cid, n, d_poses, d_scores, d_parts=0):
         _check(lib().lkg_score_device(self.h, cid, n, C.c_void_p(d_poses), C.c_void_p(d_scores),
@@ -428,6 +459,10 @@ class GSO:
     @property
     def predicted(self):
         return lib().lkg_gso_predicted(self.h)
+
+    def save(self, swarm, step, directory):
+        """Swarm `swarm` as <directory>/gso_<step>.out (swarm.rs:232-271)."""
+        _check(lib().lkg_gso_save(self.h, swarm, step, os.fsencode(directory)))
 
     def timing(self):
         """Wall seconds in exact scoring, host movement, surrogate inference

@@ -12,7 +12,9 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
 #include <cstring>
+#include <string>
 #include <unordered_map>
 #include <vector>
 
@@ -331,10 +333,13 @@ inline double now_s() {
 // Train (or fine-tune) the surrogate of group gi on its exact pairs (the
 // last `recent` of them when recent > 0; at most 65,536 are kept), in a
 // seeded shuffled order.
+// most recent exact (pose, score) pairs kept per group for training
+constexpr size_t TRAIN_CAP = 65536;
+
 int train_group(lkg_gso* G, int gi, int epochs, size_t recent) {
     auto& P = G->tr_pose[gi];
     auto& S0 = G->tr_score[gi];
-    const size_t cap = 65536;
+    const size_t cap = TRAIN_CAP;
     if (S0.size() > cap) {
         const size_t drop = S0.size() - cap;
         P.erase(P.begin(), P.begin() + 7 * drop);
@@ -572,13 +577,32 @@ int lkg_gso_set_screen(lkg_gso* G, const lkg_screen* cfg) {
     G->tr_score.assign(ng, {});
     G->scaled.assign(ng, false);
     G->rank_rng.seed_from_u64(cfg->seed);
-    if (!cfg->random_rank)
-        for (int gi = 0; gi < ng; ++gi) {
-            lkg_surrogate* s = nullptr;
-            int st = lkg_surrogate_create(G->ctx, G->group_complex[gi], cfg->seed + (uint64_t)gi, &s);
-            if (st) return st;
-            G->sur.push_back(s);
-        }
+    // every buffer the screened steps use is allocated here, at its final
+    // size: growing one inside the step loop would reallocate (each free
+    // synchronises the device) and a fresh allocation maps new pages
+    size_t total = 0;
+    for (int gi = 0; gi < ng; ++gi) {
+        size_t ng_glow = 0;
+        for (int s = G->group_first_swarm[gi]; s < G->group_first_swarm[gi] + G->group_nswarm[gi]; ++s)
+            ng_glow += G->swarms[s].g.size();
+        total += ng_glow * (size_t)(cfg->candidates + 1);
+        if (cfg->random_rank) continue;
+        lkg_surrogate* s = nullptr;
+        int st = lkg_surrogate_create(G->ctx, G->group_complex[gi], cfg->seed + (uint64_t)gi, &s);
+        if (st) return st;
+        G->sur.push_back(s);
+        const int batch = cfg->batch > 0 ? cfg->batch : 1024;
+        if ((st = lkg_surrogate_reserve(s, (int)std::min<size_t>(ng_glow * (cfg->candidates + 1), INT32_MAX), batch)))
+            return st;
+    }
+    LKG_CK(G->h_cand.reserve(total * 7 * sizeof(double)), "candidate staging");
+    LKG_CK(G->h_pred.reserve(total * sizeof(double)), "candidate staging");
+    if (!cfg->random_rank) {
+        LKG_CK(G->d_cand.reserve(total * 7 * sizeof(double)), "candidate staging");
+        LKG_CK(G->d_pred.reserve(total * sizeof(double)), "candidate staging");
+        LKG_CK(G->d_tp.reserve(TRAIN_CAP * 7 * sizeof(double)), "surrogate training set");
+        LKG_CK(G->d_ts.reserve(TRAIN_CAP * sizeof(double)), "surrogate training set");
+    }
     G->screen = true;
     return set_ok();
 }
@@ -607,6 +631,46 @@ int lkg_gso_state(lkg_gso* G, double* trans, double* rot, double* luc, double* s
             if (nneigh) nneigh[row] = (int32_t)g.nb.size();
             ++row;
         }
+    return set_ok();
+}
+
+// Swarm::save (swarm.rs:232-271): one swarm's glowworms as gso_<step>.out.
+// Rust's {:.N} prints the correctly rounded fixed-point decimal of the f64
+// (ties to even), as glibc's %.Nf does; NaN and infinities are spelled the
+// Rust way.
+static void put_fixed(std::string& out, double v, int prec) {
+    if (std::isnan(v)) { out += "NaN"; return; }
+    if (std::isinf(v)) { out += v < 0 ? "-inf" : "inf"; return; }
+    char b[400];
+    std::snprintf(b, sizeof(b), "%.*f", prec, v);
+    out += b;
+}
+
+int lkg_gso_save(lkg_gso* G, int swarm, int step, const char* directory) {
+    if (!G || !directory || swarm < 0 || swarm >= (int)G->swarms.size() || step < 0)
+        return set_error(LKG_ERR_ARG, "bad save arguments");
+    std::string text = "#Coordinates  RecID  LigID  Luciferin  Neighbor's number  Vision Range  Scoring\n";
+    for (const Glow& g : G->swarms[swarm].g) {
+        const double v[7] = {g.t[0], g.t[1], g.t[2], g.r.w, g.r.x, g.r.y, g.r.z};
+        text += "(";
+        for (int k = 0; k < 7; ++k) {
+            if (k) text += ", ";
+            put_fixed(text, v[k], 7);
+        }
+        text += ")    0    0   ";
+        put_fixed(text, g.luciferin, 8);
+        text += "  " + std::to_string(g.nb.size()) + " ";
+        put_fixed(text, g.vision, 3);
+        text += " ";
+        put_fixed(text, g.scoring, 8);
+        text += "\n";
+    }
+    const std::string path = std::string(directory) + "/gso_" + std::to_string(step) + ".out";
+    FILE* f = std::fopen(path.c_str(), "wb");
+    if (!f) return set_error(LKG_ERR_ARG, "cannot create %s", path.c_str());
+    const size_t w = std::fwrite(text.data(), 1, text.size(), f);
+    const int c = std::fclose(f);
+    if (w != text.size() || c != 0) return set_error(LKG_ERR_ARG, "cannot write %s", path.c_str());
     return set_ok();
 }
 

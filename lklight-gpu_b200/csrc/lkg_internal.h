@@ -60,7 +60,22 @@ struct ComplexDev {
     // desolvation
     int hcap;                // receptor-minimum hash capacity (power of two)
     double solv_const;       // sum over asa<0 atoms of asa*des (CPU-grid semantics)
+    // interface flags (active restraints, membrane): per pose, one bit per
+    // receptor restraint residue, ligand restraint residue and membrane bead
+    // (in that order) set when one of its atoms lies within 3.9 A of an
+    // atom of the other molecule; null tags = no restraints or membrane
+    const int2* rtag;        // sorted receptor atom -> (restraint bit, membrane bit), -1 = none
+    const int* ltag;         // bisection-ordered ligand atom -> restraint bit, -1 = none
+    int nres_r, nres_l, nmem;
+    int iface_words;         // 32-bit words of one pose's interface bits (0: none)
+    int iface_form;          // IF_* score combination of the family
 };
+
+// how the restraint fractions and the membrane penalty enter the score
+//   IF_DNA: s += pr*s + pl*s - pen              (dna.rs:989-995)
+//   IF_SUM: s = s + pr*s + pl*s - pen           (pydock.rs:440-445, cpydock.rs:670-675)
+//   IF_VDW: s = s + pr*s + pl*s, no membrane    (vdw.rs:146-149)
+enum { IF_NONE = 0, IF_DNA = 1, IF_SUM = 2, IF_VDW = 3 };
 
 // One launch over a batch of (complex, pose range) items.
 struct LaunchParams {
@@ -90,6 +105,14 @@ struct LaunchParams {
     // optional [N]: poses whose byte is 0 are skipped (their score and parts
     // keep their previous values: the device GSO's unmoved glowworms)
     const unsigned char* pose_mask;
+    // interface bits: iface_stride words per pose (global pose index),
+    // all zero between launches (the pose's last unit clears them);
+    // null when no complex of the launch has restraints or a membrane
+    unsigned* iface;
+    int iface_stride;
+    // optional [N x 3]: restraint fractions (receptor, ligand) and membrane
+    // intersection of each scored pose
+    double* iface_out;
 };
 
 constexpr double FACTOR = 332.0;
@@ -100,6 +123,9 @@ constexpr float NEAR_R = 10.0f;
 constexpr float SCAN_R = 10.001f;   // candidate radius (superset margin over 10 A)
 constexpr float SOLV2_F = 40.96f;   // 6.4^2 as the reference GPU writes it
 constexpr double SOLV2_D = 6.4 * 6.4;
+constexpr double IFACE2_D = 3.9 * 3.9;   // INTERFACE_CUTOFF^2 (constants.rs:14-15)
+constexpr float IFACE2_F = 15.2115f;    // f32 prefilter, 1e-4 above IFACE2_D
+constexpr double MEMBRANE_PENALTY = 999.0;   // MEMBRANE_PENALTY_SCORE (constants.rs:21)
 
 // launches (defined in lkg_kernels_*.cu)
 cudaError_t launch_score_fast(const LaunchParams& p, int threads, int blocks, cudaStream_t s);

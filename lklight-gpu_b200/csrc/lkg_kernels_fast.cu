@@ -8,13 +8,19 @@ namespace lkg {
 template <int G>
 static size_t warp_smem() { return (size_t)(WK_THREADS / 32) * sizeof(WSlots<G>); }
 
+// IFACE: the variant that also collects the interface bits (launches with
+// restraint or membrane complexes)
+template <int G, bool IFACE>
+static cudaError_t launch_warp_gi(const LaunchParams& p, int blocks, cudaStream_t s) {
+    const size_t sm = warp_smem<G>();
+    cudaError_t e = cudaFuncSetAttribute(k_score_warp<G, IFACE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    if (e != cudaSuccess) return e;
+    k_score_warp<G, IFACE><<<blocks, WK_THREADS, sm, s>>>(p);
+    return cudaGetLastError();
+}
 template <int G>
 static cudaError_t launch_warp_g(const LaunchParams& p, int blocks, cudaStream_t s) {
-    const size_t sm = warp_smem<G>();
-    cudaError_t e = cudaFuncSetAttribute(k_score_warp<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    k_score_warp<G><<<blocks, WK_THREADS, sm, s>>>(p);
-    return cudaGetLastError();
+    return p.iface ? launch_warp_gi<G, true>(p, blocks, s) : launch_warp_gi<G, false>(p, blocks, s);
 }
 
 cudaError_t launch_score_fast(const LaunchParams& p, int threads, int blocks, cudaStream_t s) {
@@ -35,8 +41,8 @@ template <int G>
 static int occ_warp_g() {
     int m = 0;
     const size_t sm = warp_smem<G>();
-    cudaFuncSetAttribute(k_score_warp<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_score_warp<G>, WK_THREADS, sm);
+    cudaFuncSetAttribute(k_score_warp<G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&m, k_score_warp<G, false>, WK_THREADS, sm);
     return m;
 }
 
@@ -44,13 +50,19 @@ size_t desolv_smem_bytes(int hcap, bool /*exact*/) { return (size_t)hcap * 12; }
 
 // cpydock: the warp kernel for group sizes up to 16 (its per-warp slots and
 // the block's minimum hash fit in shared memory), the per-atom kernel above
+template <int G, bool IFACE>
+static cudaError_t launch_warp_desolv_gi(const LaunchParams& p, int blocks, int hcap, cudaStream_t s) {
+    const size_t sm = wd_smem<G>(hcap);
+    cudaError_t e = cudaFuncSetAttribute(k_score_warp_desolv<G, IFACE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sm);
+    if (e != cudaSuccess) return e;
+    k_score_warp_desolv<G, IFACE><<<blocks, WD_THREADS, sm, s>>>(p);
+    return cudaGetLastError();
+}
 template <int G>
 static cudaError_t launch_warp_desolv_g(const LaunchParams& p, int blocks, int hcap, cudaStream_t s) {
-    const size_t sm = wd_smem<G>(hcap);
-    cudaError_t e = cudaFuncSetAttribute(k_score_warp_desolv<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess) return e;
-    k_score_warp_desolv<G><<<blocks, WD_THREADS, sm, s>>>(p);
-    return cudaGetLastError();
+    return p.iface ? launch_warp_desolv_gi<G, true>(p, blocks, hcap, s)
+                   : launch_warp_desolv_gi<G, false>(p, blocks, hcap, s);
 }
 
 cudaError_t launch_desolv_fast(const LaunchParams& p, int threads, int blocks, int hcap, cudaStream_t s) {
@@ -71,8 +83,8 @@ template <int G>
 static int occ_warp_desolv_g(int hcap) {
     int n = 0;
     const size_t sm = wd_smem<G>(hcap);
-    cudaFuncSetAttribute(k_score_warp_desolv<G>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_score_warp_desolv<G>, WD_THREADS, sm);
+    cudaFuncSetAttribute(k_score_warp_desolv<G, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_score_warp_desolv<G, false>, WD_THREADS, sm);
     return n;
 }
 

@@ -427,7 +427,8 @@ struct lkg_surrogate {
     DBuf wt[3], w[3];   // BF16 layouts per GEMM layer
     // activations for a batch
     DBuf X, H1, H2, H3, dH1, dH2, dH3, y, t, loss;
-    int cap = 0;
+    int cap = 0;     // rows of X, H1..H3, y, t (forward)
+    int cap_b = 0;   // rows of dH1..dH3 (backward)
     DBuf d_step;   // Adam step count (device, 1-based)
     int tc = 1;    // forward layers on tcgen05 (1, default) or mma.sync (0)
     DBuf d_status; // tcgen05 wait time-outs (bit 2)
@@ -438,20 +439,33 @@ namespace {
 
 constexpr size_t NPARAM = (size_t)H * IN + H + 2 * ((size_t)H * H + H) + H + 1;
 
-int sur_reserve(lkg_surrogate* S, int n) {
-    if (n <= S->cap) return 0;
-    if (S->cap > 0) n = std::max(n, S->cap + S->cap / 2);   // grow geometrically
-    size_t nb = (size_t)n * sizeof(__nv_bfloat16);
-    LKG_CK(S->X.reserve(nb * IN), "surrogate alloc");
-    LKG_CK(S->H1.reserve(nb * H), "surrogate alloc");
-    LKG_CK(S->H2.reserve(nb * H), "surrogate alloc");
-    LKG_CK(S->H3.reserve(nb * H), "surrogate alloc");
-    LKG_CK(S->dH1.reserve(nb * H), "surrogate alloc");
-    LKG_CK(S->dH2.reserve(nb * H), "surrogate alloc");
-    LKG_CK(S->dH3.reserve(nb * H), "surrogate alloc");
-    LKG_CK(S->y.reserve((size_t)n * sizeof(float)), "surrogate alloc");
-    LKG_CK(S->t.reserve((size_t)n * sizeof(float)), "surrogate alloc");
-    S->cap = n;
+// predictions run in chunks of at most this many rows, so the inference
+// buffers stay bounded and are sized once
+constexpr int PRED_CHUNK = 65536;
+
+// activation buffers for n rows: forward ones always, backward ones when
+// `bwd` (training); growing reallocates (and so synchronises the device),
+// so callers that know their sizes reserve them up front
+int sur_reserve(lkg_surrogate* S, int n, bool bwd) {
+    if (n > S->cap) {
+        const int m = S->cap > 0 ? std::max(n, S->cap + S->cap / 2) : n;   // grow geometrically
+        const size_t nb = (size_t)m * sizeof(__nv_bfloat16);
+        LKG_CK(S->X.reserve(nb * IN), "surrogate alloc");
+        LKG_CK(S->H1.reserve(nb * H), "surrogate alloc");
+        LKG_CK(S->H2.reserve(nb * H), "surrogate alloc");
+        LKG_CK(S->H3.reserve(nb * H), "surrogate alloc");
+        LKG_CK(S->y.reserve((size_t)m * sizeof(float)), "surrogate alloc");
+        LKG_CK(S->t.reserve((size_t)m * sizeof(float)), "surrogate alloc");
+        S->cap = m;
+    }
+    if (bwd && n > S->cap_b) {
+        const int m = S->cap_b > 0 ? std::max(n, S->cap_b + S->cap_b / 2) : n;
+        const size_t nb = (size_t)m * sizeof(__nv_bfloat16);
+        LKG_CK(S->dH1.reserve(nb * H), "surrogate alloc");
+        LKG_CK(S->dH2.reserve(nb * H), "surrogate alloc");
+        LKG_CK(S->dH3.reserve(nb * H), "surrogate alloc");
+        S->cap_b = m;
+    }
     return 0;
 }
 
@@ -568,7 +582,7 @@ int refresh_bf16(lkg_surrogate* S) {
 }
 
 int features(lkg_surrogate* S, int n, const double* d_poses) {
-    if (sur_reserve(S, n)) return lkg_last_status();
+    if (sur_reserve(S, n, false)) return lkg_last_status();
     int st = sync_descriptors(S->ctx);
     if (st) return st;
     const int threads = 256, blocks = (int)(((size_t)n * NA + threads - 1) / threads);
@@ -703,11 +717,26 @@ int lkg_surrogate_predict(lkg_surrogate* S, int n, const double* d_poses, double
     if (n == 0) return set_ok();
     cudaSetDevice(S->ctx->device);
     int st;
-    if ((st = features(S, n, d_poses))) return st;
-    if ((st = forward(S, n))) return st;
-    k_untarget<<<(n + 255) / 256, 256, 0, S->ctx->stream>>>(S->y.as<float>(), n, S->e_scale, S->t_mu, S->t_sd, d_pred);
-    LKG_CK(cudaGetLastError(), "predict");
-    S->ctx->launches++;
+    for (int b0 = 0; b0 < n; b0 += PRED_CHUNK) {
+        const int m = std::min(PRED_CHUNK, n - b0);
+        if ((st = features(S, m, d_poses + 7 * (size_t)b0))) return st;
+        if ((st = forward(S, m))) return st;
+        k_untarget<<<(m + 255) / 256, 256, 0, S->ctx->stream>>>(S->y.as<float>(), m, S->e_scale, S->t_mu, S->t_sd,
+                                                                d_pred + b0);
+        LKG_CK(cudaGetLastError(), "predict");
+        S->ctx->launches++;
+    }
+    return set_ok();
+}
+
+// Buffers for predictions of up to n_predict poses per call and training
+// batches of train_batch rows, allocated now rather than on first use.
+int lkg_surrogate_reserve(lkg_surrogate* S, int n_predict, int train_batch) {
+    if (!S || n_predict < 0 || train_batch < 0) return set_error(LKG_ERR_ARG, "bad reserve args");
+    cudaSetDevice(S->ctx->device);
+    const int nf = std::max(std::min(n_predict, PRED_CHUNK), train_batch);
+    if (nf > 0 && sur_reserve(S, nf, false)) return lkg_last_status();
+    if (train_batch > 0 && sur_reserve(S, train_batch, true)) return lkg_last_status();
     return set_ok();
 }
 
@@ -725,7 +754,7 @@ int lkg_surrogate_train(lkg_surrogate* S, int n, const double* d_poses, const do
     const int nb = n / batch;
     // one epoch = launches only (the loss is summed on the device); it is
     // captured once in a CUDA graph and replayed `epochs` times
-    if ((st = sur_reserve(S, batch)) || (st = sync_descriptors(S->ctx))) return st ? st : lkg_last_status();
+    if ((st = sur_reserve(S, batch, true)) || (st = sync_descriptors(S->ctx))) return st ? st : lkg_last_status();
     auto epoch = [&]() -> int {
         LKG_CK(cudaMemsetAsync(S->loss.p, 0, sizeof(float), s), "mlp loss clear");
         for (int b0 = 0; b0 + batch <= n; b0 += batch) {
@@ -813,7 +842,7 @@ int lkg_surrogate_grad(lkg_surrogate* S, int n, const uint16_t* feats, const flo
                        float* grad_out, float* loss_out) {
     if (!S || n <= 0 || !feats || !targets) return set_error(LKG_ERR_ARG, "bad grad args");
     cudaSetDevice(S->ctx->device);
-    if (sur_reserve(S, n)) return lkg_last_status();
+    if (sur_reserve(S, n, true)) return lkg_last_status();
     LKG_CK(cudaMemcpy(S->X.p, feats, (size_t)n * IN * 2, cudaMemcpyHostToDevice), "grad upload");
     LKG_CK(cudaMemcpy(S->t.p, targets, (size_t)n * 4, cudaMemcpyHostToDevice), "grad upload");
     int st;

@@ -62,6 +62,7 @@ int lkg_score_device_noalloc(lkg_ctx* ctx, int complex_id, int n_pose, const dou
                                         "after the last lkg_complex_add");
     const ComplexDev& d = ctx->cx[complex_id]->d;
     if (d.flags & F_DESOLV) return set_error(LKG_ERR_ARG, "cpydock complexes are not supported without allocation");
+    if (d.iface_words) return set_error(LKG_ERR_ARG, "complexes with restraints or a membrane are not supported without allocation");
     LKG_CK(cudaSetDevice(ctx->device), "cudaSetDevice");
 
     // sizes: [work counter 16 B | status 16 B | item tables 32 B | pose counters | partials]

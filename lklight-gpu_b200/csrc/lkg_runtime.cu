@@ -311,16 +311,86 @@ int complex_create(lkg_ctx* ctx, int family, unsigned flags, int lj_form, const 
     cr->d.lj_form = lj_form;
     cr->d.solv_const = solv_const;
     ctx->cx.push_back(std::move(cr));
-    ctx->cx_dirty = true;
+    mark_dirty(ctx);
     *out_id = (int)ctx->cx.size() - 1;
     return set_ok();
 }
 
 int complex_set_ligand(lkg_ctx* ctx, int id, const MolIn& lig) {
     if (id < 0 || id >= (int)ctx->cx.size()) return set_error(LKG_ERR_ARG, "bad complex id %d", id);
-    int st = build_ligand(ctx, lig, *ctx->cx[id]);
-    ctx->cx_dirty = true;
+    ComplexRec& cr = *ctx->cx[id];
+    int st = build_ligand(ctx, lig, cr);
+    // interface tags refer to the old ligand's atoms
+    cr.d.rtag = nullptr; cr.d.ltag = nullptr;
+    cr.d.nres_r = cr.d.nres_l = cr.d.nmem = cr.d.iface_words = 0;
+    cr.d.iface_form = IF_NONE;
+    mark_dirty(ctx);
     return st;
+}
+
+// Interface tags of one complex in kernel atom order (see
+// lkg_complex_set_restraints).
+int complex_set_restraints(lkg_ctx* ctx, int id, const int32_t* rres, int nres_r, const int32_t* lres, int nres_l,
+                           const int32_t* mem, int nmem) {
+    if (id < 0 || id >= (int)ctx->cx.size()) return set_error(LKG_ERR_ARG, "bad complex id %d", id);
+    if (nres_r < 0 || nres_l < 0 || nmem < 0 || (nres_r && !rres) || (nres_l && !lres) || (nmem && !mem))
+        return set_error(LKG_ERR_ARG, "bad restraint arguments");
+    ComplexRec& cr = *ctx->cx[id];
+    const int nr = cr.d.nr, nl = cr.d.nl;
+    const long long total = (long long)nres_r + nres_l + nmem;
+    if (total > (1ll << 24)) return set_error(LKG_ERR_ARG, "too many restraint residues and membrane beads");
+    // the reference's restraint maps hold only residues that have atoms
+    auto check = [&](const int32_t* res, int n_atoms, int nres, const char* side) -> int {
+        if (!nres) return 0;
+        std::vector<char> seen(nres, 0);
+        for (int i = 0; i < n_atoms; ++i) {
+            const int r = res[i];
+            if (r < -1 || r >= nres) return set_error(LKG_ERR_ARG, "%s atom %d: residue %d out of range", side, i, r);
+            if (r >= 0) seen[r] = 1;
+        }
+        for (int r = 0; r < nres; ++r)
+            if (!seen[r]) return set_error(LKG_ERR_ARG, "%s restraint residue %d has no atom", side, r);
+        return 0;
+    };
+    int st;
+    if ((st = check(rres, nr, nres_r, "receptor")) || (st = check(lres, nl, nres_l, "ligand"))) return st;
+    std::vector<int> mbit(nr, -1);
+    for (int m = 0; m < nmem; ++m) {
+        if (mem[m] < 0 || mem[m] >= nr) return set_error(LKG_ERR_ARG, "membrane bead %d: atom %d out of range", m, mem[m]);
+        if (mbit[mem[m]] >= 0) return set_error(LKG_ERR_ARG, "membrane atom %d listed twice", mem[m]);
+        mbit[mem[m]] = nres_r + nres_l + m;
+    }
+    if (total == 0) {   // cleared
+        cr.d.rtag = nullptr; cr.d.ltag = nullptr;
+        cr.d.nres_r = cr.d.nres_l = cr.d.nmem = cr.d.iface_words = 0;
+        cr.d.iface_form = IF_NONE;
+        mark_dirty(ctx);
+        return set_ok();
+    }
+    std::vector<int> rorig(nr), lorig(nl);
+    LKG_CK(cudaStreamSynchronize(ctx->stream), "restraints");
+    LKG_CK(cudaMemcpy(rorig.data(), cr.d.rorig, nr * sizeof(int), cudaMemcpyDeviceToHost), "restraints");
+    LKG_CK(cudaMemcpy(lorig.data(), cr.d.lorig, nl * sizeof(int), cudaMemcpyDeviceToHost), "restraints");
+    std::vector<int2> rt(nr);
+    std::vector<int> lt(nl);
+    for (int k = 0; k < nr; ++k) {
+        const int o = rorig[k];
+        rt[k] = make_int2(nres_r ? rres[o] : -1, mbit[o]);
+    }
+    for (int j = 0; j < nl; ++j) {
+        const int r = nres_l ? lres[lorig[j]] : -1;
+        lt[j] = r >= 0 ? nres_r + r : -1;
+    }
+    LKG_CK(upload(cr.rtag, rt, ctx->stream), "restraint tags");
+    LKG_CK(upload(cr.ltag, lt, ctx->stream), "restraint tags");
+    LKG_CK(cudaStreamSynchronize(ctx->stream), "restraint tags");
+    cr.d.rtag = cr.rtag.as<int2>();
+    cr.d.ltag = cr.ltag.as<int>();
+    cr.d.nres_r = nres_r; cr.d.nres_l = nres_l; cr.d.nmem = nmem;
+    cr.d.iface_words = (int)((total + 31) / 32);
+    cr.d.iface_form = cr.family == LKG_DNA ? IF_DNA : cr.family == LKG_VDW ? IF_VDW : IF_SUM;
+    mark_dirty(ctx);
+    return set_ok();
 }
 
 int sync_descriptors(lkg_ctx* ctx) {
@@ -333,7 +403,7 @@ int sync_descriptors(lkg_ctx* ctx) {
     return 0;
 }
 
-cudaError_t Scratch::ensure(size_t units, size_t poses, cudaStream_t s) {
+cudaError_t Scratch::ensure(size_t units, size_t poses, cudaStream_t s, size_t iface_words) {
     cudaError_t e;
     if (!status.p) {
         if ((e = work_counter.reserve(2 * sizeof(unsigned long long))) != cudaSuccess) return e;
@@ -353,6 +423,12 @@ cudaError_t Scratch::ensure(size_t units, size_t poses, cudaStream_t s) {
         if ((e = pose_counter.reserve(poses * sizeof(int))) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(pose_counter.p, 0, poses * sizeof(int), s)) != cudaSuccess) return e;
         cap_poses = poses;
+    }
+    if (iface_words > cap_iface) {   // zero between launches (the kernels clear what they set)
+        if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
+        if ((e = iface.reserve(iface_words * sizeof(unsigned))) != cudaSuccess) return e;
+        cap_iface = iface.bytes / sizeof(unsigned);
+        if ((e = cudaMemsetAsync(iface.p, 0, iface.bytes, s)) != cudaSuccess) return e;
     }
     return cudaSuccess;
 }
@@ -385,6 +461,8 @@ int build_groups(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, G
             G.inp.push_back(counts[i]);
             G.w0.push_back(G.w0.back() + (k ? (long long)counts[i] : (long long)counts[i] * d.ntiles));
             G.hcap = std::max(G.hcap, d.hcap);
+            // one stride for both groups: a pose's bits sit at pose * stride
+            g[0].iface_words = g[1].iface_words = std::max(g[0].iface_words, d.iface_words);
         }
         pose0 += counts[i];
     }
@@ -394,7 +472,7 @@ int build_groups(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, G
 
 int launch_group(lkg_ctx* ctx, const Group& G, const char* db, Scratch& sc, const double* d_poses,
                  double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e, float* atom_v,
-                 const unsigned char* pose_mask) {
+                 const unsigned char* pose_mask, double* d_iface) {
     const bool exact = ctx->precision == LKG_PREC_EXACT;
     const int ni = (int)G.ic.size();
     LaunchParams p{};
@@ -420,6 +498,15 @@ int launch_group(lkg_ctx* ctx, const Group& G, const char* db, Scratch& sc, cons
     p.atom_elec = atom_e;
     p.atom_vdw = atom_v;
     p.pose_mask = pose_mask;
+    for (int c : G.ic)   // restraints set after the groups were built (a plan made before)
+        if (ctx->cx[c]->d.iface_words > G.iface_words)
+            return set_error(LKG_ERR_STATE, "complex %d has restraints the prepared batch has no room for", c);
+    if (G.iface_words > 0) {   // callers size sc.iface for their poses x stride
+        if (!sc.iface.p) return set_error(LKG_ERR_STATE, "interface scratch missing");
+        p.iface = sc.iface.as<unsigned>();
+        p.iface_stride = G.iface_words;
+    }
+    p.iface_out = d_iface;
     cudaError_t e;
     if (G.kind == 0) {
         int threads = ctx->tile;
@@ -443,7 +530,7 @@ int launch_group(lkg_ctx* ctx, const Group& G, const char* db, Scratch& sc, cons
 
 int launch_items(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, const double* d_poses,
                  double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e,
-                 float* atom_v) {
+                 float* atom_v, double* d_iface) {
     if (n_items <= 0) return set_ok();
     Group g[2];
     size_t n_poses = 0;
@@ -452,7 +539,7 @@ int launch_items(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, c
     if (n_poses == 0) return set_ok();
     if ((st = sync_descriptors(ctx))) return st;
     const size_t units = std::max<size_t>(g[0].w0.back(), 1);
-    LKG_CK(ctx->scratch.ensure(units, n_poses, ctx->stream), "scratch");
+    LKG_CK(ctx->scratch.ensure(units, n_poses, ctx->stream, n_poses * (size_t)g[0].iface_words), "scratch");
     const size_t b0 = (g[0].bytes() + 255) & ~(size_t)255, b1 = (g[1].bytes() + 255) & ~(size_t)255;
     std::vector<char> packed(b0 + b1, 0);
     g[0].pack(packed.data());
@@ -470,7 +557,7 @@ int launch_items(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, c
     for (int k = 0; k < 2; ++k) {
         if (g[k].ic.empty()) continue;
         st = launch_group(ctx, g[k], ctx->d_items.as<char>() + (k ? b0 : 0), ctx->scratch, d_poses, d_scores, d_parts,
-                          raw_pairs, solv_only, atom_e, atom_v);
+                          raw_pairs, solv_only, atom_e, atom_v, nullptr, d_iface);
         if (st) return st;
     }
     return set_ok();
@@ -499,6 +586,10 @@ int check_status_word(int* d_status) {
     if (h[0] & 1) {
         cudaMemset(d_status, 0, sizeof(h));
         return set_error(LKG_ERR_CAPACITY, "desolvation hash overflow (too many receptor atoms within 6.4 A of one pose)");
+    }
+    if (h[0] & 2) {
+        cudaMemset(d_status, 0, sizeof(h));
+        return set_error(LKG_ERR_STATE, "restraints or membrane set after the batch was prepared: prepare it again");
     }
     return set_ok();
 }
@@ -696,31 +787,56 @@ int lkg_score_multi_device(lkg_ctx* ctx, int n_items, const int* ids, const int*
     return launch_items(ctx, n_items, ids, counts, d_poses, d_scores, d_parts, 0, 0, nullptr, nullptr);
 }
 
-int lkg_score(lkg_ctx* ctx, int id, int n, const double* poses, double* scores, double* parts) {
+// host-buffer scoring of one complex; parts (N x 4) and iface (N x 3) optional
+static int score_host(lkg_ctx* ctx, int id, int n, const double* poses, double* scores, double* parts,
+                      double* iface) {
     if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
     if (n == 0) return set_ok();
     if (n < 0 || !poses || !scores) return set_error(LKG_ERR_ARG, "bad pose buffer");
     cudaSetDevice(ctx->device);
-    const size_t pb = (size_t)n * 7 * sizeof(double), ob = (size_t)n * sizeof(double), qb = (size_t)n * 4 * sizeof(double);
+    const size_t pb = (size_t)n * 7 * sizeof(double), ob = (size_t)n * sizeof(double),
+                 qb = (size_t)n * 4 * sizeof(double), ib = (size_t)n * 3 * sizeof(double);
     LKG_CK(ctx->h_poses.reserve(pb), "staging");
-    LKG_CK(ctx->h_out.reserve(ob + qb), "staging");
+    LKG_CK(ctx->h_out.reserve(ob + qb + ib), "staging");
     LKG_CK(ctx->d_poses.reserve(pb), "staging");
     LKG_CK(ctx->d_scores.reserve(ob), "staging");
-    LKG_CK(ctx->d_parts.reserve(qb), "staging");
+    LKG_CK(ctx->d_parts.reserve(qb + ib), "staging");
     memcpy(ctx->h_poses.p, poses, pb);
     LKG_CK(cudaMemcpyAsync(ctx->d_poses.p, ctx->h_poses.p, pb, cudaMemcpyHostToDevice, ctx->stream), "pose upload");
+    double* d_iface = iface ? (double*)(ctx->d_parts.as<char>() + qb) : nullptr;
+    if (iface) LKG_CK(cudaMemsetAsync(d_iface, 0, ib, ctx->stream), "interface output");
     int st = launch_items(ctx, 1, &id, &n, ctx->d_poses.as<double>(), ctx->d_scores.as<double>(),
-                          parts ? ctx->d_parts.as<double>() : nullptr, 0, 0, nullptr, nullptr);
+                          parts ? ctx->d_parts.as<double>() : nullptr, 0, 0, nullptr, nullptr, d_iface);
     if (st) return st;
     LKG_CK(cudaMemcpyAsync(ctx->h_out.p, ctx->d_scores.p, ob, cudaMemcpyDeviceToHost, ctx->stream), "score readback");
     if (parts)
         LKG_CK(cudaMemcpyAsync(ctx->h_out.as<char>() + ob, ctx->d_parts.p, qb, cudaMemcpyDeviceToHost, ctx->stream),
                "parts readback");
+    if (iface)
+        LKG_CK(cudaMemcpyAsync(ctx->h_out.as<char>() + ob + qb, d_iface, ib, cudaMemcpyDeviceToHost, ctx->stream),
+               "interface readback");
     if ((st = wait_stream(ctx, 300.0))) return st;
     if ((st = check_status(ctx))) return st;
     memcpy(scores, ctx->h_out.p, ob);
     if (parts) memcpy(parts, ctx->h_out.as<char>() + ob, qb);
+    if (iface) memcpy(iface, ctx->h_out.as<char>() + ob + qb, ib);
     return set_ok();
+}
+
+int lkg_score(lkg_ctx* ctx, int id, int n, const double* poses, double* scores, double* parts) {
+    return score_host(ctx, id, n, poses, scores, parts, nullptr);
+}
+
+int lkg_score_interface(lkg_ctx* ctx, int id, int n, const double* poses, double* scores, double* iface) {
+    if (!iface) return set_error(LKG_ERR_ARG, "null interface output");
+    return score_host(ctx, id, n, poses, scores, nullptr, iface);
+}
+
+int lkg_complex_set_restraints(lkg_ctx* ctx, int id, const int32_t* rec_residue, int n_rec_res,
+                               const int32_t* lig_residue, int n_lig_res, const int32_t* membrane, int n_membrane) {
+    if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
+    cudaSetDevice(ctx->device);
+    return complex_set_restraints(ctx, id, rec_residue, n_rec_res, lig_residue, n_lig_res, membrane, n_membrane);
 }
 
 int lkg_score_multi(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, const double* poses,
@@ -811,6 +927,7 @@ struct lkg_plan {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     const void* captured_cx = nullptr;
+    uint64_t captured_version = 0;
     int captured_launches = 0;
 };
 
@@ -832,8 +949,8 @@ int lkg_plan_create(lkg_ctx* ctx, int n_items, const int* ids, const int* counts
     cudaError_t e;
     if ((e = P->d_tables.reserve(b0 + b1)) != cudaSuccess ||
         (e = cudaMemcpy(P->d_tables.p, packed.data(), b0 + b1, cudaMemcpyHostToDevice)) != cudaSuccess ||
-        (e = P->scratch.ensure(std::max<size_t>(P->g[0].w0.back(), 1), std::max<size_t>(P->n_poses, 1), ctx->stream)) !=
-            cudaSuccess ||
+        (e = P->scratch.ensure(std::max<size_t>(P->g[0].w0.back(), 1), std::max<size_t>(P->n_poses, 1), ctx->stream,
+                               P->n_poses * (size_t)P->g[0].iface_words)) != cudaSuccess ||
         (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) {
         delete P;
         return set_error(cuda_to_status(e), "plan setup: %s", cudaGetErrorString(e));
@@ -844,6 +961,13 @@ int lkg_plan_create(lkg_ctx* ctx, int n_items, const int* ids, const int* counts
 
 int lkg_plan_launch(lkg_plan* P, const double* d_poses, double* d_scores, double* d_parts) {
     if (!P || !d_poses || !d_scores) return set_error(LKG_ERR_ARG, "bad plan launch");
+    if (P->ctx->cx_dirty) {   // a complex changed since the plan was made: upload its descriptor first
+        cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+        cudaStreamIsCapturing(P->ctx->stream, &cs);
+        if (cs != cudaStreamCaptureStatusNone) return set_error(LKG_ERR_STATE, "complexes changed during capture");
+        int st = sync_descriptors(P->ctx);
+        if (st) return st;
+    }
     for (int k = 0; k < 2; ++k) {
         if (P->g[k].ic.empty()) continue;
         int st = launch_group(P->ctx, P->g[k], P->d_tables.as<char>() + (k ? P->b0 : 0), P->scratch, d_poses,
@@ -889,14 +1013,15 @@ int lkg_plan_capture(lkg_plan* P, const double* d_poses, double* d_scores, doubl
     P->graph = g;
     LKG_CK(cudaGraphInstantiate(&P->exec, g, 0), "graph instantiate");
     P->captured_cx = ctx->d_cx.p;
+    P->captured_version = ctx->cx_version;
     P->captured_launches = n_launches * ((P->g[0].ic.empty() ? 0 : 1) + (P->g[1].ic.empty() ? 0 : 1));
     return set_ok();
 }
 
 int lkg_plan_replay(lkg_plan* P) {
     if (!P || !P->exec) return set_error(LKG_ERR_STATE, "no captured graph");
-    if (P->captured_cx != P->ctx->d_cx.p)
-        return set_error(LKG_ERR_STATE, "complexes were added after capture; capture again");
+    if (P->captured_cx != P->ctx->d_cx.p || P->captured_version != P->ctx->cx_version)
+        return set_error(LKG_ERR_STATE, "complexes were added or changed after capture; capture again");
     cudaSetDevice(P->ctx->device);
     LKG_CK(cudaGraphLaunch(P->exec, P->ctx->stream), "graph launch");
     P->ctx->launches += P->captured_launches;

@@ -82,6 +82,7 @@ struct ComplexRec {
     DBuf rpos, rpar, rsolv, rpos64, rpar64, rsolv64, rorig, cell_start;
     DBuf lpos, lpar, lsolv, lpos64, lpar64, lsolv64, lorig, lgrp;
     DBuf phi;
+    DBuf rtag, ltag;   // interface tags (restraints / membrane), when set
     ComplexDev d{};
     int n_cells = 0;
 };
@@ -91,9 +92,10 @@ struct Occupancy { int threads = 0, hcap = 0, blocks = 0; };
 // per-launch scratch: per-unit partial sums, per-pose counters, the work
 // counter and the status word (counters reset themselves after a launch)
 struct Scratch {
-    DBuf partials, pose_counter, work_counter, status;
-    size_t cap_units = 0, cap_poses = 0;
-    cudaError_t ensure(size_t units, size_t poses, cudaStream_t s);
+    DBuf partials, pose_counter, work_counter, status, iface;
+    size_t cap_units = 0, cap_poses = 0, cap_iface = 0;
+    // iface_words: interface bit words of the whole batch (poses x stride)
+    cudaError_t ensure(size_t units, size_t poses, cudaStream_t s, size_t iface_words = 0);
 };
 
 // one launch group's item tables: (complex, first pose, pose count) per item
@@ -103,6 +105,7 @@ struct Group {
     std::vector<int> ic, ip0, inp;
     std::vector<long long> w0{0};
     int hcap = 64;
+    int iface_words = 0;   // interface bit words per pose (the batch's largest)
     size_t bytes() const { return (ic.size() + 1) * sizeof(long long) + ic.size() * 3 * sizeof(int); }
     void pack(char* dst) const;
 };
@@ -123,6 +126,7 @@ struct lkg_ctx {
     std::vector<std::unique_ptr<lkg::ComplexRec>> cx;
     lkg::DBuf d_cx;                 // ComplexDev[] on the device
     bool cx_dirty = true;
+    uint64_t cx_version = 0;        // bumped by every change of a complex (captured graphs check it)
     lkg::Scratch scratch;
     // item tables
     lkg::DBuf d_items;
@@ -143,10 +147,15 @@ int complex_create(lkg_ctx* ctx, int family, unsigned flags, int lj_form, const 
                    int* out_id);
 // replace the ligand of an existing complex (cuda_full_score)
 int complex_set_ligand(lkg_ctx* ctx, int id, const MolIn& lig);
+// a complex changed: descriptors to upload, captured graphs out of date
+inline void mark_dirty(lkg_ctx* ctx) { ctx->cx_dirty = true; ++ctx->cx_version; }
+// interface tags (restraints / membrane) of a complex, caller atom order
+int complex_set_restraints(lkg_ctx* ctx, int id, const int32_t* rres, int nres_r, const int32_t* lres, int nres_l,
+                           const int32_t* mem, int nmem);
 // one persistent launch group over items; device pointers
 int launch_items(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, const double* d_poses,
                  double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e,
-                 float* atom_v);
+                 float* atom_v, double* d_iface = nullptr);
 int wait_stream(lkg_ctx* ctx, double timeout_s);
 int check_status(lkg_ctx* ctx);
 int check_status_word(int* d_status);
@@ -156,7 +165,7 @@ int sync_descriptors(lkg_ctx* ctx);
 // launch one prepared group (kernel launches only: stream-capturable)
 int launch_group(lkg_ctx* ctx, const Group& g, const char* d_tables, Scratch& sc, const double* d_poses,
                  double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e, float* atom_v,
-                 const unsigned char* pose_mask = nullptr);
+                 const unsigned char* pose_mask = nullptr, double* d_iface = nullptr);
 // a plan's launch group(s) scoring only the poses whose mask byte is set
 int plan_launch_masked(lkg_plan* plan, const double* d_poses, double* d_scores, const unsigned char* d_mask);
 void field_geometry(const double* coords, int n, double lo[3], int dims[3], double* spacing);

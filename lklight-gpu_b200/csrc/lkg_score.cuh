@@ -254,6 +254,67 @@ struct MinHash {
 };
 
 // ------------------------------------------------------------------------
+// interface flags (restraints and membrane; dna.rs:885-897,970-973,
+// scoring.rs:83-108): a pair within INTERFACE_CUTOFF sets the bits of both
+// atoms' restraint residues and of the receptor atom's membrane bead
+// ------------------------------------------------------------------------
+// the pose's interface bits, or null when its complex has none; a launch
+// without room for them flags status bit 2 (the host reports it)
+__device__ __forceinline__ unsigned* iface_bits(const LaunchParams& p, const ComplexDev& c, long long g) {
+    if (!c.iface_words) return nullptr;
+    if (!p.iface || c.iface_words > p.iface_stride) { atomicOr(p.status, 2); return nullptr; }
+    return p.iface + (size_t)g * p.iface_stride;
+}
+
+__device__ __forceinline__ void iface_set(unsigned* bits, int b) {
+    if (b >= 0) atomicOr(bits + (b >> 5), 1u << (b & 31));
+}
+
+// receptor atom k (sorted order) and a ligand atom with tag lt at squared
+// distance d2 (f64)
+__device__ __forceinline__ void iface_mark(const ComplexDev& c, unsigned* bits, int k, int lt, double d2) {
+    if (!(d2 <= IFACE2_D)) return;
+    const int2 rt = c.rtag[k];
+    iface_set(bits, rt.x);
+    iface_set(bits, rt.y);
+    iface_set(bits, lt);
+}
+
+// set bits in [a, b)
+__device__ __forceinline__ int iface_count(const unsigned* bits, int a, int b) {
+    int n = 0;
+    for (int w = a >> 5; a < b && w <= ((b - 1) >> 5); ++w) {
+        unsigned m = __ldcg(bits + w);
+        const int lo = w * 32;
+        if (a > lo) m &= ~0u << (a - lo);
+        if (b < lo + 32) m &= (1u << (b - lo)) - 1u;
+        n += __popc(m);
+    }
+    return n;
+}
+
+// the pose's restraint fractions and membrane intersection
+// (satisfied_restraints, membrane_intersection: scoring.rs:83-108) applied
+// to score s in the family's operation order, without contraction; the
+// bits are cleared for the next launch.  f (optional): pr, pl, intersection
+__device__ __forceinline__ double iface_apply(const ComplexDev& c, unsigned* bits, double s, double* f) {
+    const int nr = c.nres_r, nl = c.nres_l, nm = c.nmem;
+    const int cr = iface_count(bits, 0, nr), cl = iface_count(bits, nr, nr + nl);
+    const int cm = iface_count(bits, nr + nl, nr + nl + nm);
+    for (int w = 0; w < c.iface_words; ++w) bits[w] = 0u;
+    const double pr = nr ? (double)cr / (double)nr : 0.0;
+    const double pl = nl ? (double)cl / (double)nl : 0.0;
+    const double inter = nm ? (double)cm / (double)nm : 0.0;
+    const double pen = inter > 0.0 ? __dmul_rn(MEMBRANE_PENALTY, inter) : 0.0;
+    if (f) { f[0] = pr; f[1] = pl; f[2] = inter; }
+    switch (c.iface_form) {
+        case IF_DNA: return __dadd_rn(s, __dsub_rn(__dadd_rn(__dmul_rn(pr, s), __dmul_rn(pl, s)), pen));
+        case IF_VDW: return __dadd_rn(__dadd_rn(s, __dmul_rn(pr, s)), __dmul_rn(pl, s));
+        default: return __dsub_rn(__dadd_rn(__dadd_rn(s, __dmul_rn(pr, s)), __dmul_rn(pl, s)), pen);
+    }
+}
+
+// ------------------------------------------------------------------------
 // per-atom work
 // ------------------------------------------------------------------------
 template <typename R> struct Atom;
@@ -263,11 +324,11 @@ template <> struct Atom<float> {
     template <bool DESOLV>
     __device__ static void run(const ComplexDev& c, const Rot& rot, int j, AtomAcc& acc,
                                double& min_l, MinHash* hash, int* status,
-                               float* out_e, float* out_v) {
+                               float* out_e, float* out_v, unsigned* ibits) {
         float4 b = Tr<float>::lpos(c, j);
         float4 lp = Tr<float>::lpar(c, j);
         double xd, yd, zd;
-        if (DESOLV) {
+        if (DESOLV || ibits) {   // f64 base coordinates (exact distances for the minima / interface)
             double4 b64 = c.lpos64[j];
             apply(rot, b64.x, b64.y, b64.z, xd, yd, zd);
         } else {
@@ -285,6 +346,7 @@ template <> struct Atom<float> {
         // far field with the reference's f64 interpolation (per atom, cheap)
         if ((flags & F_FAR) && qj != 0.f) elec += c.lpos64[j].w * sample_phi(c, xd, yd, zd);
         int np = 0;
+        const int lt = ibits ? c.ltag[j] : -1;
         scan_rows(c, x, y, z, [&](int k) {
             float4 a = Tr<float>::rpos(c, k);
             float dx = (x - a.x) + xl, dy = (y - a.y) + yl, dz = (z - a.z) + zl;
@@ -303,6 +365,11 @@ template <> struct Atom<float> {
                     min_l = fmin(min_l, d2d);
                     if (d2d <= SOLV2_D && !hash->insert(k, d2d)) atomicOr(status, 1);
                 }
+                if (ibits && d2 <= IFACE2_F) {
+                    const double4 a64 = c.rpos64[k];
+                    const double ex = xd - a64.x, ey = yd - a64.y, ez = zd - a64.z;
+                    iface_mark(c, ibits, k, lt, ex * ex + ey * ey + ez * ez);
+                }
             }
         });
         acc.elec += elec;
@@ -317,7 +384,7 @@ template <> struct Atom<double> {
     template <bool DESOLV>
     __device__ static void run(const ComplexDev& c, const Rot& rot, int j, AtomAcc& acc,
                                double& min_l, MinHash* hash, int* status,
-                               float* out_e, float* out_v) {
+                               float* out_e, float* out_v, unsigned* ibits) {
         double4 b = Tr<double>::lpos(c, j);
         double4 lp = Tr<double>::lpar(c, j);
         double x, y, z;
@@ -330,6 +397,7 @@ template <> struct Atom<double> {
         double elec = 0.0, vdw = 0.0, far = 0.0;
         if ((flags & F_FAR) && qj != 0.0) far = qj * sample_phi(c, x, y, z);
         int np = 0;
+        const int lt = ibits ? c.ltag[j] : -1;
         scan_rows(c, (float)x, (float)y, (float)z, [&](int k) {
             double4 a = Tr<double>::rpos(c, k);
             double dx = x - a.x, dy = y - a.y, dz = z - a.z;
@@ -342,6 +410,7 @@ template <> struct Atom<double> {
                     min_l = fmin(min_l, d2);
                     if (d2 <= SOLV2_D && !hash->insert(k, d2)) atomicOr(status, 1);
                 }
+                if (ibits) iface_mark(c, ibits, k, lt, d2);
             }
         });
         acc.elec += elec + far;
@@ -398,11 +467,16 @@ __device__ __forceinline__ int find_item(const long long* __restrict__ work0, in
 // final per-pose output (family combination: gpu_score.rs:326-331,
 // gpu_family.rs:283-308, cpydock.rs:789-791; CPU-grid cpydock adds the
 // constant asa<0 term, cpydock.rs:648-668)
+// With interface bits (ibits) the score is combined with the restraint
+// fractions and the membrane penalty (iface_apply).
 __device__ __forceinline__ void write_pose(const LaunchParams& p, const ComplexDev& c, long long g,
-                                           double elec, double vdw, double solv, double np) {
-    if (p.raw_pairs) { p.scores[2 * g] = elec; p.scores[2 * g + 1] = vdw; }
-    else if (p.solv_only) { p.scores[g] = solv; }
-    else {
+                                           double elec, double vdw, double solv, double np,
+                                           unsigned* ibits = nullptr) {
+    if (p.raw_pairs || p.solv_only) {
+        if (p.raw_pairs) { p.scores[2 * g] = elec; p.scores[2 * g + 1] = vdw; }
+        else p.scores[g] = solv;
+        if (ibits) for (int w = 0; w < c.iface_words; ++w) ibits[w] = 0u;
+    } else {
         double s;
         double ek = elec * FACTOR / EPSILON;
         if (c.flags & F_DESOLV) {
@@ -414,6 +488,7 @@ __device__ __forceinline__ void write_pose(const LaunchParams& p, const ComplexD
         } else {
             s = -(ek + vdw);
         }
+        if (ibits) s = iface_apply(c, ibits, s, p.iface_out ? p.iface_out + 3 * g : nullptr);
         p.scores[g] = s;
     }
     if (p.parts) {
@@ -449,13 +524,15 @@ __global__ void __launch_bounds__(256) k_score_tiles(LaunchParams p) {
         if (p.pose_mask && !p.pose_mask[g]) continue;   // block-uniform: pose skipped
         const int j = tile * p.tile + threadIdx.x;
         AtomAcc acc{0.0, 0.0, 0};
+        unsigned* ibits = iface_bits(p, c, g);
         if (j < c.nl && threadIdx.x < p.tile) {
             const Rot rot = pose_matrix(p.poses + 7 * g);
             double dummy_min = 0.0;
             const bool atom_out = p.atom_elec && b == 0 && pose == 0;
             Atom<R>::template run<false>(c, rot, j, acc, dummy_min, nullptr, p.status,
-                                         atom_out ? p.atom_elec : nullptr, atom_out ? p.atom_vdw : nullptr);
+                                         atom_out ? p.atom_elec : nullptr, atom_out ? p.atom_vdw : nullptr, ibits);
         }
+        if (ibits) __threadfence();   // interface bits before the unit is published
         double v[3] = {acc.elec, acc.vdw, (double)acc.np};
         block_sum<3>(v, s_red);
         if (threadIdx.x == 0) {
@@ -471,7 +548,7 @@ __global__ void __launch_bounds__(256) k_score_tiles(LaunchParams p) {
                 for (int t = 0; t < c.ntiles; ++t) {
                     e += __ldcg(pp + 4 * t); vv += __ldcg(pp + 4 * t + 1); np += __ldcg(pp + 4 * t + 3);
                 }
-                write_pose(p, c, g, e, vv, 0.0, np);
+                write_pose(p, c, g, e, vv, 0.0, np, ibits);
                 p.pose_counter[g] = 0;
             }
         }
@@ -503,13 +580,14 @@ __global__ void __launch_bounds__(512) k_score_desolv(LaunchParams p) {
         hash.init(smem, c.hcap);
         __syncthreads();
         const Rot rot = pose_matrix(p.poses + 7 * g);
+        unsigned* ibits = iface_bits(p, c, g);
         AtomAcc acc{0.0, 0.0, 0};
         double solv_l = 0.0;
         const bool want_pairs = !p.solv_only;
         for (int j = threadIdx.x; j < c.nl; j += blockDim.x) {
             double min_l = 1e300;
             AtomAcc a1{0.0, 0.0, 0};
-            Atom<R>::template run<true>(c, rot, j, a1, min_l, &hash, p.status, nullptr, nullptr);
+            Atom<R>::template run<true>(c, rot, j, a1, min_l, &hash, p.status, nullptr, nullptr, ibits);
             if (want_pairs) { acc.elec += a1.elec; acc.vdw += a1.vdw; }
             acc.np += a1.np;
             double2 ls = c.lsolv64[j];
@@ -533,7 +611,7 @@ __global__ void __launch_bounds__(512) k_score_desolv(LaunchParams p) {
             long long f = 0;
             for (int i = 0; i < (int)((blockDim.x + 31) >> 5); ++i) f += s_fix[i];
             double solv = v[2] + (double)f * (1.0 / 1099511627776.0);
-            write_pose(p, c, g, v[0], v[1], solv, v[3]);
+            write_pose(p, c, g, v[0], v[1], solv, v[3], ibits);
         }
         __syncthreads();
     }

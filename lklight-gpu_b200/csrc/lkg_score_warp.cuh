@@ -60,6 +60,8 @@ struct WSlots {
     float4 lres[2 * G];         // x, y, z residuals, sqrt eps
     float4 ltest[2 * G];        // candidate test: -2 l', |l'|^2 - 100.01 (l' = l - group centre)
     float2 lpar[2 * G];         // r, heavy
+    int ltag[2 * G];            // IFACE: restraint bit of the slot atom, -1 = none
+    unsigned* ibits;            // IFACE: interface bits of the current pose (null: none)
     unsigned hit[WRing<G>::N];  // (slot << 26) | receptor index
 };
 
@@ -68,8 +70,11 @@ struct WSlots {
 // the LJ power taken as (rr^2 / d^2)^3) and the clash term selected instead
 // of branched on.  DESOLV: pairs that can lie within 6.4 A also update both
 // atoms' minimum distance in f64 (cpydock.rs:615-668), the ligand atom's in
-// its slot, the receptor atom's in the block's hash.
-template <int G, bool DESOLV>
+// its slot, the receptor atom's in the block's hash.  IFACE: pairs that can
+// lie within 3.9 A and involve a tagged atom are re-tested in f64 (the slot
+// position as f32 value + residual, ~2^-48 relative) and set the pose's
+// interface bits.
+template <int G, bool DESOLV, bool IFACE>
 __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, WDes<G>* D, MinHash* hash,
                                        int* status, unsigned e, unsigned flags, double& elec, double& vdw, int& np) {
     const int l = (int)(e >> 26), k = (int)(e & 0x3ffffffu);
@@ -105,6 +110,25 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
         atomicMin(&D->lmin[l], (unsigned long long)__double_as_longlong(d2d));
         if (d2d <= SOLV2_D && !hash->insert(k, d2d)) atomicOr(status, 1);
     }
+    if (IFACE && d2 <= IFACE2_F && W.ibits) {
+        const int2 rt = __ldg(c.rtag + k);
+        const int lt = W.ltag[l];
+        if ((rt.x & rt.y & lt) >= 0) {   // not all three -1
+            const double4 a64 = c.rpos64[k];
+            double ex, ey, ez;
+            if (DESOLV) { ex = D->lx[l] - a64.x; ey = D->ly[l] - a64.y; ez = D->lz[l] - a64.z; }
+            else {
+                ex = ((double)lp.x + (double)lr.x) - a64.x;
+                ey = ((double)lp.y + (double)lr.y) - a64.y;
+                ez = ((double)lp.z + (double)lr.z) - a64.z;
+            }
+            if (ex * ex + ey * ey + ez * ez <= IFACE2_D) {
+                iface_set(W.ibits, rt.x);
+                iface_set(W.ibits, rt.y);
+                iface_set(W.ibits, lt);
+            }
+        }
+    }
 }
 
 // receptor atom of candidate kk of the current rows: the span is the last
@@ -134,7 +158,7 @@ struct WAcc {
 // Scores groups g_first, g_first + g_step, ... (< g_end) of one pose whose
 // rotation is in W.rot, into acc (per lane).  DESOLV also adds each slot
 // atom's g(min d^2) * des to acc.solv once its hits are all evaluated.
-template <int G, bool DESOLV>
+template <int G, bool DESOLV, bool IFACE>
 __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes<G>* D, MinHash* hash, int* status,
                                          int g_first, int g_end, int g_step, WAcc& acc) {
     constexpr int RING = WRing<G>::N;
@@ -147,7 +171,7 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
     int jdes0 = -1, jdes1 = -1;   // DESOLV: this lane's slot atom in set 0 / set 1
     auto drain_partial = [&]() {
         if ((int)(tail - head) > lane)
-            w_pair<G, DESOLV>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, acc.elec, acc.vdw, acc.np);
+            w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, acc.elec, acc.vdw, acc.np);
         head = tail;
     };
     auto finalize = [&](int set) {   // DESOLV: the slot set's minima are final
@@ -175,7 +199,7 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
             const float4 b4 = valid ? __ldg(c.lpos + j) : make_float4(0.f, 0.f, 0.f, 0.f);
             const float4 lp4 = valid ? __ldg(c.lpar + j) : make_float4(0.f, 0.f, 0.f, 0.f);
             double xd, yd, zd;
-            if (DESOLV) {   // the cpydock kernels transform the f64 coordinates
+            if (DESOLV || IFACE) {   // f64 base coordinates (cpydock minima, interface flags)
                 const double4 b64 = valid ? c.lpos64[j] : make_double4(0.0, 0.0, 0.0, 0.0);
                 apply(W.rot, b64.x, b64.y, b64.z, xd, yd, zd);
             } else {
@@ -191,6 +215,7 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
             W.lpos[set + lane] = make_float4(x, y, z, b4.w);
             W.lres[set + lane] = res;
             W.lpar[set + lane] = make_float2(lp4.y, lp4.z);
+            if (IFACE) W.ltag[set + lane] = (valid && c.ltag) ? __ldg(c.ltag + j) : -1;
             if (DESOLV) {
                 D->lx[set + lane] = xd; D->ly[set + lane] = yd; D->lz[set + lane] = zd;
                 D->lmin[set + lane] = W_NOMIN;
@@ -282,7 +307,7 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
                 __syncwarp();
                 // 4. full batches of 32 hits
                 while ((int)(tail - head) >= 32) {
-                    w_pair<G, DESOLV>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, acc.elec,
+                    w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, acc.elec,
                                       acc.vdw, acc.np);
                     head += 32;
                 }
@@ -296,7 +321,7 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
     finalize(G);
 }
 
-template <int G>
+template <int G, bool IFACE>
 __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchParams p) {
     static_assert(G == 4 || G == 8 || G == 16 || G == 32, "group size");
     constexpr unsigned FULL = 0xffffffffu;
@@ -316,12 +341,16 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
         const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
         if (p.pose_mask && !p.pose_mask[g]) continue;   // pose skipped: keeps its score
         __syncwarp();   // readers of the previous unit's pose are done
-        if (lane == 0) W.rot = pose_matrix(p.poses + 7 * g);
+        if (lane == 0) {
+            W.rot = pose_matrix(p.poses + 7 * g);
+            if (IFACE) W.ibits = iface_bits(p, c, g);
+        }
         __syncwarp();
         const int gpt = p.tile / G;
         const int g0 = tile * gpt, g1 = min(g0 + gpt, (c.nl + G - 1) / G);
         WAcc acc;
-        w_groups<G, false>(c, W, nullptr, nullptr, nullptr, g0, g1, 1, acc);
+        w_groups<G, false, IFACE>(c, W, nullptr, nullptr, nullptr, g0, g1, 1, acc);
+        if (IFACE && W.ibits) __threadfence();   // interface bits before the unit is published
         const double elec = warp_sum(acc.elec), vdw = warp_sum(acc.vdw);
         const long long npl = warp_sum((long long)acc.np);
         if (lane == 0) {
@@ -337,7 +366,7 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
                 for (int t = 0; t < ntiles; ++t) {
                     e += __ldcg(pp + 4 * t); vv += __ldcg(pp + 4 * t + 1); nps += __ldcg(pp + 4 * t + 3);
                 }
-                write_pose(p, c, g, e, vv, 0.0, nps);
+                write_pose(p, c, g, e, vv, 0.0, nps, IFACE ? W.ibits : nullptr);
                 p.pose_counter[g] = 0;
             }
         }
@@ -357,7 +386,7 @@ __host__ __device__ constexpr size_t wd_smem(int hcap) {
     return (size_t)hcap * 12 + (size_t)(WD_THREADS / 32) * (sizeof(WSlots<G>) + sizeof(WDes<G>));
 }
 
-template <int G>
+template <int G, bool IFACE>
 __global__ void __launch_bounds__(WD_THREADS, 1) k_score_warp_desolv(LaunchParams p) {
     constexpr int NW = WD_THREADS / 32;
     extern __shared__ __align__(16) unsigned char wd_smem_raw[];
@@ -381,10 +410,13 @@ __global__ void __launch_bounds__(WD_THREADS, 1) k_score_warp_desolv(LaunchParam
         unsigned char* base = wd_smem_raw + (size_t)c.hcap * 12;
         WSlots<G>& W = reinterpret_cast<WSlots<G>*>(base)[wid];
         WDes<G>* D = reinterpret_cast<WDes<G>*>(base + (size_t)NW * sizeof(WSlots<G>)) + wid;
-        if (lane == 0) W.rot = pose_matrix(p.poses + 7 * g);
+        if (lane == 0) {
+            W.rot = pose_matrix(p.poses + 7 * g);
+            if (IFACE) W.ibits = iface_bits(p, c, g);
+        }
         __syncthreads();   // hash cleared, poses set
         WAcc acc;
-        w_groups<G, true>(c, W, D, &hash, p.status, wid, (c.nl + G - 1) / G, NW, acc);
+        w_groups<G, true, IFACE>(c, W, D, &hash, p.status, wid, (c.nl + G - 1) / G, NW, acc);
         __syncthreads();   // every pair has updated the hash
         // receptor side: fixed-point (2^-40) sum over hash slots; slot order
         // depends on insertion races, integer sums do not
@@ -403,7 +435,7 @@ __global__ void __launch_bounds__(WD_THREADS, 1) k_score_warp_desolv(LaunchParam
             long long f = 0;
             for (int i = 0; i < NW; ++i) f += s_fix[i];
             write_pose(p, c, g, p.solv_only ? 0.0 : v[0], p.solv_only ? 0.0 : v[1],
-                       v[2] + (double)f * (1.0 / 1099511627776.0), v[3]);
+                       v[2] + (double)f * (1.0 / 1099511627776.0), v[3], IFACE ? W.ibits : nullptr);
         }
         __syncthreads();
     }

@@ -247,3 +247,31 @@ def config4(seed=19, n_glob=12625, n_lig=12000):
     lig = globule(n_lig, seed, shift=False)
     return dict(rec=add_cpydock(rec), lig=add_cpydock(lig), family="cpydock", swarms=50, glowworms=500,
                 steps=100, seed=seed)
+
+
+def restraints(rec_coords, n_lig, centres, seed, n_rec_res=20, n_lig_res=6, n_membrane=300,
+               rec_res_atoms=10, lig_res_atoms=30, reach=20.0):
+    """Synthetic active restraints and membrane for a complex whose atoms
+    carry no residues: receptor residues are blocks of `rec_res_atoms`
+    consecutive chain atoms, ligand residues blocks of `lig_res_atoms`
+    (about one nucleotide).  Restraint residues and membrane beads are drawn
+    among receptor atoms within `reach` A of the swarm centres, so that the
+    poses touch some of them.  Returns per-atom receptor / ligand restraint
+    residue indices (-1 = none) and the membrane atom indices."""
+    rng = np.random.default_rng(seed)
+    rc = np.asarray(rec_coords, np.float64)
+    near = np.zeros(len(rc), bool)
+    for c in np.asarray(centres, np.float64).reshape(-1, 3):
+        near |= np.linalg.norm(rc - c, axis=1) < reach
+    idx = np.nonzero(near)[0]
+    rres = np.minimum(np.arange(len(rc)) // rec_res_atoms, len(rc) // rec_res_atoms - 1)
+    cand = np.unique(rres[idx])
+    ract = rng.choice(cand, min(n_rec_res, len(cand)), replace=False)
+    pos = {int(r): k for k, r in enumerate(ract)}
+    rr = np.array([pos.get(int(r), -1) for r in rres], np.int32)
+    lres = np.arange(n_lig) // lig_res_atoms
+    lact = rng.choice(lres.max() + 1, min(n_lig_res, lres.max() + 1), replace=False)
+    lpos = {int(r): k for k, r in enumerate(lact)}
+    lr = np.array([lpos.get(int(r), -1) for r in lres], np.int32)
+    mem = np.sort(rng.choice(idx, min(n_membrane, len(idx)), replace=False)).astype(np.int32)
+    return rr, lr, mem

@@ -48,6 +48,8 @@ def lib():
             "orc_model_free": (V, [P]), "orc_model_field": (P, [P, C.c_int]),
             "orc_energy_grid": (D, [P, P, P, C.c_int, P]), "orc_energy_exact": (D, [P, P, P]),
             "orc_batch_energy_grid": (V, [P, I64, P, C.c_int, C.c_int, P, P]),
+            "orc_model_set_restraints": (V, [P, P, C.c_int, P, C.c_int, P, I64]),
+            "orc_batch_energy_grid_iface": (V, [P, I64, P, C.c_int, C.c_int, P, P]),
             "orc_gso_new": (P, [P, I64, P, U64, C.c_int, C.c_int]), "orc_gso_run": (V, [P, C.c_int]),
             "orc_gso_state": (V, [P, P, P, P, P, P, P, P]), "orc_gso_scored": (I64, [P]),
             "orc_gso_free": (V, [P]),
@@ -173,6 +175,24 @@ class Model:
         pa = np.zeros((len(poses), 5)) if parts else None
         lib().orc_batch_energy_grid(self.h, len(poses), _p(poses), int(fp64), threads, _p(out), _p(pa))
         return (out, pa) if parts else out
+
+    def set_restraints(self, rec_res=None, nres_r=0, lig_res=None, nres_l=0, membrane=None):
+        """Active restraints (restraint residue index per atom, -1 = none)
+        and receptor membrane bead atom indices."""
+        rr = None if not nres_r else np.ascontiguousarray(rec_res, np.int32)
+        lr = None if not nres_l else np.ascontiguousarray(lig_res, np.int32)
+        mm = None if membrane is None or len(membrane) == 0 else np.ascontiguousarray(membrane, np.int32)
+        self._keep += [rr, lr, mm]
+        lib().orc_model_set_restraints(self.h, _p(rr), int(nres_r), _p(lr), int(nres_l), _p(mm),
+                                       0 if mm is None else len(mm))
+
+    def batch_energy_grid_iface(self, poses, fp64=False, threads=0):
+        """Scores and per-pose (pr, pl, membrane intersection)."""
+        poses = _f64(poses).reshape(-1, 7)
+        out = np.zeros(len(poses))
+        f = np.zeros((len(poses), 3))
+        lib().orc_batch_energy_grid_iface(self.h, len(poses), _p(poses), int(fp64), threads, _p(out), _p(f))
+        return out, f
 
     def __del__(self):
         if getattr(self, "h", None):

@@ -388,6 +388,8 @@ const double CLOSE_DIST2 = CLOSE_DIST * CLOSE_DIST;     // == VDW_DIST_CUTOFF2
 const double ELEC_DIST_CUTOFF2 = 30.0 * 30.0;
 const double CLASH_PENALTY_W = 6.0, CLASH_PENALTY_FRAC = 0.75;  // dna.rs:32-33
 const double SOLVATION_DISTANCE2 = 6.4 * 6.4;                   // cpydock.rs:44
+const double INTERFACE_CUTOFF2 = 3.9 * 3.9;                     // constants.rs:14-15
+const double MEMBRANE_PENALTY_SCORE = 999.0;                    // constants.rs:21
 const double VDW_WEIGHT = 0.1;                                   // cpydock.rs:45
 const double HUGE_DIST = 10000.0;                               // cpydock.rs:412
 
@@ -426,6 +428,12 @@ struct Model {
     float crec_origin[3];
     NearCells cells;
     bool built_cells = false;
+    // active restraints (restraint residue index per atom, -1 = none) and
+    // receptor membrane beads; the reference keeps residue -> atoms maps
+    // (pydock.rs:30-32), which count the same satisfied residues
+    std::vector<int32_t> rres, lres, mem;
+    int nres_r = 0, nres_l = 0;
+    bool need_iface() const { return nres_r > 0 || nres_l > 0 || !mem.empty(); }
 
     const Field* get_field(int fp64) {
         int k = fp64 ? 1 : 0;
@@ -455,8 +463,10 @@ void transform_ligand(const Mol& lig, const double t[3], const double qv[4], std
     }
 }
 
-// DNA::energy_grid CPU branch (src/dna.rs:834-998, no restraints/membrane)
-double dna_grid(Model& M, const std::vector<double>& L, const Field* fld, double parts[5]) {
+// DNA::energy_grid CPU branch (src/dna.rs:834-998); ir / il (when not null)
+// receive the interface flags of dna.rs:970-973
+double dna_grid(Model& M, const std::vector<double>& L, const Field* fld, double parts[5], uint8_t* ir,
+                uint8_t* il) {
     const Mol& R = M.rec; const Mol& G = M.lig; const Crec& c = M.crec;
     double e_sum = 0.0, v_sum = 0.0, npairs = 0.0;
     const double csp = c.sp, cox = c.lo[0], coy = c.lo[1], coz = c.lo[2];
@@ -496,6 +506,7 @@ double dna_grid(Model& M, const std::vector<double>& L, const Field* fld, double
                             v_sum += v;
                             npairs += 1.0;
                         }
+                        if (ir && d2 <= INTERFACE_CUTOFF2) { ir[i] = 1; il[j] = 1; }
                     }
                 }
             }
@@ -510,8 +521,9 @@ double dna_grid(Model& M, const std::vector<double>& L, const Field* fld, double
 }
 
 // PYDOCK::energy_grid (src/pydock.rs:353-447) and VDW::energy_grid
-// (src/vdw.rs:73-151), no restraints/membrane
-double pydock_vdw_grid(Model& M, const std::vector<double>& L, const Field* fld, double parts[5]) {
+// (src/vdw.rs:73-151); interface flags as pydock.rs:427-430, vdw.rs:139-142
+double pydock_vdw_grid(Model& M, const std::vector<double>& L, const Field* fld, double parts[5], uint8_t* ir,
+                       uint8_t* il) {
     const Mol& R = M.rec; const Mol& G = M.lig;
     const bool vdw_only = (M.family == ORC_VDW);
     double e_near = 0.0, total_vdw = 0.0, npairs = 0.0;
@@ -538,6 +550,7 @@ double pydock_vdw_grid(Model& M, const std::vector<double>& L, const Field* fld,
                     total_vdw += std::fmin(vdw_e * (p6 * p6 - 2.0 * p6), VDW_CUTOFF);
                 }
             }
+            if (ir && d2 <= INTERFACE_CUTOFF2) { ir[i] = 1; il[j] = 1; }
         });
     }
     if (vdw_only) {
@@ -552,8 +565,10 @@ double pydock_vdw_grid(Model& M, const std::vector<double>& L, const Field* fld,
     return -(total_elec + total_vdw);
 }
 
-// CPYDOCK::energy_grid (src/cpydock.rs:556-676), no restraints/membrane
-double cpydock_grid(Model& M, const std::vector<double>& L, const Field* fld, double parts[5]) {
+// CPYDOCK::energy_grid (src/cpydock.rs:556-676); interface flags as
+// cpydock.rs:639-642
+double cpydock_grid(Model& M, const std::vector<double>& L, const Field* fld, double parts[5], uint8_t* ir,
+                    uint8_t* il) {
     const Mol& R = M.rec; const Mol& G = M.lig;
     std::vector<double> min_rec(R.n, HUGE_DIST), min_lig(G.n, HUGE_DIST);
     double e_near = 0.0, total_vdw = 0.0, npairs = 0.0;
@@ -577,6 +592,7 @@ double cpydock_grid(Model& M, const std::vector<double>& L, const Field* fld, do
                 double k = vdw_e * (p6 * p6 - 2.0 * p6);
                 total_vdw += (k > VDW_CUTOFF) ? VDW_CUTOFF : k;
             }
+            if (ir && d2 <= INTERFACE_CUTOFF2) { ir[i] = 1; il[j] = 1; }
         });
     }
     double e_far = 0.0;
@@ -602,15 +618,55 @@ double cpydock_grid(Model& M, const std::vector<double>& L, const Field* fld, do
     return (total_elec_kcal + VDW_WEIGHT * total_vdw - total_solv) * -1.0;
 }
 
-double energy_grid(Model& M, const double t[3], const double q[4], int fp64, double parts[5]) {
+// satisfied_restraints (scoring.rs:83-98): restraint residues with at least
+// one interface atom over all residues of the map
+double satisfied_restraints(const std::vector<uint8_t>& iface, const std::vector<int32_t>& res, int nres) {
+    if (nres == 0) return 0.0;
+    std::vector<char> sat(nres, 0);
+    for (size_t i = 0; i < res.size(); ++i)
+        if (res[i] >= 0 && iface[i] == 1) sat[res[i]] = 1;
+    int n = 0;
+    for (char c : sat) n += c;
+    return (double)n / (double)nres;
+}
+
+// membrane_intersection (scoring.rs:100-108)
+double membrane_intersection(const std::vector<uint8_t>& iface, const std::vector<int32_t>& mem) {
+    if (mem.empty()) return 0.0;
+    int64_t n = 0;
+    for (int32_t i : mem) n += iface[i];
+    return (double)n / (double)mem.size();
+}
+
+// iface (optional): pr, pl, membrane intersection
+double energy_grid(Model& M, const double t[3], const double q[4], int fp64, double parts[5],
+                   double iface[3] = nullptr) {
     std::vector<double> L;
     transform_ligand(M.lig, t, q, L);
     const Field* fld = (M.family == ORC_VDW) ? nullptr : M.get_field(fp64);
+    const bool need = M.need_iface();
+    std::vector<uint8_t> ir(need ? M.rec.n : 0, 0), il(need ? M.lig.n : 0, 0);
+    uint8_t* pr_ = need ? ir.data() : nullptr;
+    uint8_t* pl_ = need ? il.data() : nullptr;
+    double score;
     switch (M.family) {
-        case ORC_DNA: return dna_grid(M, L, fld, parts);
-        case ORC_CPYDOCK: return cpydock_grid(M, L, fld, parts);
-        default: return pydock_vdw_grid(M, L, fld, parts);
+        case ORC_DNA: score = dna_grid(M, L, fld, parts, pr_, pl_); break;
+        case ORC_CPYDOCK: score = cpydock_grid(M, L, fld, parts, pr_, pl_); break;
+        default: score = pydock_vdw_grid(M, L, fld, parts, pr_, pl_); break;
     }
+    if (iface) iface[0] = iface[1] = iface[2] = 0.0;
+    if (!need) return score;
+    const double perc_r = satisfied_restraints(ir, M.rres, M.nres_r);
+    const double perc_l = satisfied_restraints(il, M.lres, M.nres_l);
+    const double intersection = membrane_intersection(ir, M.mem);
+    const double penalty = intersection > 0.0 ? MEMBRANE_PENALTY_SCORE * intersection : 0.0;
+    if (iface) { iface[0] = perc_r; iface[1] = perc_l; iface[2] = intersection; }
+    switch (M.family) {
+        case ORC_DNA: score += perc_r * score + perc_l * score - penalty; break;   // dna.rs:989-995
+        case ORC_VDW: score = score + perc_r * score + perc_l * score; break;      // vdw.rs:146-149
+        default: score = score + perc_r * score + perc_l * score - penalty; break; // pydock.rs:440-445, cpydock.rs:670-675
+    }
+    return score;
 }
 
 // energy_exact, all pairs (dna.rs:668-819 without the Z-window sort, which
@@ -904,6 +960,36 @@ double orc_energy_grid(void* m, const double t[3], const double q[4], int fp64, 
 
 double orc_energy_exact(void* m, const double t[3], const double q[4]) {
     return energy_exact(*(Model*)m, t, q);
+}
+
+void orc_model_set_restraints(void* mv, const int32_t* rres, int nres_r, const int32_t* lres, int nres_l,
+                              const int32_t* mem, int64_t nmem) {
+    Model& M = *(Model*)mv;
+    M.nres_r = nres_r;
+    M.nres_l = nres_l;
+    M.rres.assign(M.rec.n, -1);
+    M.lres.assign(M.lig.n, -1);
+    if (nres_r && rres) M.rres.assign(rres, rres + M.rec.n);
+    if (nres_l && lres) M.lres.assign(lres, lres + M.lig.n);
+    M.mem.assign(mem ? mem : nullptr, mem ? mem + nmem : nullptr);
+}
+
+void orc_batch_energy_grid_iface(void* mv, int64_t N, const double* poses, int fp64, int threads,
+                                 double* out, double* iface) {
+    Model& M = *(Model*)mv;
+    if (M.family != ORC_VDW) M.get_field(fp64);
+#ifdef _OPENMP
+    int nt = threads > 0 ? threads : omp_get_max_threads();
+#else
+    int nt = 1; (void)threads;
+#endif
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nt)
+    for (int64_t k = 0; k < N; ++k) {
+        const double* p = poses + 7 * k;
+        double q[4] = {p[0], p[1], p[2], p[3]};
+        double t[3] = {p[4], p[5], p[6]};
+        out[k] = energy_grid(M, t, q, fp64, nullptr, iface ? iface + 3 * k : nullptr);
+    }
 }
 
 void orc_batch_energy_grid(void* mv, int64_t N, const double* poses, int fp64, int threads,

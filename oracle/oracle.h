@@ -71,6 +71,17 @@ const void* orc_model_field(void* m, int fp64);
 /* Score::energy_grid for one pose (t = translation, q = w,x,y,z).
  * parts (may be NULL) receives {e_near_raw, e_far_raw, vdw, solv, near_pairs}. */
 double orc_energy_grid(void* m, const double t[3], const double q[4], int fp64, double parts[5]);
+/* Active restraints and membrane (dna.rs:885-897,970-995, pydock.rs:427-445,
+ * vdw.rs:139-149, cpydock.rs:639-675, scoring.rs:83-108): restraint residue
+ * index per atom (-1 = none; n x 1, NULL when the count is 0) and the
+ * receptor atom indices of the membrane beads.  energy_grid then applies the
+ * restraint fractions and the membrane penalty. */
+void orc_model_set_restraints(void* m, const int32_t* rec_res, int nres_r, const int32_t* lig_res, int nres_l,
+                              const int32_t* membrane, int64_t n_membrane);
+/* batch with the interface terms per pose (iface N x 3: pr, pl, membrane
+ * intersection; may be NULL) */
+void orc_batch_energy_grid_iface(void* m, int64_t N, const double* poses, int fp64, int threads,
+                                 double* out, double* iface);
 /* energy_exact (all-pairs reference path) */
 double orc_energy_exact(void* m, const double t[3], const double q[4]);
 /* batch of poses, N x 7 in the reference's kernel order (w,x,y,z,tx,ty,tz);

@@ -7,7 +7,8 @@ test or bench time reads the reference: only the files written here do.
 Outputs
 -------
 tests/golden/1azp_models.npz
-    Per-atom parameter arrays of the 1AZP receptor and ligand, typed the way
+    Per-atom parameter arrays of the 1AZP receptor and ligand (and each
+    atom's residue, for restraint tests), typed the way
     the reference's DNA model (``src/dna.rs:277-403``) and PYDOCK model
     (``src/pydock.rs:41-162``) type them: AMBER type lookup by
     ``RES-ATOM`` with the ``H1/H2/H3 -> RES-H`` and ``*-<element>`` fallbacks,
@@ -56,7 +57,7 @@ def parse_pdb(path):
             continue
         atoms.append(dict(
             name=line[12:16].strip(), res=line[17:20].strip(),
-            chain=line[21], resseq=int(line[22:26]),
+            chain=line[21], resseq=int(line[22:26]), icode=line[26].strip(),
             x=float(line[30:38]), y=float(line[38:46]), z=float(line[46:54]),
             element=line[76:78].strip()))
     return atoms
@@ -110,6 +111,20 @@ def main():
         arrays[f"{side}_is_h"] = np.array(
             [1 if (a["element"] == "H" if a["element"] else a["name"].startswith("H"))
              else 0 for a in atoms], np.uint8)
+    # residue of every atom: dense index (first appearance) and the id the
+    # reference keys its restraint maps by, "chain.resname.serial[icode]"
+    # (src/pydock.rs:66-69)
+    for side, atoms in (("rec", rec), ("lig", lig)):
+        ids, index = [], {}
+        per_atom = []
+        for a in atoms:
+            rid = f"{a['chain']}.{a['res']}.{a['resseq']}{a['icode']}"
+            if rid not in index:
+                index[rid] = len(ids)
+                ids.append(rid)
+            per_atom.append(index[rid])
+        arrays[f"{side}_resid"] = np.array(per_atom, np.int32)
+        arrays[f"{side}_residues"] = np.array(ids)
     np.savez_compressed(os.path.join(HERE, "1azp_models.npz"), **arrays)
 
     # DNA-family vdW type table + nucleotide maps for the synthetic generator.

@@ -2,6 +2,7 @@
 include/lkg.h declares, and its host logic (RNG, setup poses, cell-list
 packing, field geometry, SASA, synthetic inputs) behaves; no GPU calls."""
 import ctypes
+import importlib
 
 import numpy as np
 import pytest
@@ -141,3 +142,42 @@ def test_mlp_oracle_bf16_rounding():
     assert abs(r[3] + 3.140625) < 1e-12
     bits = omlp.f64_to_bf16_bits(x)
     assert np.array_equal(omlp.bf16_bits_to_f64(bits), r)
+
+
+# ------------------------------------------------- gso files and rankings
+GSO_TEXT = (
+    "#Coordinates  RecID  LigID  Luciferin  Neighbor's number  Vision Range  Scoring\n"
+    "(1.0000000, -2.5000000, 3.1250000, 0.5000000, 0.5000000, -0.5000000, 0.5000000)    0    0   "
+    "7.12345678  2 0.280 -12.50000000\n"
+    "(4.0000000, 5.0000000, 6.0000000, 1.0000000, 0.0000000, 0.0000000, 0.0000000)    0    0   "
+    "9.00000000  0 0.200 31.25000000\n"
+    "not a pose line\n"
+    "(7.0000000, 8.0000000, 9.0000000, 1.0000000, 0.0000000, 0.0000000, 0.0000000, 0.1000000)    0    0   "
+    "1.50000000  5 5.000 3.00000000\n")
+
+
+def test_parse_gso_follows_the_reference_reader(tmp_path):
+    # parse_gso_file (src/bin/lightdock.rs:123-148): ids count every non-comment line
+    rank = importlib.import_module("lklight-gpu_b200.rank")
+    p = tmp_path / "gso_3.out"
+    p.write_text(GSO_TEXT)
+    e = rank.parse_gso(str(p))
+    assert [x["glowworm"] for x in e] == [0, 1, 3]
+    assert e[0]["translation"] == [1.0, -2.5, 3.125] and e[0]["rotation"] == [0.5, 0.5, -0.5, 0.5]
+    assert e[0]["luciferin"] == 7.12345678 and e[0]["scoring"] == -12.5
+    assert e[2]["extents"] == [0.1]
+
+
+def test_rank_lists_in_the_reference_format(tmp_path):
+    # write_rank_file (src/bin/lightdock.rs:888-903)
+    rank = importlib.import_module("lklight-gpu_b200.rank")
+    for sid in range(2):
+        (tmp_path / ("swarm_%d" % sid)).mkdir()
+        (tmp_path / ("swarm_%d" % sid) / "gso_3.out").write_text(GSO_TEXT)
+    ranked = rank.rank(2, 3, str(tmp_path))
+    lines = (tmp_path / "ranking.list").read_text().split("\n")
+    assert lines[0] == "# Rank Swarm Glowworm Luciferin Scoring PDB Coords"
+    assert lines[1] == "    1    0     1     9.000000    31.250000 swarm_0/lightdock_1.pdb (4.000,5.000,6.000)"
+    assert lines[2] == "    2    1     1     9.000000    31.250000 swarm_1/lightdock_1.pdb (4.000,5.000,6.000)"
+    assert lines[6] == "    6    1     0     7.123457   -12.500000 swarm_1/lightdock_0.pdb (1.000,-2.500,3.125)"
+    assert [r["luciferin"] for r in ranked] == [9.0, 9.0, 7.12345678, 7.12345678, 1.5, 1.5]

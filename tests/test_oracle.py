@@ -143,3 +143,49 @@ def test_gso_deterministic():
         runs.append(g.state())
     assert np.array_equal(runs[0]["scoring"], runs[1]["scoring"])
     assert np.array_equal(runs[0]["translation"], runs[1]["translation"])
+
+
+@pytest.mark.parametrize("family", ["dna", "pydock", "vdw", "cpydock"])
+def test_restraints_match_all_pairs_interface(family):
+    """Interface flags collected in the near scan (dna.rs:970-973 and the
+    other families' grid paths) against an all-pairs numpy scan, and the
+    restraint / membrane combination against a restatement in Python
+    floats (scoring.rs:83-108)."""
+    from tests.lkg_helpers import azp_residues, brute_interface, combine_restraints, restraint_tags
+    rec, lig = azp(family)
+    rresid, _, lresid, _ = azp_residues()
+    base, m = model(family), model(family)
+    rng = np.random.default_rng(11)
+    ract = rng.choice(rresid.max() + 1, 9, replace=False)
+    lact = rng.choice(lresid.max() + 1, 4, replace=False)
+    rr, lr = restraint_tags(rresid, ract), restraint_tags(lresid, lact)
+    mem = np.sort(rng.choice(len(rresid), 40, replace=False)).astype(np.int32)
+    m.set_restraints(rr, len(ract), lr, len(lact), mem)
+    poses = np.zeros((12, 7))
+    q = rng.normal(size=(12, 4))
+    poses[:, :4] = q / np.linalg.norm(q, axis=1, keepdims=True)
+    poses[:, 4:] = rng.uniform(-18, 18, size=(12, 3))
+    got, frac = m.batch_energy_grid_iface(poses)
+    plain = base.batch_energy_grid(poses)
+    seen = np.zeros(3)
+    for k in range(len(poses)):
+        ir, il, border = brute_interface(rec["coords"], lig["coords"], poses[k])
+        if border < 1e-9:
+            continue
+        pr = len({int(rr[i]) for i in np.nonzero(ir)[0] if rr[i] >= 0}) / len(ract)
+        pl = len({int(lr[j]) for j in np.nonzero(il)[0] if lr[j] >= 0}) / len(lact)
+        mi = float(ir[mem].sum()) / len(mem)
+        assert (frac[k] == [pr, pl, mi]).all(), (k, frac[k], (pr, pl, mi))
+        assert got[k] == combine_restraints(family, plain[k], pr, pl, mi)
+        seen += np.array([pr, pl, mi]) > 0
+    assert (seen > 0).all()   # every term was exercised
+
+
+def test_restraints_cleared_score_equals_plain():
+    from tests.lkg_helpers import azp_residues
+    m, base = model("pydock"), model("pydock")
+    rresid = azp_residues()[0]
+    m.set_restraints(np.zeros(len(rresid), np.int32), 1, None, 0, None)
+    m.set_restraints(None, 0, None, 0, None)
+    poses = np.array([[1, 0, 0, 0, 3.0, -2.0, 1.0], [0.6, 0.8, 0, 0, -5.0, 4.0, 2.0]])
+    assert (m.batch_energy_grid(poses) == base.batch_energy_grid(poses)).all()
