@@ -459,8 +459,16 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
         st = g.state()
         res[mode] = dict(seconds=el, scored=g.scored, predicted=g.predicted, st=st, phases=g.timing())
         del g
+    # the GSO's own spread: the plain run from the same start with the next
+    # seed; its top-5 overlap with the plain run bounds what any run with a
+    # different random stream can reach
+    g = lkg.GSO(ctx, [(cid, swarms, glow)], pos, [seed + 1])
+    g.run(steps)
+    g.finalize()
+    res["plain_next_seed"] = dict(st=g.state())
+    del g
     ov = {}
-    for mode in ("screened", "ablation"):
+    for mode in ("screened", "ablation", "plain_next_seed"):
         o = []
         for k in range(swarms):
             sl = slice(k * glow, (k + 1) * glow)
@@ -484,7 +492,11 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
                          "top5_overlap_with_plain": ov["screened"], "phases_s": res["screened"]["phases"]},
             "ablation_no_network": {"seconds": res["ablation"]["seconds"], "exact_evals": res["ablation"]["scored"],
                                     "mean_best_score": best["ablation"], "top5_overlap_with_plain": ov["ablation"],
-                                    "phases_s": res["ablation"]["phases"]}}
+                                    "phases_s": res["ablation"]["phases"]},
+            "plain_next_seed": {"mean_best_score": best["plain_next_seed"],
+                                "top5_overlap_with_plain": ov["plain_next_seed"],
+                                "what": "the plain GSO from the same start with GSO seed + 1: the overlap two "
+                                        "plain runs reach"}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()

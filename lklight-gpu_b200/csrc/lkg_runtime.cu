@@ -316,11 +316,29 @@ int complex_create(lkg_ctx* ctx, int family, unsigned flags, int lj_form, const 
     return set_ok();
 }
 
+// The fast kernels find tagged receptor atoms by the sign bit of their heavy
+// flag (rpar.z is +-0 or +-1; the kernels only test it against 0): set it
+// for the atoms with a tag in rt (sorted order), clear it everywhere else.
+static int set_rpar_tag_signs(lkg_ctx* ctx, ComplexRec& cr, const std::vector<int2>* rt) {
+    const int nr = cr.d.nr;
+    if (nr <= 0) return 0;
+    std::vector<float4> par(nr);
+    LKG_CK(cudaStreamSynchronize(ctx->stream), "receptor tags");
+    LKG_CK(cudaMemcpy(par.data(), cr.rpar.p, nr * sizeof(float4), cudaMemcpyDeviceToHost), "receptor tags");
+    for (int k = 0; k < nr; ++k) {
+        const bool tagged = rt && ((*rt)[k].x >= 0 || (*rt)[k].y >= 0);
+        par[k].z = tagged ? -std::fabs(par[k].z) : std::fabs(par[k].z);
+    }
+    LKG_CK(cudaMemcpy(cr.rpar.p, par.data(), nr * sizeof(float4), cudaMemcpyHostToDevice), "receptor tags");
+    return 0;
+}
+
 int complex_set_ligand(lkg_ctx* ctx, int id, const MolIn& lig) {
     if (id < 0 || id >= (int)ctx->cx.size()) return set_error(LKG_ERR_ARG, "bad complex id %d", id);
     ComplexRec& cr = *ctx->cx[id];
     int st = build_ligand(ctx, lig, cr);
     // interface tags refer to the old ligand's atoms
+    if (!st && cr.d.iface_words && (st = set_rpar_tag_signs(ctx, cr, nullptr))) return st;
     cr.d.rtag = nullptr; cr.d.ltag = nullptr;
     cr.d.nres_r = cr.d.nres_l = cr.d.nmem = cr.d.iface_words = 0;
     cr.d.iface_form = IF_NONE;
@@ -361,6 +379,7 @@ int complex_set_restraints(lkg_ctx* ctx, int id, const int32_t* rres, int nres_r
         mbit[mem[m]] = nres_r + nres_l + m;
     }
     if (total == 0) {   // cleared
+        if ((st = set_rpar_tag_signs(ctx, cr, nullptr))) return st;
         cr.d.rtag = nullptr; cr.d.ltag = nullptr;
         cr.d.nres_r = cr.d.nres_l = cr.d.nmem = cr.d.iface_words = 0;
         cr.d.iface_form = IF_NONE;
@@ -381,6 +400,7 @@ int complex_set_restraints(lkg_ctx* ctx, int id, const int32_t* rres, int nres_r
         const int r = nres_l ? lres[lorig[j]] : -1;
         lt[j] = r >= 0 ? nres_r + r : -1;
     }
+    if ((st = set_rpar_tag_signs(ctx, cr, &rt))) return st;
     LKG_CK(upload(cr.rtag, rt, ctx->stream), "restraint tags");
     LKG_CK(upload(cr.ltag, lt, ctx->stream), "restraint tags");
     LKG_CK(cudaStreamSynchronize(ctx->stream), "restraint tags");

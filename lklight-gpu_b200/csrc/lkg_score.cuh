@@ -365,7 +365,7 @@ template <> struct Atom<float> {
                     min_l = fmin(min_l, d2d);
                     if (d2d <= SOLV2_D && !hash->insert(k, d2d)) atomicOr(status, 1);
                 }
-                if (ibits && d2 <= IFACE2_F) {
+                if (ibits && d2 <= IFACE2_F && ((__float_as_uint(pr.z) >> 31) || lt >= 0)) {
                     const double4 a64 = c.rpos64[k];
                     const double ex = xd - a64.x, ey = yd - a64.y, ez = zd - a64.z;
                     iface_mark(c, ibits, k, lt, ex * ex + ey * ey + ez * ez);

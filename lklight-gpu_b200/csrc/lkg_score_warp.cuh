@@ -53,6 +53,10 @@ struct WDes {
     int lf[2 * G];
 };
 
+// interface words a warp collects in shared memory before merging them into
+// the pose's bits (larger sets go to HBM directly)
+constexpr int W_IBUF = 32;
+
 template <int G>
 struct WSlots {
     Rot rot;                    // pose of the current work unit
@@ -61,9 +65,32 @@ struct WSlots {
     float4 ltest[2 * G];        // candidate test: -2 l', |l'|^2 - 100.01 (l' = l - group centre)
     float2 lpar[2 * G];         // r, heavy
     int ltag[2 * G];            // IFACE: restraint bit of the slot atom, -1 = none
-    unsigned* ibits;            // IFACE: interface bits of the current pose (null: none)
+    unsigned* ibits;            // IFACE: interface bits of the current pose in HBM (null: none)
+    unsigned* iset;             // IFACE: where pairs set them: ibuf, or ibits when the pose has more words
+    unsigned ibuf[W_IBUF];      // IFACE: the unit's bits, merged into ibits once at the unit's end
     unsigned hit[WRing<G>::N];  // (slot << 26) | receptor index
 };
+
+// IFACE: start a unit of pose bits `bits` (lane 0; the caller syncs the
+// warp after): collect in the warp's buffer when the pose fits in it
+template <int G>
+__device__ __forceinline__ void w_iface_begin(WSlots<G>& W, const ComplexDev& c, unsigned* bits) {
+    W.ibits = bits;
+    W.iset = !bits ? nullptr : (c.iface_words <= W_IBUF ? W.ibuf : bits);
+}
+
+// IFACE: merge the warp's buffer into the pose's bits and clear it (all
+// lanes); the buffer is all zero between units
+template <int G>
+__device__ __forceinline__ void w_iface_flush(WSlots<G>& W, const ComplexDev& c) {
+    __syncwarp();
+    if (W.iset == W.ibuf)
+        for (int w = (int)(threadIdx.x & 31); w < c.iface_words; w += 32) {
+            const unsigned v = W.ibuf[w];
+            if (v) { atomicOr(W.ibits + w, v); W.ibuf[w] = 0u; }
+        }
+    __syncwarp();
+}
 
 // pair terms of one queued hit: the exact d^2 <= 100 test on the
 // compensated d^2, then the reference formulas (those of pair_fast, with
@@ -76,7 +103,8 @@ struct WSlots {
 // interface bits.
 template <int G, bool DESOLV, bool IFACE>
 __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, WDes<G>* D, MinHash* hash,
-                                       int* status, unsigned e, unsigned flags, double& elec, double& vdw, int& np) {
+                                       int* status, unsigned e, unsigned flags, unsigned* iset, double& elec,
+                                       double& vdw, int& np) {
     const int l = (int)(e >> 26), k = (int)(e & 0x3ffffffu);
     const float4 a = __ldg(c.rpos + k);
     const float4 pr = __ldg(c.rpar + k);
@@ -110,10 +138,13 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
         atomicMin(&D->lmin[l], (unsigned long long)__double_as_longlong(d2d));
         if (d2d <= SOLV2_D && !hash->insert(k, d2d)) atomicOr(status, 1);
     }
-    if (IFACE && d2 <= IFACE2_F && W.ibits) {
+    // tagged atoms carry the sign bit on their heavy flag (receptor: rpar.z,
+    // set with the restraints; ligand slot: lpar.y), which the != 0 tests
+    // above do not see: untagged pairs cost one test
+    if (IFACE && iset && d2 <= IFACE2_F && ((__float_as_uint(pr.z) | __float_as_uint(lq.y)) >> 31)) {
         const int2 rt = __ldg(c.rtag + k);
         const int lt = W.ltag[l];
-        if ((rt.x & rt.y & lt) >= 0) {   // not all three -1
+        {
             const double4 a64 = c.rpos64[k];
             double ex, ey, ez;
             if (DESOLV) { ex = D->lx[l] - a64.x; ey = D->ly[l] - a64.y; ez = D->lz[l] - a64.z; }
@@ -123,9 +154,9 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
                 ez = ((double)lp.z + (double)lr.z) - a64.z;
             }
             if (ex * ex + ey * ey + ez * ez <= IFACE2_D) {
-                iface_set(W.ibits, rt.x);
-                iface_set(W.ibits, rt.y);
-                iface_set(W.ibits, lt);
+                iface_set(iset, rt.x);
+                iface_set(iset, rt.y);
+                iface_set(iset, lt);
             }
         }
     }
@@ -167,11 +198,13 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
     const unsigned lt_mask = (1u << lane) - 1u;
     const unsigned flags = c.flags;
     const int nl = c.nl;
+    unsigned* const iset = IFACE ? W.iset : nullptr;   // set by the caller for the unit
     unsigned head = 0, tail = 0, prev_start = 0;
     int jdes0 = -1, jdes1 = -1;   // DESOLV: this lane's slot atom in set 0 / set 1
     auto drain_partial = [&]() {
         if ((int)(tail - head) > lane)
-            w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, acc.elec, acc.vdw, acc.np);
+            w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, iset,
+                                     acc.elec, acc.vdw, acc.np);
         head = tail;
     };
     auto finalize = [&](int set) {   // DESOLV: the slot set's minima are final
@@ -214,8 +247,9 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
             if (!valid) { x = y = z = 1e30f; }   // never within reach of a receptor atom
             W.lpos[set + lane] = make_float4(x, y, z, b4.w);
             W.lres[set + lane] = res;
-            W.lpar[set + lane] = make_float2(lp4.y, lp4.z);
-            if (IFACE) W.ltag[set + lane] = (valid && c.ltag) ? __ldg(c.ltag + j) : -1;
+            const int ltg = (IFACE && valid && c.ltag) ? __ldg(c.ltag + j) : -1;
+            W.lpar[set + lane] = make_float2(lp4.y, ltg >= 0 ? -lp4.z : lp4.z);   // -0 or -1 when tagged
+            if (IFACE) W.ltag[set + lane] = ltg;
             if (DESOLV) {
                 D->lx[set + lane] = xd; D->ly[set + lane] = yd; D->lz[set + lane] = zd;
                 D->lmin[set + lane] = W_NOMIN;
@@ -307,8 +341,8 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
                 __syncwarp();
                 // 4. full batches of 32 hits
                 while ((int)(tail - head) >= 32) {
-                    w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, acc.elec,
-                                      acc.vdw, acc.np);
+                    w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, iset,
+                                             acc.elec, acc.vdw, acc.np);
                     head += 32;
                 }
             }
@@ -328,6 +362,7 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
     extern __shared__ __align__(16) unsigned char wk_smem[];
     const int lane = threadIdx.x & 31;
     WSlots<G>& W = reinterpret_cast<WSlots<G>*>(wk_smem)[threadIdx.x >> 5];
+    if (IFACE) W.ibuf[lane] = 0u;
     for (;;) {
         unsigned long long wq = 0;
         if (lane == 0) wq = atomicAdd(p.work_counter, 1ull);
@@ -343,14 +378,18 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
         __syncwarp();   // readers of the previous unit's pose are done
         if (lane == 0) {
             W.rot = pose_matrix(p.poses + 7 * g);
-            if (IFACE) W.ibits = iface_bits(p, c, g);
+            if (IFACE) w_iface_begin(W, c, iface_bits(p, c, g));
+            else if (c.iface_words) atomicOr(p.status, 2);   // a launch without room for the bits
         }
         __syncwarp();
         const int gpt = p.tile / G;
         const int g0 = tile * gpt, g1 = min(g0 + gpt, (c.nl + G - 1) / G);
         WAcc acc;
         w_groups<G, false, IFACE>(c, W, nullptr, nullptr, nullptr, g0, g1, 1, acc);
-        if (IFACE && W.ibits) __threadfence();   // interface bits before the unit is published
+        if (IFACE && W.ibits) {
+            w_iface_flush(W, c);
+            __threadfence();   // interface bits before the unit is published
+        }
         const double elec = warp_sum(acc.elec), vdw = warp_sum(acc.vdw);
         const long long npl = warp_sum((long long)acc.np);
         if (lane == 0) {
@@ -410,13 +449,16 @@ __global__ void __launch_bounds__(WD_THREADS, 1) k_score_warp_desolv(LaunchParam
         unsigned char* base = wd_smem_raw + (size_t)c.hcap * 12;
         WSlots<G>& W = reinterpret_cast<WSlots<G>*>(base)[wid];
         WDes<G>* D = reinterpret_cast<WDes<G>*>(base + (size_t)NW * sizeof(WSlots<G>)) + wid;
+        if (IFACE) W.ibuf[lane] = 0u;   // the slots move with the complex's hash size
         if (lane == 0) {
             W.rot = pose_matrix(p.poses + 7 * g);
-            if (IFACE) W.ibits = iface_bits(p, c, g);
+            if (IFACE) w_iface_begin(W, c, iface_bits(p, c, g));
+            else if (c.iface_words) atomicOr(p.status, 2);
         }
         __syncthreads();   // hash cleared, poses set
         WAcc acc;
         w_groups<G, true, IFACE>(c, W, D, &hash, p.status, wid, (c.nl + G - 1) / G, NW, acc);
+        if (IFACE && W.ibits) w_iface_flush(W, c);   // before the block's barrier below
         __syncthreads();   // every pair has updated the hash
         // receptor side: fixed-point (2^-40) sum over hash slots; slot order
         // depends on insertion races, integer sums do not

@@ -226,13 +226,7 @@ def test_multi_complex_launch_equals_single(ctx):
     out = torch.zeros(len(allp), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
     ctx.score_multi_device(cids, [len(p) for p in posesets], allp.data_ptr(), out.data_ptr())
-    lkg.lib().lkg_ctx_stream(ctx.h)
-    import ctypes
-    cudart_sync = torch.cuda.synchronize
-    # the context works on its own stream: wait for it before reading
-    assert ctypes.c_void_p(ctx.stream).value is not None
-    torch.cuda.Stream(stream_ptr=ctx.stream).synchronize()
-    cudart_sync()
+    ctx.sync()   # the context works on its own stream
     got = out.cpu().numpy()
     assert np.array_equal(got, np.concatenate(singles))
 
