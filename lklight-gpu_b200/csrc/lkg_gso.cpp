@@ -275,12 +275,15 @@ struct lkg_gso {
     lkg::HBuf h_cand, h_pred;
     // device-resident plain GSO (lkg_gso_run_device)
     lkg_plan* dplan = nullptr;
-    cudaGraphExec_t dexec = nullptr;
+    cudaGraphExec_t dexec = nullptr, sexec = nullptr;   // plain / screened device step graphs
     lkg::GsoDevState ds{}, ds_captured{};
-    lkg::DBuf dbuf[24];
+    lkg::GsoDevScreen dx{}, dx_captured{};
+    lkg::DBuf dbuf[24], sbuf[6];
+    std::vector<int> dcounts;   // glowworms per group (device order)
     ~lkg_gso() {
         for (auto* s : sur) lkg_surrogate_destroy(s);
         if (dexec) cudaGraphExecDestroy(dexec);
+        if (sexec) cudaGraphExecDestroy(sexec);
         if (dplan) lkg_plan_destroy(dplan);
     }
 };
@@ -677,17 +680,18 @@ int lkg_gso_save(lkg_gso* G, int swarm, int step, const char* directory) {
 int64_t lkg_gso_scored(lkg_gso* G) { return G ? G->scored : 0; }
 int64_t lkg_gso_predicted(lkg_gso* G) { return G ? G->predicted : 0; }
 
-// Plain GSO steps on the device: the state goes up once, every step (score
-// all glowworms, luciferin, select, move) runs as kernel launches replayed
-// from one CUDA graph, and the state comes back at the end.  Unmoved
-// glowworms are rescored with the same pose, which gives the same score.
-int lkg_gso_run_device(lkg_gso* G, int steps) {
-    if (!G || steps < 0) return set_error(LKG_ERR_ARG, "bad gso run");
-    if (G->screen) return set_error(LKG_ERR_STATE, "the device GSO runs the plain GSO only");
-    if (steps == 0) return set_ok();
+// ---------------------------------------------------------------------------
+// device-resident GSO (lkg_gso_run_device)
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+namespace {
+
+// Host state -> device arrays, the scoring plan, the GsoDevState views.
+// `screened`: the mask marks the moves chosen for exact scoring, and the
+// others carry their predicted score.
+int dev_setup(lkg_gso* G, bool screened) {
     lkg_ctx* ctx = G->ctx;
-    cudaSetDevice(ctx->device);
-    const double t0 = now_s();
     const int ns = (int)G->swarms.size(), ng = (int)G->group_complex.size();
     std::vector<int> first(ns), cnt(ns), of, counts(ng, 0);
     int n = 0, maxs = 0;
@@ -701,8 +705,7 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
     for (int gi = 0; gi < ng; ++gi)
         for (int s = G->group_first_swarm[gi]; s < G->group_first_swarm[gi] + G->group_nswarm[gi]; ++s)
             counts[gi] += cnt[s];
-    if (n == 0) return set_ok();
-    // host state -> device
+    G->dcounts = counts;
     std::vector<double> a[10];
     for (auto& v : a) v.resize(n);
     std::vector<double> pose(7 * (size_t)n);
@@ -719,14 +722,18 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
             a[7][i] = gw.luciferin; a[8][i] = gw.vision; a[9][i] = gw.scoring;
             const double row[7] = {gw.r.w, gw.r.x, gw.r.y, gw.r.z, gw.t[0], gw.t[1], gw.t[2]};
             std::memcpy(&pose[7 * (size_t)i], row, sizeof(row));
-            mask[i] = (gw.moved || gw.step == 0) ? 1 : 0;   // swarm.rs:79-85
+            if (screened) {   // score_phase: exact for the chosen moves, the prediction for the others
+                mask[i] = ((gw.moved && gw.exact_next) || gw.step == 0) ? 1 : 0;
+                if (gw.moved && !gw.exact_next && gw.step != 0) a[9][i] = gw.pred;
+            } else {
+                mask[i] = (gw.moved || gw.step == 0) ? 1 : 0;   // swarm.rs:79-85
+            }
             ++i;
         }
     }
     cudaStream_t st = ctx->stream;
     lkg::DBuf* b = G->dbuf;
-    for (int k = 0; k < 10; ++k) LKG_CK(b[k].reserve(n * sizeof(double)), "device gso");
-    for (int k = 10; k < 18; ++k) LKG_CK(b[k].reserve(n * sizeof(double)), "device gso");
+    for (int k = 0; k < 18; ++k) LKG_CK(b[k].reserve(n * sizeof(double)), "device gso");
     LKG_CK(b[18].reserve(7 * (size_t)n * sizeof(double)), "device gso");
     LKG_CK(b[19].reserve(2 * (size_t)n * sizeof(int)), "device gso");
     LKG_CK(b[20].reserve((2 * (size_t)ns + n) * sizeof(int)), "device gso");
@@ -761,8 +768,80 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
     S.draws = b[22].as<unsigned long long>();
     S.mask = b[23].as<unsigned char>();
     S.nscored = reinterpret_cast<unsigned long long*>(b[23].as<unsigned char>() + ((n + 7) & ~7));
+    if (screened) {
+        const int K = G->cfg.candidates;
+        lkg::GsoDevScreen& X = G->dx;
+        lkg::DBuf* c = G->sbuf;
+        LKG_CK(c[0].reserve((size_t)n * (K + 1) * 7 * sizeof(double)), "device gso");
+        LKG_CK(c[1].reserve((size_t)n * (K + 1) * sizeof(double)), "device gso");
+        LKG_CK(c[2].reserve((size_t)n * K * sizeof(int)), "device gso");
+        LKG_CK(c[3].reserve((size_t)n * sizeof(int)), "device gso");
+        LKG_CK(c[4].reserve((size_t)n * sizeof(double)), "device gso");
+        LKG_CK(c[5].reserve(2 * (size_t)n), "device gso");
+        LKG_CK(cudaMemsetAsync(c[5].p, 0, 2 * (size_t)n, st), "device gso");   // no pending predictions
+        X.K = K; X.reserved = 0; X.frac = G->cfg.exact_fraction;
+        X.cand = c[0].as<double>(); X.pred = c[1].as<double>(); X.knid = c[2].as<int>(); X.best = c[3].as<int>();
+        X.gain = c[4].as<double>(); X.exact = c[5].as<unsigned char>(); X.pend = X.exact + n;
+    }
     int rc;
     if (!G->dplan && (rc = lkg_plan_create(ctx, ng, G->group_complex.data(), counts.data(), &G->dplan))) return rc;
+    return set_ok();
+}
+
+// device arrays -> host state after `steps` device steps
+int dev_download(lkg_gso* G, int steps, bool screened) {
+    const lkg::GsoDevState& S = G->ds;
+    const int n = S.n, ns = S.n_swarms;
+    lkg::DBuf* b = G->dbuf;
+    std::vector<double> a[10];
+    for (int k = 0; k < 10; ++k) {
+        a[k].resize(n);
+        LKG_CK(cudaMemcpy(a[k].data(), b[k].p, n * sizeof(double), cudaMemcpyDeviceToHost), "device gso");
+    }
+    std::vector<int> nid(2 * (size_t)n);
+    LKG_CK(cudaMemcpy(nid.data(), b[19].p, nid.size() * sizeof(int), cudaMemcpyDeviceToHost), "device gso");
+    std::vector<unsigned long long> draws(ns);
+    LKG_CK(cudaMemcpy(draws.data(), S.draws, ns * sizeof(unsigned long long), cudaMemcpyDeviceToHost), "device gso");
+    std::vector<double> gain;
+    std::vector<unsigned char> ex;
+    if (screened) {
+        gain.resize(n);
+        ex.resize(2 * (size_t)n);
+        LKG_CK(cudaMemcpy(gain.data(), G->dx.gain, n * sizeof(double), cudaMemcpyDeviceToHost), "device gso");
+        LKG_CK(cudaMemcpy(ex.data(), G->dx.exact, 2 * (size_t)n, cudaMemcpyDeviceToHost), "device gso");
+    }
+    for (int s = 0, i = 0; s < ns; ++s) {
+        Swarm& sw = G->swarms[s];
+        for (size_t k = 0; k < sw.g.size(); ++k, ++i) {
+            Glow& gw = sw.g[k];
+            gw.t[0] = a[0][i]; gw.t[1] = a[1][i]; gw.t[2] = a[2][i];
+            gw.r = {a[3][i], a[4][i], a[5][i], a[6][i]};
+            gw.luciferin = a[7][i]; gw.vision = a[8][i]; gw.scoring = a[9][i];
+            if (screened) {   // as screened_movement leaves them
+                gw.moved = nid[n + i] > 0;
+                gw.exact_next = ex[i] != 0;
+                gw.pred = ex[n + i] ? gw.scoring + gain[i] : gw.scoring;
+            } else {
+                gw.moved = nid[i] != (int)k;
+                gw.exact_next = gw.moved;
+            }
+            gw.nb.assign((size_t)nid[n + i], 0u);   // the count only (state reports it)
+            gw.step += (uint32_t)steps;
+        }
+        sw.rng.set_words_used(2 * draws[s]);
+    }
+    unsigned long long nsc = 0;
+    LKG_CK(cudaMemcpy(&nsc, S.nscored, sizeof(nsc), cudaMemcpyDeviceToHost), "device gso");
+    G->scored += (int64_t)nsc;
+    return set_ok();
+}
+
+// one graph (or eager) step of the plain device GSO
+int dev_plain_steps(lkg_gso* G, int steps) {
+    lkg_ctx* ctx = G->ctx;
+    cudaStream_t st = ctx->stream;
+    lkg::GsoDevState& S = G->ds;
+    int rc;
     // first step eagerly (it also makes the plan's host-side queries)
     if ((rc = lkg::plan_launch_masked(G->dplan, S.poses, S.score, S.mask))) return rc;
     LKG_CK(lkg::gso_dev_after_scoring(S, st), "device gso step");
@@ -790,31 +869,131 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
         }
         for (int k = 1; k < steps; ++k) LKG_CK(cudaGraphLaunch(G->dexec, st), "device gso step");
     }
-    if ((rc = wait_stream(ctx, 300.0)) || (rc = check_status(ctx))) return rc;
-    // device -> host state
-    for (int k = 0; k < 10; ++k)
-        LKG_CK(cudaMemcpy(a[k].data(), b[k].p, n * sizeof(double), cudaMemcpyDeviceToHost), "device gso");
-    std::vector<int> nid(2 * (size_t)n);
-    LKG_CK(cudaMemcpy(nid.data(), b[19].p, nid.size() * sizeof(int), cudaMemcpyDeviceToHost), "device gso");
-    for (int s = 0, i = 0; s < ns; ++s) {
-        Swarm& sw = G->swarms[s];
-        for (size_t k = 0; k < sw.g.size(); ++k, ++i) {
-            Glow& gw = sw.g[k];
-            gw.t[0] = a[0][i]; gw.t[1] = a[1][i]; gw.t[2] = a[2][i];
-            gw.r = {a[3][i], a[4][i], a[5][i], a[6][i]};
-            gw.luciferin = a[7][i]; gw.vision = a[8][i]; gw.scoring = a[9][i];
-            gw.moved = nid[i] != (int)k;
-            gw.exact_next = gw.moved;
-            gw.nb.assign((size_t)nid[n + i], 0u);   // the count only (state reports it)
-            gw.step += (uint32_t)steps;
-        }
-        sw.rng.set_words_used(2 * (draws[s] + (unsigned long long)steps * sw.g.size()));
+    return set_ok();
+}
+
+// luciferin, candidates, predictions and the move of one screened step
+// (kernel launches only: capturable)
+int dev_screened_tail(lkg_gso* G) {
+    cudaStream_t st = G->ctx->stream;
+    const lkg::GsoDevState& S = G->ds;
+    const lkg::GsoDevScreen& X = G->dx;
+    LKG_CK(lkg::gso_dev_screen_propose(S, X, st), "device gso step");
+    const int ng = (int)G->group_complex.size(), R = X.K + 1;
+    for (int gi = 0, g0 = 0; gi < ng; g0 += G->dcounts[gi], ++gi) {
+        if (!G->dcounts[gi]) continue;
+        int rc = lkg_surrogate_predict(G->sur[gi], G->dcounts[gi] * R, X.cand + (size_t)g0 * R * 7,
+                                       X.pred + (size_t)g0 * R);
+        if (rc) return rc;
     }
-    unsigned long long nsc = 0;
-    LKG_CK(cudaMemcpy(&nsc, S.nscored, sizeof(nsc), cudaMemcpyDeviceToHost), "device gso");
-    G->scored += (int64_t)nsc;
-    G->step += steps;
-    G->t_exact += now_s() - t0;
+    LKG_CK(lkg::gso_dev_screen_move(S, X, st), "device gso step");
+    return set_ok();
+}
+
+// screened steps on the device: every `rescore_every` steps a full exact
+// rescoring fine-tunes the surrogates (host-driven, as gso_step does); the
+// steps between replay one captured graph
+int dev_screened_steps(lkg_gso* G, int steps) {
+    lkg_ctx* ctx = G->ctx;
+    cudaStream_t st = ctx->stream;
+    lkg::GsoDevState& S = G->ds;
+    const lkg_screen& c = G->cfg;
+    const int ng = (int)G->group_complex.size();
+    for (int k = 0; k < steps; ++k) {
+        const bool rescore = c.rescore_every > 0 && G->step > c.train_steps &&
+                             (G->step - c.train_steps) % c.rescore_every == 0;
+        int rc;
+        if (rescore) {
+            LKG_CK(cudaMemsetAsync(S.mask, 1, (size_t)S.n, st), "device gso rescoring");
+            if ((rc = lkg::plan_launch_masked(G->dplan, S.poses, S.score, S.mask))) return rc;
+            // the exact pairs train the surrogates (score_phase learn + train_group)
+            std::vector<double> hp(7 * (size_t)S.n), hs(S.n);
+            LKG_CK(cudaMemcpyAsync(hp.data(), S.poses, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
+                   "device gso rescoring");
+            LKG_CK(cudaMemcpyAsync(hs.data(), S.score, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
+                   "device gso rescoring");
+            if ((rc = wait_stream(ctx, 300.0)) || (rc = check_status(ctx))) return rc;
+            for (int gi = 0, g0 = 0; gi < ng; g0 += G->dcounts[gi], ++gi) {
+                const int m = G->dcounts[gi];
+                G->tr_pose[gi].insert(G->tr_pose[gi].end(), hp.begin() + 7 * (size_t)g0, hp.begin() + 7 * (size_t)(g0 + m));
+                G->tr_score[gi].insert(G->tr_score[gi].end(), hs.begin() + g0, hs.begin() + g0 + m);
+                if ((rc = train_group(G, gi, c.finetune_epochs, (size_t)m))) return rc;
+            }
+            if ((rc = dev_screened_tail(G))) return rc;
+        } else {
+            const bool same = G->sexec && std::memcmp(&G->ds_captured, &S, sizeof(S)) == 0 &&
+                              std::memcmp(&G->dx_captured, &G->dx, sizeof(G->dx)) == 0;
+            if (!same) {
+                if (G->sexec) { cudaGraphExecDestroy(G->sexec); G->sexec = nullptr; }
+                // one eager step first (host-side queries of the plan and the surrogate)
+                if ((rc = lkg::plan_launch_masked(G->dplan, S.poses, S.score, S.mask)) || (rc = dev_screened_tail(G)))
+                    return rc;
+                G->step++;
+                G->predicted += (int64_t)S.n * (c.candidates + 1);
+                if (++k == steps) break;
+                if (G->step > c.train_steps && c.rescore_every > 0 && (G->step - c.train_steps) % c.rescore_every == 0) {
+                    --k;   // the next step is a rescoring one: no capture yet
+                    continue;
+                }
+                LKG_CK(cudaStreamSynchronize(st), "device gso");
+                LKG_CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal), "device gso capture");
+                rc = lkg::plan_launch_masked(G->dplan, S.poses, S.score, S.mask);
+                if (!rc) rc = dev_screened_tail(G);
+                cudaGraph_t graph = nullptr;
+                const cudaError_t e2 = cudaStreamEndCapture(st, &graph);
+                if (rc) { if (graph) cudaGraphDestroy(graph); return rc; }
+                if (e2 != cudaSuccess) {
+                    if (graph) cudaGraphDestroy(graph);
+                    return set_error(cuda_to_status(e2), "device gso capture failed");
+                }
+                const cudaError_t e3 = cudaGraphInstantiate(&G->sexec, graph, 0);
+                cudaGraphDestroy(graph);
+                if (e3 != cudaSuccess) return set_error(cuda_to_status(e3), "device gso graph: %s", cudaGetErrorString(e3));
+                G->ds_captured = S;
+                G->dx_captured = G->dx;
+            }
+            LKG_CK(cudaGraphLaunch(G->sexec, st), "device gso step");
+        }
+        G->step++;
+        G->predicted += (int64_t)S.n * (c.candidates + 1);
+    }
+    return set_ok();
+}
+
+}  // namespace
+
+extern "C" {
+
+// GSO steps on the device: the state goes up once, every step runs as kernel
+// launches (steps between full rescorings replayed from one CUDA graph), and
+// the state comes back at the end.  Plain runs: score (unmoved glowworms
+// are rescored with the same pose, which gives the same score), luciferin,
+// select, move.  Screened runs: the first train_steps steps run on the host
+// (they train the surrogates), then score the chosen moves, luciferin, K
+// selections, candidate predictions, the per-swarm exact choice and the
+// move, as screened_movement does.
+int lkg_gso_run_device(lkg_gso* G, int steps) {
+    if (!G || steps < 0) return set_error(LKG_ERR_ARG, "bad gso run");
+    if (G->screen && G->cfg.random_rank)
+        return set_error(LKG_ERR_STATE, "the device GSO screens with the surrogate only (not the ablation)");
+    cudaSetDevice(G->ctx->device);
+    int rc;
+    if (G->screen)   // the training steps (and the first training) run on the host
+        while (steps > 0 && G->step < G->cfg.train_steps) {
+            if ((rc = gso_step(G))) return rc;
+            --steps;
+        }
+    if (steps == 0 || G->swarms.empty()) return set_ok();
+    const double t0 = now_s(), tt0 = G->t_train;
+    if ((rc = dev_setup(G, G->screen))) return rc;
+    if (G->ds.n == 0) return set_ok();
+    const int step0 = G->step;
+    rc = G->screen ? dev_screened_steps(G, steps) : dev_plain_steps(G, steps);
+    if (rc) return rc;
+    if ((rc = wait_stream(G->ctx, 300.0)) || (rc = check_status(G->ctx))) return rc;
+    if (!G->screen) G->step += steps;
+    if ((rc = dev_download(G, G->step - step0, G->screen))) return rc;
+    G->t_exact += now_s() - t0 - (G->t_train - tt0);
     return set_ok();
 }
 

@@ -68,10 +68,12 @@ __global__ void k_gso_luciferin(GsoDevState S) {
     S.luc[i] = (1.0 - RHO) * S.luc[i] + GAMMA * S.score[i];
 }
 
-// neighbours (brighter, within the vision range, in id order) and the
-// roulette selection with the glowworm's draw (glowworm.rs:114-142); grid:
-// (swarms, ceil(max swarm size / blockDim))
-__global__ void k_gso_select(GsoDevState S) {
+// neighbours (brighter, within the vision range, in id order) and K
+// roulette selections with the glowworm's draws li*K .. li*K + K - 1 of the
+// step (glowworm.rs:114-142); out[i*K + k]: the selected neighbour (index
+// in the swarm, the glowworm itself when it has none); grid: (swarms,
+// ceil(max swarm size / blockDim))
+__global__ void k_gso_select(GsoDevState S, int K, int* __restrict__ out) {
     __shared__ double sx[256], sy[256], sz[256], sl[256];
     const int sw = blockIdx.x;
     const int first = S.swarm_first[sw], n = S.swarm_n[sw];
@@ -99,34 +101,34 @@ __global__ void k_gso_select(GsoDevState S) {
             }
         }
     }
-    // pass 2: roulette over prob_k = (l_k - l_i) / total in id order
-    const double u = act ? chacha_f64(S.keys + 8 * sw, S.draws[sw] + (unsigned long long)li) : 0.0;
-    double sum = 0.0;
-    int sel = -1, firstnb = -1;
-    bool stop = false;
-    for (int j0 = 0; j0 < n; j0 += blockDim.x) {   // block-uniform bounds: barriers inside
-        __syncthreads();
-        if (j0 + (int)threadIdx.x < n) {
-            const int j = first + j0 + threadIdx.x;
-            sx[threadIdx.x] = S.tx[j]; sy[threadIdx.x] = S.ty[j]; sz[threadIdx.x] = S.tz[j]; sl[threadIdx.x] = S.luc[j];
-        }
-        __syncthreads();
-        const int m = min((int)blockDim.x, n - j0);
-        for (int jj = 0; jj < m; ++jj) {
-            const double dx = x - sx[jj], dy = y - sy[jj], dz = z - sz[jj];
-            if (act && j0 + jj != li && l1 < sl[jj] && dx * dx + dy * dy + dz * dz < vr2) {
-                if (firstnb < 0) firstnb = j0 + jj;
-                if (!stop) {
+    // pass 2, once per draw: roulette over prob_k = (l_k - l_i) / total in
+    // id order
+    for (int kd = 0; kd < K; ++kd) {
+        const double u = act ? chacha_f64(S.keys + 8 * sw, S.draws[sw] + (unsigned long long)li * K + kd) : 0.0;
+        double sum = 0.0;
+        int sel = -1, firstnb = -1;
+        bool stop = cnt == 0;   // nothing to select (the scan still runs: barriers inside)
+        for (int j0 = 0; j0 < n; j0 += blockDim.x) {   // block-uniform bounds
+            __syncthreads();
+            if (j0 + (int)threadIdx.x < n) {
+                const int j = first + j0 + threadIdx.x;
+                sx[threadIdx.x] = S.tx[j]; sy[threadIdx.x] = S.ty[j]; sz[threadIdx.x] = S.tz[j];
+                sl[threadIdx.x] = S.luc[j];
+            }
+            __syncthreads();
+            const int m = min((int)blockDim.x, n - j0);
+            for (int jj = 0; jj < m && !stop; ++jj) {
+                const double dx = x - sx[jj], dy = y - sy[jj], dz = z - sz[jj];
+                if (act && j0 + jj != li && l1 < sl[jj] && dx * dx + dy * dy + dz * dz < vr2) {
+                    if (firstnb < 0) firstnb = j0 + jj;
                     if (sum < u) { sum += (sl[jj] - l1) / total; sel = j0 + jj; }
                     else stop = true;
                 }
             }
         }
+        if (act) out[(size_t)i * K + kd] = cnt == 0 ? li : (sel >= 0 ? sel : firstnb);
     }
-    if (act) {
-        S.nid[i] = cnt == 0 ? li : (sel >= 0 ? sel : firstnb);
-        S.nnb[i] = cnt;
-    }
+    if (act) S.nnb[i] = cnt;
 }
 
 __device__ __forceinline__ void qnorm(double& w, double& x, double& y, double& z) {   // qt.rs:36-46
@@ -134,16 +136,12 @@ __device__ __forceinline__ void qnorm(double& w, double& x, double& y, double& z
     w /= n; x /= n; y /= n; z /= n;
 }
 
-// movement towards the selected neighbour and vision update
-// (glowworm.rs:144-166, qt.rs:80-104); reads the step's starting state,
-// writes the new one into the second buffer
-__global__ void k_gso_move(GsoDevState S) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= S.n) return;
-    const int sw = S.swarm_of[i];
-    const int nid = S.swarm_first[sw] + S.nid[i];
-    double tx = S.tx[i], ty = S.ty[i], tz = S.tz[i];
-    double w = S.qw[i], x = S.qx[i], y = S.qy[i], z = S.qz[i];
+// pose of glowworm i after a move towards glowworm nid (glowworm.rs:144-166,
+// qt.rs:80-104), from the step's starting state; nid == i: unchanged
+__device__ void moved_pose(const GsoDevState& S, int i, int nid, double& tx, double& ty, double& tz, double& w,
+                           double& x, double& y, double& z) {
+    tx = S.tx[i]; ty = S.ty[i]; tz = S.tz[i];
+    w = S.qw[i]; x = S.qx[i]; y = S.qy[i]; z = S.qz[i];
     if (nid != i) {
         const double dx = S.tx[nid] - tx, dy = S.ty[nid] - ty, dz = S.tz[nid] - tz;
         const double norm = sqrt(dx * dx + dy * dy + dz * dz);
@@ -165,10 +163,25 @@ __global__ void k_gso_move(GsoDevState S) {
         }
         qnorm(w, x, y, z);
     }
+}
+
+__device__ __forceinline__ double new_vision(const GsoDevState& S, int i) {
     const double v = S.vis[i] + BETA * (double)(MAX_NEIGHBORS - S.nnb[i]);
+    return fmin(MAX_VISION, fmax(0.0, v));
+}
+
+// movement towards the selected neighbour and vision update; reads the
+// step's starting state, writes the new one into the second buffer
+__global__ void k_gso_move(GsoDevState S) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n) return;
+    const int sw = S.swarm_of[i];
+    const int nid = S.swarm_first[sw] + S.nid[i];
+    double tx, ty, tz, w, x, y, z;
+    moved_pose(S, i, nid, tx, ty, tz, w, x, y, z);
     S.ntx[i] = tx; S.nty[i] = ty; S.ntz[i] = tz;
     S.nqw[i] = w; S.nqx[i] = x; S.nqy[i] = y; S.nqz[i] = z;
-    S.nvis[i] = fmin(MAX_VISION, fmax(0.0, v));
+    S.nvis[i] = new_vision(S, i);
     S.mask[i] = nid != i;   // the next step scores the moved glowworms
 }
 
@@ -186,13 +199,145 @@ __global__ void k_gso_commit(GsoDevState S) {
     p[4] = S.tx[i]; p[5] = S.ty[i]; p[6] = S.tz[i];
 }
 
+// ---------------------------------------------------------------------------
+// screened steps (lkg_gso.cpp screened_movement, the same operations)
+// ---------------------------------------------------------------------------
+
+// moves left unscored take their predicted score (current + predicted gain)
+// before the luciferin update; the exact ones were scored this step
+__global__ void k_gso_luciferin_screened(GsoDevState S, GsoDevScreen X) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool scored = i < S.n && S.mask[i];
+    const unsigned b = __ballot_sync(0xffffffffu, scored);
+    if ((threadIdx.x & 31) == 0 && b) atomicAdd(S.nscored, (unsigned long long)__popc(b));
+    if (i >= S.n) return;
+    if (X.pend[i]) {   // a full rescoring step scored it exactly instead
+        if (!S.mask[i]) S.score[i] = S.score[i] + X.gain[i];
+        X.pend[i] = 0;
+    }
+    S.luc[i] = (1.0 - RHO) * S.luc[i] + GAMMA * S.score[i];
+}
+
+// candidate rows of glowworm i: its current pose, then the K moves (all
+// rows the current pose when it has no neighbours); the new vision range
+__global__ void k_gso_cand(GsoDevState S, GsoDevScreen X) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n) return;
+    const int K = X.K, first = S.swarm_first[S.swarm_of[i]];
+    double* row = X.cand + (size_t)i * (K + 1) * 7;
+    const double cur[7] = {S.qw[i], S.qx[i], S.qy[i], S.qz[i], S.tx[i], S.ty[i], S.tz[i]};
+    for (int c = 0; c < 7; ++c) row[c] = cur[c];
+    for (int k = 0; k < K; ++k) {
+        double* r = row + 7 * (k + 1);
+        if (S.nnb[i] > 0) {
+            double tx, ty, tz, w, x, y, z;
+            moved_pose(S, i, first + X.knid[(size_t)i * K + k], tx, ty, tz, w, x, y, z);
+            r[0] = w; r[1] = x; r[2] = y; r[3] = z; r[4] = tx; r[5] = ty; r[6] = tz;
+        } else {
+            for (int c = 0; c < 7; ++c) r[c] = cur[c];
+        }
+    }
+    S.nvis[i] = new_vision(S, i);
+}
+
+// the best predicted move (first maximum over rows 1..K) and its gain over
+// the current pose
+__global__ void k_gso_best(GsoDevState S, GsoDevScreen X) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= S.n) return;
+    const int K = X.K;
+    const double* p = X.pred + (size_t)i * (K + 1);
+    if (S.nnb[i] == 0) { X.best[i] = 0; X.gain[i] = 0.0; return; }
+    int best = 1;
+    for (int c = 2; c <= K; ++c)
+        if (p[c] > p[best]) best = c;
+    X.best[i] = best;
+    X.gain[i] = p[best] - p[0];
+}
+
+// per swarm, the ceil(frac * movers) movers with the largest gain (ties: the
+// lower id first) are scored exactly; one block per swarm, each mover's
+// rank counted against every other mover of the swarm
+__global__ void k_gso_rank(GsoDevState S, GsoDevScreen X) {
+    __shared__ double sg[256];
+    __shared__ int sm[256];
+    __shared__ int s_cnt;
+    const int sw = blockIdx.x;
+    const int first = S.swarm_first[sw], n = S.swarm_n[sw];
+    if (threadIdx.x == 0) s_cnt = 0;
+    __syncthreads();
+    int c = 0;
+    for (int li = threadIdx.x; li < n; li += blockDim.x) c += S.nnb[first + li] > 0;
+    atomicAdd(&s_cnt, c);
+    __syncthreads();
+    const int nx = (int)ceil(X.frac * (double)s_cnt);
+    for (int l0 = 0; l0 < n; l0 += blockDim.x) {   // this thread's mover l0 + tid
+        const int li = l0 + threadIdx.x;
+        const bool mine = li < n && S.nnb[first + li] > 0;
+        const double gi = mine ? X.gain[first + li] : 0.0;
+        int rank = 0;
+        for (int j0 = 0; j0 < n; j0 += blockDim.x) {   // block-uniform bounds: barriers inside
+            __syncthreads();
+            if (j0 + (int)threadIdx.x < n) {
+                const int j = first + j0 + threadIdx.x;
+                sg[threadIdx.x] = X.gain[j];
+                sm[threadIdx.x] = S.nnb[j] > 0;
+            }
+            __syncthreads();
+            const int m = min((int)blockDim.x, n - j0);
+            if (mine)
+                for (int jj = 0; jj < m; ++jj)
+                    rank += sm[jj] && (sg[jj] > gi || (sg[jj] == gi && j0 + jj < li));
+        }
+        if (li < n) X.exact[first + li] = mine && rank < nx;
+    }
+}
+
+// every glowworm with neighbours takes its best candidate; the exact ones
+// are scored next step, the others take current + gain before the next
+// luciferin update; the swarm's draw counter advances by K per glowworm
+__global__ void k_gso_commit_screened(GsoDevState S, GsoDevScreen X) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < S.n_swarms) S.draws[i] += (unsigned long long)X.K * S.swarm_n[i];
+    if (i >= S.n) return;
+    const bool moved = S.nnb[i] > 0;
+    if (moved) {
+        const double* r = X.cand + ((size_t)i * (X.K + 1) + X.best[i]) * 7;
+        S.qw[i] = r[0]; S.qx[i] = r[1]; S.qy[i] = r[2]; S.qz[i] = r[3];
+        S.tx[i] = r[4]; S.ty[i] = r[5]; S.tz[i] = r[6];
+    }
+    S.vis[i] = S.nvis[i];
+    S.mask[i] = moved && X.exact[i];
+    X.pend[i] = moved && !X.exact[i];
+    double* p = S.poses + 7 * (size_t)i;
+    p[0] = S.qw[i]; p[1] = S.qx[i]; p[2] = S.qy[i]; p[3] = S.qz[i];
+    p[4] = S.tx[i]; p[5] = S.ty[i]; p[6] = S.tz[i];
+}
+
 }  // namespace
+
+cudaError_t gso_dev_screen_propose(const GsoDevState& S, const GsoDevScreen& X, cudaStream_t s) {
+    const int t = 256, b = (S.n + t - 1) / t;
+    k_gso_luciferin_screened<<<b, t, 0, s>>>(S, X);
+    dim3 g(S.n_swarms, (S.max_swarm + 255) / 256);
+    k_gso_select<<<g, 256, 0, s>>>(S, X.K, X.knid);
+    k_gso_cand<<<b, t, 0, s>>>(S, X);
+    return cudaGetLastError();
+}
+
+cudaError_t gso_dev_screen_move(const GsoDevState& S, const GsoDevScreen& X, cudaStream_t s) {
+    const int t = 256, b = (S.n + t - 1) / t;
+    k_gso_best<<<b, t, 0, s>>>(S, X);
+    k_gso_rank<<<S.n_swarms, 256, 0, s>>>(S, X);
+    k_gso_commit_screened<<<(std::max(S.n, S.n_swarms) + t - 1) / t, t, 0, s>>>(S, X);
+    return cudaGetLastError();
+}
 
 cudaError_t gso_dev_after_scoring(const GsoDevState& S, cudaStream_t s) {
     const int t = 256, b = (S.n + t - 1) / t;   // full warps: the ballot in k_gso_luciferin
     k_gso_luciferin<<<b, t, 0, s>>>(S);
     dim3 g(S.n_swarms, (S.max_swarm + 255) / 256);
-    k_gso_select<<<g, 256, 0, s>>>(S);
+    k_gso_select<<<g, 256, 0, s>>>(S, 1, S.nid);
     k_gso_move<<<b, t, 0, s>>>(S);
     k_gso_commit<<<(std::max(S.n, S.n_swarms) + t - 1) / t, t, 0, s>>>(S);
     return cudaGetLastError();

@@ -171,8 +171,8 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
                 } else if (EPI == EPI_BWD) {
                     const float hm = __bfloat162float(Hmask[(size_t)gm * ldc + gn]);
                     Cb[(size_t)gm * ldc + gn] = __float2bfloat16(hm > 0.f ? v : 0.f);
-                } else {
-                    atomicAdd(Cf + (size_t)gm * ldc + gn, v);
+                } else {   // split blockIdx.z's partial tile; k_split_sum adds the splits in order
+                    Cf[(size_t)blockIdx.z * M * ldc + (size_t)gm * ldc + gn] = v;
                 }
             }
 }
@@ -328,33 +328,59 @@ __global__ void k_head(const __nv_bfloat16* __restrict__ H3, int n, const float*
     if (lane == 0) y[row] = s + b3[0];
 }
 
-// loss, dy = 2 (y - t) / n; dH3 = dy w3 x ReLU'(H3); head gradients
+// Every reduction of the backward pass adds its terms in a fixed order
+// (partials per block of rows or per split, then the partials in order), so
+// training is bitwise reproducible.
+constexpr int RB = 32;   // rows per partial sum
+
+// loss, dy = 2 (y - t) / n; dH3 = dy w3 x ReLU'(H3); per block of RB rows
+// (one thread per column) the partial head gradients sum_rows dy h (H
+// columns), sum dy and sum (y - t)^2 / n -> part[blk][H + 2]
 __global__ void k_loss(const float* __restrict__ y, const float* __restrict__ t, const __nv_bfloat16* __restrict__ H3,
-                       int n, const float* __restrict__ w3, __nv_bfloat16* __restrict__ dH3, float* __restrict__ g_w3,
-                       float* __restrict__ g_b3, float* __restrict__ loss) {
-    const int row = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
-    if (row >= n) return;
-    const float d = y[row] - t[row];
-    const float dy = 2.f * d / (float)n;
-    for (int k = lane; k < H; k += 32) {
-        const float h = __bfloat162float(H3[(size_t)row * H + k]);
-        dH3[(size_t)row * H + k] = __float2bfloat16(h > 0.f ? dy * w3[k] : 0.f);
-        atomicAdd(g_w3 + k, dy * h);
+                       int n, const float* __restrict__ w3, __nv_bfloat16* __restrict__ dH3, float* __restrict__ part) {
+    const int k = threadIdx.x, r0 = blockIdx.x * RB, r1 = min(n, r0 + RB);
+    float gw = 0.f, gb = 0.f, ls = 0.f;
+    for (int r = r0; r < r1; ++r) {
+        const float d = y[r] - t[r];
+        const float dy = 2.f * d / (float)n;
+        const float h = __bfloat162float(H3[(size_t)r * H + k]);
+        dH3[(size_t)r * H + k] = __float2bfloat16(h > 0.f ? dy * w3[k] : 0.f);
+        gw += dy * h;
+        gb += dy;
+        ls += d * d / (float)n;
     }
-    if (lane == 0) {
-        atomicAdd(g_b3, dy);
-        atomicAdd(loss, d * d / (float)n);
-    }
+    float* p = part + (size_t)blockIdx.x * (H + 2);
+    p[k] = gw;
+    if (k == 0) { p[H] = gb; p[H + 1] = ls; }
 }
 
-// bias gradients: column sums of dC [n x H]
-__global__ void k_colsum(const __nv_bfloat16* __restrict__ dC, int n, float* __restrict__ gb) {
-    const int col = blockIdx.x * blockDim.x + threadIdx.x;
-    if (col >= H) return;
-    const int r0 = blockIdx.y * 32, r1 = min(n, r0 + 32);
+// head gradients (w3, b3: contiguous) and the loss (added to the running
+// epoch sum) from the row-block partials, in block order
+__global__ void k_head_sum(const float* __restrict__ part, int nblk, float* __restrict__ g_w3b3,
+                           float* __restrict__ loss) {
+    const int k = threadIdx.x;
+    if (k > H + 1) return;
+    float s = 0.f;
+    for (int b = 0; b < nblk; ++b) s += part[(size_t)b * (H + 2) + k];
+    if (k <= H) g_w3b3[k] = s;
+    else *loss += s;
+}
+
+// bias gradients: column sums of dC [n x H] per block of RB rows -> part[blk][H]
+__global__ void k_colsum(const __nv_bfloat16* __restrict__ dC, int n, float* __restrict__ part) {
+    const int col = threadIdx.x, r0 = blockIdx.x * RB, r1 = min(n, r0 + RB);
     float s = 0.f;
     for (int r = r0; r < r1; ++r) s += __bfloat162float(dC[(size_t)r * H + col]);
-    atomicAdd(gb + col, s);
+    part[(size_t)blockIdx.x * H + col] = s;
+}
+
+// out[i] = sum over z = 0, 1, ... of part[z * count + i]
+__global__ void k_split_sum(const float* __restrict__ part, int nz, int count, float* __restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    float s = 0.f;
+    for (int z = 0; z < nz; ++z) s += part[(size_t)z * count + i];
+    out[i] = s;
 }
 
 // the three GEMM layers inside the flat parameter vector
@@ -427,6 +453,7 @@ struct lkg_surrogate {
     DBuf wt[3], w[3];   // BF16 layouts per GEMM layer
     // activations for a batch
     DBuf X, H1, H2, H3, dH1, dH2, dH3, y, t, loss;
+    DBuf wpart, rpart;   // backward partial sums: per split (weight gradients), per row block
     int cap = 0;     // rows of X, H1..H3, y, t (forward)
     int cap_b = 0;   // rows of dH1..dH3 (backward)
     DBuf d_step;   // Adam step count (device, 1-based)
@@ -442,6 +469,10 @@ constexpr size_t NPARAM = (size_t)H * IN + H + 2 * ((size_t)H * H + H) + H + 1;
 // predictions run in chunks of at most this many rows, so the inference
 // buffers stay bounded and are sized once
 constexpr int PRED_CHUNK = 65536;
+
+// weight gradients reduce over the batch: split it so that the 16 output
+// tiles of a layer still fill the GPU
+int wgrad_splits(int n) { return std::max(1, std::min(64, n / 64)); }
 
 // activation buffers for n rows: forward ones always, backward ones when
 // `bwd` (training); growing reallocates (and so synchronises the device),
@@ -464,17 +495,22 @@ int sur_reserve(lkg_surrogate* S, int n, bool bwd) {
         LKG_CK(S->dH1.reserve(nb * H), "surrogate alloc");
         LKG_CK(S->dH2.reserve(nb * H), "surrogate alloc");
         LKG_CK(S->dH3.reserve(nb * H), "surrogate alloc");
+        LKG_CK(S->wpart.reserve((size_t)wgrad_splits(m) * H * H * sizeof(float)), "surrogate alloc");
+        LKG_CK(S->rpart.reserve((size_t)((m + RB - 1) / RB) * (H + 2) * sizeof(float)), "surrogate alloc");
         S->cap_b = m;
     }
     return 0;
 }
 
+// split-K: rows of K per split (a multiple of BK) and the number of splits
+int split_chunk(int K, int splits) { return ((K + splits - 1) / splits + BK - 1) / BK * BK; }
+int split_count(int K, int splits) { return (K + split_chunk(K, splits) - 1) / split_chunk(K, splits); }
+
 template <bool TA, bool TB, int EPI>
 cudaError_t gemm(cudaStream_t s, int M, int N, int K, const __nv_bfloat16* A, int lda, const __nv_bfloat16* B, int ldb,
                  float* Cf, __nv_bfloat16* Cb, int ldc, const float* bias, const __nv_bfloat16* Hm, int splits = 1) {
-    int kc = (K + splits - 1) / splits;
-    kc = (kc + BK - 1) / BK * BK;
-    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, (K + kc - 1) / kc);
+    const int kc = split_chunk(K, splits);
+    dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM, split_count(K, splits));
     k_gemm<TA, TB, EPI><<<grid, 128, 0, s>>>(M, N, K, A, lda, B, ldb, Cf, Cb, ldc, bias, Hm, kc);
     return cudaGetLastError();
 }
@@ -523,23 +559,25 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
     cudaStream_t s = S->ctx->stream;
     LKG_CK(cudaMemsetAsync(S->g.p, 0, NPARAM * sizeof(float), s), "mlp grad clear");
     if (clear_loss) LKG_CK(cudaMemsetAsync(S->loss.p, 0, sizeof(float), s), "mlp loss clear");
-    k_loss<<<(n + 7) / 8, 256, 0, s>>>(S->y.as<float>(), S->t.as<float>(), S->H3.as<__nv_bfloat16>(), n, P(S, 6),
-                                       S->dH3.as<__nv_bfloat16>(), Gd(S, 6), Gd(S, 7), S->loss.as<float>());
+    const int nblk = (n + RB - 1) / RB;
+    float* rpart = S->rpart.as<float>();
+    float* wpart = S->wpart.as<float>();
+    k_loss<<<nblk, H, 0, s>>>(S->y.as<float>(), S->t.as<float>(), S->H3.as<__nv_bfloat16>(), n, P(S, 6),
+                              S->dH3.as<__nv_bfloat16>(), rpart);
+    k_head_sum<<<1, H + 2, 0, s>>>(rpart, nblk, Gd(S, 6), S->loss.as<float>());
     LKG_CK(cudaGetLastError(), "mlp loss");
-    // weight gradients reduce over the batch: split it so that the 16 output
-    // tiles of a layer still fill the GPU (split-K partial sums meet in FP32
-    // atomics)
-    const int splits = std::max(1, std::min(64, n / 64));
+    const int splits = wgrad_splits(n);
     const __nv_bfloat16* acts[3] = {S->H1.as<__nv_bfloat16>(), S->H2.as<__nv_bfloat16>(), S->H3.as<__nv_bfloat16>()};
     __nv_bfloat16* dacts[3] = {S->dH1.as<__nv_bfloat16>(), S->dH2.as<__nv_bfloat16>(), S->dH3.as<__nv_bfloat16>()};
     for (int L = 2; L >= 0; --L) {
         const int kin = L == 0 ? IN : H;
         const __nv_bfloat16* ain = L == 0 ? S->X.as<__nv_bfloat16>() : acts[L - 1];
         // dW_L[o][i] = sum_n dC[n][o] * A_in[n][i]   (A = dC^T, B = A_in^T)
-        LKG_CK((gemm<true, true, EPI_WGRAD>(s, H, kin, n, dacts[L], H, ain, kin, Gd(S, 2 * L), nullptr, kin, nullptr,
+        LKG_CK((gemm<true, true, EPI_WGRAD>(s, H, kin, n, dacts[L], H, ain, kin, wpart, nullptr, kin, nullptr,
                                             nullptr, splits)), "mlp wgrad");
-        dim3 cg((H + 255) / 256, (n + 31) / 32);
-        k_colsum<<<cg, 256, 0, s>>>(dacts[L], n, Gd(S, 2 * L + 1));
+        k_split_sum<<<(H * kin + 255) / 256, 256, 0, s>>>(wpart, split_count(n, splits), H * kin, Gd(S, 2 * L));
+        k_colsum<<<nblk, H, 0, s>>>(dacts[L], n, rpart);
+        k_split_sum<<<1, H, 0, s>>>(rpart, nblk, H, Gd(S, 2 * L + 1));
         LKG_CK(cudaGetLastError(), "mlp bias grad");
         if (L > 0) {
             // dA_in[n][i] = (sum_o dC[n][o] W_L[o][i]) x ReLU'(A_in)
@@ -547,7 +585,7 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
                                                 dacts[L - 1], H, nullptr, acts[L - 1])), "mlp bwd");
         }
     }
-    S->ctx->launches += 10;
+    S->ctx->launches += 14;
     return 0;
 }
 
