@@ -71,6 +71,45 @@ struct WSlots {
     unsigned hit[WRing<G>::N];  // (slot << 26) | receptor index
 };
 
+// Receptor-side minima of the fast cpydock kernel: one 64-bit word per slot,
+// the minimum d^2 quantised to 37 bits (0 .. SOLV2_D in steps of 3e-10 A^2)
+// above the 27-bit receptor index, so one atomicMin updates a slot (the key
+// bits are equal) and a slot costs 8 bytes of shared memory instead of 12.
+// Only pairs with d^2 <= SOLV2_D are inserted; the receptor term's
+// sqrt(d^2) then moves by < 1e-10 A.
+struct MinHash64 {
+    static constexpr unsigned long long EMPTY = ~0ull;
+    static constexpr unsigned long long KEY_MASK = (1ull << 27) - 1;
+    static constexpr double SCALE = (double)((1ull << 37) - 1) / SOLV2_D;
+    unsigned long long* slot;
+    int cap;
+    __device__ void init(char* smem, int cap_) {
+        cap = cap_;
+        slot = reinterpret_cast<unsigned long long*>(smem);
+        for (int s = threadIdx.x; s < cap; s += blockDim.x) slot[s] = EMPTY;
+    }
+    // k < 2^26 (the receptor index limit); 0 <= d2 <= SOLV2_D
+    __device__ bool insert(int k, double d2) {
+        const unsigned long long w = (__double2ull_rn(d2 * SCALE) << 27) | (unsigned long long)k;
+        unsigned h = ((unsigned)k * 2654435761u) & (unsigned)(cap - 1);
+        for (int probe = 0; probe < cap; ++probe) {
+            unsigned long long v = slot[h];
+            if (v == EMPTY) {
+                v = atomicCAS(slot + h, EMPTY, w);
+                if (v == EMPTY) return true;
+            }
+            if ((v & KEY_MASK) == (unsigned long long)k) {
+                atomicMin(slot + h, w);
+                return true;
+            }
+            h = (h + 1) & (unsigned)(cap - 1);
+        }
+        return false;
+    }
+    __device__ int key(int s) const { return slot[s] == EMPTY ? -1 : (int)(slot[s] & KEY_MASK); }
+    __device__ double value(int s) const { return fmin((double)(slot[s] >> 27) / SCALE, SOLV2_D); }
+};
+
 // IFACE: start a unit of pose bits `bits` (lane 0; the caller syncs the
 // warp after): collect in the warp's buffer when the pose fits in it
 template <int G>
@@ -102,7 +141,7 @@ __device__ __forceinline__ void w_iface_flush(WSlots<G>& W, const ComplexDev& c)
 // position as f32 value + residual, ~2^-48 relative) and set the pose's
 // interface bits.
 template <int G, bool DESOLV, bool IFACE>
-__device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, WDes<G>* D, MinHash* hash,
+__device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, WDes<G>* D, MinHash64* hash,
                                        int* status, unsigned e, unsigned flags, unsigned* iset, double& elec,
                                        double& vdw, int& np) {
     const int l = (int)(e >> 26), k = (int)(e & 0x3ffffffu);
@@ -180,6 +219,7 @@ __device__ __forceinline__ void w_fetch(const ComplexDev& c, int st, int excl, i
 
 constexpr unsigned long long W_NOMIN = 0x7fefffffffffffffull;   // largest finite double
 
+
 // The warp's sums over its groups.
 struct WAcc {
     double elec = 0.0, vdw = 0.0, solv = 0.0;
@@ -190,7 +230,7 @@ struct WAcc {
 // rotation is in W.rot, into acc (per lane).  DESOLV also adds each slot
 // atom's g(min d^2) * des to acc.solv once its hits are all evaluated.
 template <int G, bool DESOLV, bool IFACE>
-__device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes<G>* D, MinHash* hash, int* status,
+__device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes<G>* D, MinHash64* hash, int* status,
                                          int g_first, int g_end, int g_step, WAcc& acc) {
     constexpr int RING = WRing<G>::N;
     constexpr unsigned FULL = 0xffffffffu;
@@ -417,16 +457,19 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
 // cpydock: one block per pose (the receptor-side minima live in the block's
 // shared-memory hash); warp k takes the pose's groups k, k + NW, ... (a fixed
 // assignment: the sums do not depend on scheduling).  Block layout of the
-// dynamic shared memory: hash (hcap x 12 B), then NW x WSlots, NW x WDes.
-constexpr int WD_THREADS = 512;
+// dynamic shared memory: hash (hcap x 8 B), then NW x WSlots, NW x WDes.
+// 12 warps a block: with groups of 8 and the largest hash (64 KB) two
+// blocks fit an SM (24 warps resident, registers capped for it).
+constexpr int WD_THREADS = 384;
+constexpr int WD_BLOCKS = 2;
 
 template <int G>
 __host__ __device__ constexpr size_t wd_smem(int hcap) {
-    return (size_t)hcap * 12 + (size_t)(WD_THREADS / 32) * (sizeof(WSlots<G>) + sizeof(WDes<G>));
+    return (size_t)hcap * sizeof(unsigned long long) + (size_t)(WD_THREADS / 32) * (sizeof(WSlots<G>) + sizeof(WDes<G>));
 }
 
 template <int G, bool IFACE>
-__global__ void __launch_bounds__(WD_THREADS, 1) k_score_warp_desolv(LaunchParams p) {
+__global__ void __launch_bounds__(WD_THREADS, WD_BLOCKS) k_score_warp_desolv(LaunchParams p) {
     constexpr int NW = WD_THREADS / 32;
     extern __shared__ __align__(16) unsigned char wd_smem_raw[];
     __shared__ long long s_work;
@@ -444,9 +487,9 @@ __global__ void __launch_bounds__(WD_THREADS, 1) k_score_warp_desolv(LaunchParam
         const int pose = (int)(w - __ldg(p.item_work0 + b));
         const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
         if (p.pose_mask && !p.pose_mask[g]) continue;   // block-uniform: pose skipped
-        MinHash hash;
+        MinHash64 hash;
         hash.init(reinterpret_cast<char*>(wd_smem_raw), c.hcap);
-        unsigned char* base = wd_smem_raw + (size_t)c.hcap * 12;
+        unsigned char* base = wd_smem_raw + (size_t)c.hcap * sizeof(unsigned long long);
         WSlots<G>& W = reinterpret_cast<WSlots<G>*>(base)[wid];
         WDes<G>* D = reinterpret_cast<WDes<G>*>(base + (size_t)NW * sizeof(WSlots<G>)) + wid;
         if (IFACE) W.ibuf[lane] = 0u;   // the slots move with the complex's hash size
@@ -464,7 +507,7 @@ __global__ void __launch_bounds__(WD_THREADS, 1) k_score_warp_desolv(LaunchParam
         // depends on insertion races, integer sums do not
         long long fix = 0;
         for (int s = threadIdx.x; s < c.hcap; s += blockDim.x) {
-            const int k = hash.keys[s];
+            const int k = hash.key(s);
             if (k < 0) continue;
             const double2 rs = c.rsolv64[k];
             fix += __double2ll_rn(solv_term(hash.value(s), rs.y) * rs.x * 1099511627776.0);
