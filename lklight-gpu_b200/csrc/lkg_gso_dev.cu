@@ -71,64 +71,77 @@ __global__ void k_gso_luciferin(GsoDevState S) {
 // neighbours (brighter, within the vision range, in id order) and K
 // roulette selections with the glowworm's draws li*K .. li*K + K - 1 of the
 // step (glowworm.rs:114-142); out[i*K + k]: the selected neighbour (index
-// in the swarm, the glowworm itself when it has none); grid: (swarms,
-// ceil(max swarm size / blockDim))
+// in the swarm, the glowworm itself when it has none).
+//
+// One warp per glowworm.  The lanes test 32 swarm members at a time (the
+// exact f64 test of the host); the neighbours of a chunk (a ballot) are then
+// walked in id order with every lane doing the same f64 additions, so the
+// total and the running sum are the host's, bit for bit.  Lane k keeps draw
+// k (and k + 32): the roulette for a draw stops at the first neighbour whose
+// running sum before it is not below the draw, as the host's loop does; the
+// sums of the draws agree until they stop, so one running sum serves all.
 __global__ void k_gso_select(GsoDevState S, int K, int* __restrict__ out) {
-    __shared__ double sx[256], sy[256], sz[256], sl[256];
-    const int sw = blockIdx.x;
-    const int first = S.swarm_first[sw], n = S.swarm_n[sw];
-    const int li = blockIdx.y * blockDim.x + threadIdx.x;
-    const bool act = li < n;
-    const int i = first + (act ? li : 0);
+    const int lane = threadIdx.x & 31;
+    const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    if (i >= S.n) return;   // warp-uniform
+    const int sw = S.swarm_of[i];
+    const int first = S.swarm_first[sw], n = S.swarm_n[sw], li = i - first;
     const double x = S.tx[i], y = S.ty[i], z = S.tz[i], l1 = S.luc[i], v = S.vis[i];
     const double vr2 = v * v;
+    // pass 1: count and total of the luciferin differences, id order
     int cnt = 0;
     double total = 0.0;
-    // pass 1: count and total of the luciferin differences, id order
-    for (int j0 = 0; j0 < n; j0 += blockDim.x) {
-        __syncthreads();
-        if (j0 + (int)threadIdx.x < n) {
-            const int j = first + j0 + threadIdx.x;
-            sx[threadIdx.x] = S.tx[j]; sy[threadIdx.x] = S.ty[j]; sz[threadIdx.x] = S.tz[j]; sl[threadIdx.x] = S.luc[j];
+    for (int j0 = 0; j0 < n; j0 += 32) {
+        const int jl = j0 + lane;
+        bool nb = false;
+        double lj = 0.0;
+        if (jl < n) {
+            const int j = first + jl;
+            const double dx = x - S.tx[j], dy = y - S.ty[j], dz = z - S.tz[j];
+            lj = S.luc[j];
+            nb = jl != li && l1 < lj && dx * dx + dy * dy + dz * dz < vr2;
         }
-        __syncthreads();
-        const int m = min((int)blockDim.x, n - j0);
-        for (int jj = 0; jj < m; ++jj) {
-            const double dx = x - sx[jj], dy = y - sy[jj], dz = z - sz[jj];
-            if (act && j0 + jj != li && l1 < sl[jj] && dx * dx + dy * dy + dz * dz < vr2) {
-                ++cnt;
-                total += sl[jj] - l1;
-            }
+        unsigned m = __ballot_sync(0xffffffffu, nb);
+        cnt += __popc(m);
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            total += __shfl_sync(0xffffffffu, lj, b) - l1;
         }
     }
-    // pass 2, once per draw: roulette over prob_k = (l_k - l_i) / total in
-    // id order
-    for (int kd = 0; kd < K; ++kd) {
-        const double u = act ? chacha_f64(S.keys + 8 * sw, S.draws[sw] + (unsigned long long)li * K + kd) : 0.0;
-        double sum = 0.0;
-        int sel = -1, firstnb = -1;
-        bool stop = cnt == 0;   // nothing to select (the scan still runs: barriers inside)
-        for (int j0 = 0; j0 < n; j0 += blockDim.x) {   // block-uniform bounds
-            __syncthreads();
-            if (j0 + (int)threadIdx.x < n) {
-                const int j = first + j0 + threadIdx.x;
-                sx[threadIdx.x] = S.tx[j]; sy[threadIdx.x] = S.ty[j]; sz[threadIdx.x] = S.tz[j];
-                sl[threadIdx.x] = S.luc[j];
-            }
-            __syncthreads();
-            const int m = min((int)blockDim.x, n - j0);
-            for (int jj = 0; jj < m && !stop; ++jj) {
-                const double dx = x - sx[jj], dy = y - sy[jj], dz = z - sz[jj];
-                if (act && j0 + jj != li && l1 < sl[jj] && dx * dx + dy * dy + dz * dz < vr2) {
-                    if (firstnb < 0) firstnb = j0 + jj;
-                    if (sum < u) { sum += (sl[jj] - l1) / total; sel = j0 + jj; }
-                    else stop = true;
-                }
-            }
+    // pass 2: the roulettes over prob = (l_j - l_i) / total in id order
+    const unsigned long long d0 = S.draws[sw] + (unsigned long long)li * K;
+    const double u0 = lane < K ? chacha_f64(S.keys + 8 * sw, d0 + lane) : 0.0;
+    const double u1 = lane + 32 < K ? chacha_f64(S.keys + 8 * sw, d0 + lane + 32) : 0.0;
+    int sel0 = -1, sel1 = -1, firstnb = -1;
+    bool stop0 = lane >= K, stop1 = lane + 32 >= K;
+    double sum = 0.0;
+    for (int j0 = 0; j0 < n && cnt > 0 && !__all_sync(0xffffffffu, stop0 && stop1); j0 += 32) {
+        const int jl = j0 + lane;
+        bool nb = false;
+        double lj = 0.0;
+        if (jl < n) {
+            const int j = first + jl;
+            const double dx = x - S.tx[j], dy = y - S.ty[j], dz = z - S.tz[j];
+            lj = S.luc[j];
+            nb = jl != li && l1 < lj && dx * dx + dy * dy + dz * dz < vr2;
         }
-        if (act) out[(size_t)i * K + kd] = cnt == 0 ? li : (sel >= 0 ? sel : firstnb);
+        unsigned m = __ballot_sync(0xffffffffu, nb);
+        while (m) {
+            const int b = __ffs(m) - 1;
+            m &= m - 1;
+            const int jn = j0 + b;
+            const double p = (__shfl_sync(0xffffffffu, lj, b) - l1) / total;
+            if (firstnb < 0) firstnb = jn;
+            if (!stop0) { if (sum < u0) sel0 = jn; else stop0 = true; }
+            if (!stop1) { if (sum < u1) sel1 = jn; else stop1 = true; }
+            sum += p;
+        }
     }
-    if (act) S.nnb[i] = cnt;
+    int* o = out + (size_t)i * K;
+    if (lane < K) o[lane] = cnt == 0 ? li : (sel0 >= 0 ? sel0 : firstnb);
+    if (lane + 32 < K) o[lane + 32] = cnt == 0 ? li : (sel1 >= 0 ? sel1 : firstnb);
+    if (lane == 0) S.nnb[i] = cnt;
 }
 
 __device__ __forceinline__ void qnorm(double& w, double& x, double& y, double& z) {   // qt.rs:36-46
@@ -256,41 +269,31 @@ __global__ void k_gso_best(GsoDevState S, GsoDevScreen X) {
 }
 
 // per swarm, the ceil(frac * movers) movers with the largest gain (ties: the
-// lower id first) are scored exactly; one block per swarm, each mover's
-// rank counted against every other mover of the swarm
+// lower id first) are scored exactly.  One warp per glowworm counts, 32
+// swarm members at a time, the movers and the movers ranked ahead of it.
 __global__ void k_gso_rank(GsoDevState S, GsoDevScreen X) {
-    __shared__ double sg[256];
-    __shared__ int sm[256];
-    __shared__ int s_cnt;
-    const int sw = blockIdx.x;
-    const int first = S.swarm_first[sw], n = S.swarm_n[sw];
-    if (threadIdx.x == 0) s_cnt = 0;
-    __syncthreads();
-    int c = 0;
-    for (int li = threadIdx.x; li < n; li += blockDim.x) c += S.nnb[first + li] > 0;
-    atomicAdd(&s_cnt, c);
-    __syncthreads();
-    const int nx = (int)ceil(X.frac * (double)s_cnt);
-    for (int l0 = 0; l0 < n; l0 += blockDim.x) {   // this thread's mover l0 + tid
-        const int li = l0 + threadIdx.x;
-        const bool mine = li < n && S.nnb[first + li] > 0;
-        const double gi = mine ? X.gain[first + li] : 0.0;
-        int rank = 0;
-        for (int j0 = 0; j0 < n; j0 += blockDim.x) {   // block-uniform bounds: barriers inside
-            __syncthreads();
-            if (j0 + (int)threadIdx.x < n) {
-                const int j = first + j0 + threadIdx.x;
-                sg[threadIdx.x] = X.gain[j];
-                sm[threadIdx.x] = S.nnb[j] > 0;
-            }
-            __syncthreads();
-            const int m = min((int)blockDim.x, n - j0);
-            if (mine)
-                for (int jj = 0; jj < m; ++jj)
-                    rank += sm[jj] && (sg[jj] > gi || (sg[jj] == gi && j0 + jj < li));
+    const int lane = threadIdx.x & 31;
+    const int i = (int)((blockIdx.x * (size_t)blockDim.x + threadIdx.x) >> 5);
+    if (i >= S.n) return;   // warp-uniform
+    const int sw = S.swarm_of[i];
+    const int first = S.swarm_first[sw], n = S.swarm_n[sw], li = i - first;
+    const bool mine = S.nnb[i] > 0;
+    const double gi = X.gain[i];
+    int movers = 0, ahead = 0;
+    for (int j0 = 0; j0 < n; j0 += 32) {
+        const int jl = j0 + lane;
+        bool mv = false, up = false;
+        if (jl < n) {
+            const int j = first + jl;
+            mv = S.nnb[j] > 0;
+            const double gj = X.gain[j];
+            up = mv && (gj > gi || (gj == gi && jl < li));
         }
-        if (li < n) X.exact[first + li] = mine && rank < nx;
+        movers += __popc(__ballot_sync(0xffffffffu, mv));
+        ahead += __popc(__ballot_sync(0xffffffffu, up));
     }
+    const int nx = (int)ceil(X.frac * (double)movers);
+    if (lane == 0) X.exact[i] = mine && ahead < nx;
 }
 
 // every glowworm with neighbours takes its best candidate; the exact ones
@@ -319,8 +322,8 @@ __global__ void k_gso_commit_screened(GsoDevState S, GsoDevScreen X) {
 cudaError_t gso_dev_screen_propose(const GsoDevState& S, const GsoDevScreen& X, cudaStream_t s) {
     const int t = 256, b = (S.n + t - 1) / t;
     k_gso_luciferin_screened<<<b, t, 0, s>>>(S, X);
-    dim3 g(S.n_swarms, (S.max_swarm + 255) / 256);
-    k_gso_select<<<g, 256, 0, s>>>(S, X.K, X.knid);
+    const int wb = (int)(((size_t)S.n * 32 + 255) / 256);   // one warp per glowworm
+    k_gso_select<<<wb, 256, 0, s>>>(S, X.K, X.knid);
     k_gso_cand<<<b, t, 0, s>>>(S, X);
     return cudaGetLastError();
 }
@@ -328,7 +331,7 @@ cudaError_t gso_dev_screen_propose(const GsoDevState& S, const GsoDevScreen& X, 
 cudaError_t gso_dev_screen_move(const GsoDevState& S, const GsoDevScreen& X, cudaStream_t s) {
     const int t = 256, b = (S.n + t - 1) / t;
     k_gso_best<<<b, t, 0, s>>>(S, X);
-    k_gso_rank<<<S.n_swarms, 256, 0, s>>>(S, X);
+    k_gso_rank<<<(int)(((size_t)S.n * 32 + 255) / 256), 256, 0, s>>>(S, X);
     k_gso_commit_screened<<<(std::max(S.n, S.n_swarms) + t - 1) / t, t, 0, s>>>(S, X);
     return cudaGetLastError();
 }
@@ -336,8 +339,7 @@ cudaError_t gso_dev_screen_move(const GsoDevState& S, const GsoDevScreen& X, cud
 cudaError_t gso_dev_after_scoring(const GsoDevState& S, cudaStream_t s) {
     const int t = 256, b = (S.n + t - 1) / t;   // full warps: the ballot in k_gso_luciferin
     k_gso_luciferin<<<b, t, 0, s>>>(S);
-    dim3 g(S.n_swarms, (S.max_swarm + 255) / 256);
-    k_gso_select<<<g, 256, 0, s>>>(S, 1, S.nid);
+    k_gso_select<<<(int)(((size_t)S.n * 32 + 255) / 256), 256, 0, s>>>(S, 1, S.nid);   // a warp per glowworm
     k_gso_move<<<b, t, 0, s>>>(S);
     k_gso_commit<<<(std::max(S.n, S.n_swarms) + t - 1) / t, t, 0, s>>>(S);
     return cudaGetLastError();
