@@ -322,12 +322,16 @@ int lkg_gso_create(lkg_ctx* ctx, int n_groups, const int* complex_ids, const int
                    const int* n_glow, const double* positions, const uint64_t* seeds, lkg_gso** out);
 /* steps x (score moved glowworms of all swarms in one launch group; move) */
 int lkg_gso_run(lkg_gso* gso, int steps);
-/* The same plain GSO steps with the whole step on the device (no
- * counterpart in the reference): every glowworm scored, luciferin,
- * neighbour selection (the swarm's StdRng stream, drawn on the device) and
- * movement as kernel launches replayed from one CUDA graph.  Its f64
- * arithmetic is the host GSO's except acos / sin in the slerp (device
- * library), so runs agree closely at first and then drift apart. */
+/* The same GSO steps with the whole step on the device (no counterpart in
+ * the reference): scoring, luciferin, neighbour selection (the swarm's
+ * StdRng stream, drawn on the device) and movement as kernel launches
+ * replayed from one CUDA graph.  Its f64 arithmetic is the host GSO's
+ * except acos / sin in the slerp (device library), so runs agree closely at
+ * first and then drift apart.  On a screened GSO (lkg_gso_set_screen) the
+ * training steps run on the host and the screened steps after them on the
+ * device (candidates, predictions, the exact choice, the move; a full
+ * rescoring fine-tunes from the host); the no-network ablation is refused
+ * (LKG_ERR_STATE).  Host and device steps can be mixed. */
 int lkg_gso_run_device(lkg_gso* gso, int steps);
 int lkg_gso_state(lkg_gso* gso, double* trans, double* rot, double* luc, double* scoring,
                   double* vision, int32_t* nneigh);

@@ -372,8 +372,10 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
 #pragma unroll
                 for (int l = 0; l < G; ++l) {
                     const float4 t = W.ltest[set + l];
-                    const float q = fmaf(ax, t.x, fmaf(ay, t.y, fmaf(az, t.z, aa + t.w)));
-                    const bool h = q <= 0.f;
+                    // |a'|^2 - 2 a'.l' <= -(|l'|^2 - 100.01): three FMAs, the
+                    // slot's constant on the right (invalid slots: -3e30)
+                    const float q = fmaf(ax, t.x, fmaf(ay, t.y, fmaf(az, t.z, aa)));
+                    const bool h = q <= -t.w;
                     const unsigned b = __ballot_sync(FULL, h);
                     if (h) W.hit[(tail + __popc(b & lt_mask)) & (RING - 1)] = enc + ((unsigned)l << 26);
                     tail += (unsigned)__popc(b);
