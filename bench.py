@@ -56,6 +56,8 @@ def parse():
                              "restraints"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--gso-loop-steps", type=int, default=100,
+                    help="GSO steps of the step-loop measurement (batched workload; 0: skip it)")
     ap.add_argument("--tile", type=int, default=0)
     ap.add_argument("--cell", type=float, default=0.0)
     ap.add_argument("--group", type=int, default=0)
@@ -337,6 +339,30 @@ def main():
         plain = {"value": npose / (pms / 1e3), "unit": "poses/s", "ms_per_step": pms,
                  "what": "lkg_score per complex, host buffers, one launch and sync per complex"}
 
+    # the whole GSO step loop of the batched workload: every swarm of every
+    # complex as one device-resident GSO (one persistent scoring launch of
+    # the moved glowworms per step plus the GSO kernels, graph-replayed);
+    # exact poses / s over the loop, wall time including set-up and the
+    # state's read-back
+    gso_loop = None
+    if args.workload == "config2" and args.gso_loop_steps > 0:
+        groups = [(cid, it["swarms"], it["glowworms"]) for cid, it in zip(ids, items)]
+        host_pos = np.hstack([allp[:, 4:7], allp[:, 0:4]])   # (tx, ty, tz, qw, qx, qy, qz)
+        g = lkg.GSO(ctx, groups, host_pos, [it["seed"] for it in items])
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        g.run(args.gso_loop_steps, device=True)
+        torch.cuda.synchronize()
+        el = time.perf_counter() - t0
+        t_gso = max_over_ranks(el, dist, "cuda")
+        gso_loop = {"value": job_rate(g.scored, world, t_gso * 1e3), "unit": "exact poses/s",
+                    "steps": args.gso_loop_steps, "seconds": t_gso, "exact_evals_per_rank": int(g.scored),
+                    "glowworms": int(len(host_pos)),
+                    "what": "device-resident GSO over every swarm of every complex: per step one persistent "
+                            "scoring launch of the moved glowworms plus the GSO kernels, replayed from one CUDA "
+                            "graph; wall time including set-up and read-back"}
+        del g
+
     peaks = {}
     try:
         with open(os.path.join(REPO, "MEASURED_PEAKS.json")) as f:
@@ -376,6 +402,8 @@ def main():
             "step": "CUDA graph replay of one persistent launch group" if not args.no_graph else "plan launch"}
     if plain:
         line["plain_single_complex"] = plain
+    if gso_loop:
+        line["gso_step_loop"] = gso_loop
     if any("restraints" in it for it in items):
         # the same poses without restraints / membrane: the cost of the
         # interface bits; and the fractions seen, to show they were exercised
