@@ -14,7 +14,9 @@
 //   k_colsum     bias gradients
 //   k_adam_all   Adam on the FP32 master weights (one launch), refreshes both
 //                BF16 layouts of the GEMM weights
+#include <cuda.h>
 #include <cuda_bf16.h>
+#include <cudaTypedefs.h>
 
 #include <algorithm>
 
@@ -178,109 +180,115 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
 }
 
 // ---------------------------------------------------------------------------
-// Forward layer on the 5th-generation tensor cores (tcgen05, sm_100a):
-//   Y[M x 256] = ReLU(X[M x K] W^T + b) -> bf16, W [256 x K] (K = 64 or 256)
-// One CTA (4 warps) per 128-row tile and the full width N = 256: the A tile
-// and all of W are staged in shared memory in the canonical K-major layout
-// without swizzle (8-row x 16-byte core matrices, core matrices along K
-// 128 B apart, 8-row groups (K / 8) * 128 B apart); one elected thread issues
-// K / 16 tcgen05.mma (M = 128, N = 256, K = 16, BF16 in, FP32 accumulate)
-// into a 128-lane x 256-column TMEM accumulator and commits them to an
-// mbarrier; each warp then reads its 32 TMEM lanes (32 rows) back with
-// tcgen05.ld, adds the bias, applies ReLU and stores bf16.  The mbarrier
-// wait is bounded: a wait that runs out sets status bit 2 and the CTA skips
-// the epilogue (the accumulator is freed after the commit has been waited
-// for with the same bound).
+// Layers on the 5th-generation tensor cores (tcgen05, sm_100a):
+//   Y[M x 256] = epi(A[M x K] B^T), A [M x K] and B [256 x K] both K-major
+//   bf16 (K = 64 or 256), FP32 accumulation; epilogues: EPI_FWD (+ bias,
+//   ReLU; B = W, a forward layer) and EPI_BWD (x ReLU'(Hm); B = W^T, the
+//   backward-data product dA_in = dC W).
+// One CTA (4 warps) per 128-row tile and the full width N = 256.  The
+// operands arrive by TMA: one 2D tiled copy per 64-element K slab of A (128
+// rows) and of B (256 rows), 128-byte swizzled, into 1024-byte aligned
+// shared memory, all completing on one mbarrier (expect_tx); rows past M
+// are zero-filled by the copy.  One elected thread then issues K / 16
+// tcgen05.mma (M = 128, N = 256, K = 16, BF16 in, FP32 accumulate) with
+// SW128 K-major descriptors (8-row groups 1024 B apart; a K step of 16 moves
+// the start address by 32 B inside the swizzle atom) into a 128-lane x
+// 256-column TMEM accumulator and commits them to a second mbarrier; each
+// warp reads its 32 TMEM lanes (rows) back with tcgen05.ld and applies the
+// epilogue.  Both waits are bounded: a wait that runs out sets status bit 2,
+// the CTA skips the rest, and the accumulator is still freed.
 // ---------------------------------------------------------------------------
-constexpr int TC_BM = 128, TC_N = 256, TC_KMAX = 256;
-constexpr size_t TC_SMEM = (size_t)(TC_BM + TC_N) * TC_KMAX * 2 + 128;   // A, B tiles + barrier / TMEM address
+constexpr int TC_BM = 128, TC_N = 256, TC_KMAX = 256, TC_KS = 64;   // K slab of one TMA copy (128 B)
+constexpr size_t TC_SMEM = (size_t)(TC_BM + TC_N) * TC_KMAX * 2 + 1024;   // A, B slabs + alignment slack
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
-// K-major, no swizzle: LBO = 128 B (next 8 elements of K), SBO = (K / 8) * 128 B
-// (next 8 rows); version 1 (bits 46-47); layout type 0
-__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr, int K) {
-    const uint64_t start = (saddr >> 4) & 0x3fff;
-    const uint64_t lbo = (128 >> 4) & 0x3fff;
-    const uint64_t sbo = (((uint64_t)K / 8) * 128 >> 4) & 0x3fff;
-    return start | (lbo << 16) | (sbo << 32) | (1ull << 46);
+// K-major, 128-byte swizzle: SBO = 1024 B (next 8 rows), LBO unused (1),
+// version 1 (bits 46-47), layout type SWIZZLE_128B (2, bits 61-63)
+__device__ __forceinline__ uint64_t tc_desc(uint32_t saddr) {
+    return (uint64_t)((saddr >> 4) & 0x3fff) | (1ull << 16) | ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) |
+           (2ull << 61);
 }
 
-__global__ void __launch_bounds__(128, 1)
-k_gemm_tc(int M, int K, const __nv_bfloat16* __restrict__ X, const __nv_bfloat16* __restrict__ W,
-          const float* __restrict__ bias, __nv_bfloat16* __restrict__ Y, int* __restrict__ status) {
-    extern __shared__ __align__(128) unsigned char tc_smem[];
-    __nv_bfloat16* sA = reinterpret_cast<__nv_bfloat16*>(tc_smem);
-    __nv_bfloat16* sB = sA + (size_t)TC_BM * K;
-    unsigned long long* bar = reinterpret_cast<unsigned long long*>(tc_smem + (size_t)(TC_BM + TC_N) * TC_KMAX * 2);
-    uint32_t* tmem_slot = reinterpret_cast<uint32_t*>(bar + 1);
-    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * TC_BM;
-    const int kc = K / 8;   // 16-byte chunks per row
-    // 1. TMEM: 256 columns (the FP32 accumulator); mbarrier
-    if (warp == 0) {
-        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     :: "r"(smem_u32(tmem_slot)), "r"(TC_N));
-        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
-    }
-    if (tid == 0) {
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(bar)), "r"(1));
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    // 2. operand tiles, 16-byte chunks in the canonical core-matrix layout
-    for (int e = tid; e < TC_BM * kc; e += 128) {
-        const int r = e / kc, c = e % kc, gm = m0 + r;
-        uint4 v = make_uint4(0u, 0u, 0u, 0u);
-        if (gm < M) v = *reinterpret_cast<const uint4*>(X + (size_t)gm * K + 8 * c);
-        *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(sA) + (size_t)(r >> 3) * kc * 128 + c * 128 +
-                                  (r & 7) * 16) = v;
-    }
-    for (int e = tid; e < TC_N * kc; e += 128) {
-        const int r = e / kc, c = e % kc;
-        const uint4 v = *reinterpret_cast<const uint4*>(W + (size_t)r * K + 8 * c);
-        *reinterpret_cast<uint4*>(reinterpret_cast<unsigned char*>(sB) + (size_t)(r >> 3) * kc * 128 + c * 128 +
-                                  (r & 7) * 16) = v;
-    }
-    // generic-proxy stores -> visible to the tensor core's async proxy
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-    __syncthreads();
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    const uint32_t tmem = *tmem_slot;
-    // 3. one thread issues the MMAs and commits them to the barrier
-    if (tid == 0) {
-        // kind::f16 descriptor: D f32 (bits 4-5 = 1), A bf16 (7-9 = 1), B bf16
-        // (10-12 = 1), both K-major, N >> 3 at 17-22, M >> 4 at 24-28
-        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
-                               ((uint32_t)(TC_BM >> 4) << 24);
-        const uint32_t a0 = smem_u32(sA), b0 = smem_u32(sB);
-        for (int ks = 0; ks < K / 16; ++ks) {
-            const uint64_t ad = tc_desc(a0 + ks * 256, K), bd = tc_desc(b0 + ks * 256, K);
-            const uint32_t acc = ks > 0 ? 1u : 0u;
-            asm volatile(
-                "{\n\t.reg .pred p;\n\t"
-                "setp.ne.b32 p, %4, 0;\n\t"
-                "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
-                :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
-        }
-        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
-                     :: "r"(smem_u32(bar)) : "memory");
-    }
-    // 4. bounded wait for the accumulator (phase 0)
-    bool done = false;
-    for (int it = 0; it < (1 << 22) && !done; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t phase) {
+    for (int it = 0; it < (1 << 22); ++it) {
         uint32_t ok;
         asm volatile("{\n\t.reg .pred P1;\n\t"
                      "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
                      "selp.b32 %0, 1, 0, P1;\n\t}\n"
-                     : "=r"(ok) : "r"(smem_u32(bar)), "r"(0u) : "memory");
-        done = ok != 0;
+                     : "=r"(ok) : "r"(bar), "r"(phase) : "memory");
+        if (ok) return true;
     }
+    return false;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
+    asm volatile("cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];"
+                 :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar) : "memory");
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(128, 1)
+k_gemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int M, int K,
+          const float* __restrict__ bias, const __nv_bfloat16* __restrict__ Hm, __nv_bfloat16* __restrict__ Y,
+          int* __restrict__ status) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ __align__(8) unsigned long long bars[2];   // operands loaded, accumulator ready
+    __shared__ uint32_t tmem_slot;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * TC_BM, nslab = K / TC_KS;
+    const uint32_t base = (smem_u32(tc_smem) + 1023u) & ~1023u;   // SW128 atoms are 1024-byte aligned
+    const uint32_t sA = base, sB = base + (uint32_t)(nslab * TC_BM * 128);
+    const uint32_t bar_ld = smem_u32(&bars[0]), bar_mma = smem_u32(&bars[1]);
+    // 1. TMEM: 256 columns (the FP32 accumulator); barriers; the TMA copies
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&tmem_slot)), "r"(TC_N));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar_ld), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar_mma), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        const uint32_t bytes = (uint32_t)(nslab * (TC_BM + TC_N) * 128);
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar_ld), "r"(bytes) : "memory");
+        for (int sl = 0; sl < nslab; ++sl) {
+            tma_load_2d(sA + (uint32_t)(sl * TC_BM * 128), &mapA, sl * TC_KS, m0, bar_ld);
+            tma_load_2d(sB + (uint32_t)(sl * TC_N * 128), &mapB, sl * TC_KS, 0, bar_ld);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    if (!done) {
+    const uint32_t tmem = tmem_slot;
+    bool ok = mbar_wait(bar_ld, 0);
+    // 2. one thread issues the MMAs and commits them to the second barrier
+    if (ok && tid == 0) {
+        // kind::f16 descriptor: D f32 (bits 4-5 = 1), A bf16 (7-9 = 1), B bf16
+        // (10-12 = 1), both K-major, N >> 3 at 17-22, M >> 4 at 24-28
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                               ((uint32_t)(TC_BM >> 4) << 24);
+        for (int sl = 0; sl < nslab; ++sl)
+            for (int ks = 0; ks < TC_KS / 16; ++ks) {
+                const uint64_t ad = tc_desc(sA + (uint32_t)(sl * TC_BM * 128 + ks * 32));
+                const uint64_t bd = tc_desc(sB + (uint32_t)(sl * TC_N * 128 + ks * 32));
+                const uint32_t acc = (sl | ks) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                    :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(bar_mma) : "memory");
+    }
+    // 3. bounded wait for the accumulator
+    if (ok) ok = mbar_wait(bar_mma, 0);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
         if (lane == 0) atomicOr(status, 4);
     } else {
-        // 5. epilogue: warp w holds rows 32w .. 32w + 31 (TMEM lanes)
+        // 4. epilogue: warp w holds rows 32w .. 32w + 31 (TMEM lanes)
         const int row = m0 + warp * 32 + lane;
         for (int c0 = 0; c0 < TC_N; c0 += 32) {
             uint32_t r[32];
@@ -297,10 +305,20 @@ k_gemm_tc(int M, int K, const __nv_bfloat16* __restrict__ X, const __nv_bfloat16
             asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
             if (row < M) {
                 __align__(16) __nv_bfloat16 o[32];
+                if (EPI == EPI_FWD) {
 #pragma unroll
-                for (int j = 0; j < 32; ++j) {
-                    const float v = __uint_as_float(r[j]) + bias[c0 + j];
-                    o[j] = __float2bfloat16(v > 0.f ? v : 0.f);
+                    for (int j = 0; j < 32; ++j) {
+                        const float v = __uint_as_float(r[j]) + bias[c0 + j];
+                        o[j] = __float2bfloat16(v > 0.f ? v : 0.f);
+                    }
+                } else {
+                    __align__(16) __nv_bfloat16 hm[32];
+                    const uint4* src = reinterpret_cast<const uint4*>(Hm + (size_t)row * TC_N + c0);
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) reinterpret_cast<uint4*>(hm)[q] = src[q];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j)
+                        o[j] = __float2bfloat16(__bfloat162float(hm[j]) > 0.f ? __uint_as_float(r[j]) : 0.f);
                 }
                 uint4* dst = reinterpret_cast<uint4*>(Y + (size_t)row * TC_N + c0);
 #pragma unroll
@@ -308,7 +326,7 @@ k_gemm_tc(int M, int K, const __nv_bfloat16* __restrict__ X, const __nv_bfloat16
             }
         }
     }
-    // 6. free the accumulator
+    // 5. free the accumulator
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
@@ -519,11 +537,40 @@ float* P(lkg_surrogate* S, int k) { return S->p.as<float>() + S->off[k]; }
 float* Gd(lkg_surrogate* S, int k) { return S->g.as<float>() + S->off[k]; }
 
 // forward of n feature rows already in S->X; y in S->y
-cudaError_t gemm_tc(lkg_surrogate* S, int n, int K, const __nv_bfloat16* X, const __nv_bfloat16* W, const float* b,
-                    __nv_bfloat16* Y) {
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+// 2D tiled tensor map of a row-major [rows x K] bf16 matrix for the tcgen05
+// kernel: boxes of 64 K elements x box_rows rows, 128-byte swizzled; the
+// rows past `rows` read as zeros
+bool tc_map(CUtensorMap* m, const void* base, int rows, int K, int box_rows) {
+    static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+    if (!encode) {
+        void* fn = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess || !fn)
+            return false;
+        encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+    }
+    const cuuint64_t dims[2] = {(cuuint64_t)K, (cuuint64_t)rows};
+    const cuuint64_t strides[1] = {(cuuint64_t)K * 2};
+    const cuuint32_t box[2] = {(cuuint32_t)TC_KS, (cuuint32_t)box_rows};
+    const cuuint32_t estr[2] = {1, 1};
+    return encode(m, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void*>(base), dims, strides, box, estr,
+                  CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+}
+
+// Y[n x 256] = epi(A[n x K] B^T), B [256 x K]
+template <int EPI>
+cudaError_t gemm_tc(lkg_surrogate* S, int n, int K, const __nv_bfloat16* A, const __nv_bfloat16* B, const float* b,
+                    const __nv_bfloat16* Hm, __nv_bfloat16* Y) {
+    if (n <= 0) return cudaSuccess;
+    alignas(64) CUtensorMap ma, mb;
+    if (K % TC_KS || K > TC_KMAX || !tc_map(&ma, A, n, K, TC_BM) || !tc_map(&mb, B, TC_N, K, TC_N))
+        return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
     if (e != cudaSuccess) return e;
-    k_gemm_tc<<<(n + TC_BM - 1) / TC_BM, 128, TC_SMEM, S->ctx->stream>>>(n, K, X, W, b, Y, S->d_status.as<int>());
+    k_gemm_tc<EPI><<<(n + TC_BM - 1) / TC_BM, 128, TC_SMEM, S->ctx->stream>>>(ma, mb, n, K, b, Hm, Y,
+                                                                               S->d_status.as<int>());
     return cudaGetLastError();
 }
 
@@ -531,11 +578,12 @@ int forward(lkg_surrogate* S, int n) {
     cudaStream_t s = S->ctx->stream;
     const __nv_bfloat16* X = S->X.as<__nv_bfloat16>();
     if (S->tc) {
-        LKG_CK(gemm_tc(S, n, IN, X, S->wt[0].as<__nv_bfloat16>(), P(S, 1), S->H1.as<__nv_bfloat16>()), "mlp fwd tc");
-        LKG_CK(gemm_tc(S, n, H, S->H1.as<__nv_bfloat16>(), S->wt[1].as<__nv_bfloat16>(), P(S, 3),
-                       S->H2.as<__nv_bfloat16>()), "mlp fwd tc");
-        LKG_CK(gemm_tc(S, n, H, S->H2.as<__nv_bfloat16>(), S->wt[2].as<__nv_bfloat16>(), P(S, 5),
-                       S->H3.as<__nv_bfloat16>()), "mlp fwd tc");
+        LKG_CK(gemm_tc<EPI_FWD>(S, n, IN, X, S->wt[0].as<__nv_bfloat16>(), P(S, 1), nullptr,
+                                S->H1.as<__nv_bfloat16>()), "mlp fwd tc");
+        LKG_CK(gemm_tc<EPI_FWD>(S, n, H, S->H1.as<__nv_bfloat16>(), S->wt[1].as<__nv_bfloat16>(), P(S, 3), nullptr,
+                                S->H2.as<__nv_bfloat16>()), "mlp fwd tc");
+        LKG_CK(gemm_tc<EPI_FWD>(S, n, H, S->H2.as<__nv_bfloat16>(), S->wt[2].as<__nv_bfloat16>(), P(S, 5), nullptr,
+                                S->H3.as<__nv_bfloat16>()), "mlp fwd tc");
         k_head<<<(n + 7) / 8, 256, 0, s>>>(S->H3.as<__nv_bfloat16>(), n, P(S, 6), P(S, 7), S->y.as<float>());
         LKG_CK(cudaGetLastError(), "mlp head");
         S->ctx->launches += 4;
@@ -580,9 +628,13 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
         k_split_sum<<<1, H, 0, s>>>(rpart, nblk, H, Gd(S, 2 * L + 1));
         LKG_CK(cudaGetLastError(), "mlp bias grad");
         if (L > 0) {
-            // dA_in[n][i] = (sum_o dC[n][o] W_L[o][i]) x ReLU'(A_in)
-            LKG_CK((gemm<false, false, EPI_BWD>(s, n, H, H, dacts[L], H, S->w[L].as<__nv_bfloat16>(), H, nullptr,
-                                                dacts[L - 1], H, nullptr, acts[L - 1])), "mlp bwd");
+            // dA_in[n][i] = (sum_o dC[n][o] W_L[o][i]) x ReLU'(A_in); w[L] is W_L^T [in x out]
+            if (S->tc)
+                LKG_CK(gemm_tc<EPI_BWD>(S, n, H, dacts[L], S->w[L].as<__nv_bfloat16>(), nullptr, acts[L - 1],
+                                        dacts[L - 1]), "mlp bwd tc");
+            else
+                LKG_CK((gemm<false, false, EPI_BWD>(s, n, H, H, dacts[L], H, S->w[L].as<__nv_bfloat16>(), H, nullptr,
+                                                    dacts[L - 1], H, nullptr, acts[L - 1])), "mlp bwd");
         }
     }
     S->ctx->launches += 14;

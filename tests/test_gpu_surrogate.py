@@ -113,8 +113,8 @@ def test_online_training_learns_exact_energies(sur):
 
 @pytest.mark.parametrize("n", [100, 1000, 4096])
 def test_tcgen05_forward_matches_mma_sync_and_the_oracle(sur, n):
-    # the forward layers on tcgen05 (TMEM accumulators) against the mma.sync
-    # kernel and the FP64 oracle; the backward pass reuses their activations
+    # the forward layers and the backward-data products on tcgen05 (TMA-fed,
+    # TMEM accumulators) against the mma.sync kernels and the FP64 oracle
     _, _, s = sur
     rng = np.random.default_rng(100 + n)
     p = omlp.he_params(7 + n)
@@ -136,6 +136,9 @@ def test_tcgen05_forward_matches_mma_sync_and_the_oracle(sur, n):
     assert np.abs(y1 - y_ref).max() < 1e-2 * (1.0 + np.abs(y_ref).max())
     cos = float(g1 @ g_ref / (np.linalg.norm(g1) * np.linalg.norm(g_ref)))
     assert cos > 0.999, cos
+    for k, (a, b) in enumerate(zip(_blocks(g1.astype(np.float64)), _blocks(g0.astype(np.float64)))):
+        err = np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-12)
+        assert err < 3e-2, (k, err)
 
 
 def test_tcgen05_predict_throughput_is_reported(sur):
