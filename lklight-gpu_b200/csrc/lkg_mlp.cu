@@ -38,8 +38,17 @@ constexpr int IN = 64, H = 256, NA = 16;   // features, width, anchors
 // per pose: [w, x, y, z, tx/s, ty/s, tz/s, then per anchor a:
 //            phi(x_a) * 100, log1p(receptor atoms in the anchor's 3x3x3
 //            fine cells), log1p(atoms in its own cell)], 1.0, zero padding
+// Training batches also write the standardised targets (tgt not null):
+// t = (asinh(score / e_scale) - mu) / sd.
+struct TargetArgs {
+    const double* scores;
+    float e_scale, mu, sd;
+    float* t;
+};
+
 __global__ void k_features(const ComplexDev* __restrict__ cxs, int cid, const double* __restrict__ poses, int n,
-                           const int* __restrict__ anchors, float tscale, __nv_bfloat16* __restrict__ feat) {
+                           const int* __restrict__ anchors, float tscale, __nv_bfloat16* __restrict__ feat,
+                           TargetArgs tgt) {
     const ComplexDev& c = cxs[cid];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int pose = t / NA, a = t % NA;
@@ -48,6 +57,7 @@ __global__ void k_features(const ComplexDev* __restrict__ cxs, int cid, const do
     const Rot rot = pose_matrix(pq);
     __nv_bfloat16* f = feat + (size_t)pose * IN;
     if (a == 0) {
+        if (tgt.t) tgt.t[pose] = (asinhf((float)(tgt.scores[pose] / tgt.e_scale)) - tgt.mu) / tgt.sd;
         for (int k = 0; k < 4; ++k) f[k] = __float2bfloat16((float)pq[k]);
         for (int k = 0; k < 3; ++k) f[4 + k] = __float2bfloat16((float)(pq[4 + k] / tscale));
         f[7 + 3 * NA] = __float2bfloat16(1.0f);
@@ -392,13 +402,21 @@ __global__ void k_colsum(const __nv_bfloat16* __restrict__ dC, int n, float* __r
     part[(size_t)blockIdx.x * H + col] = s;
 }
 
-// out[i] = sum over z = 0, 1, ... of part[z * count + i]
-__global__ void k_split_sum(const float* __restrict__ part, int nz, int count, float* __restrict__ out) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= count) return;
+// out[i] = sum over z = 0, 1, ... of part[z * count + i], for two such
+// reductions in one launch (threads past count1 serve the second)
+struct SplitSum {
+    const float* part;
+    int nz, count;
+    float* out;
+};
+__global__ void k_split_sum(SplitSum a, SplitSum b) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const SplitSum& r = i < a.count ? a : b;
+    if (i >= a.count) i -= a.count;
+    if (i >= r.count) return;
     float s = 0.f;
-    for (int z = 0; z < nz; ++z) s += part[(size_t)z * count + i];
-    out[i] = s;
+    for (int z = 0; z < r.nz; ++z) s += r.part[(size_t)z * r.count + i];
+    r.out[i] = s;
 }
 
 // the three GEMM layers inside the flat parameter vector
@@ -411,13 +429,24 @@ struct AdamLayers {
 // Adam over the whole flat parameter vector in one launch; GEMM-layer
 // entries also refresh both BF16 layouts
 // The step count t (1-based) lives on the device so that training steps can
-// be replayed from a CUDA graph; k_adam_next advances it after each step.
+// be replayed from a CUDA graph; the kernel's last block advances it.
+// step[0]: the step count t; step[1]: blocks done (the last block to
+// finish advances t, after every block has read it, and resets the count)
 __global__ void k_adam_all(float* __restrict__ p, const float* __restrict__ gr, float* __restrict__ m1,
                            float* __restrict__ m2, int n, float lr, float b1, float b2, float eps,
-                           const int* __restrict__ step, AdamLayers L) {
+                           int* __restrict__ step, AdamLayers L) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const float t = (float)*reinterpret_cast<volatile int*>(step);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        const unsigned v = atomicAdd(reinterpret_cast<unsigned*>(step + 1), 1u);
+        if (v == gridDim.x - 1) {
+            step[0] += 1;
+            step[1] = 0;
+        }
+    }
     if (i >= n) return;
-    const float t = (float)*step;
     const float bc1 = 1.f - powf(b1, t), bc2 = 1.f - powf(b2, t);
     const float gg = gr[i];
     const float a = b1 * m1[i] + (1.f - b1) * gg, v = b2 * m2[i] + (1.f - b2) * gg * gg;
@@ -434,10 +463,6 @@ __global__ void k_adam_all(float* __restrict__ p, const float* __restrict__ gr, 
             L.w[k][(size_t)c * H + r] = __float2bfloat16(np);
         }
     }
-}
-
-__global__ void k_adam_next(int* step) {
-    if (threadIdx.x == 0 && blockIdx.x == 0) *step += 1;
 }
 
 __global__ void k_f2bf(const float* __restrict__ src, __nv_bfloat16* __restrict__ dst, int n) {
@@ -474,7 +499,7 @@ struct lkg_surrogate {
     DBuf wpart, rpart;   // backward partial sums: per split (weight gradients), per row block
     int cap = 0;     // rows of X, H1..H3, y, t (forward)
     int cap_b = 0;   // rows of dH1..dH3 (backward)
-    DBuf d_step;   // Adam step count (device, 1-based)
+    DBuf d_step;   // Adam step count (device, 1-based) and the Adam kernel's block counter
     int tc = 1;    // forward layers on tcgen05 (1, default) or mma.sync (0)
     DBuf d_status; // tcgen05 wait time-outs (bit 2)
     size_t off[9];   // block offsets of W0 b0 W1 b1 W2 b2 w3 b3, and the total
@@ -623,9 +648,10 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
         // dW_L[o][i] = sum_n dC[n][o] * A_in[n][i]   (A = dC^T, B = A_in^T)
         LKG_CK((gemm<true, true, EPI_WGRAD>(s, H, kin, n, dacts[L], H, ain, kin, wpart, nullptr, kin, nullptr,
                                             nullptr, splits)), "mlp wgrad");
-        k_split_sum<<<(H * kin + 255) / 256, 256, 0, s>>>(wpart, split_count(n, splits), H * kin, Gd(S, 2 * L));
         k_colsum<<<nblk, H, 0, s>>>(dacts[L], n, rpart);
-        k_split_sum<<<1, H, 0, s>>>(rpart, nblk, H, Gd(S, 2 * L + 1));
+        const SplitSum wsum{wpart, split_count(n, splits), H * kin, Gd(S, 2 * L)};
+        const SplitSum bsum{rpart, nblk, H, Gd(S, 2 * L + 1)};
+        k_split_sum<<<(H * kin + H + 255) / 256, 256, 0, s>>>(wsum, bsum);
         LKG_CK(cudaGetLastError(), "mlp bias grad");
         if (L > 0) {
             // dA_in[n][i] = (sum_o dC[n][o] W_L[o][i]) x ReLU'(A_in); w[L] is W_L^T [in x out]
@@ -637,7 +663,7 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
                                                     dacts[L - 1], H, nullptr, acts[L - 1])), "mlp bwd");
         }
     }
-    S->ctx->launches += 14;
+    S->ctx->launches += 13;   // loss, head sums, 3 x (weight grads, column sums, split sums), 2 x backward data
     return 0;
 }
 
@@ -654,9 +680,8 @@ int adam(lkg_surrogate* S, float lr) {
     const int n = (int)NPARAM;
     k_adam_all<<<(n + 255) / 256, 256, 0, s>>>(S->p.as<float>(), S->g.as<float>(), S->m1.as<float>(),
                                                S->m2.as<float>(), n, lr, b1, b2, eps, S->d_step.as<int>(), L);
-    k_adam_next<<<1, 32, 0, s>>>(S->d_step.as<int>());
     LKG_CK(cudaGetLastError(), "mlp adam");
-    S->ctx->launches += 2;
+    S->ctx->launches += 1;
     return 0;
 }
 
@@ -671,24 +696,23 @@ int refresh_bf16(lkg_surrogate* S) {
     return 0;
 }
 
-int features(lkg_surrogate* S, int n, const double* d_poses) {
+// features of n device poses into S->X; with d_scores also their
+// standardised targets into S->t (training)
+int features(lkg_surrogate* S, int n, const double* d_poses, const double* d_scores = nullptr) {
     if (sur_reserve(S, n, false)) return lkg_last_status();
     int st = sync_descriptors(S->ctx);
     if (st) return st;
     const int threads = 256, blocks = (int)(((size_t)n * NA + threads - 1) / threads);
+    const TargetArgs tgt{d_scores, S->e_scale, S->t_mu, S->t_sd, d_scores ? S->t.as<float>() : nullptr};
     k_features<<<blocks, threads, 0, S->ctx->stream>>>(S->ctx->d_cx.as<ComplexDev>(), S->cid, d_poses, n,
-                                                       S->anchors.as<int>(), S->tscale, S->X.as<__nv_bfloat16>());
+                                                       S->anchors.as<int>(), S->tscale, S->X.as<__nv_bfloat16>(), tgt);
     LKG_CK(cudaGetLastError(), "features");
     S->ctx->launches++;
     return 0;
 }
 
-// standardised target transform: t = (asinh(score / e_scale) - mu) / sd
-__global__ void k_target(const double* __restrict__ sc, int n, float e_scale, float mu, float sd, float* __restrict__ t) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) t[i] = (asinhf((float)(sc[i] / e_scale)) - mu) / sd;
-}
-
+// predictions back to score units: the inverse of the standardised target
+// t = (asinh(score / e_scale) - mu) / sd that k_features writes in training
 __global__ void k_untarget(const float* __restrict__ y, int n, float e_scale, float mu, float sd, double* __restrict__ out) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = (double)(sinhf(y[i] * sd + mu) * e_scale);
@@ -749,7 +773,7 @@ int lkg_surrogate_create(lkg_ctx* ctx, int complex_id, uint64_t seed, lkg_surrog
     if ((e = S->p.reserve(NPARAM * 4)) != cudaSuccess || (e = S->g.reserve(NPARAM * 4)) != cudaSuccess ||
         (e = S->m1.reserve(NPARAM * 4)) != cudaSuccess || (e = S->m2.reserve(NPARAM * 4)) != cudaSuccess ||
         (e = S->anchors.reserve(NA * sizeof(int))) != cudaSuccess || (e = S->loss.reserve(sizeof(float))) != cudaSuccess ||
-        (e = S->d_step.reserve(sizeof(int))) != cudaSuccess || (e = S->d_status.reserve(sizeof(int))) != cudaSuccess) {
+        (e = S->d_step.reserve(2 * sizeof(int))) != cudaSuccess || (e = S->d_status.reserve(sizeof(int))) != cudaSuccess) {
         delete S;
         return set_error(cuda_to_status(e), "surrogate alloc: %s", cudaGetErrorString(e));
     }
@@ -764,7 +788,8 @@ int lkg_surrogate_create(lkg_ctx* ctx, int complex_id, uint64_t seed, lkg_surrog
     cudaMemset(S->m1.p, 0, NPARAM * 4);
     cudaMemset(S->m2.p, 0, NPARAM * 4);
     const int one = 1;
-    cudaMemcpy(S->d_step.p, &one, sizeof(int), cudaMemcpyHostToDevice);
+    const int step0[2] = {one, 0};   // t = 1, no block done
+    cudaMemcpy(S->d_step.p, step0, sizeof(step0), cudaMemcpyHostToDevice);
     cudaMemset(S->d_status.p, 0, sizeof(int));
     cudaMemcpy(S->anchors.p, anc.data(), NA * sizeof(int), cudaMemcpyHostToDevice);
     if ((rc = refresh_bf16(S))) { delete S; return rc; }
@@ -849,9 +874,7 @@ int lkg_surrogate_train(lkg_surrogate* S, int n, const double* d_poses, const do
         LKG_CK(cudaMemsetAsync(S->loss.p, 0, sizeof(float), s), "mlp loss clear");
         for (int b0 = 0; b0 + batch <= n; b0 += batch) {
             int r;
-            if ((r = features(S, batch, d_poses + 7 * (size_t)b0))) return r;
-            k_target<<<(batch + 255) / 256, 256, 0, s>>>(d_scores + b0, batch, S->e_scale, S->t_mu, S->t_sd,
-                                                         S->t.as<float>());
+            if ((r = features(S, batch, d_poses + 7 * (size_t)b0, d_scores + b0))) return r;
             if ((r = forward(S, batch))) return r;
             if ((r = backward(S, batch, false))) return r;
             if ((r = adam(S, lr))) return r;
