@@ -328,9 +328,10 @@ int lkg_gso_run(lkg_gso* gso, int steps);
  * replayed from one CUDA graph.  Its f64 arithmetic is the host GSO's
  * except acos / sin in the slerp (device library), so runs agree closely at
  * first and then drift apart.  On a screened GSO (lkg_gso_set_screen) the
- * training steps run on the host and the screened steps after them on the
- * device (candidates, predictions, the exact choice, the move; a full
- * rescoring fine-tunes from the host); the no-network ablation is refused
+ * training steps are plain device steps whose exact pairs train the
+ * surrogates, and the screened steps after them run on the device too
+ * (candidates, predictions, the exact choice, the move; a full rescoring
+ * fine-tunes from the host); the no-network ablation is refused
  * (LKG_ERR_STATE).  Host and device steps can be mixed. */
 int lkg_gso_run_device(lkg_gso* gso, int steps);
 int lkg_gso_state(lkg_gso* gso, double* trans, double* rot, double* luc, double* scoring,

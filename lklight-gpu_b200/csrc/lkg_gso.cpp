@@ -890,6 +890,59 @@ int dev_screened_tail(lkg_gso* G) {
     return set_ok();
 }
 
+// the exactly scored (pose, score) pairs of the step just scored (mask set)
+// appended to the groups' training sets, in the host's order
+int dev_learn(lkg_gso* G, bool all) {
+    lkg_ctx* ctx = G->ctx;
+    const lkg::GsoDevState& S = G->ds;
+    cudaStream_t st = ctx->stream;
+    std::vector<double> hp(7 * (size_t)S.n), hs(S.n);
+    std::vector<unsigned char> hm(S.n, 1);
+    LKG_CK(cudaMemcpyAsync(hp.data(), S.poses, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "device gso learn");
+    LKG_CK(cudaMemcpyAsync(hs.data(), S.score, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st), "device gso learn");
+    if (!all) LKG_CK(cudaMemcpyAsync(hm.data(), S.mask, hm.size(), cudaMemcpyDeviceToHost, st), "device gso learn");
+    int rc;
+    if ((rc = wait_stream(ctx, 300.0)) || (rc = check_status(ctx))) return rc;
+    const int ng = (int)G->group_complex.size();
+    G->last_counts.assign(ng, 0);
+    for (int gi = 0, g0 = 0; gi < ng; g0 += G->dcounts[gi], ++gi)
+        for (int i = g0; i < g0 + G->dcounts[gi]; ++i) {
+            if (!hm[i]) continue;
+            G->tr_pose[gi].insert(G->tr_pose[gi].end(), hp.begin() + 7 * (size_t)i, hp.begin() + 7 * (size_t)(i + 1));
+            G->tr_score[gi].push_back(hs[i]);
+            G->last_counts[gi]++;
+        }
+    return set_ok();
+}
+
+// the training steps of a screened run on the device (eagerly): plain steps
+// whose exact pairs join the training sets; the last one also trains the
+// surrogates and makes the first screened move (gso_step does the same on
+// the host).  Returns the steps done in *done.
+int dev_training_steps(lkg_gso* G, int steps, int* done) {
+    cudaStream_t st = G->ctx->stream;
+    lkg::GsoDevState& S = G->ds;
+    const lkg_screen& c = G->cfg;
+    const int ng = (int)G->group_complex.size();
+    int rc;
+    *done = 0;
+    while (*done < steps && G->step < c.train_steps) {
+        if ((rc = lkg::plan_launch_masked(G->dplan, S.poses, S.score, S.mask)) || (rc = dev_learn(G, false)))
+            return rc;
+        if (G->step == c.train_steps - 1) {
+            for (int gi = 0; gi < ng; ++gi)
+                if ((rc = train_group(G, gi, c.train_epochs, 0))) return rc;
+            if ((rc = dev_screened_tail(G))) return rc;
+            G->predicted += (int64_t)S.n * (c.candidates + 1);
+        } else {
+            LKG_CK(lkg::gso_dev_after_scoring(S, st), "device gso step");
+        }
+        G->step++;
+        ++*done;
+    }
+    return set_ok();
+}
+
 // screened steps on the device: every `rescore_every` steps a full exact
 // rescoring fine-tunes the surrogates (host-driven, as gso_step does); the
 // steps between replay one captured graph
@@ -907,18 +960,9 @@ int dev_screened_steps(lkg_gso* G, int steps) {
             LKG_CK(cudaMemsetAsync(S.mask, 1, (size_t)S.n, st), "device gso rescoring");
             if ((rc = lkg::plan_launch_masked(G->dplan, S.poses, S.score, S.mask))) return rc;
             // the exact pairs train the surrogates (score_phase learn + train_group)
-            std::vector<double> hp(7 * (size_t)S.n), hs(S.n);
-            LKG_CK(cudaMemcpyAsync(hp.data(), S.poses, hp.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
-                   "device gso rescoring");
-            LKG_CK(cudaMemcpyAsync(hs.data(), S.score, hs.size() * sizeof(double), cudaMemcpyDeviceToHost, st),
-                   "device gso rescoring");
-            if ((rc = wait_stream(ctx, 300.0)) || (rc = check_status(ctx))) return rc;
-            for (int gi = 0, g0 = 0; gi < ng; g0 += G->dcounts[gi], ++gi) {
-                const int m = G->dcounts[gi];
-                G->tr_pose[gi].insert(G->tr_pose[gi].end(), hp.begin() + 7 * (size_t)g0, hp.begin() + 7 * (size_t)(g0 + m));
-                G->tr_score[gi].insert(G->tr_score[gi].end(), hs.begin() + g0, hs.begin() + g0 + m);
-                if ((rc = train_group(G, gi, c.finetune_epochs, (size_t)m))) return rc;
-            }
+            if ((rc = dev_learn(G, true))) return rc;
+            for (int gi = 0; gi < ng; ++gi)
+                if ((rc = train_group(G, gi, c.finetune_epochs, (size_t)G->dcounts[gi]))) return rc;
             if ((rc = dev_screened_tail(G))) return rc;
         } else {
             const bool same = G->sexec && std::memcmp(&G->ds_captured, &S, sizeof(S)) == 0 &&
@@ -978,21 +1022,23 @@ int lkg_gso_run_device(lkg_gso* G, int steps) {
         return set_error(LKG_ERR_STATE, "the device GSO screens with the surrogate only (not the ablation)");
     cudaSetDevice(G->ctx->device);
     int rc;
-    if (G->screen)   // the training steps (and the first training) run on the host
-        while (steps > 0 && G->step < G->cfg.train_steps) {
-            if ((rc = gso_step(G))) return rc;
-            --steps;
-        }
     if (steps == 0 || G->swarms.empty()) return set_ok();
     const double t0 = now_s(), tt0 = G->t_train;
     if ((rc = dev_setup(G, G->screen))) return rc;
     if (G->ds.n == 0) return set_ok();
     const int step0 = G->step;
-    rc = G->screen ? dev_screened_steps(G, steps) : dev_plain_steps(G, steps);
-    if (rc) return rc;
+    if (G->screen) {
+        int done = 0;
+        if (G->step < G->cfg.train_steps && (rc = dev_training_steps(G, steps, &done))) return rc;
+        if (done < steps && (rc = dev_screened_steps(G, steps - done))) return rc;
+    } else if ((rc = dev_plain_steps(G, steps))) {
+        return rc;
+    }
     if ((rc = wait_stream(G->ctx, 300.0)) || (rc = check_status(G->ctx))) return rc;
     if (!G->screen) G->step += steps;
-    if ((rc = dev_download(G, G->step - step0, G->screen))) return rc;
+    // a screened run that stopped inside its training steps left a plain move
+    const bool screened_move = G->screen && G->step >= G->cfg.train_steps;
+    if ((rc = dev_download(G, G->step - step0, screened_move))) return rc;
     G->t_exact += now_s() - t0 - (G->t_train - tt0);
     return set_ok();
 }

@@ -1,10 +1,10 @@
 """Device-resident screened GSO against the host screened GSO.
 
-After the training steps (on the host in both runs), the device run does
-whole screened steps on the GPU: K selections per glowworm from the swarm's
-stream, candidate poses, surrogate predictions, the per-swarm choice of the
-moves scored exactly, the move, and a full rescoring with fine-tuning every
-`rescore_every` steps.  Training is bitwise reproducible (fixed-order
+The device run does whole GSO steps on the GPU: the training steps (plain
+steps whose exact pairs train the surrogate), then screened steps with K
+selections per glowworm from the swarm's stream, candidate poses, surrogate
+predictions, the per-swarm choice of the moves scored exactly, the move, and
+a full rescoring with fine-tuning every `rescore_every` steps.  Training is bitwise reproducible (fixed-order
 reductions), so host screened runs repeat exactly; the device run agrees
 with the host run up to the slerp's acos / sin (device library vs glibc):
 a last-place difference in a candidate pose can move a BF16 feature and
@@ -52,9 +52,12 @@ def test_host_screened_runs_repeat_exactly(setup):
     assert a["scored"] == b["scored"]
 
 
-def test_device_screened_steps_follow_the_host(setup):
+@pytest.mark.parametrize("plan", [[(9, True)], [(4, False), (5, True)]])
+def test_device_screened_steps_follow_the_host(setup, plan):
+    # all on the device (training steps 0-3 too), or the training steps on
+    # the host; a full rescoring at step 7 in both
     host = _run(setup, [(9, False)])
-    dev = _run(setup, [(9, True)])   # steps 0-3 on the host (training), 4-8 on the device, one rescoring at 7
+    dev = _run(setup, plan)
     close = np.all(np.abs(dev["translation"] - host["translation"]) <= 1e-6 * np.maximum(1.0, np.abs(host["translation"])),
                    axis=1)
     assert close.mean() >= 0.9, close.mean()
