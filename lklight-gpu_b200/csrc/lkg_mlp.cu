@@ -237,34 +237,37 @@ __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map
                  :: "r"(dst), "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar) : "memory");
 }
 
-template <int EPI>
+// TN: output columns of a CTA (256, or 128 with blockIdx.y picking the half
+// when the row tiles alone would leave most SMs idle)
+template <int EPI, int TN>
 __global__ void __launch_bounds__(128, 1)
 k_gemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int M, int K,
           const float* __restrict__ bias, const __nv_bfloat16* __restrict__ Hm, __nv_bfloat16* __restrict__ Y,
           int* __restrict__ status) {
+    static_assert(TN == 128 || TN == 256, "tile width");
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     __shared__ __align__(8) unsigned long long bars[2];   // operands loaded, accumulator ready
     __shared__ uint32_t tmem_slot;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    const int m0 = blockIdx.x * TC_BM, nslab = K / TC_KS;
+    const int m0 = blockIdx.x * TC_BM, n0 = blockIdx.y * TN, nslab = K / TC_KS;
     const uint32_t base = (smem_u32(tc_smem) + 1023u) & ~1023u;   // SW128 atoms are 1024-byte aligned
     const uint32_t sA = base, sB = base + (uint32_t)(nslab * TC_BM * 128);
     const uint32_t bar_ld = smem_u32(&bars[0]), bar_mma = smem_u32(&bars[1]);
     // 1. TMEM: 256 columns (the FP32 accumulator); barriers; the TMA copies
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     :: "r"(smem_u32(&tmem_slot)), "r"(TC_N));
+                     :: "r"(smem_u32(&tmem_slot)), "r"(TN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar_ld), "r"(1));
         asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar_mma), "r"(1));
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        const uint32_t bytes = (uint32_t)(nslab * (TC_BM + TC_N) * 128);
+        const uint32_t bytes = (uint32_t)(nslab * (TC_BM + TN) * 128);
         asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar_ld), "r"(bytes) : "memory");
         for (int sl = 0; sl < nslab; ++sl) {
             tma_load_2d(sA + (uint32_t)(sl * TC_BM * 128), &mapA, sl * TC_KS, m0, bar_ld);
-            tma_load_2d(sB + (uint32_t)(sl * TC_N * 128), &mapB, sl * TC_KS, 0, bar_ld);
+            tma_load_2d(sB + (uint32_t)(sl * TN * 128), &mapB, sl * TC_KS, n0, bar_ld);
         }
     }
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
@@ -276,12 +279,12 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
     if (ok && tid == 0) {
         // kind::f16 descriptor: D f32 (bits 4-5 = 1), A bf16 (7-9 = 1), B bf16
         // (10-12 = 1), both K-major, N >> 3 at 17-22, M >> 4 at 24-28
-        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
                                ((uint32_t)(TC_BM >> 4) << 24);
         for (int sl = 0; sl < nslab; ++sl)
             for (int ks = 0; ks < TC_KS / 16; ++ks) {
                 const uint64_t ad = tc_desc(sA + (uint32_t)(sl * TC_BM * 128 + ks * 32));
-                const uint64_t bd = tc_desc(sB + (uint32_t)(sl * TC_N * 128 + ks * 32));
+                const uint64_t bd = tc_desc(sB + (uint32_t)(sl * TN * 128 + ks * 32));
                 const uint32_t acc = (sl | ks) ? 1u : 0u;
                 asm volatile(
                     "{\n\t.reg .pred p;\n\t"
@@ -300,9 +303,10 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
     } else {
         // 4. epilogue: warp w holds rows 32w .. 32w + 31 (TMEM lanes)
         const int row = m0 + warp * 32 + lane;
-        for (int c0 = 0; c0 < TC_N; c0 += 32) {
+        for (int cl = 0; cl < TN; cl += 32) {
             uint32_t r[32];
-            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c0;
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cl;
+            const int c0 = n0 + cl;   // output column
             asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
                          "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
                          "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
@@ -341,7 +345,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
     __syncthreads();
     if (warp == 0) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TC_N));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TN));
     }
 }
 
@@ -359,16 +363,19 @@ __global__ void k_head(const __nv_bfloat16* __restrict__ H3, int n, const float*
 // Every reduction of the backward pass adds its terms in a fixed order
 // (partials per block of rows or per split, then the partials in order), so
 // training is bitwise reproducible.
-constexpr int RB = 32;   // rows per partial sum
+constexpr int RB = 32;   // rows per partial sum (bias gradients)
+constexpr int RL = 8;    // rows per partial sum of the loss kernel (more blocks: its rows are serial)
 
-// loss, dy = 2 (y - t) / n; dH3 = dy w3 x ReLU'(H3); per block of RB rows
+// loss, dy = 2 (y - t) / n; dH3 = dy w3 x ReLU'(H3); per block of RL rows
 // (one thread per column) the partial head gradients sum_rows dy h (H
 // columns), sum dy and sum (y - t)^2 / n -> part[blk][H + 2]
 __global__ void k_loss(const float* __restrict__ y, const float* __restrict__ t, const __nv_bfloat16* __restrict__ H3,
                        int n, const float* __restrict__ w3, __nv_bfloat16* __restrict__ dH3, float* __restrict__ part) {
-    const int k = threadIdx.x, r0 = blockIdx.x * RB, r1 = min(n, r0 + RB);
+    const int k = threadIdx.x, r0 = blockIdx.x * RL, r1 = min(n, r0 + RL);
     float gw = 0.f, gb = 0.f, ls = 0.f;
-    for (int r = r0; r < r1; ++r) {
+#pragma unroll
+    for (int r = r0; r < r0 + RL; ++r) {
+        if (r >= r1) break;
         const float d = y[r] - t[r];
         const float dy = 2.f * d / (float)n;
         const float h = __bfloat162float(H3[(size_t)r * H + k]);
@@ -539,7 +546,7 @@ int sur_reserve(lkg_surrogate* S, int n, bool bwd) {
         LKG_CK(S->dH2.reserve(nb * H), "surrogate alloc");
         LKG_CK(S->dH3.reserve(nb * H), "surrogate alloc");
         LKG_CK(S->wpart.reserve((size_t)wgrad_splits(m) * H * H * sizeof(float)), "surrogate alloc");
-        LKG_CK(S->rpart.reserve((size_t)((m + RB - 1) / RB) * (H + 2) * sizeof(float)), "surrogate alloc");
+        LKG_CK(S->rpart.reserve((size_t)((m + RL - 1) / RL) * (H + 2) * sizeof(float)), "surrogate alloc");
         S->cap_b = m;
     }
     return 0;
@@ -589,13 +596,17 @@ template <int EPI>
 cudaError_t gemm_tc(lkg_surrogate* S, int n, int K, const __nv_bfloat16* A, const __nv_bfloat16* B, const float* b,
                     const __nv_bfloat16* Hm, __nv_bfloat16* Y) {
     if (n <= 0) return cudaSuccess;
+    // few row tiles (training batches): two CTAs of 128 columns per tile
+    const int tiles = (n + TC_BM - 1) / TC_BM;
+    const bool split = 2 * tiles <= S->ctx->sm_count;
+    const int tn = split ? 128 : TC_N;
     alignas(64) CUtensorMap ma, mb;
-    if (K % TC_KS || K > TC_KMAX || !tc_map(&ma, A, n, K, TC_BM) || !tc_map(&mb, B, TC_N, K, TC_N))
+    if (K % TC_KS || K > TC_KMAX || !tc_map(&ma, A, n, K, TC_BM) || !tc_map(&mb, B, TC_N, K, tn))
         return cudaErrorInvalidValue;
-    cudaError_t e = cudaFuncSetAttribute(k_gemm_tc<EPI>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
+    auto kern = split ? k_gemm_tc<EPI, 128> : k_gemm_tc<EPI, 256>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TC_SMEM);
     if (e != cudaSuccess) return e;
-    k_gemm_tc<EPI><<<(n + TC_BM - 1) / TC_BM, 128, TC_SMEM, S->ctx->stream>>>(ma, mb, n, K, b, Hm, Y,
-                                                                               S->d_status.as<int>());
+    kern<<<dim3(tiles, TC_N / tn), 128, TC_SMEM, S->ctx->stream>>>(ma, mb, n, K, b, Hm, Y, S->d_status.as<int>());
     return cudaGetLastError();
 }
 
@@ -632,12 +643,12 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
     cudaStream_t s = S->ctx->stream;
     LKG_CK(cudaMemsetAsync(S->g.p, 0, NPARAM * sizeof(float), s), "mlp grad clear");
     if (clear_loss) LKG_CK(cudaMemsetAsync(S->loss.p, 0, sizeof(float), s), "mlp loss clear");
-    const int nblk = (n + RB - 1) / RB;
+    const int nblk = (n + RB - 1) / RB, nlblk = (n + RL - 1) / RL;
     float* rpart = S->rpart.as<float>();
     float* wpart = S->wpart.as<float>();
-    k_loss<<<nblk, H, 0, s>>>(S->y.as<float>(), S->t.as<float>(), S->H3.as<__nv_bfloat16>(), n, P(S, 6),
-                              S->dH3.as<__nv_bfloat16>(), rpart);
-    k_head_sum<<<1, H + 2, 0, s>>>(rpart, nblk, Gd(S, 6), S->loss.as<float>());
+    k_loss<<<nlblk, H, 0, s>>>(S->y.as<float>(), S->t.as<float>(), S->H3.as<__nv_bfloat16>(), n, P(S, 6),
+                               S->dH3.as<__nv_bfloat16>(), rpart);
+    k_head_sum<<<1, H + 2, 0, s>>>(rpart, nlblk, Gd(S, 6), S->loss.as<float>());
     LKG_CK(cudaGetLastError(), "mlp loss");
     const int splits = wgrad_splits(n);
     const __nv_bfloat16* acts[3] = {S->H1.as<__nv_bfloat16>(), S->H2.as<__nv_bfloat16>(), S->H3.as<__nv_bfloat16>()};
