@@ -152,8 +152,8 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     d.ox = o[0]; d.oy = o[1]; d.oz = o[2]; d.h = h; d.inv_h = inv_h; d.hx = hx; d.inv_hx = inv_hx;
     cr.n_cells = (int)ncell;
     // desolvation hash capacity: >= 2 x receptor atoms up to 8192 slots
-    // (96 KB of shared memory); a pose touching more receptor atoms within
-    // 6.4 A reports LKG_ERR_CAPACITY
+    // (64 KB of shared memory in the fast kernel, 96 KB in the exact one); a
+    // pose touching more receptor atoms within 6.4 A reports LKG_ERR_CAPACITY
     int cap = 64;
     while (cap < 2 * n && cap < 8192) cap <<= 1;
     d.hcap = cap;
