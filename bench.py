@@ -39,9 +39,9 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 FLOPS_PER_PAIR = {"dna": 24, "pydock": 23, "vdw": 19, "cpydock": 25}
-# DRAM bytes per pose of the fast kernel (67.5 MB per 24,000-pose launch of
+# DRAM bytes per pose of the fast kernel (69.2 MB per 24,000-pose launch of
 # the 4-complex profiling case under ncu)
-TRAFFIC_PER_POSE = 67.52e6 / 24000
+TRAFFIC_PER_POSE = 69.25e6 / 24000
 FAR_FLOPS = 30
 
 
