@@ -338,6 +338,24 @@ def main():
         pms = (time.perf_counter() - t0) * 1e3 / reps
         plain = {"value": npose / (pms / 1e3), "unit": "poses/s", "ms_per_step": pms,
                  "what": "lkg_score per complex, host buffers, one launch and sync per complex"}
+        # the same kernel launched once per complex on device buffers (no
+        # persistent batch, no graph, one wait per step), device-timed
+        offs = np.concatenate([[0], np.cumsum(counts)])
+        def per_complex():
+            for k, cid in enumerate(ids):
+                ctx.score_device(cid, counts[k], d_poses.data_ptr() + 56 * int(offs[k]),
+                                 d_scores.data_ptr() + 8 * int(offs[k]))
+        per_complex()
+        stream.synchronize()
+        e6, e7 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e6.record(stream)
+        for _ in range(reps):
+            per_complex()
+        e7.record(stream)
+        e7.synchronize()
+        dms = e6.elapsed_time(e7) / reps
+        plain["device_buffers"] = {"value": npose / (dms / 1e3), "unit": "poses/s", "ms_per_step": dms,
+                                   "what": "lkg_score_device per complex (one launch each), device buffers"}
 
     # the whole GSO step loop of the batched workload: every swarm of every
     # complex as one device-resident GSO (one persistent scoring launch of
