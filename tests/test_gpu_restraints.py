@@ -196,3 +196,39 @@ def test_plans_made_before_restraints_are_refused():
         plan.close()
     finally:
         ctx.close()
+
+
+def test_gso_with_restraints_host_and_device_agree():
+    # the GSO drivers score restrained complexes through the same launches:
+    # a few device steps follow the host steps (up to the slerp's last place)
+    c = config0()
+    pos = synth.setup_poses(c["rec"]["coords"], 2, 150, 13)
+    rr, lr, mem = _config0_restraints(c, synth.to_kernel_poses(pos), 6)
+    ctx = lkg.Context()
+    try:
+        cid = ctx.add_complex("dna", c["rec"], c["lig"])
+        ctx.set_restraints(cid, rr, lr, mem)
+        out = []
+        for dev in (False, True):
+            g = lkg.GSO(ctx, [(cid, 2, 150)], pos, [13])
+            g.run(4, device=dev)
+            out.append(g.state())
+            del g
+        a, b = out
+        for k in ("translation", "luciferin", "scoring"):
+            d = np.abs(a[k] - b[k]) / np.maximum(np.abs(a[k]), 1.0)
+            assert d.max() < 1e-9, (k, d.max())
+        assert np.array_equal(a["neighbors"], b["neighbors"])
+        # and the restraint terms took part: the scores differ from plain ones
+        ctx.set_restraints(cid)
+        g = lkg.GSO(ctx, [(cid, 2, 150)], pos, [13])
+        g.run(1)
+        plain = g.state()["scoring"]
+        del g
+        g = lkg.GSO(ctx, [(cid, 2, 150)], pos, [13])
+        ctx.set_restraints(cid, rr, lr, mem)
+        g.run(1)
+        assert not np.array_equal(g.state()["scoring"], plain)
+        del g
+    finally:
+        ctx.close()
