@@ -48,7 +48,7 @@ def test_reference_kernel_and_liblkg_agree_on_config0(reflib):
     s_lkg = -(raw_lkg[:, 0] * 83.0 + raw_lkg[:, 1])
     # the reference kernel sums in f32 per thread and block (full_score.cu
     # :296-335): it drifts from the exact energy further than liblkg does.
-    # Judge both against the oracle (the reference's CPU grid path) on the
+    # Compare both with the oracle (the reference's CPU grid path) on the
     # poses where they disagree most, plus a plain sample
     import oracle
     worst = np.argsort(-rel_err(s_lkg, s_ref))[:100]
