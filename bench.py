@@ -214,6 +214,20 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def pick_shape(args, items, local):
+    """The warp kernel's tile shape: the command line's, else the
+    autotuner's (CUDA-graph replays of a sample of the workload's complexes
+    and poses per candidate shape; cached per device and batch signature)."""
+    shape = dict(tile=args.tile, group=args.group, cell=args.cell, xsub=args.xsub, source="command line")
+    if not (args.tile or args.group or args.cell or args.xsub):
+        if args.no_autotune:
+            shape["source"] = "library default"
+        else:
+            autotune = importlib.import_module("lklight-gpu_b200.autotune")
+            shape = autotune.autotune(items, device=local)
+    return shape
+
+
 def main():
     args = parse()
     rank = int(os.environ.get("RANK", "0"))
@@ -236,12 +250,7 @@ def main():
     items = workload(args.workload)
     if args.complexes:
         items = items[:args.complexes]
-    shape = dict(tile=args.tile, group=args.group, cell=args.cell, xsub=args.xsub, source="command line")
-    if not (args.tile or args.group or args.cell or args.xsub) and not args.no_autotune and len(items) > 1:
-        # tile shapes picked by the autotuner (a sample of the batch, CUDA-graph
-        # replays per candidate shape; cached per device and batch signature)
-        autotune = importlib.import_module("lklight-gpu_b200.autotune")
-        shape = autotune.autotune(items, device=local)
+    shape = pick_shape(args, items, local)
     ctx = lkg.Context(device=local, tile=shape["tile"], cell=shape["cell"], group=shape["group"], xsub=shape["xsub"])
     stream = torch.cuda.ExternalStream(ctx.stream)
     ids = [ctx.add_complex(it["family"], it["rec"], it["lig"]) for it in items]
@@ -487,9 +496,11 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
     else:
         c = synth.config0()
         family, swarms, glow, steps, seed = "dna", 10, 1000, args.gso_steps, 3
-    ctx = lkg.Context(device=local, tile=args.tile, cell=args.cell, group=args.group, xsub=args.xsub)
-    cid = ctx.add_complex(family, c["rec"], c["lig"])
     pos = synth.setup_poses(c["rec"]["coords"], swarms, glow, seed)
+    shape = pick_shape(args, [dict(family=family, rec=c["rec"], lig=c["lig"], poses=synth.to_kernel_poses(pos))],
+                       local)
+    ctx = lkg.Context(device=local, tile=shape["tile"], cell=shape["cell"], group=shape["group"], xsub=shape["xsub"])
+    cid = ctx.add_complex(family, c["rec"], c["lig"])
     res = {}
     for mode in ("plain", "device", "screened", "screened_device", "ablation"):
         g = lkg.GSO(ctx, [(cid, swarms, glow)], pos, [seed])
@@ -529,7 +540,8 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
             "what": "the faster plain GSO (host or device steps) over the faster screened GSO",
             "higher_is_better": True, "data": "synthetic",
             "config": {"workload": args.workload, "family": family, "swarms": swarms, "glowworms": glow, "steps": steps,
-                       "candidates": 4, "exact_fraction": 0.25, "rescore_every": 10, "train_steps": 20},
+                       "candidates": 4, "exact_fraction": 0.25, "rescore_every": 10, "train_steps": 20,
+                       "tile_shape": {k: shape.get(k) for k in ("tile", "group", "cell", "xsub", "source")}},
             "plain": {"seconds": res["plain"]["seconds"], "exact_evals": res["plain"]["scored"],
                       "mean_best_score": best["plain"], "phases_s": res["plain"]["phases"]},
             "plain_device_gso": {"seconds": res["device"]["seconds"], "exact_evals": res["device"]["scored"],

@@ -365,6 +365,11 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
                 if (k0 + 32 < total) w_fetch(c, st, excl, total, k0 + 32 + lane, an, rn);
                 const float ax = a.x - gx, ay = a.y - gy, az = a.z - gz;
                 const float aa = ax * ax + ay * ay + az * az;
+                // cpydock kernel: a candidate farther than R = 10.001 + rho
+                // from the group centre is more than 10 A from every slot atom
+                // (|l'| <= rho), so a chunk with none closer is skipped (the
+                // test pays off there, not in the plain kernel)
+                if (DESOLV && !__any_sync(FULL, aa <= R2)) continue;
                 // test slot by slot; one ballot per slot appends that slot's
                 // hits to the ring in lane order (consecutive words: no bank
                 // conflicts, no prefix scan)
@@ -377,8 +382,10 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
                     const float q = fmaf(ax, t.x, fmaf(ay, t.y, fmaf(az, t.z, aa)));
                     const bool h = q <= -t.w;
                     const unsigned b = __ballot_sync(FULL, h);
-                    if (h) W.hit[(tail + __popc(b & lt_mask)) & (RING - 1)] = enc + ((unsigned)l << 26);
-                    tail += (unsigned)__popc(b);
+                    if (!DESOLV || b) {   // cpydock kernel: slots without a hit skip the append
+                        if (h) W.hit[(tail + __popc(b & lt_mask)) & (RING - 1)] = enc + ((unsigned)l << 26);
+                        tail += (unsigned)__popc(b);
+                    }
                 }
                 __syncwarp();
                 // 4. full batches of 32 hits

@@ -57,6 +57,17 @@ def config0():
     return synth.config0()
 
 
+@functools.lru_cache(maxsize=1)
+def config2_items():
+    """The batched workload: 64 complexes (dna, then pydock) with their
+    20 x 300 kernel-layout poses each (seed 11)."""
+    items = synth.config2()
+    for it in items:
+        it["poses"] = synth.to_kernel_poses(synth.setup_poses(it["rec"]["coords"], it["swarms"], it["glowworms"],
+                                                              it["seed"]))
+    return items
+
+
 @functools.lru_cache(maxsize=2)
 def config0_cpydock():
     return synth.config1("cpydock", base=config0())

@@ -10,26 +10,15 @@ the oracle to score everything:
   (the oracle's CPU far-field build for this receptor alone takes minutes;
   the exact path is pinned to the oracle on the smaller complexes).
 """
-import functools
-
 import numpy as np
 import pytest
 
 import oracle
-from tests.lkg_helpers import lkg, rel_err, synth
+from tests.lkg_helpers import config2_items, lkg, rel_err, synth
 
 pytestmark = pytest.mark.gpu
 
 FAST_TOL = 1e-5
-
-
-@functools.lru_cache(maxsize=1)
-def _config2():
-    items = synth.config2()
-    for it in items:
-        it["poses"] = synth.to_kernel_poses(synth.setup_poses(it["rec"]["coords"], it["swarms"], it["glowworms"],
-                                                              it["seed"]))
-    return items
 
 
 def _device_scores(ctx, ids, counts, allp):
@@ -42,7 +31,7 @@ def _device_scores(ctx, ids, counts, allp):
 
 
 def test_batched_workload_full_size():
-    items = _config2()
+    items = config2_items()
     ctx = lkg.Context()
     try:
         ids = [ctx.add_complex(it["family"], it["rec"], it["lig"]) for it in items]

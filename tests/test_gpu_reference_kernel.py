@@ -16,7 +16,7 @@ import time
 import numpy as np
 import pytest
 
-from tests.lkg_helpers import compat, config0, lkg, rel_err, synth
+from tests.lkg_helpers import compat, config0, config2_items, lkg, rel_err, synth
 
 pytestmark = pytest.mark.gpu
 
@@ -69,3 +69,63 @@ def test_reference_kernel_and_liblkg_agree_on_config0(reflib):
           "(%.0f poses/s), liblkg %.2f ms (%.0f poses/s), ratio %.1fx" % (
               t["reference"] * 1e3, len(pos) / t["reference"], t["liblkg"] * 1e3, len(pos) / t["liblkg"],
               t["reference"] / t["liblkg"]))
+
+
+FAMILY_FLAGS = {"dna": 7, "pydock": 3}   # full_score.cu:21-22
+
+
+def test_reference_kernel_per_complex_on_the_batched_workload(reflib):
+    """The batched workload (64 complexes of uneven size, dna and pydock,
+    6,000 poses each) through the reference's GPU path the way
+    gpu_family.rs:196-262 drives it, one cuda_batch_score call per complex,
+    against liblkg's batched launch group over all 64 (host buffers in both;
+    the reference's buffer cache is warm for every timed call: a first,
+    untimed call uploads the complex).  Also checks that the two libraries
+    agree on every complex through the same C ABI."""
+    items = config2_items()
+    t_ref, t_plain, diffs = 0.0, 0.0, []
+    for it in items:
+        rec, lig = it["rec"], it["lig"]
+        crec = compat.CudaReceptor(rec["coords"], rec["ele"], np.sqrt(rec["vdw"]), rec["radius"], rec["heavy"])
+        clig = compat.CudaLigand(lig["coords"], lig["ele"], np.sqrt(lig["vdw"]), lig["radius"], lig["heavy"])
+        field = lkg.field_build(rec["coords"], rec["ele"])
+        flags = FAMILY_FLAGS[it["family"]]
+        pos = it["poses"]
+        for name, L in (("reference", reflib), ("liblkg", None)):
+            raw = compat.batch_raw(field, crec, clig, pos, flags, library=L)
+            t0 = time.perf_counter()
+            raw2 = compat.batch_raw(field, crec, clig, pos, flags, library=L)
+            dt = time.perf_counter() - t0
+            if name == "reference":
+                t_ref += dt
+                s_ref = -(raw2[:, 0] * 83.0 + raw2[:, 1])
+            else:
+                t_plain += dt
+                assert np.array_equal(raw, raw2)
+                s_lkg = -(raw2[:, 0] * 83.0 + raw2[:, 1])
+        diffs.append(rel_err(s_ref, s_lkg))
+    # the reference kernel sums f32 per-atom terms in f32 blocks
+    # (full_score.cu:270-335): on scores that cancel from large terms it
+    # drifts to ~1e-3 relative; liblkg is pinned to the oracle elsewhere
+    diffs = np.concatenate(diffs)
+    worst, med = float(diffs.max()), float(np.median(diffs))
+    assert worst < 1e-2 and med < 1e-5, (worst, med)
+    ctx = lkg.Context()
+    try:
+        ids = [ctx.add_complex(it["family"], it["rec"], it["lig"]) for it in items]
+        counts = [len(it["poses"]) for it in items]
+        allp = np.vstack([it["poses"] for it in items])
+        out = np.zeros(len(allp))
+        ctx.score_multi(ids, counts, allp, out)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            ctx.score_multi(ids, counts, allp, out)
+        t_batch = (time.perf_counter() - t0) / 3
+    finally:
+        ctx.close()
+    n = len(allp)
+    print("batched workload, %d poses over %d complexes (host buffers): reference cuda_batch_score per complex "
+          "%.1f ms (%.0f poses/s), liblkg cuda_batch_score per complex %.1f ms (%.0f poses/s), liblkg batched "
+          "launch group %.1f ms (%.0f poses/s); batched / reference %.1fx; rel diff reference vs liblkg: max %.1e, "
+          "median %.1e" % (n, len(items), t_ref * 1e3, n / t_ref, t_plain * 1e3, n / t_plain, t_batch * 1e3,
+                           n / t_batch, t_ref / t_batch, worst, med))
