@@ -502,11 +502,12 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
     ctx = lkg.Context(device=local, tile=shape["tile"], cell=shape["cell"], group=shape["group"], xsub=shape["xsub"])
     cid = ctx.add_complex(family, c["rec"], c["lig"])
     res = {}
-    for mode in ("plain", "device", "screened", "screened_device", "ablation"):
+    for mode in ("plain", "device", "screened", "screened_device", "ablation", "screened_carry"):
         g = lkg.GSO(ctx, [(cid, swarms, glow)], pos, [seed])
-        if mode in ("screened", "screened_device", "ablation"):
+        if mode != "plain" and mode != "device":
             g.set_screen(candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=20,
-                         finetune_epochs=2, lr=1e-3, seed=seed, random_rank=(mode == "ablation"), batch=1024)
+                         finetune_epochs=2, lr=1e-3, seed=seed, random_rank=(mode == "ablation"), batch=1024,
+                         carry_prediction=(mode == "screened_carry"))
         torch.cuda.synchronize()
         t0 = time.perf_counter()
         g.run(steps, device=mode in ("device", "screened_device"))
@@ -525,7 +526,7 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
     res["plain_next_seed"] = dict(st=g.state())
     del g
     ov = {}
-    for mode in ("screened", "screened_device", "ablation", "plain_next_seed"):
+    for mode in ("screened", "screened_device", "ablation", "screened_carry", "plain_next_seed"):
         o = []
         for k in range(swarms):
             sl = slice(k * glow, (k + 1) * glow)
@@ -561,7 +562,14 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
                                 "what": "the screened GSO with its steps after training on the device"},
             "ablation_no_network": {"seconds": res["ablation"]["seconds"], "exact_evals": res["ablation"]["scored"],
                                     "mean_best_score": best["ablation"], "top5_overlap_with_plain": ov["ablation"],
-                                    "phases_s": res["ablation"]["phases"]},
+                                    "phases_s": res["ablation"]["phases"],
+                                    "what": "the screened search with seeded random ranks instead of the network"},
+            "screened_carry_prediction": {"seconds": res["screened_carry"]["seconds"],
+                                          "exact_evals": res["screened_carry"]["scored"],
+                                          "mean_best_score": best["screened_carry"],
+                                          "top5_overlap_with_plain": ov["screened_carry"],
+                                          "what": "the screened GSO whose unscored moves take current score + "
+                                                  "predicted gain (the default keeps the last exact score)"},
             "plain_next_seed": {"mean_best_score": best["plain_next_seed"],
                                 "top5_overlap_with_plain": ov["plain_next_seed"],
                                 "what": "the plain GSO from the same start with GSO seed + 1: the overlap two "

@@ -349,7 +349,8 @@ int lkg_gso_destroy(lkg_gso* gso);
  * on every glowworm with neighbours draws `candidates` moves from its
  * neighbour distribution, the surrogate ranks them, the glowworm takes the
  * best, and per swarm the exact_fraction of moves with the largest
- * predicted gain is scored exactly (the others carry the prediction); every
+ * predicted gain is scored exactly (the others keep their last exact score,
+ * or with carry_prediction = 1 take it plus the predicted gain); every
  * rescore_every steps all glowworms are rescored exactly and the surrogate
  * is fine-tuned on them.  random_rank = 1 is the same search without the
  * network (seeded random ranks; unscored moves keep their previous score),
@@ -365,6 +366,7 @@ typedef struct {
     uint64_t seed;            /* surrogate initialisation, shuffles, ablation ranks */
     int32_t random_rank;
     int32_t batch;            /* training minibatch (1024; 0 = 1024) */
+    int32_t carry_prediction; /* 1: unscored moves score current + predicted gain (0) */
 } lkg_screen;
 int lkg_gso_set_screen(lkg_gso* gso, const lkg_screen* cfg);
 /* exact rescoring of every glowworm (the final poses of a screened run) */

@@ -152,7 +152,8 @@ class Screen(C.Structure):
     """``lkg_screen``: surrogate screening of GSO moves."""
     _fields_ = [("candidates", C.c_int32), ("exact_fraction", C.c_double), ("rescore_every", C.c_int32),
                 ("train_steps", C.c_int32), ("train_epochs", C.c_int32), ("finetune_epochs", C.c_int32),
-                ("lr", C.c_float), ("seed", C.c_uint64), ("random_rank", C.c_int32), ("batch", C.c_int32)]
+                ("lr", C.c_float), ("seed", C.c_uint64), ("random_rank", C.c_int32), ("batch", C.c_int32),
+                ("carry_prediction", C.c_int32)]
 
 
 class Context:
@@ -441,11 +442,13 @@ class GSO:
         return dict(translation=t, rotation=r, luciferin=luc, scoring=sc, vision=vis, neighbors=nn)
 
     def set_screen(self, candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=20,
-                   finetune_epochs=2, lr=1e-3, seed=0, random_rank=False, batch=1024):
+                   finetune_epochs=2, lr=1e-3, seed=0, random_rank=False, batch=1024, carry_prediction=False):
         """Screen moves with the surrogate (random_rank: the same search with
-        random candidate ranks instead of the network, for ablations)."""
+        random candidate ranks instead of the network, for ablations;
+        carry_prediction: unscored moves score current + predicted gain
+        instead of keeping their last exact score)."""
         cfg = Screen(candidates, exact_fraction, rescore_every, train_steps, train_epochs, finetune_epochs, lr, seed,
-                     1 if random_rank else 0, batch)
+                     1 if random_rank else 0, batch, 1 if carry_prediction else 0)
         _check(lib().lkg_gso_set_screen(self.h, C.byref(cfg)))
 
     def finalize(self):

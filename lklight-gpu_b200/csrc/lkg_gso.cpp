@@ -399,7 +399,7 @@ int score_phase(lkg_gso* G, bool all, bool learn) {
                 if (all || gw.step == 0 || (gw.moved && gw.exact_next)) {  // swarm.rs:79-85
                     G->need_idx.push_back((s << 20) | (int)k);
                     counts[gi]++;
-                } else if (gw.moved && G->screen && !G->cfg.random_rank) {
+                } else if (gw.moved && G->screen && !G->cfg.random_rank && G->cfg.carry_prediction) {
                     gw.scoring = gw.pred;
                 }
             }
@@ -570,7 +570,7 @@ int lkg_gso_set_screen(lkg_gso* G, const lkg_screen* cfg) {
     if (G->step != 0) return set_error(LKG_ERR_STATE, "screening must be set before the first step");
     if (cfg->candidates < 1 || cfg->candidates > 64 || !(cfg->exact_fraction > 0.0 && cfg->exact_fraction <= 1.0) ||
         cfg->rescore_every < 0 || cfg->train_steps < 1 || cfg->train_epochs < 0 || cfg->finetune_epochs < 0 ||
-        !(cfg->lr > 0.f))
+        !(cfg->lr > 0.f) || (cfg->carry_prediction != 0 && cfg->carry_prediction != 1))
         return set_error(LKG_ERR_ARG, "bad screen configuration");
     for (auto* s : G->sur) lkg_surrogate_destroy(s);
     G->sur.clear();
@@ -722,9 +722,9 @@ int dev_setup(lkg_gso* G, bool screened) {
             a[7][i] = gw.luciferin; a[8][i] = gw.vision; a[9][i] = gw.scoring;
             const double row[7] = {gw.r.w, gw.r.x, gw.r.y, gw.r.z, gw.t[0], gw.t[1], gw.t[2]};
             std::memcpy(&pose[7 * (size_t)i], row, sizeof(row));
-            if (screened) {   // score_phase: exact for the chosen moves, the prediction for the others
+            if (screened) {   // score_phase: exact for the chosen moves, the carried prediction for the others
                 mask[i] = ((gw.moved && gw.exact_next) || gw.step == 0) ? 1 : 0;
-                if (gw.moved && !gw.exact_next && gw.step != 0) a[9][i] = gw.pred;
+                if (G->cfg.carry_prediction && gw.moved && !gw.exact_next && gw.step != 0) a[9][i] = gw.pred;
             } else {
                 mask[i] = (gw.moved || gw.step == 0) ? 1 : 0;   // swarm.rs:79-85
             }
@@ -779,7 +779,7 @@ int dev_setup(lkg_gso* G, bool screened) {
         LKG_CK(c[4].reserve((size_t)n * sizeof(double)), "device gso");
         LKG_CK(c[5].reserve(2 * (size_t)n), "device gso");
         LKG_CK(cudaMemsetAsync(c[5].p, 0, 2 * (size_t)n, st), "device gso");   // no pending predictions
-        X.K = K; X.reserved = 0; X.frac = G->cfg.exact_fraction;
+        X.K = K; X.carry = G->cfg.carry_prediction ? 1 : 0; X.frac = G->cfg.exact_fraction;
         X.cand = c[0].as<double>(); X.pred = c[1].as<double>(); X.knid = c[2].as<int>(); X.best = c[3].as<int>();
         X.gain = c[4].as<double>(); X.exact = c[5].as<unsigned char>(); X.pend = X.exact + n;
     }

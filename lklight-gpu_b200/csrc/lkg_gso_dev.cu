@@ -216,8 +216,9 @@ __global__ void k_gso_commit(GsoDevState S) {
 // screened steps (lkg_gso.cpp screened_movement, the same operations)
 // ---------------------------------------------------------------------------
 
-// moves left unscored take their predicted score (current + predicted gain)
-// before the luciferin update; the exact ones were scored this step
+// with X.carry, moves left unscored take their predicted score (current +
+// predicted gain) before the luciferin update; without it they keep their
+// last exact score.  The exact ones were scored this step
 __global__ void k_gso_luciferin_screened(GsoDevState S, GsoDevScreen X) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     const bool scored = i < S.n && S.mask[i];
@@ -297,8 +298,9 @@ __global__ void k_gso_rank(GsoDevState S, GsoDevScreen X) {
 }
 
 // every glowworm with neighbours takes its best candidate; the exact ones
-// are scored next step, the others take current + gain before the next
-// luciferin update; the swarm's draw counter advances by K per glowworm
+// are scored next step, the others (with X.carry) take current + gain
+// before the next luciferin update; the swarm's draw counter advances by K
+// per glowworm
 __global__ void k_gso_commit_screened(GsoDevState S, GsoDevScreen X) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < S.n_swarms) S.draws[i] += (unsigned long long)X.K * S.swarm_n[i];
@@ -311,7 +313,7 @@ __global__ void k_gso_commit_screened(GsoDevState S, GsoDevScreen X) {
     }
     S.vis[i] = S.nvis[i];
     S.mask[i] = moved && X.exact[i];
-    X.pend[i] = moved && !X.exact[i];
+    X.pend[i] = X.carry && moved && !X.exact[i];
     double* p = S.poses + 7 * (size_t)i;
     p[0] = S.qw[i]; p[1] = S.qx[i]; p[2] = S.qy[i]; p[3] = S.qz[i];
     p[4] = S.tx[i]; p[5] = S.ty[i]; p[6] = S.tz[i];

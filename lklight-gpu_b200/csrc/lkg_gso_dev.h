@@ -31,7 +31,7 @@ cudaError_t gso_dev_after_scoring(const GsoDevState& S, cudaStream_t s);
 // swarm scored exactly in the next step
 struct GsoDevScreen {
     int K;                   // candidates per glowworm
-    int reserved;            // keeps the struct free of padding (compared bytewise)
+    int carry;               // 1: unscored moves take current + gain (also keeps the struct free of padding)
     double frac;             // exact fraction per swarm
     double* cand;            // n x (K + 1) x 7 candidate poses (w, x, y, z, tx, ty, tz)
     double* pred;            // n x (K + 1) predicted scores
@@ -39,7 +39,7 @@ struct GsoDevScreen {
     int* best;               // n: chosen candidate row (1..K), 0 without neighbours
     double* gain;            // n: prediction at the chosen move minus at the current pose
     unsigned char* exact;    // n: the move is scored exactly in the next step
-    unsigned char* pend;     // n: score += gain before the next luciferin update
+    unsigned char* pend;     // n: score += gain before the next luciferin update (carry only)
 };
 
 // luciferin update (with the pending predicted scores), K selections per

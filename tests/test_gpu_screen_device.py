@@ -32,10 +32,10 @@ def setup():
     ctx.close()
 
 
-def _run(setup, plan):
+def _run(setup, plan, **extra):
     ctx, cid, pos = setup
     g = lkg.GSO(ctx, [(cid, SWARMS, GLOW)], pos, [SEED])
-    g.set_screen(**SCREEN)
+    g.set_screen(**SCREEN, **extra)
     for steps, dev in plan:
         g.run(steps, device=dev)
     st = g.state()
@@ -52,12 +52,14 @@ def test_host_screened_runs_repeat_exactly(setup):
     assert a["scored"] == b["scored"]
 
 
+@pytest.mark.parametrize("carry", [False, True])
 @pytest.mark.parametrize("plan", [[(9, True)], [(4, False), (5, True)]])
-def test_device_screened_steps_follow_the_host(setup, plan):
+def test_device_screened_steps_follow_the_host(setup, plan, carry):
     # all on the device (training steps 0-3 too), or the training steps on
-    # the host; a full rescoring at step 7 in both
-    host = _run(setup, [(9, False)])
-    dev = _run(setup, plan)
+    # the host; a full rescoring at step 7 in both; unscored moves keep
+    # their last exact score, or (carry) take the predicted gain
+    host = _run(setup, [(9, False)], carry_prediction=carry)
+    dev = _run(setup, plan, carry_prediction=carry)
     close = np.all(np.abs(dev["translation"] - host["translation"]) <= 1e-6 * np.maximum(1.0, np.abs(host["translation"])),
                    axis=1)
     assert close.mean() >= 0.9, close.mean()
