@@ -108,18 +108,22 @@ def cpy_flag(hyd):
     return f
 
 
-def cpydock_solv(rec, lig, poses, r_flag, l_flag, r_des, r_asa, l_des, l_asa):
-    """cuda_cpydock_solv: per-pose desolvation S."""
+def cpydock_solv(rec, lig, poses, r_flag, l_flag, r_des, r_asa, l_des, l_asa, library=None):
+    """cuda_cpydock_solv: per-pose desolvation S.  ``library``: another
+    ctypes library exporting the same symbol (as for batch_raw)."""
     poses = np.ascontiguousarray(poses, np.float64).reshape(-1, 7)
     n = len(poses)
     out = np.zeros(n)
     a = [np.ascontiguousarray(x, dt) for x, dt in ((r_flag, np.uint8), (l_flag, np.uint8), (r_des, np.float32),
                                                    (r_asa, np.float32), (l_des, np.float32), (l_asa, np.float32))]
-    r = lib().cuda_cpydock_solv(ptr(rec.r_coords), ptr(a[0]), rec.nr, ptr(rec.cell_start), ptr(rec.cell_atoms),
-                                rec.ncx, rec.ncy, rec.ncz, rec.c_o[0], rec.c_o[1], rec.c_o[2], rec.c_sp,
-                                ptr(lig.base), ptr(poses), ptr(a[1]), ptr(lig.ele), lig.nl, n,
-                                ptr(a[2]), ptr(a[3]), ptr(a[4]), ptr(a[5]), ptr(out))
+    L = library if library is not None else lib()
+    r = L.cuda_cpydock_solv(ptr(rec.r_coords), ptr(a[0]), rec.nr, ptr(rec.cell_start), ptr(rec.cell_atoms),
+                            rec.ncx, rec.ncy, rec.ncz, rec.c_o[0], rec.c_o[1], rec.c_o[2], rec.c_sp,
+                            ptr(lig.base), ptr(poses), ptr(a[1]), ptr(lig.ele), lig.nl, n,
+                            ptr(a[2]), ptr(a[3]), ptr(a[4]), ptr(a[5]), ptr(out))
     if r != 0:
+        if library is not None:
+            raise RuntimeError("cuda_cpydock_solv returned %d" % r)
         raise LkgError(lib().lkg_last_status(), lib().lkg_last_error().decode())
     return out
 

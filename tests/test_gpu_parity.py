@@ -110,7 +110,8 @@ def test_config0_fast_200_poses(ctx):
 
 @pytest.mark.parametrize("tile,group,xsub,cell", [(64, 8, 1, 2.5), (128, 16, 4, 2.0), (256, 32, 8, 3.33),
                                                     (128, 8, 4, 2.5), (256, 16, 2, 2.5), (128, 4, 8, 4.0),
-                                                    (128, 8, 8, 5.0)])
+                                                    (128, 8, 8, 5.0), (128, 8, 8, 6.0), (128, 8, 8, 7.0),
+                                                    (256, 8, 8, 6.0)])
 def test_config0_fast_kernel_shapes(tile, group, xsub, cell):
     # every tile / group / x-sub-cell / cell shape of the warp kernel finds
     # the same near pairs (exact counts) and energies within the f32 budget
@@ -142,6 +143,25 @@ def test_config1_cpydock_fast(ctx):
     assert (np.abs(got - ref) / np.maximum(np.abs(ref), 10.0)).max() < FAST_TOL
     # desolvation is evaluated in f64 on both sides
     assert np.abs(parts[:, 2] - rparts[:, 3]).max() < 1e-9 * max(1.0, np.abs(rparts[:, 3]).max())
+
+
+@pytest.mark.parametrize("group,cell", [(8, 4.0), (8, 6.0), (8, 7.0), (16, 5.0), (4, 4.0)])
+def test_config1_cpydock_fast_kernel_shapes(group, cell):
+    # the autotuner's group / cell candidates on the fused desolvation kernel:
+    # the same bound as the default shape, desolvation to f64 rounding
+    c1 = config0_cpydock()
+    m = oracle.Model("cpydock", c1["rec"], c1["lig"])
+    pos = synth.to_kernel_poses(synth.setup_poses(c1["rec"]["coords"], 2, 20, 7))
+    ref, rparts = m.batch_energy_grid(pos, parts=True)
+    c = lkg.Context(tile=128, group=group, xsub=8, cell=cell)
+    try:
+        cid = c.add_complex("cpydock", c1["rec"], c1["lig"])
+        got, parts = c.score(cid, pos, parts=True)
+    finally:
+        c.close()
+    assert (np.abs(got - ref) / np.maximum(np.abs(ref), 10.0)).max() < FAST_TOL
+    assert np.abs(parts[:, 2] - rparts[:, 3]).max() < 1e-9 * max(1.0, np.abs(rparts[:, 3]).max())
+    assert np.all(np.abs(parts[:, 3] - rparts[:, 4]) <= 2)  # near pairs (f32 boundary cases only)
 
 
 def test_config1_cpydock_exact(ctx_exact):

@@ -7,7 +7,10 @@ Both compute the pair terms in f32; liblkg sums in f64 and stays within the
 drift further (both errors are printed).  The test also times both for the
 record (printed).
 Calls keep N constant: the reference caches its output buffer at the size of
-its first call.
+its first call.  Its cache also keys on host pointers (full_score.cu:375-387):
+the packed inputs of the last complex each test hands it stay alive until
+the module ends (_KEEP), so a later complex can never be allocated at the
+same addresses and be served another complex's device arrays.
 """
 import ctypes as C
 import os
@@ -16,9 +19,11 @@ import time
 import numpy as np
 import pytest
 
-from tests.lkg_helpers import compat, config0, config2_items, lkg, rel_err, synth
+from tests.lkg_helpers import compat, config0, config0_cpydock, config2_items, lkg, rel_err, synth
 
 pytestmark = pytest.mark.gpu
+
+_KEEP = []
 
 REF = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "libref_cuda.so")
 
@@ -28,9 +33,10 @@ def reflib():
     if not os.path.exists(REF):
         pytest.skip("reference kernels not built (oracle/Makefile ref needs the reference tree)")
     L = C.CDLL(REF)
-    ours = lkg.lib().cuda_batch_score
-    L.cuda_batch_score.argtypes = ours.argtypes
-    L.cuda_batch_score.restype = ours.restype
+    for name in ("cuda_batch_score", "cuda_cpydock_solv"):
+        ours = getattr(lkg.lib(), name)
+        getattr(L, name).argtypes = ours.argtypes
+        getattr(L, name).restype = ours.restype
     return L
 
 
@@ -65,6 +71,7 @@ def test_reference_kernel_and_liblkg_agree_on_config0(reflib):
         for _ in range(3):
             compat.batch_raw(field, crec, clig, pos, flags, library=L)
         t[name] = (time.perf_counter() - t0) / 3
+    _KEEP.append((field, crec, clig, pos))
     print("cuda_batch_score, 6000 poses of the config-0 complex (host buffers, per call): reference %.2f ms "
           "(%.0f poses/s), liblkg %.2f ms (%.0f poses/s), ratio %.1fx" % (
               t["reference"] * 1e3, len(pos) / t["reference"], t["liblkg"] * 1e3, len(pos) / t["liblkg"],
@@ -104,6 +111,7 @@ def test_reference_kernel_per_complex_on_the_batched_workload(reflib):
                 assert np.array_equal(raw, raw2)
                 s_lkg = -(raw2[:, 0] * 83.0 + raw2[:, 1])
         diffs.append(rel_err(s_ref, s_lkg))
+    _KEEP.append((field, crec, clig, pos))
     # the reference kernel sums f32 per-atom terms in f32 blocks
     # (full_score.cu:270-335): on scores that cancel from large terms it
     # drifts to ~1e-3 relative; liblkg is pinned to the oracle elsewhere
@@ -129,3 +137,54 @@ def test_reference_kernel_per_complex_on_the_batched_workload(reflib):
           "launch group %.1f ms (%.0f poses/s); batched / reference %.1fx; rel diff reference vs liblkg: max %.1e, "
           "median %.1e" % (n, len(items), t_ref * 1e3, n / t_ref, t_plain * 1e3, n / t_plain, t_batch * 1e3,
                            n / t_batch, t_ref / t_batch, worst, med))
+
+
+def test_reference_cpydock_path_on_config1(reflib):
+    """cpydock through the reference's GPU path as gpu_family.rs:196-262 and
+    :352-411 drive it (cuda_batch_score for the electrostatics and LJ terms,
+    then cuda_cpydock_solv for the desolvation: three kernels and two host
+    round trips), against the same two entry points of liblkg and against
+    liblkg's fused cpydock kernel (all three terms in one launch, through
+    Context.score), on the config-1 cpydock complex (6 x 300 poses)."""
+    c1 = config0_cpydock()
+    rec, lig = c1["rec"], c1["lig"]
+    crec = compat.CudaReceptor(rec["coords"], rec["ele"], np.sqrt(rec["vdw"]), rec["radius"])
+    clig = compat.CudaLigand(lig["coords"], lig["ele"], np.sqrt(lig["vdw"]), lig["radius"])
+    field = lkg.field_build(rec["coords"], rec["ele"])
+    pos = synth.to_kernel_poses(synth.setup_poses(rec["coords"], 6, 300, 7))
+    rf, lf = compat.cpy_flag(rec["hyd"]), compat.cpy_flag(lig["hyd"])
+    flags = lkg.FLAGS["cpydock"]
+
+    def path(L):
+        raw = compat.batch_raw(field, crec, clig, pos, flags, library=L)
+        s = compat.cpydock_solv(crec, clig, pos, rf, lf, rec["des"], rec["asa"], lig["des"], lig["asa"], library=L)
+        return raw, s
+
+    out, t = {}, {}
+    for name, L in (("reference", reflib), ("liblkg", None)):
+        path(L)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            out[name] = path(L)
+        t[name] = (time.perf_counter() - t0) / 3
+    _KEEP.append((field, crec, clig, pos, rf, lf))
+    (raw_r, s_r), (raw_l, s_l) = out["reference"], out["liblkg"]
+    # f32 sums in the reference's kernels (full_score.cu:320-335, :551-566)
+    assert np.abs(raw_r - raw_l).max() < 1e-3 * max(1.0, np.abs(raw_l).max())
+    assert np.abs(s_r - s_l).max() < 1e-3 * max(1.0, np.abs(s_l).max())
+    ctx = lkg.Context()
+    try:
+        cid = ctx.add_complex("cpydock", rec, lig)
+        ctx.score(cid, pos)
+        t0 = time.perf_counter()
+        for _ in range(3):
+            ctx.score(cid, pos)
+        t["fused"] = (time.perf_counter() - t0) / 3
+    finally:
+        ctx.close()
+    n = len(pos)
+    print("cpydock, %d poses of the config-1 complex (host buffers, per call): reference cuda_batch_score + "
+          "cuda_cpydock_solv %.2f ms (%.0f poses/s), liblkg's same entry points %.2f ms (%.0f poses/s), liblkg "
+          "fused kernel %.2f ms (%.0f poses/s); fused / reference %.1fx" % (
+              n, t["reference"] * 1e3, n / t["reference"], t["liblkg"] * 1e3, n / t["liblkg"], t["fused"] * 1e3,
+              n / t["fused"], t["reference"] / t["fused"]))
