@@ -44,7 +44,13 @@ Compat& compat() {
 int ensure_ctx(Compat& C) {
     if (C.ctx) return 0;
     cudaGetLastError();  // drain a stale sticky error (full_score.cu:375)
-    return lkg_ctx_create(0, &C.ctx);
+    int st = lkg_ctx_create(0, &C.ctx);
+    if (st) return st;
+    // the reference's GSO calls these entry points once per swarm and step
+    // (swarm.rs:70-100: a few hundred poses): work units of 64 ligand atoms
+    // spread such a call over twice the warps of 128-atom units (a 300-pose
+    // call takes ~320 instead of ~400 us on the batched workload's complexes)
+    return lkg_ctx_set_tiles(C.ctx, 64, 0);
 }
 
 void clear_locked(Compat& C) {
