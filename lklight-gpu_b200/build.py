@@ -3,7 +3,7 @@
 nvcc -gencode arch=compute_100a,code=sm_100a; the f64 exact-path kernels and
 the far-field builder are compiled with --fmad=false so their f64 arithmetic
 follows the reference's operation order.  The CUDA runtime is linked
-statically, so the library needs only the driver at run time.
+statically, so the library needs only the CUDA driver at run time.
 """
 import concurrent.futures as cf
 import os
