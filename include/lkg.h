@@ -349,7 +349,7 @@ int lkg_gso_destroy(lkg_gso* gso);
  * on every glowworm with neighbours draws `candidates` moves from its
  * neighbour distribution, the surrogate ranks them, the glowworm takes the
  * best, and per swarm the exact_fraction of moves with the largest
- * predicted gain is scored exactly (the others keep their last exact score,
+ * predicted change |gain| is scored exactly (the others keep their last exact score,
  * or with carry_prediction = 1 take it plus the predicted gain); every
  * rescore_every steps all glowworms are rescored exactly and the surrogate
  * is fine-tuned on them.  random_rank = 1 is the same search without the

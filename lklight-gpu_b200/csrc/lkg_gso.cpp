@@ -506,7 +506,10 @@ int screened_movement(lkg_gso* G) {
             const double g = hpred[off[s] + best] - hpred[off[s] + c0];
             gw.pred = gw.scoring + g;
             gw.moved = true;
-            gain.push_back({g, i});
+            // the moves whose predicted score changes most are scored
+            // exactly: an unscored move keeps a score that is off by about
+            // its change, so the stale scores left are the smallest ones
+            gain.push_back({std::fabs(g), i});
         }
         std::sort(gain.begin(), gain.end(), [](const std::pair<double, uint32_t>& a, const std::pair<double, uint32_t>& b) {
             return a.first > b.first || (a.first == b.first && a.second < b.second);

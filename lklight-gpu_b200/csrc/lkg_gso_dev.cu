@@ -269,8 +269,8 @@ __global__ void k_gso_best(GsoDevState S, GsoDevScreen X) {
     X.gain[i] = p[best] - p[0];
 }
 
-// per swarm, the ceil(frac * movers) movers with the largest gain (ties: the
-// lower id first) are scored exactly.  One warp per glowworm counts, 32
+// per swarm, the ceil(frac * movers) movers with the largest |gain| (ties:
+// the lower id first) are scored exactly (the host GSO's rule).  One warp per glowworm counts, 32
 // swarm members at a time, the movers and the movers ranked ahead of it.
 __global__ void k_gso_rank(GsoDevState S, GsoDevScreen X) {
     const int lane = threadIdx.x & 31;
@@ -279,7 +279,7 @@ __global__ void k_gso_rank(GsoDevState S, GsoDevScreen X) {
     const int sw = S.swarm_of[i];
     const int first = S.swarm_first[sw], n = S.swarm_n[sw], li = i - first;
     const bool mine = S.nnb[i] > 0;
-    const double gi = X.gain[i];
+    const double gi = fabs(X.gain[i]);
     int movers = 0, ahead = 0;
     for (int j0 = 0; j0 < n; j0 += 32) {
         const int jl = j0 + lane;
@@ -287,7 +287,7 @@ __global__ void k_gso_rank(GsoDevState S, GsoDevScreen X) {
         if (jl < n) {
             const int j = first + jl;
             mv = S.nnb[j] > 0;
-            const double gj = X.gain[j];
+            const double gj = fabs(X.gain[j]);
             up = mv && (gj > gi || (gj == gi && jl < li));
         }
         movers += __popc(__ballot_sync(0xffffffffu, mv));
