@@ -475,8 +475,12 @@ class GSO:
         return dict(exact=t[0], movement=t[1], inference=t[2], training=t[3])
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().lkg_gso_destroy(self.h)
+        h, self.h = getattr(self, "h", None), None
+        if h:
+            try:
+                lib().lkg_gso_destroy(h)
+            except Exception:   # interpreter shutdown: the module's globals are gone
+                pass
 
 
 class Rng:
@@ -489,8 +493,12 @@ class Rng:
         return lib().lkg_rng_f64(self.h)
 
     def __del__(self):
-        if getattr(self, "h", None):
-            lib().lkg_rng_free(self.h)
+        h, self.h = getattr(self, "h", None), None
+        if h:
+            try:
+                lib().lkg_rng_free(h)
+            except Exception:   # interpreter shutdown: the module's globals are gone
+                pass
 
 
 def field_build(coords, charges):
