@@ -181,3 +181,30 @@ def test_rank_lists_in_the_reference_format(tmp_path):
     assert lines[2] == "    2    1     1     9.000000    31.250000 swarm_1/lightdock_1.pdb (4.000,5.000,6.000)"
     assert lines[6] == "    6    1     0     7.123457   -12.500000 swarm_1/lightdock_0.pdb (1.000,-2.500,3.125)"
     assert [r["luciferin"] for r in ranked] == [9.0, 9.0, 7.12345678, 7.12345678, 1.5, 1.5]
+
+
+def test_bench_tile_shape_without_the_autotuner():
+    # a shape on the command line is used as given; --no-autotune keeps the
+    # library's defaults (zeros: the context picks them)
+    import argparse
+    import bench
+    a = argparse.Namespace(tile=64, group=8, cell=6.0, xsub=8, no_autotune=False)
+    assert bench.pick_shape(a, [], 0) == dict(tile=64, group=8, cell=6.0, xsub=8, source="command line")
+    a = argparse.Namespace(tile=0, group=0, cell=0.0, xsub=0, no_autotune=True)
+    assert bench.pick_shape(a, [], 0) == dict(tile=0, group=0, cell=0.0, xsub=0, source="library default")
+
+
+def test_bench_top5_overlap_rule():
+    # tools/analyze_perf3.py:50-55: a pose of run A counts when some top-5
+    # pose of run B lies within 2 A on every axis; ranks by descending score
+    import bench
+    tr_a = np.array([[0.0, 0, 0], [10, 0, 0], [20, 0, 0], [30, 0, 0], [40, 0, 0], [50, 0, 0]])
+    sc_a = np.array([6.0, 5, 4, 3, 2, 1])
+    tr_b = tr_a + np.array([1.9, -1.9, 0.0])
+    assert bench.top5_overlap(tr_a, sc_a, tr_b, sc_a) == 1.0
+    tr_b2 = tr_a.copy()
+    tr_b2[0] += [2.1, 0, 0]
+    assert bench.top5_overlap(tr_a, sc_a, tr_b2, sc_a) == 0.8
+    # run B's top 5 exclude its lowest-scored pose
+    sc_b = np.array([1.0, 5, 4, 3, 2, 6])
+    assert bench.top5_overlap(tr_a, sc_a, tr_a, sc_b) == 0.8
