@@ -70,10 +70,15 @@ def parse():
     return ap.parse_args()
 
 
-def workload(name):
+def workload(name, gen=None):
+    """The workload's complexes with their setup poses.  gen: the chain and
+    StdRng generators (None: liblkg's; the CPU reference arm passes the
+    oracle's, so that it never loads the product library)."""
     synth = importlib.import_module("lklight-gpu_b200.synth")
+    if gen is not None and name not in ("config0", "config2"):
+        raise SystemExit("the CPU reference arm covers the config0 and config2 workloads")
     if name == "config0":
-        c0 = synth.config0()
+        c0 = synth.config0(gen=gen)
         items = [dict(rec=c0["rec"], lig=c0["lig"], family="dna", swarms=1, glowworms=200, seed=42)]
     elif name == "config1":
         base = synth.config0()
@@ -90,10 +95,10 @@ def workload(name):
         c0 = synth.config0()
         items = [dict(rec=c0["rec"], lig=c0["lig"], family="dna", swarms=10, glowworms=1000, seed=3)]
     else:
-        items = synth.config2()
+        items = synth.config2(gen=gen)
     for it in items:
         it["poses"] = synth.to_kernel_poses(
-            synth.setup_poses(it["rec"]["coords"], it["swarms"], it["glowworms"], it["seed"]))
+            synth.setup_poses(it["rec"]["coords"], it["swarms"], it["glowworms"], it["seed"], gen=gen))
     if name == "restraints":
         it = items[0]
         centres = it["poses"][::it["glowworms"], 4:7]
@@ -145,39 +150,87 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(items, min_seconds=10.0, threads=0, max_complexes=2):
-    """Oracle poses/s on a bounded sample: the first dna and the first pydock
-    complex, poses from their setup sets, batches until min_seconds pass."""
+def cpu_models(items):
+    """Oracle models of every complex with their far fields built (set-up,
+    as the reference builds its ReceptorField once per receptor)."""
     import oracle
-    picks = []
-    for fam in ("dna", "pydock"):
-        for k, it in enumerate(items):
-            if it["family"] == fam:
-                picks.append(k)
-                break
-    picks = picks[:max_complexes]
-    models = [(k, oracle.Model(items[k]["family"], items[k]["rec"], items[k]["lig"])) for k in picks]
-    for k, m in models:
-        m.field()  # far field built before timing (setup, as the reference caches it)
-        if "restraints" in items[k]:
-            rr, lr, mem = items[k]["restraints"]
+    models = []
+    for it in items:
+        m = oracle.Model(it["family"], it["rec"], it["lig"])
+        m.field()
+        if "restraints" in it:
+            rr, lr, mem = it["restraints"]
             m.set_restraints(rr, int(rr.max()) + 1, lr, int(lr.max()) + 1, mem)
-    done, t0, batch = 0, time.perf_counter(), 8
-    off = 0
+        models.append(m)
+    return models
+
+
+def cpu_sample(items, models, min_seconds=10.0, threads=0, per_complex=32):
+    """The oracle (the reference's CPU grid path) on a bounded sample of the
+    workload itself: rounds that take `per_complex` poses from every complex
+    in turn (every complex has the same number of poses in the step, so each
+    round has the step's mix), until min_seconds pass.  Returns poses/s,
+    near pairs/s (pairs counted by the oracle), the cores used and the
+    sample's description."""
+    done, pairs, off = 0, 0.0, 0
+    t0 = time.perf_counter()
     while True:
-        for k, m in models:
-            p = items[k]["poses"]
-            sel = p[(off + np.arange(batch)) % len(p)]
-            m.batch_energy_grid(sel, threads=threads)
-            done += batch
-        off += batch
+        for it, m in zip(items, models):
+            p = it["poses"]
+            sel = p[(off + np.arange(per_complex)) % len(p)]
+            _, parts = m.batch_energy_grid(sel, threads=threads, parts=True)
+            pairs += float(parts[:, 4].sum())
+            done += len(sel)
+        off += per_complex
         el = time.perf_counter() - t0
         if el >= min_seconds:
             break
-        batch = min(batch * 2, 512)
     cores = threads if threads > 0 else os.cpu_count()
-    return done / el, cores, "poses of complexes %s (%s), %d poses, %.1f s" % (
-        picks, "/".join(items[k]["family"] for k in picks), done, el)
+    sample = "%d poses, %d from each of the %d complexes in turn (the step's mix), %.1f s" % (
+        done, done // len(items), len(items), el)
+    return dict(value=done / el, pairs_per_s=pairs / el, cores=cores, sample=sample)
+
+
+def parity_sample(items, models, scores, counts, pairs, per_complex=4, fp64_every=4, seed=23):
+    """Parity of the timed step's own scores, computed after the timed
+    region: from every complex, `per_complex` seeded random poses and the
+    pose with the most near pairs (the most crowded interface), against the
+    oracle (the reference's CPU grid path: f32 far field) and, for every
+    `fp64_every`-th complex, against the oracle's FP64 evaluation of the
+    same function (far field accumulated and stored in f64).  Relative error
+    with denominator max(|E|, 1), as the reference's grid-vs-exact test
+    (src/dna.rs:1155-1179)."""
+    rng = np.random.default_rng(seed)
+    off = np.concatenate([[0], np.cumsum(counts)])
+    e_grid, e_fp64, n_fp64 = [], [], 0
+    for k, (it, m) in enumerate(zip(items, models)):
+        n = counts[k]
+        sel = np.unique(np.concatenate([rng.choice(n, min(per_complex, n), replace=False),
+                                        [int(np.argmax(pairs[off[k]:off[k + 1]]))]]))
+        got = scores[off[k] + sel]
+        ref = m.batch_energy_grid(it["poses"][sel])
+        e_grid.append(np.abs(got - ref) / np.maximum(np.abs(ref), 1.0))
+        if k % fp64_every == 0:
+            r64 = m.batch_energy_grid(it["poses"][sel], fp64=True)
+            e_fp64.append(np.abs(got - r64) / np.maximum(np.abs(r64), 1.0))
+            n_fp64 += len(sel)
+    eg, ef = np.concatenate(e_grid), np.concatenate(e_fp64)
+    return {"vs_oracle": {"max_rel": float(eg.max()), "median_rel": float(np.median(eg)), "poses": int(len(eg))},
+            "vs_fp64": {"max_rel": float(ef.max()), "median_rel": float(np.median(ef)), "poses": int(n_fp64)},
+            "tolerance": 1e-5, "denominator": "max(|E|, 1)",
+            "sample": "from every complex %d seeded random poses of the timed step plus its most crowded pose; "
+                      "FP64 on every %d-th complex" % (per_complex, fp64_every)}
+
+
+def workload_config(args, items, world):
+    """The workload definition (identical on both arms of the comparison)."""
+    return {"workload": args.workload, "complexes": len(items),
+            "poses_per_step": int(sum(len(it["poses"]) for it in items)),
+            "families": sorted(set(it["family"] for it in items)),
+            "receptor_atoms": int(sum(len(it["rec"]["coords"]) for it in items)),
+            "ligand_atoms": int(sum(len(it["lig"]["coords"]) for it in items)),
+            "l2": "inputs larger than L2 (receptor arrays and far-field grids of all complexes)",
+            "parallelism": "replicas" if world > 1 else "single"}
 
 
 def max_over_ranks(v, dist, device):
@@ -196,20 +249,32 @@ def job_rate(units_per_rank, world, ms_max):
 
 
 def run_reference(args, rank, world):
+    """The reference's CPU grid path (the oracle port: the reference is Rust
+    and cannot be built here) on the host cores, all threads, over bounded
+    samples of the same workload: every step takes poses from every complex.
+    Inputs come from the oracle's generators, so this arm never loads
+    liblkg.  Rank 0 alone runs (the other ranks exit)."""
     if rank != 0:
         return
-    items = workload(args.workload)
-    vals = []
+    import oracle
+    items = workload(args.workload, gen=oracle.Generators)
+    if args.complexes:
+        items = items[:args.complexes]
+    models = cpu_models(items)
+    vals, prs = [], []
     for s in range(args.warmup + args.steps):
-        v, cores, sample = cpu_sample(items, min_seconds=3.0 if s < args.warmup else 6.0)
+        r = cpu_sample(items, models, min_seconds=1.0 if s < args.warmup else 3.0)
         if s >= args.warmup:
-            vals.append(v)
+            vals.append(r["value"])
+            prs.append(r["pairs_per_s"])
     v = statistics.median(vals)
     line = {"impl": "reference", "metric": "exact poses/s on 1 B200 (dna); surrogate-screened at >=95% top-5 overlap",
             "value": v, "unit": "poses/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": None, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-            "data": "synthetic", "config": {"workload": args.workload, "sample": sample},
-            "cpu_baseline": {"value": v, "unit": "poses/s", "cores": cores, "kind": "port", "sample": sample},
+            "data": "synthetic", "config": workload_config(args, items, world),
+            "pair_rate": {"value": statistics.median(prs), "unit": "near pairs/s"},
+            "cpu_baseline": {"value": v, "unit": "poses/s", "cores": r["cores"], "kind": "port",
+                             "sample": r["sample"] + " per step (median of %d steps)" % args.steps},
             "e2e": {"value": v, "unit": "poses/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
@@ -312,6 +377,7 @@ def main():
     clk = clocks.stop()
     launches = ctx.launches - l0
     ms = ev0.elapsed_time(ev1) / args.steps
+    timed_scores = d_scores.cpu().numpy()   # the last timed step's scores (read after the timed region)
     ms_max = max_over_ranks(ms, dist, "cuda")
     value = job_rate(npose, world, ms_max)
 
@@ -404,14 +470,10 @@ def main():
             "value": value, "unit": "poses/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 pair math, f64 transform and sums", "data": "synthetic",
-            "config": {"workload": args.workload, "complexes": len(items), "poses_per_step": npose,
-                       "families": sorted(set(it["family"] for it in items)),
-                       "receptor_atoms": int(sum(len(it["rec"]["coords"]) for it in items)),
-                       "ligand_atoms": int(sum(len(it["lig"]["coords"]) for it in items)),
-                       "near_pairs_per_step": float(pairs.sum()), "near_pairs_by_family": fam_pairs,
-                       "l2": "inputs larger than L2 (receptor arrays and far-field grids of all complexes)",
-                       "parallelism": "replicas" if world > 1 else "single",
-                       "tile_shape": {k: shape.get(k) for k in ("tile", "group", "cell", "xsub", "source")}},
+            "config": workload_config(args, items, world),
+            "work": {"near_pairs_per_step": float(pairs.sum()), "near_pairs_by_family": fam_pairs,
+                     "counted_by": "the exact (f64) path's near-pair counts, equal to the oracle's by test",
+                     "tile_shape": {k: shape.get(k) for k in ("tile", "group", "cell", "xsub", "source")}},
             "roofline": {"bound": "fp32", "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
                          "frac": achieved / fp32_peak,
                          "traffic": TRAFFIC_PER_POSE * npose if args.workload == "config2" else None,
@@ -436,7 +498,7 @@ def main():
         # interface bits; and the fractions seen, to show they were exercised
         h_iface = ctx.score_interface(ids[0], items[0]["poses"])[1]
         rr, lr, mem = items[0]["restraints"]
-        line["config"]["restraints"] = {
+        line["work"]["restraints"] = {
             "receptor_residues": int(rr.max()) + 1, "ligand_residues": int(lr.max()) + 1, "membrane_beads": len(mem),
             "poses_with": {k: int((h_iface[:, i] > 0).sum()) for i, k in enumerate(("rec", "lig", "membrane"))}}
         plan.close()
@@ -457,14 +519,17 @@ def main():
                                       "restraint_overhead": ms / pms - 1.0}
         for cid, it in zip(ids, items):
             ctx.set_restraints(cid, *it["restraints"])
-    # (the oracle's CPU far-field build for the 101k-atom cpydock receptor
-    # alone takes minutes: no CPU sample for that workload)
-    if rank == 0 and world == 1 and not args.no_cpu_baseline and args.workload != "config4":
-        v, cores, sample = cpu_sample(items)
-        line["cpu_baseline"] = {"value": v, "unit": "poses/s", "cores": cores, "kind": "port", "sample": sample}
-        v1, _, sample1 = cpu_sample(items, min_seconds=5.0, threads=1)
-        line["cpu_baseline_single_thread"] = {"value": v1, "unit": "poses/s", "cores": 1, "kind": "port",
-                                              "sample": sample1}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        models = cpu_models(items)
+        line["parity"] = parity_sample(items, models, timed_scores, counts, pairs)
+        r = cpu_sample(items, models)
+        line["cpu_baseline"] = {"value": r["value"], "unit": "poses/s", "cores": r["cores"], "kind": "port",
+                                "sample": r["sample"], "pair_rate": {"value": r["pairs_per_s"],
+                                                                     "unit": "near pairs/s"}}
+        r1 = cpu_sample(items, models, min_seconds=5.0, threads=1, per_complex=4)
+        line["cpu_baseline_single_thread"] = {"value": r1["value"], "unit": "poses/s", "cores": 1, "kind": "port",
+                                              "sample": r1["sample"],
+                                              "pair_rate": {"value": r1["pairs_per_s"], "unit": "near pairs/s"}}
     if rank == 0:
         print(json.dumps(line), flush=True)
     plan.close()

@@ -223,19 +223,23 @@ int lkg_score_multi(lkg_ctx* ctx, int n_items, const int* complex_ids, const int
  * where allocation calls are not allowed).  The fast tile kernel's scratch
  * lives in a fixed 8 MiB array inside liblkg (held on every GPU that loads
  * the library); a batch needing more (32 B per pose and ligand tile + 4 B
- * per pose + 64 B) fails with LKG_ERR_CAPACITY.  The first call on a device
- * looks the array's address up (cudaGetSymbolAddress): make it before any
- * stream capture.  Each call clears the counters it uses; calls overlapping
- * on the GPU race on the shared array.  The complex must be resident and
- * already scored once through a regular entry point; cpydock complexes are
- * refused.  Asynchronous on the context stream. */
+ * per pose rounded up to a multiple of 8 + 64 B) fails with
+ * LKG_ERR_CAPACITY.  The first call on a device looks the array's address
+ * up (cudaGetSymbolAddress) and keeps it: make that call before any stream
+ * capture, and do not use the entry point across a cudaDeviceReset.  Each
+ * call clears the counters it uses; calls overlapping on the GPU race on
+ * the shared array.  The complex must be resident and already scored once
+ * through a regular entry point; cpydock complexes and complexes with
+ * restraints are refused.  Asynchronous on the context stream: lkg_ctx_sync
+ * waits for it and reports the kernel's status word. */
 int lkg_score_device_noalloc(lkg_ctx* ctx, int complex_id, int n_pose, const double* d_poses,
                              double* d_scores, double* d_parts);
 
 /* Kernel launches made by this context so far (for launch accounting). */
 int64_t lkg_ctx_launches(lkg_ctx* ctx);
 /* Wait (bounded host poll) for the context stream and check the device
- * status word (LKG_ERR_CAPACITY after a desolvation-hash overflow). */
+ * status words: the context's (LKG_ERR_CAPACITY after a desolvation-hash
+ * overflow) and, after lkg_score_device_noalloc, that entry point's. */
 int lkg_ctx_sync(lkg_ctx* ctx);
 
 /* Plans: one batch (complexes x pose counts) prepared once — descriptors,

@@ -113,7 +113,15 @@ struct LaunchParams {
     // optional [N x 3]: restraint fractions (receptor, ligand) and membrane
     // intersection of each scored pose
     double* iface_out;
+    // desolvation spill tables: one region of spill_cap slots per block
+    // (SPILL_SLOT_BYTES each), all slots empty between poses; null: none
+    unsigned char* spill;
+    int spill_cap;
 };
+
+// bytes per spill slot: the exact kernel's 8-byte value + 4-byte key (the
+// fast kernel's packed 8-byte slots use the first 8 x spill_cap bytes)
+constexpr int SPILL_SLOT_BYTES = 12;
 
 constexpr double FACTOR = 332.0;
 constexpr double EPSILON = 4.0;

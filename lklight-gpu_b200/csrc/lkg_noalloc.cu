@@ -14,17 +14,25 @@
 // Limits and rules:
 //   * The array holds LKG_NOALLOC_SCRATCH_BYTES (8 MiB) on every GPU that
 //     loads liblkg, for the life of the process.  A call needs
-//     32 bytes per (pose, ligand tile) + 4 bytes per pose + 64 bytes;
-//     larger batches are rejected with LKG_ERR_CAPACITY before any work.
+//     32 bytes per (pose, ligand tile) + 4 bytes per pose (rounded up to a
+//     multiple of 8) + 64 bytes; larger batches are rejected with
+//     LKG_ERR_CAPACITY before any work.
 //   * The host cannot use the array's name as a device address; on the
 //     first call on each device (with that device current) the entry point
-//     looks the address up once with cudaGetSymbolAddress.  Make that first
-//     call before any stream capture.
+//     looks the address up once with cudaGetSymbolAddress and keeps it for
+//     the process.  Make that first call before any stream capture, and do
+//     not use the entry point across a cudaDeviceReset (the reset unloads
+//     the module and the kept address would be stale).
 //   * Every call shares the one array and it keeps the last call's
 //     contents, so each call clears the counters it needs with
-//     cudaMemsetAsync on its stream first.  Calls whose kernels overlap on
-//     the GPU (different streams, or several contexts on one device) race
-//     on the array: serialise them.
+//     cudaMemsetAsync on its stream and writes its one-item work table with
+//     a one-thread kernel (values passed by value: nothing is read from
+//     host memory).  Calls whose kernels overlap on the GPU (different
+//     streams, or several contexts on one device) race on the array:
+//     serialise them.
+//   * The kernel reports errors in a status word inside the array;
+//     lkg_ctx_sync (which waits for the context stream) reads and clears it
+//     after a no-allocation call, as it does the context's own word.
 //   * The complex must already be resident (lkg_complex_add) and its device
 //     descriptor uploaded by an earlier scoring call of the context; the
 //     fast (f32) tile kernel is used; cpydock complexes (shared-memory
@@ -44,7 +52,35 @@ __device__ __align__(256) static unsigned char g_noalloc_scratch[LKG_NOALLOC_SCR
 std::mutex g_mu;
 void* g_addr[64] = {nullptr};  // per-device address of g_noalloc_scratch
 
+// byte offsets inside the array
+constexpr size_t OFF_WORK = 0, OFF_STATUS = 16, OFF_WORK0 = 32, OFF_ITEMS = 48, OFF_HEAD = 64;
+
+// the call's one-item work table, written on the device from values
+// passed by value: (work0[0], work0[1]) = (0, total), items = (complex, first
+// pose, pose count, 0)
+__global__ void k_noalloc_table(unsigned char* base, int complex_id, int n_pose, long long total) {
+    long long* w0 = reinterpret_cast<long long*>(base + OFF_WORK0);
+    int* it = reinterpret_cast<int*>(base + OFF_ITEMS);
+    w0[0] = 0;
+    w0[1] = total;
+    it[0] = complex_id; it[1] = 0; it[2] = n_pose; it[3] = 0;
+}
+
 }  // namespace
+
+namespace lkg {
+// status word of the last no-allocation call on the context's device (the
+// context's stream has been waited for by the caller)
+int noalloc_check_status(lkg_ctx* ctx) {
+    void* base = nullptr;
+    {
+        std::lock_guard<std::mutex> g(g_mu);
+        if (ctx->device >= 0 && ctx->device < 64) base = g_addr[ctx->device];
+    }
+    if (!base) return set_ok();
+    return check_status_word(reinterpret_cast<int*>(static_cast<char*>(base) + OFF_STATUS));
+}
+}  // namespace lkg
 
 using namespace lkg;
 
@@ -66,8 +102,8 @@ int lkg_score_device_noalloc(lkg_ctx* ctx, int complex_id, int n_pose, const dou
     LKG_CK(cudaSetDevice(ctx->device), "cudaSetDevice");
 
     // sizes: [work counter 16 B | status 16 B | item tables 32 B | pose counters | partials]
-    const size_t head = 64;
-    const size_t counters = ((size_t)n_pose * sizeof(int) + 255) & ~(size_t)255;
+    const size_t head = OFF_HEAD;
+    const size_t counters = ((size_t)n_pose * sizeof(int) + 7) & ~(size_t)7;   // partials stay 8-byte aligned
     const size_t partials = (size_t)n_pose * d.ntiles * 4 * sizeof(double);
     if (head + counters + partials > LKG_NOALLOC_SCRATCH_BYTES)
         return set_error(LKG_ERR_CAPACITY,
@@ -88,28 +124,29 @@ int lkg_score_device_noalloc(lkg_ctx* ctx, int complex_id, int n_pose, const dou
         base = (char*)g_addr[ctx->device];
     }
     cudaStream_t s = ctx->stream;
-    // the array keeps the previous call's contents: zero the counters, the
-    // status word and the item table region before this launch
+    // the array keeps the previous call's contents: zero the work counter,
+    // the status word and the pose counters, then write this call's table
+    const long long total = (long long)n_pose * d.ntiles;
     LKG_CK(cudaMemsetAsync(base, 0, head + counters, s), "scratch clear");
-    long long work0[2] = {0, (long long)n_pose * d.ntiles};
-    int items[4] = {complex_id, 0, n_pose, 0};
-    LKG_CK(cudaMemcpyAsync(base + 32, work0, sizeof(work0), cudaMemcpyHostToDevice, s), "item table");
-    LKG_CK(cudaMemcpyAsync(base + 48, items, sizeof(items), cudaMemcpyHostToDevice, s), "item table");
+    k_noalloc_table<<<1, 1, 0, s>>>((unsigned char*)base, complex_id, n_pose, total);
+    LKG_CK(cudaGetLastError(), "work table");
+    ctx->launches++;
+    ctx->noalloc_used = true;
 
     LaunchParams p{};
     p.cx = ctx->d_cx.as<ComplexDev>();
-    p.item_work0 = (const long long*)(base + 32);
-    p.item_complex = (const int*)(base + 48);
+    p.item_work0 = (const long long*)(base + OFF_WORK0);
+    p.item_complex = (const int*)(base + OFF_ITEMS);
     p.item_pose0 = p.item_complex + 1;
     p.item_npose = p.item_complex + 2;
     p.n_items = 1;
-    p.total_work = work0[1];
+    p.total_work = total;
     p.tile = ctx->tile;
     p.poses = d_poses;
     p.scores = d_scores;
     p.parts = d_parts;
-    p.work_counter = (unsigned long long*)base;
-    p.status = (int*)(base + 16);
+    p.work_counter = (unsigned long long*)(base + OFF_WORK);
+    p.status = (int*)(base + OFF_STATUS);
     p.pose_counter = (int*)(base + head);
     p.partials = (double*)(base + head + counters);
     p.max_tiles = d.ntiles;

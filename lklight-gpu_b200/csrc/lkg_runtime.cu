@@ -153,7 +153,8 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     cr.n_cells = (int)ncell;
     // desolvation hash capacity: >= 2 x receptor atoms up to 8192 slots
     // (64 KB of shared memory in the fast kernel, 96 KB in the exact one); a
-    // pose touching more receptor atoms within 6.4 A reports LKG_ERR_CAPACITY
+    // pose touching more receptor atoms within 6.4 A continues in the launch
+    // group's global spill tables (more slots than receptor atoms)
     int cap = 64;
     while (cap < 2 * n && cap < 8192) cap <<= 1;
     d.hcap = cap;
@@ -453,6 +454,14 @@ cudaError_t Scratch::ensure(size_t units, size_t poses, cudaStream_t s, size_t i
     return cudaSuccess;
 }
 
+cudaError_t Scratch::ensure_spill(size_t bytes, cudaStream_t s) {
+    if (bytes == 0 || (spill.p && bytes <= spill.bytes)) return cudaSuccess;
+    cudaError_t e;
+    if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;   // a launch may still use the old tables
+    if ((e = spill.reserve(bytes)) != cudaSuccess) return e;
+    return cudaMemsetAsync(spill.p, 0xff, spill.bytes, s);
+}
+
 void Group::pack(char* dst) const {
     const size_t ni = ic.size();
     memcpy(dst, w0.data(), (ni + 1) * sizeof(long long));
@@ -481,6 +490,11 @@ int build_groups(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, G
             G.inp.push_back(counts[i]);
             G.w0.push_back(G.w0.back() + (k ? (long long)counts[i] : (long long)counts[i] * d.ntiles));
             G.hcap = std::max(G.hcap, d.hcap);
+            if (k) {   // spill slots: more than the receptor has atoms, so a spill insert always succeeds
+                int sc = 64;
+                while (sc <= d.nr) sc <<= 1;
+                G.spill_cap = std::max(G.spill_cap, sc);
+            }
             // one stride for both groups: a pose's bits sit at pose * stride
             g[0].iface_words = g[1].iface_words = std::max(g[0].iface_words, d.iface_words);
         }
@@ -488,6 +502,19 @@ int build_groups(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, G
     }
     *n_poses = (size_t)pose0;
     return set_ok();
+}
+
+long long group_blocks(lkg_ctx* ctx, const Group& G, bool exact) {
+    const long long work = std::max(1LL, G.w0.back());
+    long long blocks;
+    if (G.kind == 0) blocks = (long long)ctx->sm_count * occupancy(ctx, false, exact, ctx->tile, 0);
+    else blocks = (long long)ctx->sm_count * occupancy(ctx, true, exact, ctx->desolv_threads, G.hcap);
+    return std::max(1LL, std::min(blocks, work));
+}
+
+size_t group_spill_bytes(lkg_ctx* ctx, const Group& G, bool exact) {
+    if (G.kind != 1 || G.ic.empty()) return 0;
+    return (size_t)group_blocks(ctx, G, exact) * (size_t)G.spill_cap * SPILL_SLOT_BYTES;
 }
 
 int launch_group(lkg_ctx* ctx, const Group& G, const char* db, Scratch& sc, const double* d_poses,
@@ -528,18 +555,25 @@ int launch_group(lkg_ctx* ctx, const Group& G, const char* db, Scratch& sc, cons
     }
     p.iface_out = d_iface;
     cudaError_t e;
+    const long long blocks = group_blocks(ctx, G, exact);
     if (G.kind == 0) {
-        int threads = ctx->tile;
-        long long blocks = (long long)ctx->sm_count * occupancy(ctx, false, exact, threads, 0);
-        blocks = std::max(1LL, std::min(blocks, p.total_work));
-        e = exact ? launch_score_exact(p, threads, (int)blocks, ctx->stream)
-                  : launch_score_fast(p, threads, (int)blocks, ctx->stream);
+        e = exact ? launch_score_exact(p, ctx->tile, (int)blocks, ctx->stream)
+                  : launch_score_fast(p, ctx->tile, (int)blocks, ctx->stream);
     } else {
         int threads = ctx->desolv_threads;
         size_t smem = desolv_smem_bytes(G.hcap, exact);
         if (smem > 227 * 1024) return set_error(LKG_ERR_CAPACITY, "desolvation hash too large");
-        long long blocks = (long long)ctx->sm_count * occupancy(ctx, true, exact, threads, G.hcap);
-        blocks = std::max(1LL, std::min(blocks, p.total_work));
+        const size_t need = group_spill_bytes(ctx, G, exact);
+        if (need > sc.spill.bytes || !sc.spill.p) {
+            // tables are sized before capture by the callers; grow here only outside a capture
+            cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+            cudaStreamIsCapturing(ctx->stream, &cs);
+            if (cs != cudaStreamCaptureStatusNone)
+                return set_error(LKG_ERR_STATE, "desolvation spill tables not sized before the capture");
+            LKG_CK(sc.ensure_spill(need, ctx->stream), "spill tables");
+        }
+        p.spill = sc.spill.as<unsigned char>();
+        p.spill_cap = G.spill_cap;
         e = exact ? launch_desolv_exact(p, threads, (int)blocks, G.hcap, ctx->stream)
                   : launch_desolv_fast(p, threads, (int)blocks, G.hcap, ctx->stream);
     }
@@ -971,6 +1005,8 @@ int lkg_plan_create(lkg_ctx* ctx, int n_items, const int* ids, const int* counts
         (e = cudaMemcpy(P->d_tables.p, packed.data(), b0 + b1, cudaMemcpyHostToDevice)) != cudaSuccess ||
         (e = P->scratch.ensure(std::max<size_t>(P->g[0].w0.back(), 1), std::max<size_t>(P->n_poses, 1), ctx->stream,
                                P->n_poses * (size_t)P->g[0].iface_words)) != cudaSuccess ||
+        (e = P->scratch.ensure_spill(std::max(group_spill_bytes(ctx, P->g[1], false),
+                                              group_spill_bytes(ctx, P->g[1], true)), ctx->stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(ctx->stream)) != cudaSuccess) {
         delete P;
         return set_error(cuda_to_status(e), "plan setup: %s", cudaGetErrorString(e));
@@ -1063,7 +1099,9 @@ int lkg_ctx_sync(lkg_ctx* ctx) {
     cudaSetDevice(ctx->device);
     int st = wait_stream(ctx, 300.0);
     if (st) return st;
-    return check_status(ctx);
+    st = check_status(ctx);
+    if (st) return st;
+    return ctx->noalloc_used ? noalloc_check_status(ctx) : set_ok();
 }
 
 int lkg_plan_sync(lkg_plan* P) {

@@ -94,8 +94,12 @@ struct Occupancy { int threads = 0, hcap = 0, blocks = 0; };
 struct Scratch {
     DBuf partials, pose_counter, work_counter, status, iface;
     size_t cap_units = 0, cap_poses = 0, cap_iface = 0;
+    // desolvation spill tables (every slot empty between launches)
+    DBuf spill;
     // iface_words: interface bit words of the whole batch (poses x stride)
     cudaError_t ensure(size_t units, size_t poses, cudaStream_t s, size_t iface_words = 0);
+    // at least `bytes` of spill tables, all slots empty (0xff bytes)
+    cudaError_t ensure_spill(size_t bytes, cudaStream_t s);
 };
 
 // one launch group's item tables: (complex, first pose, pose count) per item
@@ -105,6 +109,7 @@ struct Group {
     std::vector<int> ic, ip0, inp;
     std::vector<long long> w0{0};
     int hcap = 64;
+    int spill_cap = 0;     // desolvation spill slots per block: a power of two above the largest receptor
     int iface_words = 0;   // interface bit words per pose (the batch's largest)
     size_t bytes() const { return (ic.size() + 1) * sizeof(long long) + ic.size() * 3 * sizeof(int); }
     void pack(char* dst) const;
@@ -137,6 +142,7 @@ struct lkg_ctx {
     lkg::HBuf h_poses, h_out;
     int64_t launches = 0;
     lkg::Occupancy occ_tiles[2], occ_desolv[2];
+    bool noalloc_used = false;      // lkg_score_device_noalloc ran on this context (its status word is checked)
 };
 
 namespace lkg {
@@ -159,9 +165,15 @@ int launch_items(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, c
 int wait_stream(lkg_ctx* ctx, double timeout_s);
 int check_status(lkg_ctx* ctx);
 int check_status_word(int* d_status);
+// status word of the no-allocation entry point's array on the context's device
+int noalloc_check_status(lkg_ctx* ctx);
 // item tables of the two launch groups for a batch
 int build_groups(lkg_ctx* ctx, int n_items, const int* ids, const int* counts, Group g[2], size_t* n_poses);
 int sync_descriptors(lkg_ctx* ctx);
+// persistent grid of a launch group at the given precision
+long long group_blocks(lkg_ctx* ctx, const Group& g, bool exact);
+// spill table bytes of a desolvation group at the given precision
+size_t group_spill_bytes(lkg_ctx* ctx, const Group& g, bool exact);
 // launch one prepared group (kernel launches only: stream-capturable)
 int launch_group(lkg_ctx* ctx, const Group& g, const char* d_tables, Scratch& sc, const double* d_poses,
                  double* d_scores, double* d_parts, int raw_pairs, int solv_only, float* atom_e, float* atom_v,

@@ -231,24 +231,42 @@ __device__ __forceinline__ double solv_term(double d2, double asa) {
 
 // receptor-minimum hash in shared memory (open addressing, bounded probes):
 // key = position-sorted receptor index, value = f64 bits of the minimum d^2
-// (non-negative doubles order like their bit patterns, so atomicMin works)
+// (non-negative doubles order like their bit patterns, so atomicMin works).
+// Spill: as the fast kernel's table (MinHash64), a pose that fills the
+// shared table continues in the block's global table (values, then keys;
+// more slots than receptor atoms), whose keys are disjoint from the shared
+// table's; the block empties the global slots when it sums them.
 struct MinHash {
+    static constexpr unsigned long long NOMIN = 0x7fefffffffffffffull;
     int* keys; unsigned long long* vals; int cap;
-    __device__ void init(char* smem, int cap_) {
+    int* skeys; unsigned long long* svals; int scap;   // the block's global table, or null
+    int* spilled;
+    __device__ void init(char* smem, int cap_, unsigned char* spill, int spill_cap, int* spilled_) {
         cap = cap_; vals = (unsigned long long*)smem; keys = (int*)(vals + cap);
-        for (int s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = -1; vals[s] = 0x7fefffffffffffffull; }
+        for (int s = threadIdx.x; s < cap; s += blockDim.x) { keys[s] = -1; vals[s] = NOMIN; }
+        svals = spill ? reinterpret_cast<unsigned long long*>(spill) : nullptr;
+        skeys = spill ? reinterpret_cast<int*>(svals + spill_cap) : nullptr;
+        scap = spill_cap;
+        spilled = spilled_;
+        if (threadIdx.x == 0) *spilled = 0;
     }
-    __device__ bool insert(int k, double d2) {
-        unsigned h = ((unsigned)k * 2654435761u) & (unsigned)(cap - 1);
-        for (int probe = 0; probe < cap; ++probe) {
-            int prev = atomicCAS(keys + h, -1, k);
+    __device__ static bool put(int* kt, unsigned long long* vt, int n, int k, double d2) {
+        unsigned h = ((unsigned)k * 2654435761u) & (unsigned)(n - 1);
+        for (int probe = 0; probe < n; ++probe) {
+            int prev = atomicCAS(kt + h, -1, k);
             if (prev == -1 || prev == k) {
-                atomicMin(vals + h, (unsigned long long)__double_as_longlong(d2));
+                atomicMin(vt + h, (unsigned long long)__double_as_longlong(d2));
                 return true;
             }
-            h = (h + 1) & (unsigned)(cap - 1);
+            h = (h + 1) & (unsigned)(n - 1);
         }
         return false;
+    }
+    __device__ bool insert(int k, double d2) {
+        if (put(keys, vals, cap, k, d2)) return true;
+        if (!skeys) return false;
+        *spilled = 1;
+        return put(skeys, svals, scap, k, d2);
     }
     __device__ double value(int s) const { return __longlong_as_double((long long)vals[s]); }
 };
@@ -565,6 +583,8 @@ __global__ void __launch_bounds__(512) k_score_desolv(LaunchParams p) {
     __shared__ long long s_work;
     __shared__ double s_red[4][32];
     __shared__ long long s_fix[32];
+    __shared__ int s_spilled;
+    unsigned char* const spill = p.spill ? p.spill + (size_t)blockIdx.x * p.spill_cap * SPILL_SLOT_BYTES : nullptr;
     for (;;) {
         if (threadIdx.x == 0) s_work = (long long)atomicAdd(p.work_counter, 1ull);
         __syncthreads();
@@ -577,7 +597,7 @@ __global__ void __launch_bounds__(512) k_score_desolv(LaunchParams p) {
         const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
         if (p.pose_mask && !p.pose_mask[g]) continue;   // block-uniform: pose skipped
         MinHash hash;
-        hash.init(smem, c.hcap);
+        hash.init(smem, c.hcap, spill, p.spill_cap, &s_spilled);
         __syncthreads();
         const Rot rot = pose_matrix(p.poses + 7 * g);
         unsigned* ibits = iface_bits(p, c, g);
@@ -603,6 +623,17 @@ __global__ void __launch_bounds__(512) k_score_desolv(LaunchParams p) {
             double2 rs = c.rsolv64[k];
             fix += __double2ll_rn(solv_term(hash.value(s), rs.y) * rs.x * 1099511627776.0);
         }
+        if (s_spilled)   // block-uniform: read after the barrier above
+            for (int s = threadIdx.x; s < hash.scap; s += blockDim.x) {
+                // the atomics acted in L2: read around L1
+                const int k = __ldcg(hash.skeys + s);
+                if (k < 0) continue;
+                const double d2 = __longlong_as_double((long long)__ldcg(hash.svals + s));
+                __stcg(hash.skeys + s, -1);                 // empty again for the block's next pose
+                __stcg(hash.svals + s, MinHash::NOMIN);
+                double2 rs = c.rsolv64[k];
+                fix += __double2ll_rn(solv_term(d2, rs.y) * rs.x * 1099511627776.0);
+            }
         fix = warp_sum(fix);
         if ((threadIdx.x & 31) == 0) s_fix[threadIdx.x >> 5] = fix;
         double v[4] = {acc.elec, acc.vdw, solv_l, (double)acc.np};

@@ -77,37 +77,64 @@ struct WSlots {
 // bits are equal) and a slot costs 8 bytes of shared memory instead of 12.
 // Only pairs with d^2 <= SOLV2_D are inserted; the receptor term's
 // sqrt(d^2) then moves by < 1e-10 A.
+// Spill: a pose that touches more receptor atoms within 6.4 A than the
+// shared table holds (a ligand sunk into a large receptor) continues in the
+// block's own table in global memory, of more slots than the complex has
+// receptor atoms, so an insert there always finds its key or an empty slot.
+// A key enters the global table only after the shared table was found full
+// without it, and a full shared table stays full, so the two tables hold
+// disjoint keys and the receptor sum runs over both.  The block empties the
+// global slots it used when it sums them.
 struct MinHash64 {
     static constexpr unsigned long long EMPTY = ~0ull;
     static constexpr unsigned long long KEY_MASK = (1ull << 27) - 1;
     static constexpr double SCALE = (double)((1ull << 37) - 1) / SOLV2_D;
     unsigned long long* slot;
     int cap;
-    __device__ void init(char* smem, int cap_) {
+    unsigned long long* spill;   // the block's global table (all EMPTY between poses), or null
+    int spill_cap;
+    int* spilled;                // shared flag: the pose used the global table
+    __device__ void init(char* smem, int cap_, unsigned long long* spill_, int spill_cap_, int* spilled_) {
         cap = cap_;
         slot = reinterpret_cast<unsigned long long*>(smem);
+        spill = spill_;
+        spill_cap = spill_cap_;
+        spilled = spilled_;
         for (int s = threadIdx.x; s < cap; s += blockDim.x) slot[s] = EMPTY;
+        if (threadIdx.x == 0) *spilled = 0;
+    }
+    // linear probing over tab[0..n) (n a power of two); false when full.
+    // GLOBAL: the table is in global memory, where the atomics act in L2:
+    // plain reads there bypass L1 (__ldcg), which could hold a stale line
+    template <bool GLOBAL>
+    __device__ static bool put(unsigned long long* tab, int n, int k, unsigned long long w) {
+        unsigned h = ((unsigned)k * 2654435761u) & (unsigned)(n - 1);
+        for (int probe = 0; probe < n; ++probe) {
+            unsigned long long v = GLOBAL ? __ldcg(tab + h) : tab[h];
+            if (v == EMPTY) {
+                v = atomicCAS(tab + h, EMPTY, w);
+                if (v == EMPTY) return true;
+            }
+            if ((v & KEY_MASK) == (unsigned long long)k) {
+                atomicMin(tab + h, w);
+                return true;
+            }
+            h = (h + 1) & (unsigned)(n - 1);
+        }
+        return false;
     }
     // k < 2^26 (the receptor index limit); 0 <= d2 <= SOLV2_D
     __device__ bool insert(int k, double d2) {
         const unsigned long long w = (__double2ull_rn(d2 * SCALE) << 27) | (unsigned long long)k;
-        unsigned h = ((unsigned)k * 2654435761u) & (unsigned)(cap - 1);
-        for (int probe = 0; probe < cap; ++probe) {
-            unsigned long long v = slot[h];
-            if (v == EMPTY) {
-                v = atomicCAS(slot + h, EMPTY, w);
-                if (v == EMPTY) return true;
-            }
-            if ((v & KEY_MASK) == (unsigned long long)k) {
-                atomicMin(slot + h, w);
-                return true;
-            }
-            h = (h + 1) & (unsigned)(cap - 1);
-        }
-        return false;
+        if (put<false>(slot, cap, k, w)) return true;
+        if (!spill) return false;
+        *spilled = 1;
+        return put<true>(spill, spill_cap, k, w);
     }
-    __device__ int key(int s) const { return slot[s] == EMPTY ? -1 : (int)(slot[s] & KEY_MASK); }
-    __device__ double value(int s) const { return fmin((double)(slot[s] >> 27) / SCALE, SOLV2_D); }
+    __device__ static int key_of(unsigned long long v) { return v == EMPTY ? -1 : (int)(v & KEY_MASK); }
+    __device__ static double value_of(unsigned long long v) { return fmin((double)(v >> 27) / SCALE, SOLV2_D); }
+    __device__ int key(int s) const { return key_of(slot[s]); }
+    __device__ double value(int s) const { return value_of(slot[s]); }
 };
 
 // IFACE: start a unit of pose bits `bits` (lane 0; the caller syncs the
@@ -484,7 +511,11 @@ __global__ void __launch_bounds__(WD_THREADS, WD_BLOCKS) k_score_warp_desolv(Lau
     __shared__ long long s_work;
     __shared__ double s_red[4][32];
     __shared__ long long s_fix[32];
+    __shared__ int s_spilled;
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    unsigned long long* const spill =
+        p.spill ? reinterpret_cast<unsigned long long*>(p.spill + (size_t)blockIdx.x * p.spill_cap * SPILL_SLOT_BYTES)
+                : nullptr;
     for (;;) {
         if (threadIdx.x == 0) s_work = (long long)atomicAdd(p.work_counter, 1ull);
         __syncthreads();
@@ -497,7 +528,7 @@ __global__ void __launch_bounds__(WD_THREADS, WD_BLOCKS) k_score_warp_desolv(Lau
         const long long g = (long long)__ldg(p.item_pose0 + b) + pose;
         if (p.pose_mask && !p.pose_mask[g]) continue;   // block-uniform: pose skipped
         MinHash64 hash;
-        hash.init(reinterpret_cast<char*>(wd_smem_raw), c.hcap);
+        hash.init(reinterpret_cast<char*>(wd_smem_raw), c.hcap, spill, p.spill_cap, &s_spilled);
         unsigned char* base = wd_smem_raw + (size_t)c.hcap * sizeof(unsigned long long);
         WSlots<G>& W = reinterpret_cast<WSlots<G>*>(base)[wid];
         WDes<G>* D = reinterpret_cast<WDes<G>*>(base + (size_t)NW * sizeof(WSlots<G>)) + wid;
@@ -521,6 +552,15 @@ __global__ void __launch_bounds__(WD_THREADS, WD_BLOCKS) k_score_warp_desolv(Lau
             const double2 rs = c.rsolv64[k];
             fix += __double2ll_rn(solv_term(hash.value(s), rs.y) * rs.x * 1099511627776.0);
         }
+        if (s_spilled)   // block-uniform: read after the barrier above
+            for (int s = threadIdx.x; s < p.spill_cap; s += blockDim.x) {
+                const unsigned long long v = __ldcg(spill + s);
+                if (v == MinHash64::EMPTY) continue;
+                __stcg(spill + s, MinHash64::EMPTY);   // empty again for the block's next pose
+                const int k = MinHash64::key_of(v);
+                const double2 rs = c.rsolv64[k];
+                fix += __double2ll_rn(solv_term(MinHash64::value_of(v), rs.y) * rs.x * 1099511627776.0);
+            }
         fix = warp_sum(fix);
         if (lane == 0) s_fix[wid] = fix;
         double v[4] = {acc.elec, acc.vdw, acc.solv, (double)acc.np};

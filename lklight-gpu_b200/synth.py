@@ -22,6 +22,11 @@ value distributions of the five benchmark configurations:
 
 Random streams: the chain uses std::mt19937_64(seed) in C++; types, charges
 and sequences use numpy's PCG64(seed); poses use the reference's StdRng.
+
+``gen``: the generators of the chain and of StdRng.  None uses liblkg's
+(``lkg_synth_chain``, ``lkg_rng_*``); a caller that must not load the library
+passes an object with the same ``chain(n, seed, r0=...)`` and ``Rng(seed)``
+(the benchmark's CPU reference arm passes the oracle's).
 """
 import functools
 import json
@@ -60,7 +65,9 @@ for names, v in ((("C", "CD", "CT", "CY", "CZ"), 1.95),
         _RASP[n] = v
 
 
-def chain(n, seed, r0=30.0, bond=1.5, min_sep=3.0, patience=10000):
+def chain(n, seed, r0=30.0, bond=1.5, min_sep=3.0, patience=10000, gen=None):
+    if gen is not None:
+        return gen.chain(n, seed, r0=r0, bond=bond, min_sep=min_sep, patience=patience)
     out = np.zeros((n, 3))
     rf = C.c_double()
     _check(lib().lkg_synth_chain(seed, n, r0, bond, min_sep, patience, ptr(out), C.byref(rf)))
@@ -79,9 +86,9 @@ def _f32(a):
     return np.asarray(a, np.float32).astype(np.float64)
 
 
-def globule(n, seed, r0=30.0, net_charge=10.0, shift=True):
+def globule(n, seed, r0=30.0, net_charge=10.0, shift=True, gen=None):
     """Random-chain globule receptor with uniform DNA-table types."""
-    coords, radius = chain(n, seed, r0=r0)
+    coords, radius = chain(n, seed, r0=r0, gen=gen)
     rng = np.random.default_rng(seed)
     names = [tables()["types"][i][0] for i in rng.integers(0, len(tables()["types"]), n)]
     eps, rad, heavy = _params(names)
@@ -167,13 +174,13 @@ def fib_sphere(n, r):
     return out
 
 
-def setup_poses(rec_coords, n_swarms, n_glow, seed, swarm_radius=3.0):
+def setup_poses(rec_coords, n_swarms, n_glow, seed, swarm_radius=3.0, gen=None):
     """``LKlight setup`` initial positions: (n_swarms * n_glow) x 7 rows of
     (tx, ty, tz, qw, qx, qy, qz), 6-decimal text precision."""
     c = np.asarray(rec_coords, np.float64)
     avg_r = float(np.mean(np.sqrt((c * c).sum(axis=1))))
     centers = fib_sphere(max(n_swarms * 5, 2000), avg_r + swarm_radius)[:n_swarms]
-    rng = Rng(seed)
+    rng = (gen.Rng if gen is not None else Rng)(seed)
     rows = []
     two_pi = 2.0 * math.pi
     for cx, cy, cz in centers:
@@ -200,9 +207,9 @@ def to_kernel_poses(positions):
 # ---------------------------------------------------------------------------
 # benchmark configurations
 # ---------------------------------------------------------------------------
-def config0(n_rec=12625, n_bp=20, seed=42):
+def config0(n_rec=12625, n_bp=20, seed=42, gen=None):
     """Plain scorer, dna: 12,625-atom globule + 20 bp duplex; 1 x 200, seed 42."""
-    rec = globule(n_rec, seed)
+    rec = globule(n_rec, seed, gen=gen)
     lig = duplex(n_bp, seed)
     return dict(rec=rec, lig=lig, family="dna", swarms=1, glowworms=200, steps=100, seed=seed)
 
@@ -216,7 +223,7 @@ def config1(family, seed=7, base=None):
     return dict(rec=rec, lig=lig, family=family, swarms=6, glowworms=300, steps=100, seed=seed)
 
 
-def config2(n_complex=64, seed=11, swarms=20, glowworms=300):
+def config2(n_complex=64, seed=11, swarms=20, glowworms=300, gen=None):
     """64 complexes, receptors log-uniform 2k-40k atoms, ligands 300-5k atoms;
     first half dna, second half pydock."""
     rng = np.random.default_rng(seed)
@@ -225,7 +232,7 @@ def config2(n_complex=64, seed=11, swarms=20, glowworms=300):
         nr = int(round(math.exp(rng.uniform(math.log(2000), math.log(40000)))))
         nl = int(round(math.exp(rng.uniform(math.log(300), math.log(5000)))))
         n_bp = max(2, int(round(nl / 62.0)))
-        rec = globule(nr, seed * 1000 + k, r0=30.0 * (nr / 12625.0) ** (1.0 / 3.0))
+        rec = globule(nr, seed * 1000 + k, r0=30.0 * (nr / 12625.0) ** (1.0 / 3.0), gen=gen)
         lig = duplex(n_bp, seed * 1000 + k)
         out.append(dict(rec=rec, lig=lig, family="dna" if k < n_complex // 2 else "pydock",
                         swarms=swarms, glowworms=glowworms, steps=100, seed=seed))

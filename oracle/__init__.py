@@ -39,7 +39,8 @@ def lib():
             "orc_rng_u64": (U64, [P]),
             "orc_quat_random": (V, [P, P]), "orc_quat_slerp": (V, [P, P, D, P]),
             "orc_quat_normalize": (V, [P]),
-            "orc_field_new": (P, [P, P, I64, C.c_int]), "orc_field_info": (V, [P, P, P, P]),
+            "orc_field_new": (P, [P, P, I64, C.c_int]), "orc_field_new_scatter": (P, [P, P, I64, C.c_int]),
+            "orc_field_info": (V, [P, P, P, P]),
             "orc_field_phi32": (P, [P]), "orc_field_phi64": (P, [P]),
             "orc_field_sample": (D, [P, D, D, D]), "orc_field_free": (V, [P]),
             "orc_crec_build": (I64, [P, I64, P, P, P, P, P]),
@@ -53,6 +54,7 @@ def lib():
             "orc_gso_new": (P, [P, I64, P, U64, C.c_int, C.c_int]), "orc_gso_run": (V, [P, C.c_int]),
             "orc_gso_state": (V, [P, P, P, P, P, P, P, P]), "orc_gso_scored": (I64, [P]),
             "orc_gso_free": (V, [P]),
+            "orc_synth_chain": (C.c_int, [U64, I32, D, D, D, I32, P, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -92,6 +94,23 @@ class Rng:
             lib().orc_rng_free(self.h)
 
 
+def synth_chain(n, seed, r0=30.0, bond=1.5, min_sep=3.0, patience=10000):
+    """The benchmark's synthetic receptor chain (liblkg's generator, restated
+    here): n x 3 coordinates and the final confinement radius."""
+    out, rf = np.zeros((n, 3)), C.c_double()
+    if lib().orc_synth_chain(seed, n, r0, bond, min_sep, patience, _p(out), C.byref(rf)) != 0:
+        raise ValueError("random chain did not fit (%d atoms, r0 %.1f)" % (n, r0))
+    return out, rf.value
+
+
+class Generators:
+    """Input generators for the CPU reference arm: the synthetic chain and
+    StdRng from the oracle, so that its complexes and poses are made without
+    loading the product library (``synth`` functions take ``gen=``)."""
+    chain = staticmethod(synth_chain)
+    Rng = None   # set below
+
+
 def slerp(a, b, t):
     a, b, out = _f64(a), _f64(b), np.zeros(4)
     lib().orc_quat_slerp(_p(a), _p(b), t, _p(out))
@@ -99,14 +118,17 @@ def slerp(a, b, t):
 
 
 class Field:
-    """``ReceptorField`` (grid_dna.rs); fp64 keeps phi in double."""
+    """``ReceptorField`` (grid_dna.rs); fp64 keeps phi in double.  scatter:
+    build by the plain single-threaded per-atom scatter instead of the
+    parallel brick order (the same bits; a check of the brick order)."""
 
-    def __init__(self, coords, charges, fp64=False, _handle=None, _owner=None):
+    def __init__(self, coords, charges, fp64=False, _handle=None, _owner=None, scatter=False):
         if _handle is not None:
             self.h, self._owner = _handle, _owner
         else:
             c, q = _f64(coords), _f64(charges)
-            self.h, self._owner = lib().orc_field_new(_p(c), _p(q), len(q), int(fp64)), None
+            new = lib().orc_field_new_scatter if scatter else lib().orc_field_new
+            self.h, self._owner = new(_p(c), _p(q), len(q), int(fp64)), None
         o, d, s = np.zeros(3), np.zeros(3, np.int64), C.c_double()
         lib().orc_field_info(self.h, _p(o), _p(d), C.byref(s))
         self.origin, self.dims, self.spacing, self.fp64 = o, d, s.value, fp64
@@ -126,6 +148,9 @@ class Field:
     def __del__(self):
         if getattr(self, "h", None) and self._owner is None:
             lib().orc_field_free(self.h)
+
+
+Generators.Rng = Rng
 
 
 def crec_build(coords):

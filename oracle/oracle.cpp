@@ -17,7 +17,10 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <random>
+#include <unordered_map>
 #include <vector>
+#include <immintrin.h>
 #ifdef _OPENMP
 #include <omp.h>
 #endif
@@ -161,10 +164,11 @@ struct Field {
     std::vector<double> phi64;
 };
 
-Field* field_build(const double* coords, const double* q, int64_t na, int fp64) {
-    Field* f = new Field();
-    f->fp64 = fp64;
-    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+// Grid extent of ReceptorField::new (grid_dna.rs:44-70): 30 A + 2 spacings
+// beyond the atoms, floored / ceiled to whole Angstroms.
+void field_extent(const double* coords, int64_t na, double lo[3], int64_t n[3]) {
+    double hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int a = 0; a < 3; ++a) lo[a] = INFINITY;
     for (int64_t i = 0; i < na; ++i)
         for (int a = 0; a < 3; ++a) {
             lo[a] = std::fmin(lo[a], coords[3 * i + a]);
@@ -174,65 +178,178 @@ Field* field_build(const double* coords, const double* q, int64_t na, int fp64) 
         lo[a] = std::floor(lo[a] - FIELD_RMAX - 2.0 * SPACING);
         hi[a] = std::ceil(hi[a] + FIELD_RMAX + 2.0 * SPACING);
     }
-    int64_t n[3];
     for (int a = 0; a < 3; ++a) n[a] = (int64_t)((hi[a] - lo[a]) / SPACING) + 1;
+}
+
+// One grid row of one atom: points xl..xh, 10 < d <= 30, += (T)(q / d^2),
+// with the reference's expressions: dx = lo + (double)ix * s - c,
+// d2 = dx * dx + dyz^2.  On hosts with AVX2 four points go at a time: the
+// same IEEE operations lane by lane ((double)ix as an exact f64 counter),
+// and a point outside the shell adds +0, which leaves its value's bits
+// unchanged (a grid value is never -0: it starts at +0 and every term is
+// nonzero), so both versions give the same bits.
+template <typename T>
+inline void field_row_scalar(T* row, int64_t xl, int64_t xh, double lo0, double s, double c0, double dyz2,
+                             double qk) {
+    const double r2min = CLOSE_DIST * CLOSE_DIST, r2max = FIELD_RMAX * FIELD_RMAX;
+    for (int64_t ix = xl; ix <= xh; ++ix) {
+        double dx = lo0 + (double)ix * s - c0;
+        double d2 = dx * dx + dyz2;
+        if (d2 > r2min && d2 <= r2max) row[ix] += (T)(qk / d2);
+    }
+}
+
+template <typename T>
+__attribute__((target("avx2"))) void field_row_avx2(T* row, int64_t xl, int64_t xh, double lo0, double s,
+                                                     double c0, double dyz2, double qk) {
+    const __m256d vlo = _mm256_set1_pd(lo0), vs = _mm256_set1_pd(s), vc = _mm256_set1_pd(c0);
+    const __m256d vyz = _mm256_set1_pd(dyz2), vq = _mm256_set1_pd(qk), four = _mm256_set1_pd(4.0);
+    const __m256d vmin = _mm256_set1_pd(CLOSE_DIST * CLOSE_DIST), vmax = _mm256_set1_pd(FIELD_RMAX * FIELD_RMAX);
+    __m256d fx = _mm256_setr_pd((double)xl, (double)(xl + 1), (double)(xl + 2), (double)(xl + 3));
+    int64_t ix = xl;
+    for (; ix + 3 <= xh; ix += 4) {
+        const __m256d dx = _mm256_sub_pd(_mm256_add_pd(vlo, _mm256_mul_pd(fx, vs)), vc);
+        const __m256d d2 = _mm256_add_pd(_mm256_mul_pd(dx, dx), vyz);
+        const __m256d in = _mm256_and_pd(_mm256_cmp_pd(d2, vmin, _CMP_GT_OQ), _mm256_cmp_pd(d2, vmax, _CMP_LE_OQ));
+        const __m256d t = _mm256_and_pd(_mm256_div_pd(vq, d2), in);
+        if constexpr (sizeof(T) == 4) {
+            float* p = reinterpret_cast<float*>(row) + ix;
+            _mm_storeu_ps(p, _mm_add_ps(_mm_loadu_ps(p), _mm256_cvtpd_ps(t)));
+        } else {
+            double* p = reinterpret_cast<double*>(row) + ix;
+            _mm256_storeu_pd(p, _mm256_add_pd(_mm256_loadu_pd(p), t));
+        }
+        fx = _mm256_add_pd(fx, four);
+    }
+    field_row_scalar(row, ix, xh, lo0, s, c0, dyz2, qk);
+}
+
+const bool HAVE_AVX2 = __builtin_cpu_supports("avx2");
+
+template <typename T>
+inline void field_row(T* row, int64_t xl, int64_t xh, double lo0, double s, double c0, double dyz2, double qk) {
+    if (HAVE_AVX2) field_row_avx2(row, xl, xh, lo0, s, c0, dyz2, qk);
+    else field_row_scalar(row, xl, xh, lo0, s, c0, dyz2, qk);
+}
+
+// One atom's contribution to the grid points of the box [b0, b1] (inclusive
+// per axis), exactly as the per-atom scatter of grid_dna.rs:71-149 visits
+// them: the atom's +-spread box, the row test dyz^2 < 30^2, the row's x
+// range from sqrt(30^2 - dyz^2), then 10 < d <= 30 per point, adding
+// (qk / d^2) as f32 (or f64).  Restricting the scatter to a box changes
+// neither the set of points an atom reaches nor the value added there.
+template <typename T, bool SCALAR = false>
+inline void field_atom_into(T* phi, const double lo[3], const int64_t n[3], const double* c, double qk,
+                            const int64_t b0[3], const int64_t b1[3]) {
+    const double s = SPACING;
+    const int64_t spread = (int64_t)std::ceil(FIELD_RMAX / s) + 2;
+    const double r2max = FIELD_RMAX * FIELD_RMAX;
+    int64_t gi[3], gh[3];
+    for (int a = 0; a < 3; ++a) {
+        int64_t fl = (int64_t)std::floor((c[a] - lo[a]) / s);
+        gi[a] = std::max<int64_t>(fl - spread, 0);
+        gh[a] = std::min<int64_t>(fl + spread, n[a] - 1);
+    }
+    const int64_t zlo = std::max(gi[2], b0[2]), zhi = std::min(gh[2], b1[2]);
+    const int64_t ylo = std::max(gi[1], b0[1]), yhi = std::min(gh[1], b1[1]);
+    if (zlo > zhi || ylo > yhi || gi[0] > b1[0] || gh[0] < b0[0]) return;
+    const double cxi_f = (c[0] - lo[0]) / s;
+    const int64_t nx = n[0], ny = n[1];
+    for (int64_t iz = zlo; iz <= zhi; ++iz) {
+        double zz = lo[2] + (double)iz * s;
+        double dz = zz - c[2];
+        for (int64_t iy = ylo; iy <= yhi; ++iy) {
+            double yy = lo[1] + (double)iy * s;
+            double dy = yy - c[1];
+            double dyz2 = dy * dy + dz * dz;
+            if (dyz2 >= r2max) continue;
+            double b = std::sqrt(r2max - dyz2);
+            int64_t xl = std::max<int64_t>((int64_t)std::floor(cxi_f - b / s) - 1, gi[0]);
+            int64_t xh = std::min<int64_t>((int64_t)std::ceil(cxi_f + b / s) + 1, gh[0]);
+            if (xl > gh[0] || xh < gi[0]) continue;
+            xl = std::max(std::max(xl, gi[0]), b0[0]);
+            xh = std::min(std::min(xh, gh[0]), b1[0]);
+            T* row = phi + (iz * ny + iy) * nx;
+            if (SCALAR) field_row_scalar(row, xl, xh, lo[0], s, c[0], dyz2, qk);
+            else field_row(row, xl, xh, lo[0], s, c[0], dyz2, qk);
+        }
+    }
+}
+
+// ReceptorField::build (grid_dna.rs:44-149).  The reference scatters atom by
+// atom; every grid point therefore receives its q/d^2 terms in atom order,
+// and that order fixes the f32 bits.  Here the grid is cut into bricks of
+// 32^3 points (128 KB of f32, cache resident) built in parallel; each brick
+// walks the atoms in index order and applies the scatter restricted to
+// itself, so every point still adds its terms in atom order: the result is
+// bitwise the reference's (checked against the plain scatter,
+// field_build_scatter, in tests/test_oracle.py).
+#ifndef BX
+#define BX 128
+#define BY 16
+#define BZ 16
+#endif
+Field* field_build(const double* coords, const double* q, int64_t na, int fp64) {
+    Field* f = new Field();
+    f->fp64 = fp64;
+    double lo[3];
+    int64_t n[3];
+    field_extent(coords, na, lo, n);
     size_t total = (size_t)n[0] * n[1] * n[2];
     if (fp64) f->phi64.assign(total, 0.0); else f->phi.assign(total, 0.0f);
     const double s = SPACING;
     const int64_t spread = (int64_t)std::ceil(FIELD_RMAX / s) + 2;
-    const double r2min = CLOSE_DIST * CLOSE_DIST, r2max = FIELD_RMAX * FIELD_RMAX;
-    const int64_t nx = n[0], ny = n[1];
-    // Parallel over z-slabs of the grid: each thread owns whole grid planes
-    // and walks the atoms in index order, so every grid point still receives
-    // its q/d^2 terms in atom order (the f32 accumulation order is unchanged).
-#pragma omp parallel
-    {
-        int nt = 1, tid = 0;
-#ifdef _OPENMP
-        nt = omp_get_num_threads(); tid = omp_get_thread_num();
-#endif
-        int64_t z0 = n[2] * tid / nt, z1 = n[2] * (tid + 1) / nt;
-        for (int64_t k = 0; k < na; ++k) {
-            double qk = q[k];
-            if (qk == 0.0) continue;
-            const double* c = coords + 3 * k;
-            int64_t gi[3], gh[3];
-            for (int a = 0; a < 3; ++a) {
-                int64_t fl = (int64_t)std::floor((c[a] - lo[a]) / s);
-                gi[a] = std::max<int64_t>(fl - spread, 0);
-                gh[a] = std::min<int64_t>(fl + spread, n[a] - 1);
-            }
-            double cxi_f = (c[0] - lo[0]) / s;
-            int64_t zlo = std::max(gi[2], z0), zhi = std::min(gh[2], z1 - 1);
-            for (int64_t iz = zlo; iz <= zhi; ++iz) {
-                double zz = lo[2] + (double)iz * s;
-                double dz = zz - c[2];
-                for (int64_t iy = gi[1]; iy <= gh[1]; ++iy) {
-                    double yy = lo[1] + (double)iy * s;
-                    double dy = yy - c[1];
-                    double dyz2 = dy * dy + dz * dz;
-                    if (dyz2 >= r2max) continue;
-                    double b = std::sqrt(r2max - dyz2);
-                    int64_t xl = std::max<int64_t>((int64_t)std::floor(cxi_f - b / s) - 1, gi[0]);
-                    int64_t xh = std::min<int64_t>((int64_t)std::ceil(cxi_f + b / s) + 1, gh[0]);
-                    if (xl > gh[0] || xh < gi[0]) continue;
-                    xl = std::max(xl, gi[0]);
-                    xh = std::min(xh, gh[0]);
-                    int64_t base = (iz * ny + iy) * nx;
-                    for (int64_t ix = xl; ix <= xh; ++ix) {
-                        double dx = lo[0] + (double)ix * s - c[0];
-                        double d2 = dx * dx + dyz2;
-                        if (d2 > r2min && d2 <= r2max) {
-                            if (fp64) f->phi64[base + ix] += qk / d2;
-                            else f->phi[base + ix] += (float)(qk / d2);
-                        }
-                    }
-                }
-            }
+    // charged atoms with their grid cell, for the per-brick atom test
+    std::vector<int64_t> idx;
+    std::vector<int64_t> cell;
+    for (int64_t k = 0; k < na; ++k) {
+        if (q[k] == 0.0) continue;
+        idx.push_back(k);
+        for (int a = 0; a < 3; ++a) cell.push_back((int64_t)std::floor((coords[3 * k + a] - lo[a]) / s));
+    }
+    const int64_t B[3] = {BX, BY, BZ};
+    const int64_t nb[3] = {(n[0] + B[0] - 1) / B[0], (n[1] + B[1] - 1) / B[1], (n[2] + B[2] - 1) / B[2]};
+    const int64_t nbricks = nb[0] * nb[1] * nb[2];
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int64_t br = 0; br < nbricks; ++br) {
+        const int64_t bx = br % nb[0], by = (br / nb[0]) % nb[1], bz = br / (nb[0] * nb[1]);
+        const int64_t b0[3] = {bx * B[0], by * B[1], bz * B[2]};
+        const int64_t b1[3] = {std::min(b0[0] + B[0], n[0]) - 1, std::min(b0[1] + B[1], n[1]) - 1,
+                               std::min(b0[2] + B[2], n[2]) - 1};
+        for (size_t m = 0; m < idx.size(); ++m) {
+            const int64_t* cl = &cell[3 * m];
+            // the atom's +-spread box misses the brick: no point of it is reached
+            if (cl[0] + spread < b0[0] || cl[0] - spread > b1[0] || cl[1] + spread < b0[1] ||
+                cl[1] - spread > b1[1] || cl[2] + spread < b0[2] || cl[2] - spread > b1[2])
+                continue;
+            const int64_t k = idx[m];
+            if (fp64) field_atom_into(f->phi64.data(), lo, n, coords + 3 * k, q[k], b0, b1);
+            else field_atom_into(f->phi.data(), lo, n, coords + 3 * k, q[k], b0, b1);
         }
     }
     for (int a = 0; a < 3; ++a) { f->origin[a] = lo[a]; f->n[a] = n[a]; }
     f->spacing = s;
+    return f;
+}
+
+// The plain per-atom scatter of grid_dna.rs:71-149 (single thread, scalar
+// rows), kept as the check of field_build's brick order and AVX2 rows.
+Field* field_build_scatter(const double* coords, const double* q, int64_t na, int fp64) {
+    Field* f = new Field();
+    f->fp64 = fp64;
+    double lo[3];
+    int64_t n[3];
+    field_extent(coords, na, lo, n);
+    size_t total = (size_t)n[0] * n[1] * n[2];
+    if (fp64) f->phi64.assign(total, 0.0); else f->phi.assign(total, 0.0f);
+    const int64_t b0[3] = {0, 0, 0}, b1[3] = {n[0] - 1, n[1] - 1, n[2] - 1};
+    for (int64_t k = 0; k < na; ++k) {
+        if (q[k] == 0.0) continue;
+        if (fp64) field_atom_into<double, true>(f->phi64.data(), lo, n, coords + 3 * k, q[k], b0, b1);
+        else field_atom_into<float, true>(f->phi.data(), lo, n, coords + 3 * k, q[k], b0, b1);
+    }
+    for (int a = 0; a < 3; ++a) { f->origin[a] = lo[a]; f->n[a] = n[a]; }
+    f->spacing = SPACING;
     return f;
 }
 
@@ -848,12 +965,111 @@ void gso_movement(Gso& S) {  // swarm.rs:105-174
     }
 }
 
+// ---------------------------------------------------------------------------
+// Synthetic receptor chain for the CPU reference arm of the benchmark, so
+// that its inputs are made without the product library.  Same algorithm and
+// std::mt19937_64 stream as liblkg's lkg_synth_chain (a seeded
+// self-avoiding walk, not reference code): bond vectors uniform on the
+// sphere, rejected outside radius R or within min_sep of an atom more than
+// two bonds back; every 200 consecutive rejections the end is either given
+// 0.5 A more radius (stuck at the boundary with no new length for
+// `patience` attempts) or backed off by 1, 2, 4, ... atoms.  Checked bit
+// for bit against the library's generator in tests/test_host.py.
+// ---------------------------------------------------------------------------
+struct ChainGrid {
+    double cs;
+    std::unordered_map<int64_t, std::vector<int>> cells;
+    static int64_t pack(int64_t ix, int64_t iy, int64_t iz) {
+        return ((ix + (1 << 20)) << 42) | ((iy + (1 << 20)) << 21) | (iz + (1 << 20));
+    }
+    int64_t cell_of(double x, double y, double z) const {
+        return pack((int64_t)std::floor(x / cs), (int64_t)std::floor(y / cs), (int64_t)std::floor(z / cs));
+    }
+};
+
+int synth_chain(uint64_t seed, int32_t n, double r0, double bond, double min_sep, int32_t patience,
+                double* coords, double* r_final) {
+    if (n <= 0 || !coords || r0 <= 0 || bond <= 0 || min_sep < 0 || patience <= 0) return -1;
+    std::mt19937_64 gen(seed);
+    auto unit = [&]() { return (double)(gen() >> 11) * (1.0 / 9007199254740992.0); };
+    const double two_pi = 2.0 * M_PI;
+    double R = r0;
+    ChainGrid G{std::max(min_sep, 1.0), {}};
+    std::vector<double> c{0.0, 0.0, 0.0};
+    c.reserve(3 * (size_t)n);
+    G.cells[G.cell_of(0, 0, 0)].push_back(0);
+    int fails = 0, longest = 1, back = 1;
+    long long tries = 0, since_longest = 0;
+    const long long max_tries = 4000LL * n + 100000000LL;
+    const double sep2 = min_sep * min_sep;
+    while ((int)(c.size() / 3) < n) {
+        const int k = (int)(c.size() / 3);
+        const double u = 2.0 * unit() - 1.0;
+        const double phi = two_pi * unit();
+        const double sn = std::sqrt(std::max(0.0, 1.0 - u * u));
+        const double* e = &c[3 * (k - 1)];
+        const double x = e[0] + bond * sn * std::cos(phi), y = e[1] + bond * sn * std::sin(phi), z = e[2] + bond * u;
+        bool ok = x * x + y * y + z * z <= R * R;
+        if (ok) {
+            const int64_t bx = (int64_t)std::floor(x / G.cs), by = (int64_t)std::floor(y / G.cs),
+                          bz = (int64_t)std::floor(z / G.cs);
+            for (int64_t dz = -1; dz <= 1 && ok; ++dz)
+                for (int64_t dy = -1; dy <= 1 && ok; ++dy)
+                    for (int64_t dx = -1; dx <= 1 && ok; ++dx) {
+                        auto it = G.cells.find(ChainGrid::pack(bx + dx, by + dy, bz + dz));
+                        if (it == G.cells.end()) continue;
+                        for (int a : it->second) {
+                            if (a >= k - 2) continue;
+                            const double ex = x - c[3 * a], ey = y - c[3 * a + 1], ez = z - c[3 * a + 2];
+                            if (ex * ex + ey * ey + ez * ez < sep2) { ok = false; break; }
+                        }
+                    }
+        }
+        if (ok) {
+            c.insert(c.end(), {x, y, z});
+            G.cells[G.cell_of(x, y, z)].push_back(k);
+            fails = 0;
+            if (k + 1 > longest) { longest = k + 1; since_longest = 0; back = 1; }
+            continue;
+        }
+        if (++tries > max_tries) return -1;
+        if (++fails % 200 == 0 && k > 1) {
+            const double* t = &c[3 * (k - 1)];
+            const double rt = std::sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+            if (rt > R - 2.0 * min_sep && since_longest >= patience) {
+                R += 0.5;
+                since_longest = 0;
+            } else {
+                const int m = std::min(back, k - 1);
+                for (int i = 0; i < m; ++i) {
+                    const int last = (int)(c.size() / 3) - 1;
+                    auto& v = G.cells[G.cell_of(c[3 * last], c[3 * last + 1], c[3 * last + 2])];
+                    v.erase(std::remove(v.begin(), v.end(), last), v.end());
+                    c.resize(c.size() - 3);
+                }
+                back = std::min(back * 2, 256);
+            }
+            fails = 0;
+        }
+        ++since_longest;
+    }
+    std::copy(c.begin(), c.end(), coords);
+    if (r_final) *r_final = R;
+    return 0;
+}
+
 }  // namespace
+
 
 // ---------------------------------------------------------------------------
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
+
+int orc_synth_chain(uint64_t seed, int32_t n, double r0, double bond, double min_sep, int32_t patience,
+                    double* coords, double* r_final) {
+    return synth_chain(seed, n, r0, bond, min_sep, patience, coords, r_final);
+}
 
 void* orc_rng_new(uint64_t seed) { Rng* r = new Rng(); rng_seed(*r, seed); return r; }
 void orc_rng_free(void* r) { delete (Rng*)r; }
@@ -883,6 +1099,9 @@ void orc_quat_normalize(double q[4]) {
 
 void* orc_field_new(const double* coords, const double* q, int64_t n, int fp64) {
     return field_build(coords, q, n, fp64);
+}
+void* orc_field_new_scatter(const double* coords, const double* q, int64_t n, int fp64) {
+    return field_build_scatter(coords, q, n, fp64);
 }
 void orc_field_info(const void* fv, double origin[3], int64_t dims[3], double* spacing) {
     const Field* f = (const Field*)fv;

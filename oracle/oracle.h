@@ -28,6 +28,12 @@ void   orc_rng_free(void* rng);
 double orc_rng_f64(void* rng);          /* Rng::gen::<f64>() */
 uint64_t orc_rng_u64(void* rng);
 
+/* synthetic receptor chain of the benchmark inputs (the generator liblkg's
+ * lkg_synth_chain runs, restated so that the CPU reference arm makes its
+ * inputs without the product library); 0 = ok, -1 = bad arguments or no fit */
+int orc_synth_chain(uint64_t seed, int32_t n, double r0, double bond, double min_sep, int32_t patience,
+                    double* coords, double* r_final);
+
 /* quaternions (src/qt.rs) */
 void orc_quat_random(void* rng, double out[4]);                       /* qt.rs:106-117 */
 void orc_quat_slerp(const double a[4], const double b[4], double t, double out[4]); /* qt.rs:80-104 */
@@ -36,6 +42,9 @@ void orc_quat_normalize(double q[4]);                                 /* qt.rs:4
 /* receptor far field (src/grid_dna.rs).  fp64 != 0 accumulates and stores
  * phi in double (the "FP64 evaluation of the same function"). */
 void*  orc_field_new(const double* coords, const double* q, int64_t n, int fp64);
+/* the same field by the plain single-threaded per-atom scatter (the check
+ * of orc_field_new's parallel brick order) */
+void*  orc_field_new_scatter(const double* coords, const double* q, int64_t n, int fp64);
 void   orc_field_info(const void* f, double origin[3], int64_t dims[3], double* spacing);
 const float*  orc_field_phi32(const void* f);
 const double* orc_field_phi64(const void* f);

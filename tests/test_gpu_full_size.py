@@ -1,20 +1,25 @@
-"""Parity at the benchmark's full sizes, through properties that do not need
-the oracle to score everything:
+"""Parity at the benchmark's full sizes:
 * the batched workload (64 complexes, 384,000 poses in one launch group):
   bitwise reproducible, equal to one launch per complex, a sample of poses
-  from every complex against the exact path, and samples of the four
-  smallest complexes against the oracle (1e-5 relative; the oracle's CPU
-  far-field builds for all 64 receptors would take about ten minutes);
+  from every complex against the exact path, samples of the four smallest
+  complexes against the oracle, and of the four LARGEST (34k-40k-atom
+  receptors: the long rows and crowded interfaces) against the oracle and
+  its FP64 evaluation;
 * the config-4 cpydock complex (101k-atom receptor, 12k-atom ligand,
-  25,000 poses): bitwise reproducible, and a sample against the exact path
-  (the oracle's CPU far-field build for this receptor alone takes minutes;
-  the exact path is pinned to the oracle on the smaller complexes).
+  25,000 poses): bitwise reproducible, a sample against the exact path, and
+  random plus the most crowded poses against the oracle and its FP64
+  evaluation;
+* the config-1 vdw and pydock runs on the config-0 complex (6 x 300 poses)
+  against the oracle, every pose.
+The FP64 evaluation accumulates and stores the far field in f64 (the
+reference's grid path stores it in f32); on these complexes the two differ
+by < 4e-8 relative, so both comparisons hold the same 1e-5 budget.
 """
 import numpy as np
 import pytest
 
 import oracle
-from tests.lkg_helpers import config2_items, lkg, rel_err, synth
+from tests.lkg_helpers import config0, config2_items, lkg, pose_matrix, random_poses, rel_err, synth
 
 pytestmark = pytest.mark.gpu
 
@@ -80,3 +85,112 @@ def test_cpydock_large_complex_full_size():
     finally:
         ctx.close()
         ctx_x.close()
+
+
+def _crowded_and_random(parts, n_top, n_rand, seed):
+    """The n_top poses with the most near pairs (the most crowded
+    interfaces) and n_rand seeded random ones."""
+    top = np.argsort(-parts[:, 3], kind="stable")[:n_top]
+    rnd = np.random.default_rng(seed).choice(len(parts), n_rand, replace=False)
+    return np.unique(np.concatenate([top, rnd]))
+
+
+def test_batched_workload_largest_complexes_against_oracle_and_fp64():
+    items = config2_items()
+    largest = np.argsort([len(it["rec"]["coords"]) for it in items])[::-1][:4]
+    ctx = lkg.Context()
+    ctx_x = lkg.Context(precision="exact")
+    try:
+        for k in largest:
+            it = items[k]
+            cid = ctx.add_complex(it["family"], it["rec"], it["lig"])
+            got_all, parts = ctx.score(cid, it["poses"], parts=True)
+            sel = _crowded_and_random(parts, 8, 8, int(k))
+            m = oracle.Model(it["family"], it["rec"], it["lig"])
+            ref, rparts = m.batch_energy_grid(it["poses"][sel], parts=True)
+            r64 = m.batch_energy_grid(it["poses"][sel], fp64=True)
+            ex, xparts = ctx_x.score(ctx_x.add_complex(it["family"], it["rec"], it["lig"]), it["poses"][sel],
+                                     parts=True)
+            e_fast, e_fast64 = rel_err(got_all[sel], ref).max(), rel_err(got_all[sel], r64).max()
+            e_ex, e_ex64 = rel_err(ex, ref).max(), rel_err(ex, r64).max()
+            print("complex %d (%s, %d receptor atoms, up to %d near pairs a pose): fast vs oracle %.2e, vs FP64 "
+                  "%.2e; exact vs oracle %.2e, vs FP64 %.2e" % (k, it["family"], len(it["rec"]["coords"]),
+                                                                 int(rparts[:, 4].max()), e_fast, e_fast64, e_ex,
+                                                                 e_ex64))
+            assert rparts[:, 4].max() > 10000                  # the crowded poses are in the sample
+            assert np.array_equal(xparts[:, 3], rparts[:, 4])  # near pairs exactly
+            assert e_fast < FAST_TOL and e_fast64 < FAST_TOL
+            assert e_ex < 1e-11 and e_ex64 < 1e-7
+    finally:
+        ctx.close()
+        ctx_x.close()
+
+
+def test_cpydock_large_complex_against_oracle_and_fp64():
+    # cpydock totals can cancel (E*332/4 + 0.1 V - S): the fast path's bound
+    # is 1e-5 of max(|E|, 10), as on the config-1 complex; the exact path
+    # holds 1e-11 of max(|E|, 1).  Besides setup poses the sample has four
+    # poses that sink the 12k-atom ligand into the 101k-atom receptor: they
+    # touch more receptor atoms within 6.4 A than the kernels' shared-memory
+    # tables hold (8,192), so their desolvation runs through the spill
+    # tables in global memory; they must score, and match the oracle.
+    c4 = synth.config4()
+    poses = synth.to_kernel_poses(synth.setup_poses(c4["rec"]["coords"], 50, 500, 19))
+    rc, lc = c4["rec"]["coords"], c4["lig"]["coords"]
+    n8 = len(rc) // 8   # the receptor's eight globules, in order: sink the ligand into four of them
+    sunk = np.vstack([random_poses(1, rc[i * n8:(i + 1) * n8].mean(axis=0), 3.0, 8 + i) for i in range(4)])
+    ctx = lkg.Context()
+    ctx_x = lkg.Context(precision="exact")
+    try:
+        cid = ctx.add_complex("cpydock", c4["rec"], c4["lig"])
+        got_all, parts = ctx.score(cid, np.vstack([poses, sunk]), parts=True)
+        # receptor atoms within 6.4 A of each sunk pose's ligand: more than
+        # the shared table's 8,192 slots
+        from scipy.spatial import cKDTree
+        tree = cKDTree(rc)
+        touched = []
+        for p in sunk:
+            near = tree.query_ball_point(lc @ pose_matrix(p).T + p[4:7], 6.4)
+            touched.append(len(set(i for lst in near for i in lst)))
+        assert min(touched) > 8192
+        poses = np.vstack([poses, sunk])
+        sel = np.concatenate([_crowded_and_random(parts[:-4], 16, 16, 4), len(poses) - 4 + np.arange(4)])
+        m = oracle.Model("cpydock", c4["rec"], c4["lig"])
+        ref, rparts = m.batch_energy_grid(poses[sel], parts=True)
+        r64 = m.batch_energy_grid(poses[sel], fp64=True)
+        ex, xparts = ctx_x.score(ctx_x.add_complex("cpydock", c4["rec"], c4["lig"]), poses[sel], parts=True)
+
+        def err(a, b):
+            return (np.abs(a - b) / np.maximum(np.abs(b), 10.0)).max()
+        e_fast, e_fast64 = err(got_all[sel], ref), err(got_all[sel], r64)
+        e_ex, e_ex64 = rel_err(ex, ref).max(), rel_err(ex, r64).max()
+        print("config 4 (%d poses, up to %d near pairs a pose; sunk poses touch %d receptor atoms within 6.4 A): "
+              "fast vs oracle %.2e, vs FP64 %.2e; exact vs oracle %.2e, vs FP64 %.2e; desolvation fast vs oracle "
+              "%.2e" % (len(sel), int(rparts[:, 4].max()), min(touched), e_fast, e_fast64, e_ex, e_ex64,
+                        np.abs(parts[sel, 2] - rparts[:, 3]).max()))
+        assert np.array_equal(xparts[:, 3], rparts[:, 4])
+        assert np.all(np.abs(parts[sel, 3] - rparts[:, 4]) <= 2)   # f32 boundary cases only
+        assert np.abs(parts[sel, 2] - rparts[:, 3]).max() < 1e-9 * max(1.0, np.abs(rparts[:, 3]).max())
+        assert e_fast < FAST_TOL and e_fast64 < FAST_TOL
+        assert e_ex < 1e-11 and e_ex64 < 1e-7
+    finally:
+        ctx.close()
+        ctx_x.close()
+
+
+@pytest.mark.parametrize("family", ["vdw", "pydock"])
+def test_config1_every_pose_against_oracle(family):
+    c1 = synth.config1(family, base=config0())
+    poses = synth.to_kernel_poses(synth.setup_poses(c1["rec"]["coords"], 6, 300, 7))
+    m = oracle.Model(family, c1["rec"], c1["lig"])
+    ref, rparts = m.batch_energy_grid(poses, parts=True)
+    ctx = lkg.Context()
+    try:
+        got, parts = ctx.score(ctx.add_complex(family, c1["rec"], c1["lig"]), poses, parts=True)
+    finally:
+        ctx.close()
+    e = rel_err(got, ref)
+    print("config 1 %s, %d poses: max %.2e, median %.2e" % (family, len(poses), e.max(), np.median(e)))
+    assert len(poses) == 1800 and rparts[:, 4].sum() > 0
+    assert e.max() < FAST_TOL
+    assert np.all(np.abs(parts[:, 3] - rparts[:, 4]) <= 2)

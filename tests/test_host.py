@@ -106,6 +106,18 @@ def test_synthetic_config0_shape_and_charges():
     assert np.array_equal(c0b["rec"]["coords"], rec["coords"])
 
 
+def test_reference_arm_generators_equal_the_library_ones():
+    # the benchmark's CPU reference arm makes its inputs with the oracle's
+    # chain and StdRng instead of liblkg's: the same bits, including a chain
+    # long enough to grow its confining radius (config 0: 30 -> 58 A)
+    for n, seed, r0 in ((2000, 5, 30.0), (12625, 42, 30.0), (800, 11003, 12.0)):
+        a, ra = synth.chain(n, seed, r0=r0)
+        b, rb = synth.chain(n, seed, r0=r0, gen=oracle.Generators)
+        assert ra == rb and np.array_equal(a.view(np.uint64), b.view(np.uint64))
+    c = np.random.default_rng(0).normal(size=(100, 3)) * 20
+    assert np.array_equal(synth.setup_poses(c, 3, 10, 7), synth.setup_poses(c, 3, 10, 7, gen=oracle.Generators))
+
+
 def test_cpy_flag_matches_reference_view():
     hyd = np.array([1, 0, 1, 1, 0, 0, 1])
     f = compat.cpy_flag(hyd)

@@ -55,6 +55,23 @@ def test_field_unit_charge():
     assert abs(f.sample(35, 0, 0)) < 1e-9
 
 
+@pytest.mark.parametrize("fp64", [False, True])
+def test_field_brick_order_equals_atom_scatter(fp64):
+    # grid_dna.rs:71-149 scatters atom by atom; the oracle builds the grid in
+    # parallel bricks (and AVX2 rows where the host has them) that keep each
+    # point's atom order: the bits must equal the plain scalar scatter
+    import importlib
+    synth = importlib.import_module("lklight-gpu_b200.synth")
+    rec, _ = azp("dna")
+    glob = synth.globule(1200, 31)
+    for c, q in ((rec["coords"], rec["ele"]), (glob["coords"], glob["ele"])):
+        a = oracle.Field(c, q, fp64=fp64)
+        b = oracle.Field(c, q, fp64=fp64, scatter=True)
+        view = np.uint64 if fp64 else np.uint32
+        assert np.array_equal(a.dims, b.dims) and np.array_equal(a.origin, b.origin)
+        assert np.array_equal(a.phi.view(view), b.phi.view(view))
+
+
 def test_nearcell_matches_allpairs():
     # src/nearcell.rs:120-160: xorshift coordinates, 300 atoms, cell 5
     state = 7

@@ -9,8 +9,11 @@ kernel with its scratch (per-tile partial sums, per-pose counters, work
 counter) in a fixed 8 MiB device array compiled into liblkg.
 
 The test calls it through the C ABI twice in a row on the same inputs and
-checks each result against the regular entry point (``lkg_score_device``),
-then checks that a batch too large for the fixed array is refused up front.
+checks each result against the regular entry point (``lkg_score_device``):
+scores on both calls, the per-pose parts (raw electrostatics, LJ, near
+pairs) on the second, the kernel's status word (read by ``lkg_ctx_sync``),
+and once against the oracle (the reference's CPU grid path).  Then it
+checks that a batch too large for the fixed array is refused up front.
 This file is named to be collected last.
 """
 import ctypes
@@ -18,6 +21,7 @@ import ctypes
 import numpy as np
 import pytest
 
+import oracle
 from tests.lkg_helpers import azp_model, lkg, random_poses, rel_err
 
 pytestmark = pytest.mark.gpu
@@ -40,22 +44,33 @@ def test_noalloc_matches_regular_entry_point_on_two_calls():
     rec, lig = azp_model("dna")
     cid = ctx.add_complex("dna", rec, lig)
     n = 300
-    d_poses = torch.tensor(random_poses(n, [0, 0, 0], 6.0, 21), dtype=torch.float64, device="cuda")
+    poses = random_poses(n, [0, 0, 0], 6.0, 21)
+    d_poses = torch.tensor(poses, dtype=torch.float64, device="cuda")
     ref = torch.zeros(n, dtype=torch.float64, device="cuda")
+    ref_parts = torch.zeros((n, 4), dtype=torch.float64, device="cuda")
     torch.cuda.synchronize()
     # the regular entry point (also puts the complex descriptor on the device)
-    ctx.score_device(cid, n, d_poses.data_ptr(), ref.data_ptr())
+    ctx.score_device(cid, n, d_poses.data_ptr(), ref.data_ptr(), ref_parts.data_ptr())
     stream.synchronize()
-    ref_h = ref.cpu().numpy()
-    for _ in range(2):
+    ref_h, ref_parts_h = ref.cpu().numpy(), ref_parts.cpu().numpy()
+    for call in range(2):
         out = torch.full((n,), float("nan"), dtype=torch.float64, device="cuda")
+        parts = torch.full((n, 4), float("nan"), dtype=torch.float64, device="cuda")
         torch.cuda.synchronize()
-        rc = noalloc(ctx.h, cid, n, d_poses.data_ptr(), out.data_ptr(), None)
+        rc = noalloc(ctx.h, cid, n, d_poses.data_ptr(), out.data_ptr(), parts.data_ptr() if call else None)
         assert rc == 0, lkg.lib().lkg_last_error().decode()
-        stream.synchronize()
+        ctx.sync()   # waits for the call and checks its status word (raises if set)
         got = out.cpu().numpy()
         assert np.all(np.isfinite(got))
         assert rel_err(got, ref_h).max() < TOL
+        if call:
+            p = parts.cpu().numpy()
+            assert rel_err(p[:, 0] * 83.0, ref_parts_h[:, 0] * 83.0).max() < TOL   # raw electrostatics
+            assert rel_err(p[:, 1], ref_parts_h[:, 1]).max() < TOL                  # LJ + clash
+            assert np.all(np.abs(p[:, 3] - ref_parts_h[:, 3]) <= 2)                 # near pairs
+        else:
+            # the reference's CPU grid path on the same poses
+            assert rel_err(got, oracle.Model("dna", rec, lig).batch_energy_grid(poses)).max() < TOL
     ctx.close()
 
 
