@@ -55,6 +55,7 @@ def lib():
             "orc_gso_state": (V, [P, P, P, P, P, P, P, P]), "orc_gso_scored": (I64, [P]),
             "orc_gso_free": (V, [P]),
             "orc_synth_chain": (C.c_int, [U64, I32, D, D, D, I32, P, P]),
+            "orc_lr_sasa": (V, [P, P, I32, P]),
         }
         for name, (res, args) in sig.items():
             f = getattr(L, name)
@@ -92,6 +93,14 @@ class Rng:
     def __del__(self):
         if getattr(self, "h", None):
             lib().orc_rng_free(self.h)
+
+
+def lr_sasa(coords, radii):
+    """Lee & Richards per-atom SASA (src/lr_sasa.rs: probe 1.4 A, 20 slices)."""
+    c, r = _f64(coords).reshape(-1, 3), _f64(radii)
+    out = np.zeros(len(r))
+    lib().orc_lr_sasa(_p(c), _p(r), len(r), _p(out))
+    return out
 
 
 def synth_chain(n, seed, r0=30.0, bond=1.5, min_sep=3.0, patience=10000):

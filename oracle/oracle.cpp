@@ -1058,6 +1058,153 @@ int synth_chain(uint64_t seed, int32_t n, double r0, double bond, double min_sep
     return 0;
 }
 
+// ---------------------------------------------------------------------------
+// Lee & Richards solvent-accessible surface area (src/lr_sasa.rs:27-291, the
+// freesasa 2.2 algorithm with probe 1.4 A and 20 slices), restated here
+// independently of liblkg's copy so that the cpydock reference areas are
+// checked against the reference's own algorithm.
+// ---------------------------------------------------------------------------
+struct LrNb {
+    std::vector<std::vector<int>> idx;       // neighbours of each atom, in discovery order
+    std::vector<std::vector<double>> dxy;    // sqrt(dx^2 + dy^2)
+    std::vector<std::vector<double>> dx, dy; // neighbour minus atom
+};
+
+// lr_sasa.rs:27-145: cells of edge 2 max(R), atoms in index order per cell,
+// each cell paired with the neighbouring cells whose offset sums to >= 0
+// (and itself, from the next atom on), pairs kept when d^2 < (Ri + Rj)^2
+LrNb lr_neighbours(const double* c, const std::vector<double>& R) {
+    const int n = (int)R.size();
+    LrNb nb;
+    nb.idx.resize(n); nb.dxy.resize(n); nb.dx.resize(n); nb.dy.resize(n);
+    double rmax = 0.0;
+    for (double r : R) rmax = std::fmax(rmax, r);
+    const double d = 2.0 * rmax;
+    double lo[3] = {c[0], c[1], c[2]}, hi[3] = {c[0], c[1], c[2]};
+    for (int i = 1; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            lo[a] = std::fmin(lo[a], c[3 * i + a]);
+            hi[a] = std::fmax(hi[a], c[3 * i + a]);
+        }
+    int64_t nc[3];
+    for (int a = 0; a < 3; ++a) {
+        lo[a] -= d / 2.0;
+        hi[a] += d / 2.0;
+        nc[a] = (int64_t)std::ceil((hi[a] - lo[a]) / d);
+    }
+    auto cell_index = [&](int64_t ix, int64_t iy, int64_t iz) { return ix + nc[0] * (iy + nc[1] * iz); };
+    std::vector<std::vector<int>> cell(nc[0] * nc[1] * nc[2]);
+    for (int i = 0; i < n; ++i) {
+        int64_t g[3];
+        for (int a = 0; a < 3; ++a)
+            g[a] = std::min<int64_t>(std::max<int64_t>((int64_t)((c[3 * i + a] - lo[a]) / d), 0), nc[a] - 1);
+        cell[cell_index(g[0], g[1], g[2])].push_back(i);
+    }
+    for (int64_t iz = 0; iz < nc[2]; ++iz)
+        for (int64_t iy = 0; iy < nc[1]; ++iy)
+            for (int64_t ix = 0; ix < nc[0]; ++ix) {
+                const std::vector<int>& A = cell[cell_index(ix, iy, iz)];
+                // neighbour cells in x-outer, z-inner order, as lr_sasa.rs:84-102 lists them
+                for (int64_t jx = std::max<int64_t>(ix - 1, 0); jx <= std::min(ix + 1, nc[0] - 1); ++jx)
+                    for (int64_t jy = std::max<int64_t>(iy - 1, 0); jy <= std::min(iy + 1, nc[1] - 1); ++jy)
+                        for (int64_t jz = std::max<int64_t>(iz - 1, 0); jz <= std::min(iz + 1, nc[2] - 1); ++jz) {
+                            if ((jx - ix) + (jy - iy) + (jz - iz) < 0) continue;
+                            const bool same = jx == ix && jy == iy && jz == iz;
+                            const std::vector<int>& B = cell[cell_index(jx, jy, jz)];
+                            for (size_t ii = 0; ii < A.size(); ++ii) {
+                                const int a = A[ii];
+                                for (size_t jj = same ? ii + 1 : 0; jj < B.size(); ++jj) {
+                                    const int b = B[jj];
+                                    const double cut2 = (R[a] + R[b]) * (R[a] + R[b]);
+                                    const double ex = c[3 * b] - c[3 * a], ey = c[3 * b + 1] - c[3 * a + 1],
+                                                 ez = c[3 * b + 2] - c[3 * a + 2];
+                                    if (ex * ex + ey * ey + ez * ez < cut2) {
+                                        const double exy = std::sqrt(ex * ex + ey * ey);
+                                        nb.idx[a].push_back(b); nb.idx[b].push_back(a);
+                                        nb.dxy[a].push_back(exy); nb.dxy[b].push_back(exy);
+                                        nb.dx[a].push_back(ex); nb.dx[b].push_back(-ex);
+                                        nb.dy[a].push_back(ey); nb.dy[b].push_back(-ey);
+                                    }
+                                }
+                            }
+                        }
+            }
+    return nb;
+}
+
+// exposed length of the full circle given m buried intervals (start, end)
+// in arc[0 .. 2m): intervals sorted by start (insertion sort), then the gaps
+// between the running union's end and the next start are summed
+// (lr_sasa.rs:150-185)
+double lr_exposed(std::vector<double>& arc, int m) {
+    const double two_pi = 2.0 * M_PI;
+    if (m == 0) return two_pi;
+    for (int i = 2; i < 2 * m; i += 2) {
+        const double s0 = arc[i], s1 = arc[i + 1];
+        int j = i;
+        for (; j > 0 && arc[j - 2] > s0; j -= 2) {
+            arc[j] = arc[j - 2];
+            arc[j + 1] = arc[j - 1];
+        }
+        arc[j] = s0;
+        arc[j + 1] = s1;
+    }
+    double total = arc[0], end = arc[1];
+    for (int i = 2; i < 2 * m; i += 2) {
+        if (end < arc[i]) total += arc[i] - end;
+        if (arc[i + 1] > end) end = arc[i + 1];
+    }
+    return total + two_pi - end;
+}
+
+// area of atom i: n_slices planes across its sphere, each plane's exposed
+// arc of the atom's circle times delta * R_i (lr_sasa.rs:187-268)
+double lr_area(int i, const double* c, const std::vector<double>& R, const LrNb& nb, int n_slices) {
+    const double two_pi = 2.0 * M_PI;
+    const std::vector<int>& J = nb.idx[i];
+    const int m = (int)J.size();
+    const double zi = c[3 * i + 2], ri = R[i];
+    const double delta = 2.0 * ri / n_slices;
+    double z = zi - ri - 0.5 * delta, area = 0.0;
+    std::vector<double> arc(4 * std::max(m, 1));
+    for (int s = 0; s < n_slices; ++s) {
+        z += delta;
+        const double di = std::fabs(zi - z);
+        const double ri_p2 = ri * ri - di * di;
+        if (ri_p2 < 0.0) continue;
+        const double ri_p = std::sqrt(ri_p2);
+        if (ri_p <= 0.0) continue;
+        int arcs = 0;
+        bool buried = false;
+        for (int k = 0; k < m; ++k) {
+            const double dj = std::fabs(c[3 * J[k] + 2] - z);
+            const double rj = R[J[k]];
+            if (!(dj < rj)) continue;
+            const double rj_p2 = rj * rj - dj * dj;
+            const double rj_p = std::sqrt(rj_p2);
+            const double dij = nb.dxy[i][k];
+            if (dij >= ri_p + rj_p) continue;                // circles apart
+            if (dij + ri_p < rj_p) { buried = true; break; }  // circle i inside circle j
+            if (dij + rj_p < ri_p) continue;                  // circle j inside circle i
+            const double alpha = std::acos((ri_p2 + dij * dij - rj_p2) / (2.0 * ri_p * dij));
+            const double beta = std::atan2(nb.dy[i][k], nb.dx[i][k]) + M_PI;
+            double a0 = beta - alpha, a1 = beta + alpha;
+            if (a0 < 0.0) a0 += two_pi;
+            if (a1 > 2.0 * M_PI) a1 -= two_pi;
+            if (a1 < a0) {   // the interval wraps through 0: two pieces
+                arc[2 * arcs] = 0.0; arc[2 * arcs + 1] = a1;
+                arc[2 * arcs + 2] = a0; arc[2 * arcs + 3] = two_pi;
+                arcs += 2;
+            } else {
+                arc[2 * arcs] = a0; arc[2 * arcs + 1] = a1;
+                arcs += 1;
+            }
+        }
+        if (!buried) area += delta * ri * lr_exposed(arc, arcs);
+    }
+    return area;
+}
+
 }  // namespace
 
 
@@ -1065,6 +1212,14 @@ int synth_chain(uint64_t seed, int32_t n, double r0, double bond, double min_sep
 // C ABI
 // ---------------------------------------------------------------------------
 extern "C" {
+
+void orc_lr_sasa(const double* coords, const double* radii, int32_t n, double* out) {
+    if (n <= 0) return;
+    std::vector<double> R(n);
+    for (int i = 0; i < n; ++i) R[i] = radii[i] + 1.4;   // probe radius
+    const LrNb nb = lr_neighbours(coords, R);
+    for (int i = 0; i < n; ++i) out[i] = lr_area(i, coords, R, nb, 20);
+}
 
 int orc_synth_chain(uint64_t seed, int32_t n, double r0, double bond, double min_sep, int32_t patience,
                     double* coords, double* r_final) {

@@ -34,6 +34,10 @@ uint64_t orc_rng_u64(void* rng);
 int orc_synth_chain(uint64_t seed, int32_t n, double r0, double bond, double min_sep, int32_t patience,
                     double* coords, double* r_final);
 
+/* Lee & Richards SASA (src/lr_sasa.rs: probe 1.4 A, 20 slices): per-atom
+ * areas of n atoms with bare radii `radii` */
+void orc_lr_sasa(const double* coords, const double* radii, int32_t n, double* out);
+
 /* quaternions (src/qt.rs) */
 void orc_quat_random(void* rng, double out[4]);                       /* qt.rs:106-117 */
 void orc_quat_slerp(const double a[4], const double b[4], double t, double out[4]); /* qt.rs:80-104 */

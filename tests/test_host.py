@@ -87,6 +87,31 @@ def test_lr_sasa_isolated_and_buried():
     assert b[0] == 0.0 and b[1] > 0
 
 
+def test_lr_sasa_equals_the_oracle_restatement():
+    # liblkg's Lee & Richards areas (the cpydock reference ASA) against the
+    # oracle's own restatement of src/lr_sasa.rs, atom by atom: the 1AZP
+    # heavy atoms, the config-0 duplex ligand and a 3000-atom globule with
+    # the radius_per_asp radii cpydock uses (cpydock.rs:59-70, 269-332)
+    from tests.golden_models import azp
+    rec, _ = azp("pydock")
+    heavy = rec["is_h"] == 0
+    cases = [(rec["coords"][heavy], rec["radius"][heavy])]
+    for m in (synth.duplex(20, 42), synth.globule(3000, 5)):
+        h = np.asarray(m["heavy"]).astype(bool)
+        cases.append((np.asarray(m["coords"])[h], np.array([synth._RASP.get(t, 0.0)
+                                                            for t, k in zip(m["types"], h) if k])))
+    for c, r in cases:
+        assert np.array_equal(lkg.lr_sasa(c, r), oracle.lr_sasa(c, r))
+    # and the cpydock side arrays synth builds from them (hydrogens get -1)
+    lig = synth.duplex(6, 3)
+    cp = synth.add_cpydock(lig)
+    h = np.asarray(lig["heavy"]).astype(bool)
+    ref = np.full(len(h), -1.0)
+    ref[h] = oracle.lr_sasa(np.asarray(lig["coords"])[h],
+                            np.array([synth._RASP.get(t, 0.0) for t, k in zip(lig["types"], h) if k]))
+    assert np.array_equal(cp["asa"], ref)
+
+
 def test_synthetic_config0_shape_and_charges():
     c0 = synth.config0()
     rec, lig = c0["rec"], c0["lig"]

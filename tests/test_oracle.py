@@ -72,6 +72,25 @@ def test_field_brick_order_equals_atom_scatter(fp64):
         assert np.array_equal(a.phi.view(view), b.phi.view(view))
 
 
+def test_lr_sasa_analytic_spheres():
+    # Lee & Richards (src/lr_sasa.rs, probe 1.4 A, 20 slices): an isolated
+    # sphere's slices sum to 4 pi R^2 exactly; two overlapping spheres side
+    # by side (slices cut both) approach the analytic exposed areas
+    # 4 pi R^2 - 2 pi R h (h: height of the cap inside the other sphere)
+    # within the 20-slice discretisation; a sphere inside another is buried
+    a = oracle.lr_sasa(np.zeros((1, 3)), [1.6])
+    assert abs(a[0] - 4 * np.pi * 3.0 ** 2) < 1e-9
+    for r1, r2, d in ((1.6, 1.9, 3.0), (1.8, 1.8, 4.5), (1.4, 2.0, 2.2)):
+        got = oracle.lr_sasa(np.array([[0.0, 0, 0], [d, 0, 0]]), [r1, r2])
+        p1, p2 = r1 + 1.4, r2 + 1.4
+        h1 = p1 - (d * d + p1 * p1 - p2 * p2) / (2 * d)
+        h2 = p2 - (d * d + p2 * p2 - p1 * p1) / (2 * d)
+        exact = [4 * np.pi * p1 * p1 - 2 * np.pi * p1 * h1, 4 * np.pi * p2 * p2 - 2 * np.pi * p2 * h2]
+        assert np.all(np.abs(got - exact) / exact < 0.01)
+    b = oracle.lr_sasa(np.array([[0.0, 0, 0], [0.1, 0, 0]]), [0.5, 4.0])
+    assert b[0] == 0.0 and b[1] > 0
+
+
 def test_nearcell_matches_allpairs():
     # src/nearcell.rs:120-160: xorshift coordinates, 300 atoms, cell 5
     state = 7
