@@ -65,6 +65,9 @@ def parse():
     ap.add_argument("--no-graph", action="store_true")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--gso-steps", type=int, default=200)
+    ap.add_argument("--seeds", type=int, default=1,
+                    help="screened workloads: GSO seeds over which the screened run, the random-rank ablation and "
+                         "the plain run with the next seed are compared with the plain run (mean and spread)")
     ap.add_argument("--complexes", type=int, default=0,
                     help="score only the first K complexes of the workload (profiling-size cases)")
     return ap.parse_args()
@@ -567,6 +570,7 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
     ctx = lkg.Context(device=local, tile=shape["tile"], cell=shape["cell"], group=shape["group"], xsub=shape["xsub"])
     cid = ctx.add_complex(family, c["rec"], c["lig"])
     res = {}
+    clocks = Clocks(local)   # sampled over every timed run below
     for mode in ("plain", "device", "screened", "screened_device", "ablation", "screened_carry"):
         g = lkg.GSO(ctx, [(cid, swarms, glow)], pos, [seed])
         if mode != "plain" and mode != "device":
@@ -582,6 +586,7 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
         st = g.state()
         res[mode] = dict(seconds=el, scored=g.scored, predicted=g.predicted, st=st, phases=g.timing())
         del g
+    clk = clocks.stop()
     # the GSO's own spread: the plain run from the same start with the next
     # seed; its top-5 overlap with the plain run bounds what any run with a
     # different random stream can reach
@@ -638,12 +643,62 @@ def run_screened(args, lkg, torch, local, rank, world, dist):
             "plain_next_seed": {"mean_best_score": best["plain_next_seed"],
                                 "top5_overlap_with_plain": ov["plain_next_seed"],
                                 "what": "the plain GSO from the same start with GSO seed + 1: the overlap two "
-                                        "plain runs reach"}}
+                                        "plain runs reach"},
+            "clocks": clk}
+    if args.seeds > 1:
+        line["seeds"] = seed_spread(lkg, ctx, cid, pos, swarms, glow, steps, seed, args.seeds)
     if rank == 0:
         print(json.dumps(line), flush=True)
     ctx.close()
     if dist:
         dist.destroy_process_group()
+
+
+def seed_spread(lkg, ctx, cid, pos, swarms, glow, steps, seed0, n_seeds):
+    """The screened run (device steps), the random-rank ablation and the
+    plain run with the next GSO seed, each against the plain run of the same
+    seed, over GSO seeds seed0 .. seed0 + n_seeds - 1 from the same start:
+    mean and standard deviation of the top-5 overlap and of the mean best
+    score per swarm, and the per-seed values."""
+    def run(seed, mode):
+        g = lkg.GSO(ctx, [(cid, swarms, glow)], pos, [seed])
+        if mode in ("screened", "ablation"):
+            g.set_screen(candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=20, train_epochs=20,
+                         finetune_epochs=2, lr=1e-3, seed=seed, random_rank=(mode == "ablation"), batch=1024)
+        g.run(steps, device=(mode == "screened"))
+        g.finalize()
+        st = g.state()
+        del g
+        return st
+
+    def overlap(a, b):
+        o = []
+        for k in range(swarms):
+            sl = slice(k * glow, (k + 1) * glow)
+            o.append(top5_overlap(a["translation"][sl], a["scoring"][sl], b["translation"][sl], b["scoring"][sl]))
+        return float(np.mean(o))
+
+    def best(st):
+        return float(np.mean(st["scoring"].reshape(swarms, glow).max(axis=1)))
+
+    plain = [run(seed0 + i, "plain") for i in range(n_seeds + 1)]
+    per = {"screened": [], "ablation": [], "plain_next_seed": []}
+    for i in range(n_seeds):
+        s = seed0 + i
+        for mode in ("screened", "ablation"):
+            st = run(s, mode)
+            per[mode].append({"seed": s, "top5_overlap": overlap(st, plain[i]), "mean_best_score": best(st)})
+        per["plain_next_seed"].append({"seed": s + 1, "top5_overlap": overlap(plain[i + 1], plain[i]),
+                                       "mean_best_score": best(plain[i + 1])})
+    out = {"seeds": [seed0 + i for i in range(n_seeds)],
+           "plain_mean_best_score": [best(p) for p in plain[:n_seeds]]}
+    for mode, rows in per.items():
+        ov = np.array([r["top5_overlap"] for r in rows])
+        bs = np.array([r["mean_best_score"] for r in rows])
+        out[mode] = {"top5_overlap_mean": float(ov.mean()), "top5_overlap_std": float(ov.std()),
+                     "mean_best_score_mean": float(bs.mean()), "mean_best_score_std": float(bs.std()),
+                     "per_seed": rows}
+    return out
 
 
 if __name__ == "__main__":

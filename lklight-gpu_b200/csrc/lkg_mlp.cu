@@ -2,13 +2,18 @@
 // BF16 weights and activations and FP32 accumulation, trained online on the
 // exact scorer's energies and used to screen candidate GSO moves.
 //
-// Kernels (all hand-written, tensor cores through mma.sync m16n8k16 bf16):
+// Kernels (all hand-written; the GEMM layers on tcgen05 by default, the
+// mma.sync m16n8k16 bf16 kernel k_gemm kept as the second backend):
 //   k_features   pose parameters + far-field potential and receptor atom
 //                counts at 16 ligand anchor atoms -> 64 bf16 features
 //   k_gemm       C = A * B^T tiles of 64 x 64, K step 32, four warps; A / B
 //                read [rows][k] or transposed from global; epilogues: bias +
 //                ReLU -> bf16 (forward), x ReLU'(H) -> bf16 (backward data),
 //                split-K atomic FP32 (weight gradients)
+//   k_gemm_tc    tcgen05 + TMA layers (forward, backward data): 128-row tiles,
+//                K-major SW128 operands, FP32 accumulator in TMEM
+//   k_wgrad_tc   tcgen05 + TMA weight gradients: MN-major SW128 operands,
+//                reduction over the batch split across CTAs
 //   k_head       last layer (256 -> 1) dot products, FP32
 //   k_loss       MSE on the standardised target, dy, head gradients
 //   k_colsum     bias gradients
@@ -206,7 +211,8 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
 // 256-column TMEM accumulator and commits them to a second mbarrier; each
 // warp reads its 32 TMEM lanes (rows) back with tcgen05.ld and applies the
 // epilogue.  Both waits are bounded: a wait that runs out sets status bit 2,
-// the CTA skips the rest, and the accumulator is still freed.
+// the CTA skips the rest, waits (bounded again) for the copies or MMAs it
+// still has in flight, and the accumulator is still freed.
 // ---------------------------------------------------------------------------
 constexpr int TC_BM = 128, TC_N = 256, TC_KMAX = 256, TC_KS = 64;   // K slab of one TMA copy (128 B)
 constexpr size_t TC_SMEM = (size_t)(TC_BM + TC_N) * TC_KMAX * 2 + 1024;   // A, B slabs + alignment slack
@@ -274,9 +280,9 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_slot;
-    bool ok = mbar_wait(bar_ld, 0);
+    const bool ld_ok = mbar_wait(bar_ld, 0);
     // 2. one thread issues the MMAs and commits them to the second barrier
-    if (ok && tid == 0) {
+    if (ld_ok && tid == 0) {
         // kind::f16 descriptor: D f32 (bits 4-5 = 1), A bf16 (7-9 = 1), B bf16
         // (10-12 = 1), both K-major, N >> 3 at 17-22, M >> 4 at 24-28
         const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TN >> 3) << 17) |
@@ -296,7 +302,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
                      :: "r"(bar_mma) : "memory");
     }
     // 3. bounded wait for the accumulator
-    if (ok) ok = mbar_wait(bar_mma, 0);
+    const bool ok = ld_ok && mbar_wait(bar_mma, 0);
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     if (!ok) {
         if (lane == 0) atomicOr(status, 4);
@@ -340,7 +346,130 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
             }
         }
     }
-    // 5. free the accumulator
+    // 5. free the accumulator.  After a wait that ran out, first wait out
+    //    (bounded again) what this CTA still has in flight: the TMA copies
+    //    into its shared memory, or the MMAs into its TMEM
+    if (!ld_ok) mbar_wait(bar_ld, 0);
+    else if (!ok) mbar_wait(bar_mma, 0);
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(TN));
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Weight gradients on tcgen05: dW[o][i] = sum_r dC[r][o] * A_in[r][i] over
+// the batch rows r.  Both operands are stored row by row ([r][o], [r][i]),
+// so for the reduction over r they are MN-major: A (M = o, 128 per CTA)
+// and B (N = i: 64 or 256) arrive by TMA as boxes of 64 contiguous
+// elements x 64 batch rows, 128-byte swizzled (8 rows per 1024-byte atom).
+// The descriptors are MN-major SW128: SBO = 1024 B to the next 8 rows (K),
+// LBO = 64 rows x 128 B to the next 64 elements (MN); one K step of 16 rows
+// moves the start address by 2048 B (two whole atoms).  Each CTA reduces a
+// chunk of TCW_ROWS batch rows (all its slabs resident, one expect_tx
+// barrier) and writes its FP32 partial tile to part[split][o][i]; the
+// splits are added in order afterwards (k_split_sum), so training stays
+// bitwise reproducible.  Waits are bounded as in k_gemm_tc.
+// ---------------------------------------------------------------------------
+constexpr int TCW_ROWS = 128;                       // batch rows per CTA (two 64-row slabs)
+constexpr int TCW_SLAB = 64;                        // batch rows per TMA box
+constexpr size_t TCW_SMEM = (size_t)(TC_BM + TC_N) * TCW_ROWS * 2 + 1024;
+
+__device__ __forceinline__ uint64_t tc_desc_mn(uint32_t saddr, uint32_t lbo_bytes) {
+    return (uint64_t)((saddr >> 4) & 0x3fff) | ((uint64_t)((lbo_bytes >> 4) & 0x3fff) << 16) |
+           ((uint64_t)(1024 >> 4) << 32) | (1ull << 46) | (2ull << 61);
+}
+
+template <int TN>
+__global__ void __launch_bounds__(128, 1)
+k_wgrad_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int rows,
+           float* __restrict__ part, int* __restrict__ status) {
+    static_assert(TN == 64 || TN == 256, "input width");
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ __align__(8) unsigned long long bars[2];
+    __shared__ uint32_t tmem_slot;
+    constexpr int NSLAB = TCW_ROWS / TCW_SLAB;
+    constexpr uint32_t A_SLAB = TC_BM * TCW_SLAB * 2, B_SLAB = TN * TCW_SLAB * 2;   // bytes per slab
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int m0 = blockIdx.x * TC_BM, r0 = blockIdx.y * TCW_ROWS;
+    const uint32_t base = (smem_u32(tc_smem) + 1023u) & ~1023u;
+    const uint32_t sA = base, sB = base + (uint32_t)NSLAB * A_SLAB;
+    const uint32_t bar_ld = smem_u32(&bars[0]), bar_mma = smem_u32(&bars[1]);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&tmem_slot)), "r"(TN));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar_ld), "r"(1));
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(bar_mma), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                     :: "r"(bar_ld), "r"((uint32_t)NSLAB * (A_SLAB + B_SLAB)) : "memory");
+        // slab sl: A boxes of 64 output rows (o) and B boxes of 64 inputs (i),
+        // 64 batch rows each; box b of a slab sits b x 64 x 128 B in
+        for (int sl = 0; sl < NSLAB; ++sl) {
+            const int y = r0 + sl * TCW_SLAB;
+            for (int b = 0; b < TC_BM / 64; ++b)
+                tma_load_2d(sA + (uint32_t)sl * A_SLAB + (uint32_t)b * (TCW_SLAB * 128), &mapA, m0 + 64 * b, y, bar_ld);
+            for (int b = 0; b < TN / 64; ++b)
+                tma_load_2d(sB + (uint32_t)sl * B_SLAB + (uint32_t)b * (TCW_SLAB * 128), &mapB, 64 * b, y, bar_ld);
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    const bool ld_ok = mbar_wait(bar_ld, 0);
+    if (ld_ok && tid == 0) {
+        // kind::f16: D f32, A and B bf16, both MN-major (bits 15, 16), N >> 3, M >> 4
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 15) | (1u << 16) |
+                               ((uint32_t)(TN >> 3) << 17) | ((uint32_t)(TC_BM >> 4) << 24);
+        for (int sl = 0; sl < NSLAB; ++sl)
+            for (int ks = 0; ks < TCW_SLAB / 16; ++ks) {
+                const uint64_t ad = tc_desc_mn(sA + (uint32_t)sl * A_SLAB + (uint32_t)ks * 2048, TCW_SLAB * 128);
+                const uint64_t bd = tc_desc_mn(sB + (uint32_t)sl * B_SLAB + (uint32_t)ks * 2048, TCW_SLAB * 128);
+                const uint32_t acc = (sl | ks) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                    :: "r"(tmem), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u), "r"(0u));
+            }
+        asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                     :: "r"(bar_mma) : "memory");
+    }
+    const bool ok = ld_ok && mbar_wait(bar_mma, 0);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    if (!ok) {
+        if (lane == 0) atomicOr(status, 4);
+    } else {
+        // warp w: output rows o = m0 + 32 w + lane (TMEM lanes), 32 columns at a time
+        float* out = part + (size_t)blockIdx.y * H * TN + (size_t)(m0 + warp * 32 + lane) * TN;
+        for (int cl = 0; cl < TN; cl += 32) {
+            uint32_t r[32];
+            const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)cl;
+            asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                         "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                         "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                         : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                           "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                           "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]),
+                           "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]),
+                           "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+                         : "r"(taddr));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            float4* dst = reinterpret_cast<float4*>(out + cl);
+#pragma unroll
+            for (int q = 0; q < 8; ++q)
+                dst[q] = make_float4(__uint_as_float(r[4 * q]), __uint_as_float(r[4 * q + 1]),
+                                     __uint_as_float(r[4 * q + 2]), __uint_as_float(r[4 * q + 3]));
+        }
+    }
+    if (!ld_ok) mbar_wait(bar_ld, 0);
+    else if (!ok) mbar_wait(bar_mma, 0);
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
     if (warp == 0) {
@@ -507,7 +636,7 @@ struct lkg_surrogate {
     int cap = 0;     // rows of X, H1..H3, y, t (forward)
     int cap_b = 0;   // rows of dH1..dH3 (backward)
     DBuf d_step;   // Adam step count (device, 1-based) and the Adam kernel's block counter
-    int tc = 1;    // forward layers on tcgen05 (1, default) or mma.sync (0)
+    int tc = 1;    // GEMM layers (forward, backward data, weight gradients) on tcgen05 (1, default) or mma.sync (0)
     DBuf d_status; // tcgen05 wait time-outs (bit 2)
     size_t off[9];   // block offsets of W0 b0 W1 b1 W2 b2 w3 b3, and the total
 };
@@ -545,7 +674,8 @@ int sur_reserve(lkg_surrogate* S, int n, bool bwd) {
         LKG_CK(S->dH1.reserve(nb * H), "surrogate alloc");
         LKG_CK(S->dH2.reserve(nb * H), "surrogate alloc");
         LKG_CK(S->dH3.reserve(nb * H), "surrogate alloc");
-        LKG_CK(S->wpart.reserve((size_t)wgrad_splits(m) * H * H * sizeof(float)), "surrogate alloc");
+        const size_t splits = std::max<size_t>(wgrad_splits(m), (size_t)(m + TCW_ROWS - 1) / TCW_ROWS);
+        LKG_CK(S->wpart.reserve(splits * H * H * sizeof(float)), "surrogate alloc");
         LKG_CK(S->rpart.reserve((size_t)((m + RL - 1) / RL) * (H + 2) * sizeof(float)), "surrogate alloc");
         S->cap_b = m;
     }
@@ -610,6 +740,22 @@ cudaError_t gemm_tc(lkg_surrogate* S, int n, int K, const __nv_bfloat16* A, cons
     return cudaGetLastError();
 }
 
+// dW[H x kin] partials: part[split][o][i] = sum over the split's batch rows r
+// of dC[r][o] * A_in[r][i]; returns the number of splits
+cudaError_t wgrad_tc(lkg_surrogate* S, int n, int kin, const __nv_bfloat16* dC, const __nv_bfloat16* Ain, float* part,
+                     int* nsplit) {
+    const int splits = (n + TCW_ROWS - 1) / TCW_ROWS;
+    *nsplit = splits;
+    alignas(64) CUtensorMap ma, mb;
+    if ((kin != 64 && kin != H) || !tc_map(&ma, dC, n, H, TCW_SLAB) || !tc_map(&mb, Ain, n, kin, TCW_SLAB))
+        return cudaErrorInvalidValue;
+    auto kern = kin == H ? k_wgrad_tc<256> : k_wgrad_tc<64>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TCW_SMEM);
+    if (e != cudaSuccess) return e;
+    kern<<<dim3(H / TC_BM, splits), 128, TCW_SMEM, S->ctx->stream>>>(ma, mb, n, part, S->d_status.as<int>());
+    return cudaGetLastError();
+}
+
 int forward(lkg_surrogate* S, int n) {
     cudaStream_t s = S->ctx->stream;
     const __nv_bfloat16* X = S->X.as<__nv_bfloat16>();
@@ -657,10 +803,16 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
         const int kin = L == 0 ? IN : H;
         const __nv_bfloat16* ain = L == 0 ? S->X.as<__nv_bfloat16>() : acts[L - 1];
         // dW_L[o][i] = sum_n dC[n][o] * A_in[n][i]   (A = dC^T, B = A_in^T)
-        LKG_CK((gemm<true, true, EPI_WGRAD>(s, H, kin, n, dacts[L], H, ain, kin, wpart, nullptr, kin, nullptr,
-                                            nullptr, splits)), "mlp wgrad");
+        int nz = 0;
+        if (S->tc) {
+            LKG_CK(wgrad_tc(S, n, kin, dacts[L], ain, wpart, &nz), "mlp wgrad tc");
+        } else {
+            LKG_CK((gemm<true, true, EPI_WGRAD>(s, H, kin, n, dacts[L], H, ain, kin, wpart, nullptr, kin, nullptr,
+                                                nullptr, splits)), "mlp wgrad");
+            nz = split_count(n, splits);
+        }
         k_colsum<<<nblk, H, 0, s>>>(dacts[L], n, rpart);
-        const SplitSum wsum{wpart, split_count(n, splits), H * kin, Gd(S, 2 * L)};
+        const SplitSum wsum{wpart, nz, H * kin, Gd(S, 2 * L)};
         const SplitSum bsum{rpart, nblk, H, Gd(S, 2 * L + 1)};
         k_split_sum<<<(H * kin + H + 255) / 256, 256, 0, s>>>(wsum, bsum);
         LKG_CK(cudaGetLastError(), "mlp bias grad");

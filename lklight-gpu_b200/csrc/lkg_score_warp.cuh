@@ -35,8 +35,10 @@ namespace lkg {
 
 constexpr int WK_THREADS = 128;   // 4 independent warps per block
 
-// ring capacity: 31 pending + 32 * G hits of one candidate chunk must fit
-template <int G> struct WRing { static constexpr int N = (G <= 8) ? 512 : (G <= 16) ? 1024 : 2048; };
+// hit buffer: fewer than 64 pending hits (a batch of the plain kernel is 64
+// hits, two a lane) are moved to its front after each candidate chunk, so
+// the pending hits + the 32 x G hits of one chunk always fit
+template <int G> struct WRing { static constexpr int N = 32 * G + 64; };
 
 // resident blocks per SM the register budget is sized for (64 registers a
 // thread for G = 8; the larger masks of G = 16, 32 get 80)
@@ -68,7 +70,7 @@ struct WSlots {
     unsigned* ibits;            // IFACE: interface bits of the current pose in HBM (null: none)
     unsigned* iset;             // IFACE: where pairs set them: ibuf, or ibits when the pose has more words
     unsigned ibuf[W_IBUF];      // IFACE: the unit's bits, merged into ibits once at the unit's end
-    unsigned hit[WRing<G>::N];  // (slot << 26) | receptor index
+    unsigned hit[WRing<G>::N];  // (slot << 26) | receptor index, pending hits first
 };
 
 // Receptor-side minima of the fast cpydock kernel: one 64-bit word per slot,
@@ -158,6 +160,21 @@ __device__ __forceinline__ void w_iface_flush(WSlots<G>& W, const ComplexDev& c)
     __syncwarp();
 }
 
+// 1 / x and 1 / sqrt(x) by the MUFU approximations alone (PTX rcp.approx /
+// rsqrt.approx, flush-to-zero): the pair distances are far from f32
+// denormals (d^2 >= ~1 A^2 for any real pair, <= 100 here), where these
+// are within a few ulp, the budget of the f32 pair math
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+__device__ __forceinline__ float rsqrt_approx(float x) {
+    float r;
+    asm("rsqrt.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 // pair terms of one queued hit: the exact d^2 <= 100 test on the
 // compensated d^2, then the reference formulas (those of pair_fast, with
 // the LJ power taken as (rr^2 / d^2)^3) and the clash term selected instead
@@ -180,7 +197,7 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
     const float d2 = dx * dx + dy * dy + dz * dz;
     if (!(d2 <= 100.f)) return;
     ++np;
-    const float ir2 = __fdividef(1.0f, d2);
+    const float ir2 = rcp_approx(d2);
     if (flags & F_ELEC) {
         float ae = lp.w * a.w * ir2;
         ae = fminf(fmaxf(ae, -ES_CAP_F), ES_CAP_F);
@@ -192,7 +209,7 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
     const float p6 = t * t * t;
     float vp = fminf(sv * p6 * (p6 - 2.f), 1.0f);
     if (flags & F_CLASH) {   // uniform per complex: the other families skip the distance
-        const float d = d2 * rsqrtf(d2), dmin = 0.75f * rr;
+        const float d = d2 * rsqrt_approx(d2), dmin = 0.75f * rr;
         const bool clash = lq.y != 0.f && pr.z != 0.f && d < dmin;
         vp = clash ? vp + 6.f * (dmin - d) : vp;
     }
@@ -228,6 +245,77 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
     }
 }
 
+// Packed pairs of f32 (Blackwell's f32x2 FADD / FMUL / FFMA: one instruction
+// computes both lanes of the pair, each rounded as the scalar operation)
+struct F2 { unsigned long long v; };
+__device__ __forceinline__ F2 f2(float a, float b) {
+    F2 r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(r.v) : "f"(a), "f"(b));
+    return r;
+}
+__device__ __forceinline__ void f2_get(F2 x, float& a, float& b) { asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x.v)); }
+__device__ __forceinline__ F2 add2(F2 a, F2 b) { F2 r; asm("add.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v)); return r; }
+__device__ __forceinline__ F2 sub2(F2 a, F2 b) { F2 r; asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v)); return r; }
+__device__ __forceinline__ F2 mul2(F2 a, F2 b) { F2 r; asm("mul.rn.f32x2 %0, %1, %2;" : "=l"(r.v) : "l"(a.v), "l"(b.v)); return r; }
+__device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
+    F2 r;
+    asm("fma.rn.f32x2 %0, %1, %2, %3;" : "=l"(r.v) : "l"(a.v), "l"(b.v), "l"(c.v));
+    return r;
+}
+
+// two queued hits a lane (the plain kernel, no desolvation, no interface
+// bits): the pair terms of w_pair for hits e0 and e1 computed side by side
+// on packed f32 pairs, which halves the FP32 instructions of the pair math.
+// e1 counts only when v1 (a partial batch).  Same formulas and rounding
+// steps as w_pair, per hit.
+template <int G>
+__device__ __forceinline__ void w_pair2(const ComplexDev& c, const WSlots<G>& W, unsigned e0, unsigned e1, bool v1,
+                                        unsigned flags, double& elec, double& vdw, int& np) {
+    const int l0 = (int)(e0 >> 26), k0 = (int)(e0 & 0x3ffffffu);
+    const int l1 = (int)(e1 >> 26), k1 = (int)(e1 & 0x3ffffffu);
+    const float4 a0 = __ldg(c.rpos + k0), a1 = __ldg(c.rpos + k1);
+    const float4 p0 = __ldg(c.rpar + k0), p1 = __ldg(c.rpar + k1);
+    const float4 lp0 = W.lpos[l0], lp1 = W.lpos[l1], lr0 = W.lres[l0], lr1 = W.lres[l1];
+    const float2 lq0 = W.lpar[l0], lq1 = W.lpar[l1];
+    const F2 dx = add2(sub2(f2(lp0.x, lp1.x), f2(a0.x, a1.x)), f2(lr0.x, lr1.x));
+    const F2 dy = add2(sub2(f2(lp0.y, lp1.y), f2(a0.y, a1.y)), f2(lr0.y, lr1.y));
+    const F2 dz = add2(sub2(f2(lp0.z, lp1.z), f2(a0.z, a1.z)), f2(lr0.z, lr1.z));
+    const F2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
+    float d20, d21;
+    f2_get(d2, d20, d21);
+    const bool ok0 = d20 <= 100.f, ok1 = v1 && d21 <= 100.f;
+    np += (int)ok0 + (int)ok1;
+    const F2 ir2 = f2(rcp_approx(d20), rcp_approx(d21));
+    if (flags & F_ELEC) {
+        float e0f, e1f;
+        f2_get(mul2(mul2(f2(lp0.w, lp1.w), f2(a0.w, a1.w)), ir2), e0f, e1f);
+        e0f = fminf(fmaxf(e0f, -ES_CAP_F), ES_CAP_F);
+        e1f = fminf(fmaxf(e1f, -ES_CAP_F), ES_CAP_F);
+        if (ok0) elec += (double)e0f;
+        if (ok1) elec += (double)e1f;
+    }
+    const F2 sv = mul2(f2(lr0.w, lr1.w), f2(p0.x, p1.x));
+    const F2 rr = add2(f2(lq0.x, lq1.x), f2(p0.y, p1.y));
+    const F2 t = mul2(mul2(rr, rr), ir2);
+    const F2 p6 = mul2(mul2(t, t), t);
+    float v0, vv1;
+    f2_get(mul2(mul2(sv, p6), sub2(p6, f2(2.f, 2.f))), v0, vv1);
+    v0 = fminf(v0, 1.0f);
+    vv1 = fminf(vv1, 1.0f);
+    if (flags & F_CLASH) {
+        const F2 d = mul2(d2, f2(rsqrt_approx(d20), rsqrt_approx(d21)));
+        const F2 dmin = mul2(f2(0.75f, 0.75f), rr);
+        float dd0, dd1, m0, m1, c0, c1;
+        f2_get(d, dd0, dd1);
+        f2_get(dmin, m0, m1);
+        f2_get(fma2(f2(6.f, 6.f), sub2(dmin, d), f2(v0, vv1)), c0, c1);
+        v0 = (lq0.y != 0.f && p0.z != 0.f && dd0 < m0) ? c0 : v0;
+        vv1 = (lq1.y != 0.f && p1.z != 0.f && dd1 < m1) ? c1 : vv1;
+    }
+    if (ok0) vdw += (double)v0;
+    if (ok1) vdw += (double)vv1;
+}
+
 // receptor atom of candidate kk of the current rows: the span is the last
 // row whose exclusive prefix is <= kk (empty rows never qualify ahead of the
 // non-empty row that follows them); far away when kk is past the end
@@ -259,19 +347,29 @@ struct WAcc {
 template <int G, bool DESOLV, bool IFACE>
 __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes<G>* D, MinHash64* hash, int* status,
                                          int g_first, int g_end, int g_step, WAcc& acc) {
-    constexpr int RING = WRing<G>::N;
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
-    const unsigned lt_mask = (1u << lane) - 1u;
     const unsigned flags = c.flags;
     const int nl = c.nl;
     unsigned* const iset = IFACE ? W.iset : nullptr;   // set by the caller for the unit
-    unsigned head = 0, tail = 0, prev_start = 0;
+    // hits [head, tail) are pending; hits [head, prev_start) belong to the
+    // group before the previous one (whose slot set the next group reuses)
+    int head = 0, tail = 0, prev_start = 0;
     int jdes0 = -1, jdes1 = -1;   // DESOLV: this lane's slot atom in set 0 / set 1
+    // the plain kernel evaluates 64 hits a batch (two a lane, packed f32
+    // pairs); the desolvation and interface kernels 32 (one a lane)
+    constexpr bool PAIR2 = !DESOLV && !IFACE;
+    constexpr int BATCH = PAIR2 ? 64 : 32;
     auto drain_partial = [&]() {
-        if ((int)(tail - head) > lane)
-            w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, iset,
-                                     acc.elec, acc.vdw, acc.np);
+        const int n = tail - head;
+        if (n > lane) {
+            if (PAIR2)
+                w_pair2<G>(c, W, W.hit[head + lane], lane + 32 < n ? W.hit[head + 32 + lane] : W.hit[head + lane],
+                           lane + 32 < n, flags, acc.elec, acc.vdw, acc.np);
+            else
+                w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[head + lane], flags, iset, acc.elec, acc.vdw,
+                                         acc.np);
+        }
         head = tail;
     };
     auto finalize = [&](int set) {   // DESOLV: the slot set's minima are final
@@ -288,7 +386,7 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
         // slot set `set` last served the group before the previous one, whose
         // hits were queued before the previous group started: evaluate any
         // still pending
-        if ((int)(prev_start - head) > 0) drain_partial();
+        if (prev_start > head) drain_partial();
         prev_start = tail;
         __syncwarp();
         finalize(set);
@@ -397,29 +495,56 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
                 // (|l'| <= rho), so a chunk with none closer is skipped (the
                 // test pays off there, not in the plain kernel)
                 if (DESOLV && !__any_sync(FULL, aa <= R2)) continue;
-                // test slot by slot; one ballot per slot appends that slot's
-                // hits to the ring in lane order (consecutive words: no bank
-                // conflicts, no prefix scan)
-                const unsigned enc = (unsigned)ridx | enc_set;
+                // the lane's candidate against every slot: a bit per hit
+                unsigned m = 0;
 #pragma unroll
                 for (int l = 0; l < G; ++l) {
                     const float4 t = W.ltest[set + l];
                     // |a'|^2 - 2 a'.l' <= -(|l'|^2 - 100.01): three FMAs, the
                     // slot's constant on the right (invalid slots: -3e30)
                     const float q = fmaf(ax, t.x, fmaf(ay, t.y, fmaf(az, t.z, aa)));
-                    const bool h = q <= -t.w;
-                    const unsigned b = __ballot_sync(FULL, h);
-                    if (!DESOLV || b) {   // cpydock kernel: slots without a hit skip the append
-                        if (h) W.hit[(tail + __popc(b & lt_mask)) & (RING - 1)] = enc + ((unsigned)l << 26);
-                        tail += (unsigned)__popc(b);
-                    }
+                    m |= (q <= -t.w ? 1u : 0u) << l;
                 }
+                // lane-major append: each lane writes its hits (slot order)
+                // at the warp's exclusive prefix of the hit counts
+                const int nh = __popc(m);
+                int inc = nh;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const int v = __shfl_up_sync(FULL, inc, o);
+                    if (lane >= o) inc += v;
+                }
+                const int chunk_hits = __shfl_sync(FULL, inc, 31);
+                if (chunk_hits == 0) continue;
+                unsigned* dst = W.hit + tail + (inc - nh);
+                const unsigned enc = (unsigned)ridx | enc_set;
+#pragma unroll
+                for (int l = 0; l < G; ++l)
+                    if (m & (1u << l)) *dst++ = enc + ((unsigned)l << 26);
+                tail += chunk_hits;
                 __syncwarp();
-                // 4. full batches of 32 hits
-                while ((int)(tail - head) >= 32) {
-                    w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[(head + lane) & (RING - 1)], flags, iset,
-                                             acc.elec, acc.vdw, acc.np);
-                    head += 32;
+                // 4. full batches
+                while (tail - head >= BATCH) {
+                    if (PAIR2)
+                        w_pair2<G>(c, W, W.hit[head + lane], W.hit[head + 32 + lane], true, flags, acc.elec,
+                                   acc.vdw, acc.np);
+                    else
+                        w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[head + lane], flags, iset, acc.elec,
+                                                 acc.vdw, acc.np);
+                    head += BATCH;
+                }
+                // keep the buffer linear: the < BATCH pending hits move to its front
+                if (head > 0) {
+                    const int rem = tail - head;
+                    const unsigned v = lane < rem ? W.hit[head + lane] : 0u;
+                    const unsigned v2 = (PAIR2 && lane + 32 < rem) ? W.hit[head + 32 + lane] : 0u;
+                    __syncwarp();
+                    if (lane < rem) W.hit[lane] = v;
+                    if (PAIR2 && lane + 32 < rem) W.hit[32 + lane] = v2;
+                    __syncwarp();
+                    prev_start = max(prev_start - head, 0);
+                    tail = rem;
+                    head = 0;
                 }
             }
         }

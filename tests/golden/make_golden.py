@@ -1,8 +1,9 @@
 """Generate the committed golden fixtures for the oracle and parity tests.
 
-Run once in a checkout that has the LKlight-GPU reference sources mounted
-(default ``/root/reference``; override with ``LKG_REFERENCE``).  Nothing at
-test or bench time reads the reference: only the files written here do.
+Run once in a checkout that has the LKlight-GPU reference sources beside it:
+``LKG_REFERENCE`` names their directory, by default ``reference`` next to
+this repository's directory.  Nothing at test or bench time reads the
+reference: only the files written here do.
 
 Outputs
 -------
@@ -28,9 +29,9 @@ import sys
 
 import numpy as np
 
-REF = os.environ.get("LKG_REFERENCE", "/root/reference")
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
+REF = os.environ.get("LKG_REFERENCE", os.path.join(os.path.dirname(REPO), "reference"))
 
 
 def parse_tables(path):

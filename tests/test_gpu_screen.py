@@ -35,9 +35,9 @@ def runs():
     cid = ctx.add_complex("dna", c0["rec"], c0["lig"])
     pos = synth.setup_poses(c0["rec"]["coords"], SWARMS, GLOW, 3)
     out = {}
-    for mode in ("plain", "screened", "ablation"):
-        g = lkg.GSO(ctx, [(cid, SWARMS, GLOW)], pos, [3])
-        if mode != "plain":
+    for mode in ("plain", "screened", "ablation", "plain_next_seed"):
+        g = lkg.GSO(ctx, [(cid, SWARMS, GLOW)], pos, [4 if mode == "plain_next_seed" else 3])
+        if mode in ("screened", "ablation"):
             g.set_screen(candidates=4, exact_fraction=0.25, rescore_every=10, train_steps=10, train_epochs=40,
                          finetune_epochs=2, lr=1e-3, seed=5, random_rank=(mode == "ablation"))
         g.run(STEPS)
@@ -125,11 +125,23 @@ def test_network_picks_better_moves_than_the_same_choice_without_it():
     assert precision > 0.35
 
 
-def test_top5_overlap_with_plain_run_is_reported(runs):
-    p, s = runs["plain"]["state"], runs["screened"]["state"]
+def _overlaps(runs, mode):
+    p, s = runs["plain"]["state"], runs[mode]["state"]
     ov = []
     for k in range(SWARMS):
         sl = slice(k * GLOW, (k + 1) * GLOW)
         ov.append(top5_overlap(s["translation"][sl], s["scoring"][sl], p["translation"][sl], p["scoring"][sl]))
-    print("top-5 overlap per swarm", ov)
-    assert all(0.0 <= o <= 1.0 for o in ov)
+    return np.array(ov)
+
+
+def test_top5_overlap_with_plain_run_against_the_gso_floor(runs):
+    # a screened run draws its own random stream (K candidates per
+    # glowworm), so its top-5 overlap with the plain run is bounded by what
+    # two plain runs with different GSO seeds reach: the floor.  The
+    # screened run must stay within 0.35 of that floor (mean over the
+    # swarms) and find at least one of the plain run's top-5 poses
+    scr, floor, abl = _overlaps(runs, "screened"), _overlaps(runs, "plain_next_seed"), _overlaps(runs, "ablation")
+    print("top-5 overlap with the plain run, per swarm: screened %s, ablation %s, plain with the next seed %s"
+          % (scr.tolist(), abl.tolist(), floor.tolist()))
+    assert scr.mean() >= floor.mean() - 0.35
+    assert scr.max() > 0.0

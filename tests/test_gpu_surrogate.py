@@ -113,8 +113,9 @@ def test_online_training_learns_exact_energies(sur):
 
 @pytest.mark.parametrize("n", [100, 1000, 4096])
 def test_tcgen05_forward_matches_mma_sync_and_the_oracle(sur, n):
-    # the forward layers and the backward-data products on tcgen05 (TMA-fed,
-    # TMEM accumulators) against the mma.sync kernels and the FP64 oracle
+    # the forward layers, the backward-data products and the weight
+    # gradients (MN-major operands) on tcgen05 (TMA-fed, TMEM accumulators)
+    # against the mma.sync kernels and the FP64 oracle
     _, _, s = sur
     rng = np.random.default_rng(100 + n)
     p = omlp.he_params(7 + n)
