@@ -279,7 +279,64 @@ def run_reference(args, rank, world):
             "cpu_baseline": {"value": v, "unit": "poses/s", "cores": r["cores"], "kind": "port",
                              "sample": r["sample"] + " per step (median of %d steps)" % args.steps},
             "e2e": {"value": v, "unit": "poses/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    ref_gpu = reference_cuda_per_swarm(items, models)
+    if ref_gpu:
+        line["reference_cuda_kernel"] = ref_gpu
     print(json.dumps(line), flush=True)
+
+
+# cuda_batch_score (full_score.cu:359-371) as the reference's Rust bridge binds it
+_REF_SIG = ("PiiiffffPPPPPiPPiiiffffPPPPPPiiIP")
+
+
+def reference_cuda_per_swarm(items, models):
+    """The reference's own GPU scorer, src/cuda/full_score.cu compiled
+    unmodified for sm_100a (oracle/_ref, built where the reference tree is
+    present), called the way the reference's GSO calls it: one
+    cuda_batch_score per swarm and step (swarm.rs:70-100, gpu_family.rs:
+    196-262), host buffers, on every swarm of the workload, each complex's
+    first call (the upload into its buffer cache) untimed.  The far field
+    is the oracle's grid (bitwise the reference builder's), in place.
+    None when there is no CUDA device or the library was not built."""
+    import ctypes as C
+    path = os.path.join(REPO, "oracle", "_ref", "libref_cuda.so")
+    try:
+        import torch
+        if not torch.cuda.is_available() or not os.path.exists(path):
+            return None
+    except ImportError:
+        return None
+    compat = importlib.import_module("lklight-gpu_b200.compat")
+    L = C.CDLL(path)
+    T = {"P": C.c_void_p, "i": C.c_int, "f": C.c_float, "I": C.c_uint}
+    L.cuda_batch_score.argtypes = [T[ch] for ch in _REF_SIG]
+    L.cuda_batch_score.restype = C.c_int
+    flags = {"dna": 7, "pydock": 3}   # full_score.cu:21-22, gpu_family.rs:187-194
+    keep, t_total, poses_done, calls = [], 0.0, 0, 0
+    for it, m in zip(items, models):
+        if it["family"] not in flags:
+            return None
+        rec, lig = it["rec"], it["lig"]
+        crec = compat.CudaReceptor(rec["coords"], rec["ele"], np.sqrt(rec["vdw"]), rec["radius"], rec["heavy"])
+        clig = compat.CudaLigand(lig["coords"], lig["ele"], np.sqrt(lig["vdw"]), lig["radius"], lig["heavy"])
+        f = m.field()
+        field = dict(phi=f.phi_view(), dims=f.dims, origin=f.origin, spacing=f.spacing)
+        # the reference caches device copies by host pointer: every complex's
+        # arrays stay alive (and so at distinct addresses) until the end
+        keep.append((crec, clig, f, field))
+        g = it["glowworms"]
+        pos = it["poses"]
+        compat.batch_raw(field, crec, clig, pos[:g], flags[it["family"]], library=L)
+        t0 = time.perf_counter()
+        for s in range(it["swarms"]):
+            compat.batch_raw(field, crec, clig, pos[s * g:(s + 1) * g], flags[it["family"]], library=L)
+        t_total += time.perf_counter() - t0
+        poses_done += it["swarms"] * g
+        calls += it["swarms"]
+    return {"value": poses_done / t_total, "unit": "poses/s", "calls": calls, "poses_per_call": items[0]["glowworms"],
+            "seconds": t_total,
+            "what": "the reference's src/cuda/full_score.cu compiled unmodified for sm_100a, one cuda_batch_score per "
+                    "swarm (as its GSO calls it), host buffers, every swarm of the workload once, buffer cache warm"}
 
 
 def pick_shape(args, items, local):

@@ -157,6 +157,12 @@ int lkg_ctx_set_group(lkg_ctx* ctx, int group);
  * complexes with groups of 32): the near scan trims each (z, y) cell row to
  * the 10 A sphere at this finer x resolution; fixed once complexes exist. */
 int lkg_ctx_set_xsub(lkg_ctx* ctx, int xsub);
+/* No counterpart in the reference (its cell list, gpu_score.rs:75-144, is
+ * built on the host).  Where complex set-up sorts the receptor into its cell
+ * grid and packs the sorted device arrays: 1 = on the GPU (the default:
+ * counting sort, stable inside each cell), 0 = on the host.  Both give the
+ * same arrays bit for bit; the host build is kept as the check. */
+int lkg_ctx_set_setup(lkg_ctx* ctx, int on_device);
 /* Work on this CUDA stream (cudaStream_t) instead of the context's own. */
 int lkg_ctx_set_stream(lkg_ctx* ctx, void* stream);
 void* lkg_ctx_stream(lkg_ctx* ctx);

@@ -80,7 +80,9 @@ cudaError_t upload(DBuf& b, const std::vector<T>& v, cudaStream_t s) {
     return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
 }
 
-// receptor: sort by fine cell (x fastest), pack device arrays
+// receptor: sort by fine cell (x fastest), pack device arrays; the sort and
+// packing run on the GPU (lkg_cells.cu) unless the context asks for the
+// host build
 int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     ComplexDev& d = cr.d;
     const int n = R.n;
@@ -110,40 +112,46 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     }
     const size_t ncell = (size_t)nc[0] * nc[1] * nc[2];
     if (ncell > (size_t)1 << 28) return set_error(LKG_ERR_ARG, "receptor cell grid too large (%zu cells)", ncell);
-    std::vector<int> cell_of(n), cs(ncell + 1, 0);
-    for (int i = 0; i < n; ++i) {
-        int ci[3];
-        for (int a = 0; a < 3; ++a)
-            ci[a] = std::min(std::max((int)std::floor(((float)R.c[3 * i + a] - o[a]) * inv_e[a]), 0), nc[a] - 1);
-        cell_of[i] = (ci[2] * nc[1] + ci[1]) * nc[0] + ci[0];
-        cs[cell_of[i] + 1]++;
+    if (ctx->setup_on_device) {
+        const int st = build_receptor_device(ctx, R, cr, o, nc, inv_e);
+        if (st) return st;
+    } else {
+        // the host counting sort (the check of the device build)
+        std::vector<int> cell_of(n), cs(ncell + 1, 0);
+        for (int i = 0; i < n; ++i) {
+            int ci[3];
+            for (int a = 0; a < 3; ++a)
+                ci[a] = std::min(std::max((int)std::floor(((float)R.c[3 * i + a] - o[a]) * inv_e[a]), 0), nc[a] - 1);
+            cell_of[i] = (ci[2] * nc[1] + ci[1]) * nc[0] + ci[0];
+            cs[cell_of[i] + 1]++;
+        }
+        for (size_t k = 0; k < ncell; ++k) cs[k + 1] += cs[k];
+        std::vector<int> cur(cs.begin(), cs.end() - 1), order(n);
+        for (int i = 0; i < n; ++i) order[cur[cell_of[i]]++] = i;
+        std::vector<float4> pos(n), par(n);
+        std::vector<float2> sol(n);
+        std::vector<double4> pos64(n), par64(n);
+        std::vector<double2> sol64(n);
+        for (int k = 0; k < n; ++k) {
+            int i = order[k];
+            pos[k] = make_float4((float)R.c[3 * i], (float)R.c[3 * i + 1], (float)R.c[3 * i + 2], (float)R.q[i]);
+            par[k] = make_float4((float)R.svdw[i], (float)R.rad[i], R.heavy[i] ? 1.f : 0.f, R.excl[i] ? 1.f : 0.f);
+            sol[k] = make_float2((float)R.des[i], (float)R.asa[i]);
+            pos64[k] = make_double4(R.c[3 * i], R.c[3 * i + 1], R.c[3 * i + 2], R.q[i]);
+            par64[k] = make_double4(R.svdw[i], R.rad[i], R.eps[i], R.heavy[i] ? 1.0 : 0.0);
+            sol64[k] = make_double2(R.des[i], R.asa[i]);
+        }
+        cudaStream_t s = ctx->stream;
+        LKG_CK(upload(cr.rpos, pos, s), "upload receptor");
+        LKG_CK(upload(cr.rpar, par, s), "upload receptor");
+        LKG_CK(upload(cr.rsolv, sol, s), "upload receptor");
+        LKG_CK(upload(cr.rpos64, pos64, s), "upload receptor");
+        LKG_CK(upload(cr.rpar64, par64, s), "upload receptor");
+        LKG_CK(upload(cr.rsolv64, sol64, s), "upload receptor");
+        LKG_CK(upload(cr.rorig, order, s), "upload receptor");
+        LKG_CK(upload(cr.cell_start, cs, s), "upload receptor");
+        LKG_CK(cudaStreamSynchronize(s), "upload receptor");
     }
-    for (size_t k = 0; k < ncell; ++k) cs[k + 1] += cs[k];
-    std::vector<int> cur(cs.begin(), cs.end() - 1), order(n);
-    for (int i = 0; i < n; ++i) order[cur[cell_of[i]]++] = i;
-    std::vector<float4> pos(n), par(n);
-    std::vector<float2> sol(n);
-    std::vector<double4> pos64(n), par64(n);
-    std::vector<double2> sol64(n);
-    for (int k = 0; k < n; ++k) {
-        int i = order[k];
-        pos[k] = make_float4((float)R.c[3 * i], (float)R.c[3 * i + 1], (float)R.c[3 * i + 2], (float)R.q[i]);
-        par[k] = make_float4((float)R.svdw[i], (float)R.rad[i], R.heavy[i] ? 1.f : 0.f, R.excl[i] ? 1.f : 0.f);
-        sol[k] = make_float2((float)R.des[i], (float)R.asa[i]);
-        pos64[k] = make_double4(R.c[3 * i], R.c[3 * i + 1], R.c[3 * i + 2], R.q[i]);
-        par64[k] = make_double4(R.svdw[i], R.rad[i], R.eps[i], R.heavy[i] ? 1.0 : 0.0);
-        sol64[k] = make_double2(R.des[i], R.asa[i]);
-    }
-    cudaStream_t s = ctx->stream;
-    LKG_CK(upload(cr.rpos, pos, s), "upload receptor");
-    LKG_CK(upload(cr.rpar, par, s), "upload receptor");
-    LKG_CK(upload(cr.rsolv, sol, s), "upload receptor");
-    LKG_CK(upload(cr.rpos64, pos64, s), "upload receptor");
-    LKG_CK(upload(cr.rpar64, par64, s), "upload receptor");
-    LKG_CK(upload(cr.rsolv64, sol64, s), "upload receptor");
-    LKG_CK(upload(cr.rorig, order, s), "upload receptor");
-    LKG_CK(upload(cr.cell_start, cs, s), "upload receptor");
-    LKG_CK(cudaStreamSynchronize(s), "upload receptor");
     d.nr = n;
     d.rpos = cr.rpos.as<float4>(); d.rpar = cr.rpar.as<float4>(); d.rsolv = cr.rsolv.as<float2>();
     d.rpos64 = cr.rpos64.as<double4>(); d.rpar64 = cr.rpar64.as<double4>(); d.rsolv64 = cr.rsolv64.as<double2>();
@@ -745,6 +753,12 @@ int lkg_ctx_set_xsub(lkg_ctx* ctx, int xsub) {
     if (xsub < 1 || xsub > 8) return set_error(LKG_ERR_ARG, "xsub must be 1..8");
     if (!ctx->cx.empty() && xsub != ctx->xsub) return set_error(LKG_ERR_STATE, "xsub fixed once complexes exist");
     ctx->xsub = xsub;
+    return set_ok();
+}
+
+int lkg_ctx_set_setup(lkg_ctx* ctx, int on_device) {
+    if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
+    ctx->setup_on_device = on_device != 0;
     return set_ok();
 }
 

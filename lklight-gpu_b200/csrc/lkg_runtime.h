@@ -143,6 +143,7 @@ struct lkg_ctx {
     int64_t launches = 0;
     lkg::Occupancy occ_tiles[2], occ_desolv[2];
     bool noalloc_used = false;      // lkg_score_device_noalloc ran on this context (its status word is checked)
+    bool setup_on_device = true;    // receptor cell sort and packing on the GPU (false: the host build)
 };
 
 namespace lkg {
@@ -151,6 +152,10 @@ namespace lkg {
 int complex_create(lkg_ctx* ctx, int family, unsigned flags, int lj_form, const MolIn& rec,
                    const MolIn& lig, const lkg_field* field, bool build_field, double solv_const,
                    int* out_id);
+// the receptor's cell-sorted arrays and cell_start built on the GPU
+// (lkg_cells.cu), bit for bit the host build's
+int build_receptor_device(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr, const float o[3], const int nc[3],
+                          const float inv_e[3]);
 // replace the ligand of an existing complex (cuda_full_score)
 int complex_set_ligand(lkg_ctx* ctx, int id, const MolIn& lig);
 // a complex changed: descriptors to upload, captured graphs out of date

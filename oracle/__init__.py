@@ -151,6 +151,13 @@ class Field:
         ptr = lib().orc_field_phi32(self.h)
         return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float)), (n,)).copy()
 
+    def phi_view(self):
+        """The f32 grid in place (no copy): valid while this field (or the
+        model that owns it) lives."""
+        n = int(np.prod(self.dims))
+        ptr = lib().orc_field_phi32(self.h)
+        return np.ctypeslib.as_array(C.cast(ptr, C.POINTER(C.c_float)), (n,))
+
     def sample(self, x, y, z):
         return lib().orc_field_sample(self.h, x, y, z)
 

@@ -356,3 +356,30 @@ def test_gso_config0_fast_mode_against_oracle_reported():
     ref = m.batch_energy_grid(np.hstack([fin["rotation"], fin["translation"]]))
     assert rel_err(fin["scoring"], ref).max() < FAST_TOL
     assert 0.0 <= overlap <= 1.0
+
+
+@pytest.mark.parametrize("which", ["azp_dna", "config0_dna", "config0_cpydock", "small_shape"])
+def test_receptor_setup_on_gpu_equals_host_build(which):
+    # the receptor's cell sort and packing run on the GPU by default; the
+    # host build is the check: the same poses must score to the same bits
+    # (the summation order follows the receptor order, so any difference in
+    # the sort would show), with the same near-pair counts and desolvation
+    if which == "azp_dna":
+        fam, (rec, lig), kw = "dna", azp_model("dna"), {}
+        poses = _azp_poses(32, 4)
+    elif which == "small_shape":
+        fam, (rec, lig), kw = "pydock", azp_model("pydock"), dict(tile=64, group=4, xsub=2, cell=2.5)
+        poses = _azp_poses(32, 6)
+    else:
+        c = config0_cpydock() if which == "config0_cpydock" else config0()
+        fam, rec, lig, kw = ("cpydock" if which == "config0_cpydock" else "dna"), c["rec"], c["lig"], {}
+        poses = synth.to_kernel_poses(synth.setup_poses(rec["coords"], 2, 40, 13))
+    out = []
+    for host in (False, True):
+        ctx = lkg.Context(host_setup=host, **kw)
+        try:
+            out.append(ctx.score(ctx.add_complex(fam, rec, lig), poses, parts=True))
+        finally:
+            ctx.close()
+    (a, pa), (b, pb) = out
+    assert np.array_equal(a, b) and np.array_equal(pa, pb)
