@@ -63,6 +63,9 @@ def parse():
     ap.add_argument("--group", type=int, default=0)
     ap.add_argument("--xsub", type=int, default=0)
     ap.add_argument("--no-graph", action="store_true")
+    ap.add_argument("--stage", default="l1", choices=["l1", "tma"],
+                    help="how the plain kernel loads candidate receptor atoms: through L1 (default) or staged in "
+                         "shared memory by bulk copies")
     ap.add_argument("--no-autotune", action="store_true")
     ap.add_argument("--gso-steps", type=int, default=200)
     ap.add_argument("--seeds", type=int, default=1,
@@ -376,7 +379,8 @@ def main():
     if args.complexes:
         items = items[:args.complexes]
     shape = pick_shape(args, items, local)
-    ctx = lkg.Context(device=local, tile=shape["tile"], cell=shape["cell"], group=shape["group"], xsub=shape["xsub"])
+    ctx = lkg.Context(device=local, tile=shape["tile"], cell=shape["cell"], group=shape["group"], xsub=shape["xsub"],
+                      stage=args.stage)
     stream = torch.cuda.ExternalStream(ctx.stream)
     ids = [ctx.add_complex(it["family"], it["rec"], it["lig"]) for it in items]
     for cid, it in zip(ids, items):
@@ -548,7 +552,8 @@ def main():
                     "h2d_bytes_per_step": npose * 7 * 8, "d2h_bytes_per_step": npose * 8,
                     "api": "lkg_score_multi (host page-locked buffers)"},
             "gpu_launches": int(launches), "clocks": clk,
-            "step": "CUDA graph replay of one persistent launch group" if not args.no_graph else "plan launch"}
+            "step": "CUDA graph replay of one persistent launch group" if not args.no_graph else "plan launch",
+            "candidate_loads": args.stage}
     if plain:
         line["plain_single_complex"] = plain
     if gso_loop:

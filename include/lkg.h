@@ -163,6 +163,15 @@ int lkg_ctx_set_xsub(lkg_ctx* ctx, int xsub);
  * counting sort, stable inside each cell), 0 = on the host.  Both give the
  * same arrays bit for bit; the host build is kept as the check. */
 int lkg_ctx_set_setup(lkg_ctx* ctx, int on_device);
+/* No counterpart in the reference (it reads receptor atoms one thread per
+ * ligand atom, full_score.cu:279-319).  How the plain warp kernel brings the
+ * receptor atoms of its candidate row spans in: 0 (default) = coalesced
+ * float4 loads through L1, the next chunk of 32 fetched while the current
+ * one is tested; 1 = windows of 64 atoms copied into shared memory by bulk
+ * copies (cp.async.bulk, one per row span and window, completing on a
+ * per-warp mbarrier).  Same scores bit for bit; kept as the measured
+ * alternative. */
+int lkg_ctx_set_staging(lkg_ctx* ctx, int tma);
 /* Work on this CUDA stream (cudaStream_t) instead of the context's own. */
 int lkg_ctx_set_stream(lkg_ctx* ctx, void* stream);
 void* lkg_ctx_stream(lkg_ctx* ctx);

@@ -71,7 +71,7 @@ def lib():
         "lkg_version": (C.c_char_p, []),
         "lkg_ctx_create": (I, [I, P]), "lkg_ctx_destroy": (I, [P]),
         "lkg_ctx_set_precision": (I, [P, I]), "lkg_ctx_set_tiles": (I, [P, I, I]),
-        "lkg_ctx_set_stream": (I, [P, P]), "lkg_ctx_set_setup": (I, [P, I]), "lkg_ctx_set_group": (I, [P, I]), "lkg_ctx_set_xsub": (I, [P, I]), "lkg_ctx_stream": (P, [P]), "lkg_ctx_launches": (I64, [P]),
+        "lkg_ctx_set_stream": (I, [P, P]), "lkg_ctx_set_setup": (I, [P, I]), "lkg_ctx_set_staging": (I, [P, I]), "lkg_ctx_set_group": (I, [P, I]), "lkg_ctx_set_xsub": (I, [P, I]), "lkg_ctx_stream": (P, [P]), "lkg_ctx_launches": (I64, [P]),
         "lkg_complex_add": (I, [P, I, P, P, P, P]), "lkg_complex_info": (I, [P, I, P, P, P]),
         "lkg_score": (I, [P, I, I, P, P, P]), "lkg_score_device": (I, [P, I, I, P, P, P]),
         "lkg_score_interface": (I, [P, I, I, P, P, P]),
@@ -159,15 +159,20 @@ class Screen(C.Structure):
 class Context:
     """A device context: resident complexes, a stream, scratch buffers."""
 
-    def __init__(self, device=0, precision="fast", tile=0, cell=0.0, group=0, xsub=0, host_setup=False):
+    def __init__(self, device=0, precision="fast", tile=0, cell=0.0, group=0, xsub=0, host_setup=False,
+                 stage="l1"):
         """host_setup: sort and pack receptors on the host instead of the
-        GPU (the same arrays; the check of the GPU set-up)."""
+        GPU (the same arrays; the check of the GPU set-up).  stage: "l1"
+        (default) or "tma": how the plain kernel loads candidate receptor
+        atoms (lkg_ctx_set_staging)."""
         h = C.c_void_p()
         _check(lib().lkg_ctx_create(device, C.byref(h)))
         self.h = h
         self._keep = []
         if host_setup:
             _check(lib().lkg_ctx_set_setup(self.h, 0))
+        if stage != "l1":
+            _check(lib().lkg_ctx_set_staging(self.h, 1 if stage == "tma" else 0))
         if precision != "fast":
             _check(lib().lkg_ctx_set_precision(self.h, PREC_EXACT if precision == "exact" else PREC_FAST))
         if tile or cell:

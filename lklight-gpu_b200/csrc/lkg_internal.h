@@ -117,6 +117,8 @@ struct LaunchParams {
     // (SPILL_SLOT_BYTES each), all slots empty between poses; null: none
     unsigned char* spill;
     int spill_cap;
+    // plain warp kernel: stage candidates in shared memory by bulk copies
+    int stage;
 };
 
 // bytes per spill slot: the exact kernel's 8-byte value + 4-byte key (the

@@ -6,21 +6,26 @@ namespace lkg {
 // warp-independent kernel for scores; the per-thread kernel when per-atom
 // outputs are requested (cuda_full_score)
 template <int G>
-static size_t warp_smem() { return (size_t)(WK_THREADS / 32) * sizeof(WSlots<G>); }
+static size_t warp_smem(bool stage = false) {
+    return (size_t)(WK_THREADS / 32) * (sizeof(WSlots<G>) + (stage ? sizeof(WStage) : 0));
+}
 
 // IFACE: the variant that also collects the interface bits (launches with
-// restraint or membrane complexes)
-template <int G, bool IFACE>
+// restraint or membrane complexes); STAGE: candidates staged in shared
+// memory by bulk copies (contexts that ask for it)
+template <int G, bool IFACE, bool STAGE>
 static cudaError_t launch_warp_gi(const LaunchParams& p, int blocks, cudaStream_t s) {
-    const size_t sm = warp_smem<G>();
-    cudaError_t e = cudaFuncSetAttribute(k_score_warp<G, IFACE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    const size_t sm = warp_smem<G>(STAGE);
+    cudaError_t e = cudaFuncSetAttribute(k_score_warp<G, IFACE, STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sm);
     if (e != cudaSuccess) return e;
-    k_score_warp<G, IFACE><<<blocks, WK_THREADS, sm, s>>>(p);
+    k_score_warp<G, IFACE, STAGE><<<blocks, WK_THREADS, sm, s>>>(p);
     return cudaGetLastError();
 }
 template <int G>
 static cudaError_t launch_warp_g(const LaunchParams& p, int blocks, cudaStream_t s) {
-    return p.iface ? launch_warp_gi<G, true>(p, blocks, s) : launch_warp_gi<G, false>(p, blocks, s);
+    if (p.iface) return launch_warp_gi<G, true, false>(p, blocks, s);
+    return p.stage ? launch_warp_gi<G, false, true>(p, blocks, s) : launch_warp_gi<G, false, false>(p, blocks, s);
 }
 
 cudaError_t launch_score_fast(const LaunchParams& p, int threads, int blocks, cudaStream_t s) {

@@ -553,6 +553,7 @@ int launch_group(lkg_ctx* ctx, const Group& G, const char* db, Scratch& sc, cons
     p.atom_elec = atom_e;
     p.atom_vdw = atom_v;
     p.pose_mask = pose_mask;
+    p.stage = ctx->stage_tma ? 1 : 0;
     for (int c : G.ic)   // restraints set after the groups were built (a plan made before)
         if (ctx->cx[c]->d.iface_words > G.iface_words)
             return set_error(LKG_ERR_STATE, "complex %d has restraints the prepared batch has no room for", c);
@@ -652,6 +653,10 @@ int check_status_word(int* d_status) {
     if (h[0] & 2) {
         cudaMemset(d_status, 0, sizeof(h));
         return set_error(LKG_ERR_STATE, "restraints or membrane set after the batch was prepared: prepare it again");
+    }
+    if (h[0] & 8) {
+        cudaMemset(d_status, 0, sizeof(h));
+        return set_error(LKG_ERR_TIMEOUT, "a staged candidate copy did not complete in time");
     }
     return set_ok();
 }
@@ -753,6 +758,12 @@ int lkg_ctx_set_xsub(lkg_ctx* ctx, int xsub) {
     if (xsub < 1 || xsub > 8) return set_error(LKG_ERR_ARG, "xsub must be 1..8");
     if (!ctx->cx.empty() && xsub != ctx->xsub) return set_error(LKG_ERR_STATE, "xsub fixed once complexes exist");
     ctx->xsub = xsub;
+    return set_ok();
+}
+
+int lkg_ctx_set_staging(lkg_ctx* ctx, int tma) {
+    if (!ctx) return set_error(LKG_ERR_ARG, "null ctx");
+    ctx->stage_tma = tma != 0;
     return set_ok();
 }
 

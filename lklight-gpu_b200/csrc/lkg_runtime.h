@@ -144,6 +144,7 @@ struct lkg_ctx {
     lkg::Occupancy occ_tiles[2], occ_desolv[2];
     bool noalloc_used = false;      // lkg_score_device_noalloc ran on this context (its status word is checked)
     bool setup_on_device = true;    // receptor cell sort and packing on the GPU (false: the host build)
+    bool stage_tma = false;         // plain warp kernel: candidates staged by bulk copies (measured alternative)
 };
 
 namespace lkg {

@@ -73,6 +73,32 @@ struct WSlots {
     unsigned hit[WRing<G>::N];  // (slot << 26) | receptor index, pending hits first
 };
 
+// Staged candidates (the plain kernel's TMA variant, selected per context):
+// a window of STAGE_WIN receptor atoms (their float4 positions) copied from
+// the row spans into shared memory by bulk copies (cp.async.bulk, no
+// multicast) that complete on the warp's mbarrier.
+constexpr int STAGE_WIN = 64;
+struct WStage {
+    float4 a[STAGE_WIN];
+    unsigned long long bar;
+    unsigned phase;   // parity of the barrier's current phase
+};
+
+__device__ __forceinline__ uint32_t w_smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// bounded wait for phase `parity` of the mbarrier at `bar` (false: ran out)
+__device__ __forceinline__ bool w_bar_wait(uint32_t bar, uint32_t parity) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred P1;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                     : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+        if (ok) return true;
+    }
+    return false;
+}
+
 // Receptor-side minima of the fast cpydock kernel: one 64-bit word per slot,
 // the minimum d^2 quantised to 37 bits (0 .. SOLV2_D in steps of 3e-10 A^2)
 // above the 27-bit receptor index, so one atomicMin updates a slot (the key
@@ -344,9 +370,9 @@ struct WAcc {
 // Scores groups g_first, g_first + g_step, ... (< g_end) of one pose whose
 // rotation is in W.rot, into acc (per lane).  DESOLV also adds each slot
 // atom's g(min d^2) * des to acc.solv once its hits are all evaluated.
-template <int G, bool DESOLV, bool IFACE>
+template <int G, bool DESOLV, bool IFACE, bool STAGE = false>
 __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes<G>* D, MinHash64* hash, int* status,
-                                         int g_first, int g_end, int g_step, WAcc& acc) {
+                                         int g_first, int g_end, int g_step, WAcc& acc, WStage* S = nullptr) {
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned flags = c.flags;
@@ -479,22 +505,16 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
             }
             const int total = __shfl_sync(FULL, inc, 31);
             const int excl = inc - len;
-            // 3. candidate chunks; the next chunk's receptor atoms are
-            //    fetched while the current one is tested
-            float4 an = make_float4(3e30f, 3e30f, 3e30f, 0.f);
-            int rn = 0;
-            if (total > 0) w_fetch(c, st, excl, total, lane, an, rn);
-            for (int k0 = 0; k0 < total; k0 += 32) {
-                const float4 a = an;
-                const int ridx = rn;
-                if (k0 + 32 < total) w_fetch(c, st, excl, total, k0 + 32 + lane, an, rn);
+            // 3. candidate chunks of 32: each lane tests its candidate
+            //    against the group's slots and appends its hits
+            auto chunk = [&](const float4 a, const int ridx) {
                 const float ax = a.x - gx, ay = a.y - gy, az = a.z - gz;
                 const float aa = ax * ax + ay * ay + az * az;
                 // cpydock kernel: a candidate farther than R = 10.001 + rho
                 // from the group centre is more than 10 A from every slot atom
                 // (|l'| <= rho), so a chunk with none closer is skipped (the
                 // test pays off there, not in the plain kernel)
-                if (DESOLV && !__any_sync(FULL, aa <= R2)) continue;
+                if (DESOLV && !__any_sync(FULL, aa <= R2)) return;
                 // the lane's candidate against every slot: a bit per hit
                 unsigned m = 0;
 #pragma unroll
@@ -515,7 +535,7 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
                     if (lane >= o) inc += v;
                 }
                 const int chunk_hits = __shfl_sync(FULL, inc, 31);
-                if (chunk_hits == 0) continue;
+                if (chunk_hits == 0) return;
                 unsigned* dst = W.hit + tail + (inc - nh);
                 const unsigned enc = (unsigned)ridx | enc_set;
 #pragma unroll
@@ -546,6 +566,61 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
                     tail = rem;
                     head = 0;
                 }
+            };
+            if (!STAGE) {
+                // the next chunk's receptor atoms are fetched (through L1)
+                // while the current one is tested
+                float4 an = make_float4(3e30f, 3e30f, 3e30f, 0.f);
+                int rn = 0;
+                if (total > 0) w_fetch(c, st, excl, total, lane, an, rn);
+                for (int k0 = 0; k0 < total; k0 += 32) {
+                    const float4 a = an;
+                    const int ridx = rn;
+                    if (k0 + 32 < total) w_fetch(c, st, excl, total, k0 + 32 + lane, an, rn);
+                    chunk(a, ridx);
+                }
+            } else {
+                // windows of STAGE_WIN candidates: every row span's part of
+                // the window is bulk-copied into shared memory by its lane
+                const uint32_t bar = w_smem_u32(&S->bar);
+                for (int w0 = 0; w0 < total; w0 += STAGE_WIN) {
+                    const int wn = min(STAGE_WIN, total - w0);
+                    const int lo = max(excl, w0), hi = min(excl + len, w0 + wn);
+                    __syncwarp();   // the previous window is read
+                    if (lane == 0)
+                        asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                                     :: "r"(bar), "r"((uint32_t)wn * 16u) : "memory");
+                    __syncwarp();
+                    if (hi > lo) {
+                        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+                        asm volatile(
+                            "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                            :: "r"(w_smem_u32(S->a + (lo - w0))),
+                               "l"(reinterpret_cast<uint64_t>(c.rpos + st + (lo - excl))),
+                               "r"((uint32_t)(hi - lo) * 16u), "r"(bar) : "memory");
+                    }
+                    const unsigned ph = S->phase;
+                    if (!w_bar_wait(bar, ph)) {
+                        // ran out: report, and wait (bounded again) for the copies in flight
+                        if (lane == 0) atomicOr(status, 8);
+                        w_bar_wait(bar, ph);
+                    }
+                    __syncwarp();
+                    if (lane == 0) S->phase = ph ^ 1u;
+                    __syncwarp();
+                    for (int k0 = w0; k0 < w0 + wn; k0 += 32) {
+                        const int kk = k0 + lane;
+                        int rr = 0;
+#pragma unroll
+                        for (int sft = 16; sft > 0; sft >>= 1) {
+                            const int v = __shfl_sync(FULL, excl, rr + sft);
+                            if (v <= kk) rr += sft;
+                        }
+                        const int ridx = __shfl_sync(FULL, st, rr) + (kk - __shfl_sync(FULL, excl, rr));
+                        const float4 a = kk < w0 + wn ? S->a[kk - w0] : make_float4(3e30f, 3e30f, 3e30f, 0.f);
+                        chunk(a, ridx);
+                    }
+                }
             }
         }
     }
@@ -556,13 +631,26 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
     finalize(G);
 }
 
-template <int G, bool IFACE>
+// STAGE: the candidates reach shared memory by bulk copies (WStage) instead
+// of L1 loads (selected per context; the measured alternative)
+template <int G, bool IFACE, bool STAGE = false>
 __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchParams p) {
     static_assert(G == 4 || G == 8 || G == 16 || G == 32, "group size");
+    static_assert(!(STAGE && IFACE), "the staged variant is the plain kernel's");
     constexpr unsigned FULL = 0xffffffffu;
     extern __shared__ __align__(16) unsigned char wk_smem[];
     const int lane = threadIdx.x & 31;
     WSlots<G>& W = reinterpret_cast<WSlots<G>*>(wk_smem)[threadIdx.x >> 5];
+    WStage* S = STAGE ? reinterpret_cast<WStage*>(wk_smem + (WK_THREADS / 32) * sizeof(WSlots<G>)) + (threadIdx.x >> 5)
+                      : nullptr;
+    if (STAGE) {
+        if (lane == 0) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(w_smem_u32(&S->bar)), "r"(1));
+            asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+            S->phase = 0u;
+        }
+        __syncwarp();
+    }
     if (IFACE) W.ibuf[lane] = 0u;
     for (;;) {
         unsigned long long wq = 0;
@@ -586,7 +674,7 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
         const int gpt = p.tile / G;
         const int g0 = tile * gpt, g1 = min(g0 + gpt, (c.nl + G - 1) / G);
         WAcc acc;
-        w_groups<G, false, IFACE>(c, W, nullptr, nullptr, nullptr, g0, g1, 1, acc);
+        w_groups<G, false, IFACE, STAGE>(c, W, nullptr, nullptr, p.status, g0, g1, 1, acc, S);
         if (IFACE && W.ibits) {
             w_iface_flush(W, c);
             __threadfence();   // interface bits before the unit is published

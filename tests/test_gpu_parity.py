@@ -383,3 +383,25 @@ def test_receptor_setup_on_gpu_equals_host_build(which):
             ctx.close()
     (a, pa), (b, pb) = out
     assert np.array_equal(a, b) and np.array_equal(pa, pb)
+
+
+@pytest.mark.parametrize("group,cell", [(8, 6.0), (16, 4.0), (4, 2.5)])
+def test_tma_staged_candidates_equal_l1_loads(group, cell):
+    # the plain kernel's measured alternative: candidate receptor atoms copied
+    # into shared memory by bulk copies (64-atom windows, one copy per row
+    # span) instead of loaded through L1 -- the same candidates in the same
+    # order, so the same bits; and both hold the oracle's 1e-5
+    c0 = config0()
+    pos = synth.to_kernel_poses(synth.setup_poses(c0["rec"]["coords"], 1, 200, 42))[:120]
+    out = []
+    for stage in ("l1", "tma"):
+        c = lkg.Context(tile=128, group=group, xsub=8, cell=cell, stage=stage)
+        try:
+            out.append(c.score(c.add_complex("dna", c0["rec"], c0["lig"]), pos, parts=True))
+            c.sync()
+        finally:
+            c.close()
+    (a, pa), (b, pb) = out
+    assert np.array_equal(a, b) and np.array_equal(pa, pb)
+    ref = oracle.Model("dna", c0["rec"], c0["lig"]).batch_energy_grid(pos)
+    assert rel_err(b, ref).max() < FAST_TOL
