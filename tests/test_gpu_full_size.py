@@ -12,8 +12,10 @@
 * the config-1 vdw and pydock runs on the config-0 complex (6 x 300 poses)
   against the oracle, every pose.
 The FP64 evaluation accumulates and stores the far field in f64 (the
-reference's grid path stores it in f32); on these complexes the two differ
-by < 4e-8 relative, so both comparisons hold the same 1e-5 budget.
+reference's grid path stores it in f32); on the batched workload's
+complexes the two differ by < 4e-8 relative, on the config-4 complex (every
+ligand atom charged) by ~2e-7, so the fast path holds the same 1e-5 budget
+against both.
 """
 import numpy as np
 import pytest
@@ -172,7 +174,11 @@ def test_cpydock_large_complex_against_oracle_and_fp64():
         assert np.all(np.abs(parts[sel, 3] - rparts[:, 4]) <= 2)   # f32 boundary cases only
         assert np.abs(parts[sel, 2] - rparts[:, 3]).max() < 1e-9 * max(1.0, np.abs(rparts[:, 3]).max())
         assert e_fast < FAST_TOL and e_fast64 < FAST_TOL
-        assert e_ex < 1e-11 and e_ex64 < 1e-7
+        # all 12k ligand atoms are charged here, so the far field weighs more
+        # than on the batched workload: the oracle's f32 grid and its FP64
+        # grid differ by ~2e-7 relative, and the exact path follows the f32
+        # grid (the reference's) to 1e-11
+        assert e_ex < 1e-11 and e_ex64 < 1e-6
     finally:
         ctx.close()
         ctx_x.close()

@@ -64,9 +64,12 @@ def test_noalloc_matches_regular_entry_point_on_two_calls():
         assert np.all(np.isfinite(got))
         assert rel_err(got, ref_h).max() < TOL
         if call:
+            # the parts are the score's terms (score = -(83 elec + vdW)): each
+            # must agree within the fast path's budget of the score
             p = parts.cpu().numpy()
-            assert rel_err(p[:, 0] * 83.0, ref_parts_h[:, 0] * 83.0).max() < TOL   # raw electrostatics
-            assert rel_err(p[:, 1], ref_parts_h[:, 1]).max() < TOL                  # LJ + clash
+            scale = np.maximum(np.abs(ref_h), 1.0)
+            assert (np.abs(p[:, 0] - ref_parts_h[:, 0]) * 83.0 / scale).max() < TOL   # raw electrostatics
+            assert (np.abs(p[:, 1] - ref_parts_h[:, 1]) / scale).max() < TOL          # LJ + clash
             assert np.all(np.abs(p[:, 3] - ref_parts_h[:, 3]) <= 2)                 # near pairs
         else:
             # the reference's CPU grid path on the same poses
