@@ -119,6 +119,9 @@ struct LaunchParams {
     int spill_cap;
     // plain warp kernel: stage candidates in shared memory by bulk copies
     int stage;
+    // [N] far-field term of each pose from k_far_poses (fast cpydock
+    // launch groups), added to the pose's electrostatics; null: inline
+    double* far;
 };
 
 // bytes per spill slot: the exact kernel's 8-byte value + 4-byte key (the
@@ -142,6 +145,8 @@ cudaError_t launch_score_fast(const LaunchParams& p, int threads, int blocks, cu
 cudaError_t launch_desolv_fast(const LaunchParams& p, int threads, int blocks, int hcap, cudaStream_t s);
 cudaError_t launch_score_exact(const LaunchParams& p, int threads, int blocks, cudaStream_t s);
 cudaError_t launch_desolv_exact(const LaunchParams& p, int threads, int blocks, int hcap, cudaStream_t s);
+// the far-field pass of a fast cpydock launch group (fills p.far)
+cudaError_t launch_far_poses(const LaunchParams& p, int blocks, cudaStream_t s);
 size_t desolv_smem_bytes(int hcap, bool exact);
 
 // GPU far-field builder (lkg_field.cu), bit-identical to the reference's

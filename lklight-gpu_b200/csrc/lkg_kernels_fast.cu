@@ -70,6 +70,11 @@ static cudaError_t launch_warp_desolv_g(const LaunchParams& p, int blocks, int h
                    : launch_warp_desolv_gi<G, false>(p, blocks, hcap, s);
 }
 
+cudaError_t launch_far_poses(const LaunchParams& p, int blocks, cudaStream_t s) {
+    k_far_poses<<<blocks, FAR_THREADS, 0, s>>>(p);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_desolv_fast(const LaunchParams& p, int threads, int blocks, int hcap, cudaStream_t s) {
     switch (p.group) {
         case 4: return launch_warp_desolv_g<4>(p, blocks, hcap, s);

@@ -450,6 +450,7 @@ cudaError_t Scratch::ensure(size_t units, size_t poses, cudaStream_t s, size_t i
         if ((e = cudaStreamSynchronize(s)) != cudaSuccess) return e;
         poses = std::max<size_t>(poses, 1024);
         if ((e = pose_counter.reserve(poses * sizeof(int))) != cudaSuccess) return e;
+        if ((e = far.reserve(poses * sizeof(double))) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(pose_counter.p, 0, poses * sizeof(int), s)) != cudaSuccess) return e;
         cap_poses = poses;
     }
@@ -583,6 +584,15 @@ int launch_group(lkg_ctx* ctx, const Group& G, const char* db, Scratch& sc, cons
         }
         p.spill = sc.spill.as<unsigned char>();
         p.spill_cap = G.spill_cap;
+        // the fast warp kernel (groups up to 16) takes the far field from a
+        // pass of its own (k_far_poses), launched first on the same stream
+        if (!exact && ctx->group <= 16 && !solv_only) {
+            p.far = sc.far.as<double>();
+            e = launch_far_poses(p, (int)std::min<long long>(p.total_work, (long long)ctx->sm_count * 8),
+                                 ctx->stream);
+            if (e != cudaSuccess) return set_error(cuda_to_status(e), "far-field launch: %s", cudaGetErrorString(e));
+            ctx->launches++;
+        }
         e = exact ? launch_desolv_exact(p, threads, (int)blocks, G.hcap, ctx->stream)
                   : launch_desolv_fast(p, threads, (int)blocks, G.hcap, ctx->stream);
     }

@@ -93,6 +93,7 @@ struct Occupancy { int threads = 0, hcap = 0, blocks = 0; };
 // counter and the status word (counters reset themselves after a launch)
 struct Scratch {
     DBuf partials, pose_counter, work_counter, status, iface;
+    DBuf far;   // [poses] far-field terms of the fast cpydock group
     size_t cap_units = 0, cap_poses = 0, cap_iface = 0;
     // desolvation spill tables (every slot empty between launches)
     DBuf spill;

@@ -157,6 +157,22 @@ __device__ __forceinline__ void scan_rows(const ComplexDev& c, float x, float y,
 // ------------------------------------------------------------------------
 // pair terms
 // ------------------------------------------------------------------------
+// The 10 A cutoff is the one discontinuity of the pair terms (a Coulomb
+// term there is up to ~0.5 kcal/mol), so a pair whose f32 d^2 lies within
+// NEAR_BAND of 100 is decided in f64, as the reference decides it: the slot
+// atom's f64 position (its f32 value + rounding residual, ~2^-48 relative)
+// against the receptor atom's f64 coordinates, without contraction.  The
+// compensated f32 d^2 is off by ~1e-5 A^2 at most, far inside the band.
+constexpr float NEAR_BAND = 1e-3f;
+__device__ __noinline__ bool near_exact(const ComplexDev& c, int k, float x, float xr, float y, float yr, float z,
+                                           float zr) {
+    const double4 a = c.rpos64[k];
+    const double dx = __dsub_rn(__dadd_rn((double)x, (double)xr), a.x);
+    const double dy = __dsub_rn(__dadd_rn((double)y, (double)yr), a.y);
+    const double dz = __dsub_rn(__dadd_rn((double)z, (double)zr), a.z);
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)) <= 100.0;
+}
+
 struct AtomAcc {
     double elec, vdw;   // per-atom sums
     int np;             // near pairs
@@ -346,11 +362,9 @@ template <> struct Atom<float> {
         float4 b = Tr<float>::lpos(c, j);
         float4 lp = Tr<float>::lpar(c, j);
         double xd, yd, zd;
-        if (DESOLV || ibits) {   // f64 base coordinates (exact distances for the minima / interface)
-            double4 b64 = c.lpos64[j];
+        {   // from the f64 base coordinates, as the reference transforms them
+            const double4 b64 = c.lpos64[j];
             apply(rot, b64.x, b64.y, b64.z, xd, yd, zd);
-        } else {
-            apply(rot, (double)b.x, (double)b.y, (double)b.z, xd, yd, zd);
         }
         // the f64 position as a float plus its rounding residual: x - a.x is
         // (nearly) exact for nearby atoms, so adding the residual keeps the
@@ -369,7 +383,8 @@ template <> struct Atom<float> {
             float4 a = Tr<float>::rpos(c, k);
             float dx = (x - a.x) + xl, dy = (y - a.y) + yl, dz = (z - a.z) + zl;
             float d2 = dx * dx + dy * dy + dz * dz;
-            if (d2 <= 100.f) {
+            const bool in = fabsf(d2 - 100.f) < NEAR_BAND ? near_exact(c, k, x, xl, y, yl, z, zl) : d2 <= 100.f;
+            if (in) {
                 float4 pr = Tr<float>::rpar(c, k);
                 ++np;
                 pair_fast(flags, qj, svj, rj, hj, a, pr, d2, elec, vdw);

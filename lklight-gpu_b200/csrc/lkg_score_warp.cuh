@@ -221,7 +221,9 @@ __device__ __forceinline__ void w_pair(const ComplexDev& c, const WSlots<G>& W, 
     const float2 lq = W.lpar[l];
     const float dx = (lp.x - a.x) + lr.x, dy = (lp.y - a.y) + lr.y, dz = (lp.z - a.z) + lr.z;
     const float d2 = dx * dx + dy * dy + dz * dz;
-    if (!(d2 <= 100.f)) return;
+    const bool in = fabsf(d2 - 100.f) < NEAR_BAND ? near_exact(c, k, lp.x, lr.x, lp.y, lr.y, lp.z, lr.z)
+                                                  : d2 <= 100.f;
+    if (!in) return;
     ++np;
     const float ir2 = rcp_approx(d2);
     if (flags & F_ELEC) {
@@ -309,7 +311,10 @@ __device__ __forceinline__ void w_pair2(const ComplexDev& c, const WSlots<G>& W,
     const F2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
     float d20, d21;
     f2_get(d2, d20, d21);
-    const bool ok0 = d20 <= 100.f, ok1 = v1 && d21 <= 100.f;
+    const bool ok0 = fabsf(d20 - 100.f) < NEAR_BAND ? near_exact(c, k0, lp0.x, lr0.x, lp0.y, lr0.y, lp0.z, lr0.z)
+                                                    : d20 <= 100.f;
+    const bool ok1 = v1 && (fabsf(d21 - 100.f) < NEAR_BAND ? near_exact(c, k1, lp1.x, lr1.x, lp1.y, lr1.y, lp1.z, lr1.z)
+                                                           : d21 <= 100.f);
     np += (int)ok0 + (int)ok1;
     const F2 ir2 = f2(rcp_approx(d20), rcp_approx(d21));
     if (flags & F_ELEC) {
@@ -372,7 +377,8 @@ struct WAcc {
 // atom's g(min d^2) * des to acc.solv once its hits are all evaluated.
 template <int G, bool DESOLV, bool IFACE, bool STAGE = false>
 __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes<G>* D, MinHash64* hash, int* status,
-                                         int g_first, int g_end, int g_step, WAcc& acc, WStage* S = nullptr) {
+                                         int g_first, int g_end, int g_step, WAcc& acc, WStage* S = nullptr,
+                                         bool far_sep = false) {
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
     const unsigned flags = c.flags;
@@ -423,18 +429,19 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
             const float4 b4 = valid ? __ldg(c.lpos + j) : make_float4(0.f, 0.f, 0.f, 0.f);
             const float4 lp4 = valid ? __ldg(c.lpar + j) : make_float4(0.f, 0.f, 0.f, 0.f);
             double xd, yd, zd;
-            if (DESOLV || IFACE) {   // f64 base coordinates (cpydock minima, interface flags)
+            {   // from the f64 base coordinates, as the reference transforms them
                 const double4 b64 = valid ? c.lpos64[j] : make_double4(0.0, 0.0, 0.0, 0.0);
                 apply(W.rot, b64.x, b64.y, b64.z, xd, yd, zd);
-            } else {
-                apply(W.rot, (double)b4.x, (double)b4.y, (double)b4.z, xd, yd, zd);
             }
             float x = (float)xd, y = (float)yd, z = (float)zd;
             const float4 res = make_float4((float)(xd - (double)x), (float)(yd - (double)y),
                                            (float)(zd - (double)z), lp4.x);
             // far field with the reference's f64 interpolation (a per-atom
             // cost; f32 here would add up over thousands of charged atoms)
-            if (valid && (flags & F_FAR) && b4.w != 0.f) acc.elec += c.lpos64[j].w * sample_phi(c, xd, yd, zd);
+            // (the cpydock kernel takes it from k_far_poses instead when
+            // that pass ran: far_sep)
+            if (valid && (flags & F_FAR) && !(DESOLV && far_sep) && b4.w != 0.f)
+                acc.elec += c.lpos64[j].w * sample_phi(c, xd, yd, zd);
             if (!valid) { x = y = z = 1e30f; }   // never within reach of a receptor atom
             W.lpos[set + lane] = make_float4(x, y, z, b4.w);
             W.lres[set + lane] = res;
@@ -753,7 +760,8 @@ __global__ void __launch_bounds__(WD_THREADS, WD_BLOCKS) k_score_warp_desolv(Lau
         }
         __syncthreads();   // hash cleared, poses set
         WAcc acc;
-        w_groups<G, true, IFACE>(c, W, D, &hash, p.status, wid, (c.nl + G - 1) / G, NW, acc);
+        w_groups<G, true, IFACE>(c, W, D, &hash, p.status, wid, (c.nl + G - 1) / G, NW, acc, nullptr,
+                                 p.far != nullptr);
         if (IFACE && W.ibits) w_iface_flush(W, c);   // before the block's barrier below
         __syncthreads();   // every pair has updated the hash
         // receptor side: fixed-point (2^-40) sum over hash slots; slot order
@@ -781,12 +789,45 @@ __global__ void __launch_bounds__(WD_THREADS, WD_BLOCKS) k_score_warp_desolv(Lau
         if (threadIdx.x == 0) {
             long long f = 0;
             for (int i = 0; i < NW; ++i) f += s_fix[i];
-            write_pose(p, c, g, p.solv_only ? 0.0 : v[0], p.solv_only ? 0.0 : v[1],
+            const double far = p.far ? __ldcg(p.far + g) : 0.0;   // k_far_poses' far field, when it ran
+            write_pose(p, c, g, p.solv_only ? 0.0 : v[0] + far, p.solv_only ? 0.0 : v[1],
                        v[2] + (double)f * (1.0 / 1099511627776.0), v[3], IFACE ? W.ibits : nullptr);
         }
         __syncthreads();
     }
     finish_launch(p);
+}
+
+// The far field of the cpydock launch group as its own pass, before the
+// fused kernel: one block per pose, each thread a fixed stride of ligand
+// atoms (the f64 transform of the f64 base coordinates and the reference's
+// f64 interpolation, as the fused kernel does it), then a block sum in a
+// fixed order into far[pose] (deterministic).  Inside the fused kernel the
+// 8 grid gathers of every charged atom waited on memory with only 24 warps
+// per SM resident; here every thread has independent gathers in flight.
+// Skipped (masked) poses are left alone.
+constexpr int FAR_THREADS = 256;
+__global__ void __launch_bounds__(FAR_THREADS) k_far_poses(LaunchParams p) {
+    __shared__ double s_red[4][32];
+    for (long long w = blockIdx.x; w < p.total_work; w += gridDim.x) {
+        const int b = find_item(p.item_work0, p.n_items, w);
+        const ComplexDev& c = p.cx[__ldg(p.item_complex + b)];
+        const long long g = (long long)__ldg(p.item_pose0 + b) + (w - __ldg(p.item_work0 + b));
+        if (p.pose_mask && !p.pose_mask[g]) continue;   // block-uniform
+        double v[1] = {0.0};
+        if (c.flags & F_FAR) {
+            const Rot rot = pose_matrix(p.poses + 7 * g);
+            for (int j = threadIdx.x; j < c.nl; j += FAR_THREADS) {
+                if (__ldg(&c.lpos[j].w) == 0.f) continue;
+                const double4 b64 = c.lpos64[j];
+                double xd, yd, zd;
+                apply(rot, b64.x, b64.y, b64.z, xd, yd, zd);
+                v[0] += b64.w * sample_phi(c, xd, yd, zd);
+            }
+        }
+        block_sum<1>(v, s_red);
+        if (threadIdx.x == 0) p.far[g] = v[0];
+    }
 }
 
 }  // namespace lkg
