@@ -164,7 +164,7 @@ __device__ __forceinline__ void scan_rows(const ComplexDev& c, float x, float y,
 // against the receptor atom's f64 coordinates, without contraction.  The
 // compensated f32 d^2 is off by ~1e-5 A^2 at most, far inside the band.
 constexpr float NEAR_BAND = 1e-3f;
-__device__ __noinline__ bool near_exact(const ComplexDev& c, int k, float x, float xr, float y, float yr, float z,
+static __device__ __noinline__ bool near_exact(const ComplexDev& c, int k, float x, float xr, float y, float yr, float z,
                                            float zr) {
     const double4 a = c.rpos64[k];
     const double dx = __dsub_rn(__dadd_rn((double)x, (double)xr), a.x);
