@@ -36,13 +36,25 @@ def signature(items, device_name):
 
 
 def _sample(items, k):
-    order = sorted(range(len(items)), key=lambda i: len(items[i]["rec"]["coords"]) * len(items[i]["lig"]["coords"]))
+    """k complexes that stand for the batch's work: a pose's cost grows
+    with its ligand's atom count, so the picks sit at evenly spaced
+    quantiles of the cumulative ligand atoms (large-ligand complexes, which
+    dominate the step, are picked more often than by count)."""
+    order = sorted(range(len(items)), key=lambda i: len(items[i]["lig"]["coords"]))
     if len(order) <= k:
         return order
-    return [order[int(round(j * (len(order) - 1) / (k - 1)))] for j in range(k)]
+    w = np.cumsum([len(items[i]["lig"]["coords"]) for i in order], dtype=float)
+    w /= w[-1]
+    picks = []
+    for j in range(k):
+        q = (j + 0.5) / k
+        i = order[int(np.searchsorted(w, q))]
+        if i not in picks:
+            picks.append(i)
+    return picks
 
 
-def autotune(items, device=0, candidates=CANDIDATES, sample=8, poses_per_complex=2000, reps=3,
+def autotune(items, device=0, candidates=CANDIDATES, sample=12, poses_per_complex=3000, reps=3,
              cache_path=DEFAULT_CACHE, verbose=False):
     """Returns dict(tile, group, cell, xsub, ms, source) for a batch given as
     a list of dicts with ``family``, ``rec``, ``lig`` and ``poses`` (N x 7,
