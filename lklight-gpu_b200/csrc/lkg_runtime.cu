@@ -159,12 +159,16 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     d.ncx = nc[0]; d.ncy = nc[1]; d.ncz = nc[2];
     d.ox = o[0]; d.oy = o[1]; d.oz = o[2]; d.h = h; d.inv_h = inv_h; d.hx = hx; d.inv_hx = inv_hx;
     cr.n_cells = (int)ncell;
-    // desolvation hash capacity: >= 2 x receptor atoms up to 8192 slots
-    // (64 KB of shared memory in the fast kernel, 96 KB in the exact one); a
+    // desolvation hash capacity: >= 2 x receptor atoms up to 2048 slots
+    // (16 KB of shared memory in the fast kernel, 24 KB in the exact one); a
     // pose touching more receptor atoms within 6.4 A continues in the launch
-    // group's global spill tables (more slots than receptor atoms)
+    // group's global spill tables (more slots than receptor atoms).  The
+    // small table leaves room for two 12-warp blocks per SM with groups of
+    // 16 and for L1: on the 101k-atom config-4 receptor 2048 slots score
+    // 1.3x faster than 8192 (whose larger tables spilled less) and 1.24x
+    // faster than 1024 (which spill more)
     int cap = 64;
-    while (cap < 2 * n && cap < 8192) cap <<= 1;
+    while (cap < 2 * n && cap < 2048) cap <<= 1;
     d.hcap = cap;
     return set_ok();
 }

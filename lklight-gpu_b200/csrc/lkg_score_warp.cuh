@@ -58,6 +58,10 @@ struct WDes {
 // interface words a warp collects in shared memory before merging them into
 // the pose's bits (larger sets go to HBM directly)
 constexpr int W_IBUF = 32;
+// hits of the packed pair path whose f32 d^2 lies within NEAR_BAND of the
+// 10 A cutoff wait here for the f64 decision (the scalar pair path), which
+// runs before their slot set is reused
+constexpr int W_DEFER = 64;
 
 template <int G>
 struct WSlots {
@@ -71,6 +75,8 @@ struct WSlots {
     unsigned* iset;             // IFACE: where pairs set them: ibuf, or ibits when the pose has more words
     unsigned ibuf[W_IBUF];      // IFACE: the unit's bits, merged into ibits once at the unit's end
     unsigned hit[WRing<G>::N];  // (slot << 26) | receptor index, pending hits first
+    unsigned defer[W_DEFER];    // plain kernel: hits within f32 rounding of the cutoff, decided in f64 later
+    int ndefer;
 };
 
 // Staged candidates (the plain kernel's TMA variant, selected per context):
@@ -297,7 +303,7 @@ __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
 // e1 counts only when v1 (a partial batch).  Same formulas and rounding
 // steps as w_pair, per hit.
 template <int G>
-__device__ __forceinline__ void w_pair2(const ComplexDev& c, const WSlots<G>& W, unsigned e0, unsigned e1, bool v1,
+__device__ __forceinline__ void w_pair2(const ComplexDev& c, WSlots<G>& W, unsigned e0, unsigned e1, bool v1,
                                         unsigned flags, double& elec, double& vdw, int& np) {
     const int l0 = (int)(e0 >> 26), k0 = (int)(e0 & 0x3ffffffu);
     const int l1 = (int)(e1 >> 26), k1 = (int)(e1 & 0x3ffffffu);
@@ -311,10 +317,19 @@ __device__ __forceinline__ void w_pair2(const ComplexDev& c, const WSlots<G>& W,
     const F2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
     float d20, d21;
     f2_get(d2, d20, d21);
-    const bool ok0 = fabsf(d20 - 100.f) < NEAR_BAND ? near_exact(c, k0, lp0.x, lr0.x, lp0.y, lr0.y, lp0.z, lr0.z)
-                                                    : d20 <= 100.f;
-    const bool ok1 = v1 && (fabsf(d21 - 100.f) < NEAR_BAND ? near_exact(c, k1, lp1.x, lr1.x, lp1.y, lr1.y, lp1.z, lr1.z)
-                                                           : d21 <= 100.f);
+    bool ok0 = d20 <= 100.f, ok1 = v1 && d21 <= 100.f;
+    // a hit within f32 rounding of the cutoff leaves this path for the
+    // deferred list (w_flush_deferred decides it in f64); were the list full
+    // (W_DEFER such hits before their slot set is reused) it keeps the f32
+    // decision
+    if (__builtin_expect(fabsf(d20 - 100.f) < NEAR_BAND, 0)) {
+        const int i = atomicAdd(&W.ndefer, 1);
+        if (i < W_DEFER) { W.defer[i] = e0; ok0 = false; }
+    }
+    if (__builtin_expect(v1 && fabsf(d21 - 100.f) < NEAR_BAND, 0)) {
+        const int i = atomicAdd(&W.ndefer, 1);
+        if (i < W_DEFER) { W.defer[i] = e1; ok1 = false; }
+    }
     np += (int)ok0 + (int)ok1;
     const F2 ir2 = f2(rcp_approx(d20), rcp_approx(d21));
     if (flags & F_ELEC) {
@@ -345,6 +360,21 @@ __device__ __forceinline__ void w_pair2(const ComplexDev& c, const WSlots<G>& W,
     }
     if (ok0) vdw += (double)v0;
     if (ok1) vdw += (double)vv1;
+}
+
+// the deferred hits through the scalar pair path (which decides the cutoff
+// in f64 near it); out of line: it runs only when such hits exist
+template <int G>
+__device__ __noinline__ void w_flush_deferred(const ComplexDev& c, WSlots<G>& W, unsigned flags, double& elec,
+                                              double& vdw, int& np) {
+    const int lane = threadIdx.x & 31;
+    __syncwarp();
+    const int n = min(W.ndefer, W_DEFER);
+    for (int i = lane; i < n; i += 32)
+        w_pair<G, false, false>(c, W, nullptr, nullptr, nullptr, W.defer[i], flags, nullptr, elec, vdw, np);
+    __syncwarp();
+    if (lane == 0) W.ndefer = 0;
+    __syncwarp();
 }
 
 // receptor atom of candidate kk of the current rows: the span is the last
@@ -419,6 +449,10 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
         // hits were queued before the previous group started: evaluate any
         // still pending
         if (prev_start > head) drain_partial();
+        if (PAIR2) {   // the deferred hits, before their slot set is reused
+            __syncwarp();
+            if (W.ndefer) w_flush_deferred<G>(c, W, flags, acc.elec, acc.vdw, acc.np);
+        }
         prev_start = tail;
         __syncwarp();
         finalize(set);
@@ -634,6 +668,7 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
     __syncwarp();
     drain_partial();
     __syncwarp();
+    if (PAIR2 && W.ndefer) w_flush_deferred<G>(c, W, flags, acc.elec, acc.vdw, acc.np);
     finalize(0);
     finalize(G);
 }
@@ -659,6 +694,8 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
         __syncwarp();
     }
     if (IFACE) W.ibuf[lane] = 0u;
+    if (lane == 0) W.ndefer = 0;
+    __syncwarp();
     for (;;) {
         unsigned long long wq = 0;
         if (lane == 0) wq = atomicAdd(p.work_counter, 1ull);
