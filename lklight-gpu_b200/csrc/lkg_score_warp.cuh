@@ -844,7 +844,7 @@ __global__ void __launch_bounds__(WD_THREADS, WD_BLOCKS) k_score_warp_desolv(Lau
 // per SM resident; here every thread has independent gathers in flight.
 // Skipped (masked) poses are left alone.
 constexpr int FAR_THREADS = 256;
-__global__ void __launch_bounds__(FAR_THREADS) k_far_poses(LaunchParams p) {
+__global__ void __launch_bounds__(FAR_THREADS, 4) k_far_poses(LaunchParams p) {
     __shared__ double s_red[4][32];
     for (long long w = blockIdx.x; w < p.total_work; w += gridDim.x) {
         const int b = find_item(p.item_work0, p.n_items, w);
