@@ -27,11 +27,13 @@ DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "lkg", "tuning.j
 
 
 def signature(items, device_name):
-    """Batch signature: device, then (family, receptor atoms, ligand atoms)
-    of every complex."""
+    """Batch signature: device, then (family, receptor atoms, ligand atoms,
+    poses) of every complex: the best shape for 200 poses of a complex is
+    not the best for 10,000."""
     h = hashlib.sha1(device_name.encode())
     for it in items:
-        h.update(("%s:%d:%d;" % (it["family"], len(it["rec"]["coords"]), len(it["lig"]["coords"]))).encode())
+        n = len(it["poses"]) if "poses" in it else 0
+        h.update(("%s:%d:%d:%d;" % (it["family"], len(it["rec"]["coords"]), len(it["lig"]["coords"]), n)).encode())
     return h.hexdigest()
 
 
