@@ -133,4 +133,23 @@ cudaError_t launch_far_field_sum(const float* phi, int nx, int ny, int nz, float
     return cudaGetLastError();
 }
 
+__global__ void k_phi_bricks(const float* __restrict__ src, int nx, int ny, int nz, int nbx, int nby,
+                             float* __restrict__ dst, size_t total) {
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= total) return;
+    const size_t b = i >> 6;
+    const int l = (int)(i & 63);
+    const int x = (int)(b % nbx) * 4 + (l & 3);
+    const int y = (int)((b / nbx) % nby) * 4 + ((l >> 2) & 3);
+    const int z = (int)(b / ((size_t)nbx * nby)) * 4 + (l >> 4);
+    dst[i] = (x < nx && y < ny && z < nz) ? src[((size_t)z * ny + y) * nx + x] : 0.f;
+}
+
+cudaError_t phi_to_bricks(const float* src, int nx, int ny, int nz, float* dst, cudaStream_t s) {
+    const int nbx = (nx + 3) / 4, nby = (ny + 3) / 4, nbz = (nz + 3) / 4;
+    const size_t total = (size_t)nbx * nby * nbz * 64;
+    k_phi_bricks<<<(unsigned)((total + 255) / 256), 256, 0, s>>>(src, nx, ny, nz, nbx, nby, dst, total);
+    return cudaGetLastError();
+}
+
 }  // namespace lkg

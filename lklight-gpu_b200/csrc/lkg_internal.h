@@ -51,9 +51,11 @@ struct ComplexDev {
     const float4* lgrp;      // per group of `group` atoms: ligand-frame centre, radius
     int group;               // ligand atoms per candidate-search group
     int ntiles;              // ceil(nl / tile)
-    // far field
+    // far field: fnx x fny x fnz points in bricks of 4 x 4 x 4 (fbx x fby x
+    // fbz bricks, x-fastest; points x-fastest inside a brick)
     const float* phi;
     int fnx, fny, fnz;
+    int fbx, fby, fbz;
     float fox, foy, foz, fsp;
     double fox64, foy64, foz64, fsp64;
     double finv64;           // 1 / spacing when the spacing is a power of two (then x * finv64 == x / spacing), else 0
@@ -155,6 +157,9 @@ size_t desolv_smem_bytes(int hcap, bool exact);
 cudaError_t build_field_device(const double* d_coords, const double* d_q, int n,
                                const double lo[3], const int dims[3], double spacing,
                                float* d_phi, cudaStream_t s);
+// the x-fastest grid src (nx x ny x nz) rearranged into 4 x 4 x 4 bricks
+// (dst: nbx * nby * nbz * 64 floats, points past the grid 0)
+cudaError_t phi_to_bricks(const float* src, int nx, int ny, int nz, float* dst, cudaStream_t s);
 // far-field sum for cuda_far_field
 cudaError_t launch_far_field_sum(const float* phi, int nx, int ny, int nz, float ox, float oy,
                                  float oz, float sp, const float* coords, const float* q, int n,

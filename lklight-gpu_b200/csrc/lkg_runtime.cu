@@ -288,6 +288,16 @@ int build_field(lkg_ctx* ctx, const MolIn& R, const lkg_field* f, bool build, Co
         return set_ok();
     }
     LKG_CK(cudaStreamSynchronize(s), "field upload");
+    {   // the kernels read the grid in 4 x 4 x 4 bricks
+        d.fbx = (d.fnx + 3) / 4; d.fby = (d.fny + 3) / 4; d.fbz = (d.fnz + 3) / 4;
+        DBuf bricks;
+        LKG_CK(bricks.reserve((size_t)d.fbx * d.fby * d.fbz * 64 * sizeof(float)), "field bricks");
+        LKG_CK(phi_to_bricks(cr.phi.as<float>(), d.fnx, d.fny, d.fnz, bricks.as<float>(), s), "field bricks");
+        ctx->launches++;
+        LKG_CK(cudaStreamSynchronize(s), "field bricks");
+        std::swap(cr.phi.p, bricks.p);
+        std::swap(cr.phi.bytes, bricks.bytes);   // the x-fastest grid is freed with `bricks`
+    }
     d.phi = cr.phi.as<float>();
     d.fox = (float)d.fox64; d.foy = (float)d.foy64; d.foz = (float)d.foz64; d.fsp = (float)d.fsp64;
     {

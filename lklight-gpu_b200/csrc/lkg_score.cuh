@@ -73,6 +73,21 @@ __device__ __forceinline__ void apply(const Rot& r, double vx, double vy, double
 // ------------------------------------------------------------------------
 // far field
 // ------------------------------------------------------------------------
+// The grid is stored in bricks of 4 x 4 x 4 points (256 bytes: two 128-byte
+// lines), bricks x-fastest, points x-fastest inside a brick.  A sample's 8
+// corners then sit in one brick (or a few neighbouring ones), on 1-2 lines
+// instead of the 4 rows of the x-fastest layout, and the samples of a
+// compact ligand group share bricks.  Returns the offset of corner
+// (ix, iy, iz) and the steps to its +x, +y and +z neighbours.
+__device__ __forceinline__ size_t phi_brick_offsets(const ComplexDev& c, int ix, int iy, int iz, size_t& ox,
+                                                    size_t& oy, size_t& oz) {
+    const size_t bx = (size_t)c.fbx, bxy = (size_t)c.fbx * c.fby;
+    ox = (ix & 3) == 3 ? 64 - 3 : 1;
+    oy = (iy & 3) == 3 ? bx * 64 - 12 : 4;
+    oz = (iz & 3) == 3 ? bxy * 64 - 48 : 16;
+    return (((size_t)(iz >> 2) * bxy + (size_t)(iy >> 2) * bx + (size_t)(ix >> 2)) << 6) +
+           (size_t)(((iz & 3) << 4) | ((iy & 3) << 2) | (ix & 3));
+}
 __device__ __forceinline__ float sample_phi(const ComplexDev& c, float x, float y, float z) {
     float fx = (x - c.fox) / c.fsp, fy = (y - c.foy) / c.fsp, fz = (z - c.foz) / c.fsp;
     // in the box iff 0 <= f < n - 1 per axis (ix + 1 < n); compared in float
@@ -83,10 +98,10 @@ __device__ __forceinline__ float sample_phi(const ComplexDev& c, float x, float 
     int ix = (int)fx, iy = (int)fy, iz = (int)fz;
     if (ix + 1 >= c.fnx || iy + 1 >= c.fny || iz + 1 >= c.fnz) return 0.f;
     float tx = fx - ix, ty = fy - iy, tz = fz - iz;
-    size_t sy = (size_t)c.fnx, sz = (size_t)c.fnx * c.fny;
-    const float* p = c.phi + (size_t)iz * sz + (size_t)iy * sy + ix;
-    float c000 = __ldg(p), c100 = __ldg(p + 1), c010 = __ldg(p + sy), c110 = __ldg(p + sy + 1);
-    float c001 = __ldg(p + sz), c101 = __ldg(p + sz + 1), c011 = __ldg(p + sz + sy), c111 = __ldg(p + sz + sy + 1);
+    size_t ox, oy, oz;
+    const float* p = c.phi + phi_brick_offsets(c, ix, iy, iz, ox, oy, oz);
+    float c000 = __ldg(p), c100 = __ldg(p + ox), c010 = __ldg(p + oy), c110 = __ldg(p + oy + ox);
+    float c001 = __ldg(p + oz), c101 = __ldg(p + oz + ox), c011 = __ldg(p + oz + oy), c111 = __ldg(p + oz + oy + ox);
     float c00 = c000 * (1.f - tx) + c100 * tx, c10 = c010 * (1.f - tx) + c110 * tx;
     float c01 = c001 * (1.f - tx) + c101 * tx, c11 = c011 * (1.f - tx) + c111 * tx;
     float c0 = c00 * (1.f - ty) + c10 * ty, c1 = c01 * (1.f - ty) + c11 * ty;
@@ -108,10 +123,10 @@ __device__ __forceinline__ double sample_phi(const ComplexDev& c, double x, doub
     long long ix0 = (long long)ix, iy0 = (long long)iy, iz0 = (long long)iz;
     if (ix0 + 1 >= c.fnx || iy0 + 1 >= c.fny || iz0 + 1 >= c.fnz) return 0.0;
     double tx = (double)(float)(fx - ix), ty = (double)(float)(fy - iy), tz = (double)(float)(fz - iz);
-    size_t sy = (size_t)c.fnx, sz = (size_t)c.fnx * c.fny;
-    const float* p = c.phi + (size_t)iz0 * sz + (size_t)iy0 * sy + ix0;
-    double c000 = p[0], c100 = p[1], c010 = p[sy], c110 = p[sy + 1];
-    double c001 = p[sz], c101 = p[sz + 1], c011 = p[sz + sy], c111 = p[sz + sy + 1];
+    size_t ox, oy, oz;
+    const float* p = c.phi + phi_brick_offsets(c, (int)ix0, (int)iy0, (int)iz0, ox, oy, oz);
+    double c000 = p[0], c100 = p[ox], c010 = p[oy], c110 = p[oy + ox];
+    double c001 = p[oz], c101 = p[oz + ox], c011 = p[oz + oy], c111 = p[oz + oy + ox];
     double c00 = c000 * (1.0 - tx) + c100 * tx;
     double c10 = c010 * (1.0 - tx) + c110 * tx;
     double c01 = c001 * (1.0 - tx) + c101 * tx;
