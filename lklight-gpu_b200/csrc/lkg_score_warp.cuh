@@ -854,28 +854,12 @@ __global__ void __launch_bounds__(FAR_THREADS, 4) k_far_poses(LaunchParams p) {
         double v[1] = {0.0};
         if (c.flags & F_FAR) {
             const Rot rot = pose_matrix(p.poses + 7 * g);
-            // two atoms an iteration (j and j + FAR_THREADS): both samples'
-            // gathers are in flight together; they are added in atom order
-            for (int j = threadIdx.x; j < c.nl; j += 2 * FAR_THREADS) {
-                const int j2 = j + FAR_THREADS;
-                const bool q1 = __ldg(&c.lpos[j].w) != 0.f, q2 = j2 < c.nl && __ldg(&c.lpos[j2].w) != 0.f;
-                double s1 = 0.0, s2 = 0.0, w1 = 0.0, w2 = 0.0;
-                if (q1) {
-                    const double4 b = c.lpos64[j];
-                    double xd, yd, zd;
-                    apply(rot, b.x, b.y, b.z, xd, yd, zd);
-                    w1 = b.w;
-                    s1 = sample_phi(c, xd, yd, zd);
-                }
-                if (q2) {
-                    const double4 b = c.lpos64[j2];
-                    double xd, yd, zd;
-                    apply(rot, b.x, b.y, b.z, xd, yd, zd);
-                    w2 = b.w;
-                    s2 = sample_phi(c, xd, yd, zd);
-                }
-                if (q1) v[0] += w1 * s1;
-                if (q2) v[0] += w2 * s2;
+            for (int j = threadIdx.x; j < c.nl; j += FAR_THREADS) {
+                if (__ldg(&c.lpos[j].w) == 0.f) continue;
+                const double4 b64 = c.lpos64[j];
+                double xd, yd, zd;
+                apply(rot, b64.x, b64.y, b64.z, xd, yd, zd);
+                v[0] += b64.w * sample_phi(c, xd, yd, zd);
             }
         }
         block_sum<1>(v, s_red);
