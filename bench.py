@@ -11,7 +11,9 @@ plain dna configuration (1 x 200 poses) instead.
 Reported (one JSON line on rank 0):
   value     poses/s with poses resident in HBM, CUDA events on the context's
             stream, max over ranks (weak scaling: every rank scores its own
-            copy of the workload)
+            copy of the workload; with ``--partition`` the complexes are
+            split over the ranks instead, strong scaling, and the scores are
+            gathered after the timed region)
   e2e       the same through the C ABI with host buffers (``lkg_score_multi``:
             page-locked poses in, scores out, every step)
   roofline  FP32 work of the dominant kernel (near pairs x FLOPs per pair
@@ -73,6 +75,9 @@ def parse():
                          "the plain run with the next seed are compared with the plain run (mean and spread)")
     ap.add_argument("--complexes", type=int, default=0,
                     help="score only the first K complexes of the workload (profiling-size cases)")
+    ap.add_argument("--partition", action="store_true",
+                    help="under torchrun: split the workload's complexes over the ranks (strong scaling, scores "
+                         "gathered after the timed region) instead of one replica of the workload per rank")
     return ap.parse_args()
 
 
@@ -229,14 +234,16 @@ def parity_sample(items, models, scores, counts, pairs, per_complex=4, fp64_ever
 
 
 def workload_config(args, items, world):
-    """The workload definition (identical on both arms of the comparison)."""
+    """The workload definition (identical on both arms of the comparison);
+    items: the whole job's complexes."""
     return {"workload": args.workload, "complexes": len(items),
             "poses_per_step": int(sum(len(it["poses"]) for it in items)),
             "families": sorted(set(it["family"] for it in items)),
             "receptor_atoms": int(sum(len(it["rec"]["coords"]) for it in items)),
             "ligand_atoms": int(sum(len(it["lig"]["coords"]) for it in items)),
             "l2": "inputs larger than L2 (receptor arrays and far-field grids of all complexes)",
-            "parallelism": "replicas" if world > 1 else "single"}
+            "parallelism": "single" if world == 1 else
+            ("partitioned by complex" if getattr(args, "partition", False) else "replicas")}
 
 
 def max_over_ranks(v, dist, device):
@@ -245,6 +252,43 @@ def max_over_ranks(v, dist, device):
     t = torch.tensor([float(v)], dtype=torch.float64, device=device)
     if dist:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def shard_items(items, world):
+    """Complexes to ranks for a partitioned run: greedy, largest estimated
+    work first (poses x ligand atoms, the near scan's cost driver), each to
+    the rank with the least work so far.  Returns one list of item indices
+    per rank, each in workload order."""
+    order = sorted(range(len(items)), key=lambda i: -len(items[i]["poses"]) * len(items[i]["lig"]["coords"]))
+    load, out = [0.0] * world, [[] for _ in range(world)]
+    for i in order:
+        r = min(range(world), key=lambda k: (load[k], k))
+        out[r].append(i)
+        load[r] += len(items[i]["poses"]) * len(items[i]["lig"]["coords"])
+    return [sorted(o) for o in out]
+
+
+def gather_scores(local, dist):
+    """Per-complex score arrays of every rank, merged on every rank
+    ({item index: scores}); a single process returns its own."""
+    if not dist:
+        return dict(local)
+    parts = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, dict(local))
+    merged = {}
+    for p in parts:
+        merged.update(p)
+    return merged
+
+
+def sum_over_ranks(v, dist, device):
+    """The sum of a per-rank count over all ranks."""
+    if not dist:
+        return float(v)
+    import torch
+    t = torch.tensor([float(v)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
     return float(t.item())
 
 
@@ -378,6 +422,14 @@ def main():
     items = workload(args.workload)
     if args.complexes:
         items = items[:args.complexes]
+    job_items, mine = items, list(range(len(items)))
+    partitioned = args.partition and world > 1
+    if partitioned:
+        if world > len(items):
+            raise SystemExit("--partition needs at least one complex per rank (%d complexes, %d ranks)"
+                             % (len(items), world))
+        mine = shard_items(items, world)[rank]
+        items = [items[i] for i in mine]
     shape = pick_shape(args, items, local)
     ctx = lkg.Context(device=local, tile=shape["tile"], cell=shape["cell"], group=shape["group"], xsub=shape["xsub"],
                       stage=args.stage)
@@ -443,7 +495,21 @@ def main():
     ms = ev0.elapsed_time(ev1) / args.steps
     timed_scores = d_scores.cpu().numpy()   # the last timed step's scores (read after the timed region)
     ms_max = max_over_ranks(ms, dist, "cuda")
-    value = job_rate(npose, world, ms_max)
+    # replicas: every rank scores npose; partitioned: the ranks' shares sum
+    # to the workload's poses
+    npose_job = sum_over_ranks(npose, dist, "cuda") if partitioned else npose * world
+
+    def rate(ms_):
+        return npose_job / (ms_ / 1e3)
+    value = rate(ms_max)
+    gathered = None
+    if partitioned:
+        # the one collective of a partitioned run: every complex's scores of
+        # the last timed step, gathered on every rank for ranking
+        offs = np.concatenate([[0], np.cumsum(counts)])
+        merged = gather_scores({mine[k]: timed_scores[offs[k]:offs[k + 1]] for k in range(len(items))}, dist)
+        gathered = {"complexes": len(merged), "poses": int(sum(len(v) for v in merged.values())),
+                    "complexes_on_rank0": len(mine), "how": "all_gather_object after the timed region"}
 
     # e2e: host buffers through the C ABI, copies inside the timed region
     h_poses = torch.from_numpy(allp).pin_memory()
@@ -462,7 +528,7 @@ def main():
     ev3.record(stream)
     ev3.synchronize()
     e2e_ms_max = max_over_ranks(ev2.elapsed_time(ev3) / args.steps, dist, "cuda")
-    e2e_value = job_rate(npose, world, e2e_ms_max)
+    e2e_value = rate(e2e_ms_max)
 
     # plain single-complex scorer: one host-buffer call (one launch) per complex
     plain = None
@@ -512,7 +578,8 @@ def main():
         torch.cuda.synchronize()
         el = time.perf_counter() - t0
         t_gso = max_over_ranks(el, dist, "cuda")
-        gso_loop = {"value": job_rate(g.scored, world, t_gso * 1e3), "unit": "exact poses/s",
+        scored_job = sum_over_ranks(g.scored, dist, "cuda") if partitioned else g.scored * world
+        gso_loop = {"value": scored_job / t_gso, "unit": "exact poses/s",
                     "steps": args.gso_loop_steps, "seconds": t_gso, "exact_evals_per_rank": int(g.scored),
                     "glowworms": int(len(host_pos)),
                     "what": "device-resident GSO over every swarm of every complex: per step one persistent "
@@ -532,9 +599,9 @@ def main():
 
     line = {"metric": "exact poses/s on 1 B200 (dna); surrogate-screened at >=95% top-5 overlap",
             "value": value, "unit": "poses/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-            "dtype": "f32 pair math, f64 transform and sums", "data": "synthetic",
-            "config": workload_config(args, items, world),
+            "ms_per_step": ms_max, "higher_is_better": True, "scaling": "strong" if partitioned else "weak",
+            "vs_baseline": None, "dtype": "f32 pair math, f64 transform and sums", "data": "synthetic",
+            "config": workload_config(args, job_items, world),
             "work": {"near_pairs_per_step": float(pairs.sum()), "near_pairs_by_family": fam_pairs,
                      "counted_by": "the exact (f64) path's near-pair counts, equal to the oracle's by test",
                      "tile_shape": {k: shape.get(k) for k in ("tile", "group", "cell", "xsub", "source")}},
@@ -554,6 +621,8 @@ def main():
             "gpu_launches": int(launches), "clocks": clk,
             "step": "CUDA graph replay of one persistent launch group" if not args.no_graph else "plan launch",
             "candidate_loads": args.stage}
+    if gathered:
+        line["gathered"] = gathered
     if plain:
         line["plain_single_complex"] = plain
     if gso_loop:
