@@ -20,7 +20,7 @@ import numpy as np
 CANDIDATES = [
     (128, 8, 4.0, 8), (128, 8, 5.0, 8), (128, 8, 6.0, 8), (128, 8, 7.0, 8),
     (128, 16, 4.0, 8), (128, 16, 5.0, 8), (128, 16, 6.0, 8), (128, 16, 7.0, 8),
-    (256, 16, 6.0, 8), (128, 32, 6.0, 8), (256, 32, 7.0, 8),
+    (128, 16, 8.0, 8), (256, 16, 6.0, 8), (256, 16, 7.0, 8), (256, 16, 8.0, 8), (128, 32, 6.0, 8), (256, 32, 7.0, 8),
     (128, 4, 4.0, 8), (64, 8, 4.0, 8), (256, 8, 6.0, 8),
 ]
 DEFAULT_CACHE = os.path.join(os.path.expanduser("~"), ".cache", "lkg", "tuning.json")

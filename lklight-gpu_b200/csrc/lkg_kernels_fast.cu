@@ -7,7 +7,7 @@ namespace lkg {
 // outputs are requested (cuda_full_score)
 template <int G>
 static size_t warp_smem(bool stage = false) {
-    return (size_t)(WK_THREADS / 32) * (sizeof(WSlots<G>) + (stage ? sizeof(WStage) : 0));
+    return (size_t)(WK_THREADS / 32) * (sizeof(WSlots<G>) + sizeof(WQueue) + (stage ? sizeof(WStage) : 0));
 }
 
 // IFACE: the variant that also collects the interface bits (launches with

@@ -40,9 +40,10 @@ constexpr int WK_THREADS = 128;   // 4 independent warps per block
 // the pending hits + the 32 x G hits of one chunk always fit
 template <int G> struct WRing { static constexpr int N = 32 * G + 64; };
 
-// resident blocks per SM the register budget is sized for (64 registers a
-// thread for G = 8; the larger masks of G = 16, 32 get 80)
-template <int G> struct WOcc { static constexpr int N = (G <= 8) ? 8 : 6; };
+// resident blocks per SM the register budget is sized for: 64 registers a
+// thread for G = 8, 72 for G = 16 (measured 1.4 % faster than 80 at 6
+// blocks, 64 at 8 blocks 1.3 % slower), 80 for G = 32
+template <int G> struct WOcc { static constexpr int N = (G <= 8) ? 8 : (G == 16 ? 7 : 6); };
 
 // per-warp desolvation state of the two slot sets (cpydock): the slot
 // atoms' f64 positions, their running minimum d^2 to non-excluded receptor
@@ -62,6 +63,14 @@ constexpr int W_IBUF = 32;
 // 10 A cutoff wait here for the f64 decision (the scalar pair path), which
 // runs before their slot set is reused
 constexpr int W_DEFER = 64;
+// plain and interface kernels: candidates of the current group within its
+// sphere (x, y, z relative to the group centre, receptor index in w), tested
+// 32 at a time: a ring of 64, since fewer than 32 wait when a chunk of 32
+// more arrives
+constexpr int W_CQ = 64;
+struct WQueue {
+    float4 a[W_CQ];
+};
 
 template <int G>
 struct WSlots {
@@ -407,10 +416,11 @@ struct WAcc {
 // atom's g(min d^2) * des to acc.solv once its hits are all evaluated.
 template <int G, bool DESOLV, bool IFACE, bool STAGE = false>
 __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes<G>* D, MinHash64* hash, int* status,
-                                         int g_first, int g_end, int g_step, WAcc& acc, WStage* S = nullptr,
-                                         bool far_sep = false) {
+                                         int g_first, int g_end, int g_step, WAcc& acc, WQueue* Q,
+                                         WStage* S = nullptr, bool far_sep = false) {
     constexpr unsigned FULL = 0xffffffffu;
     const int lane = threadIdx.x & 31;
+    const unsigned lt_mask = (1u << lane) - 1u;
     const unsigned flags = c.flags;
     const int nl = c.nl;
     unsigned* const iset = IFACE ? W.iset : nullptr;   // set by the caller for the unit
@@ -515,6 +525,88 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
         const int nbox = (nyr > 0 && nzr > 0) ? nyr * nzr : 0;
         const float inv_nyr = 1.0f / (float)max(nyr, 1);
         const unsigned enc_set = (unsigned)set << 26;
+        // 3. queued candidates, 32 a time: each lane tests its candidate
+        //    (relative to the group centre) against the group's slots and
+        //    appends its hits
+        auto test_chunk = [&](const float ax, const float ay, const float az, const int ridx) {
+            const float aa = ax * ax + ay * ay + az * az;
+            // the lane's candidate against every slot: a bit per hit
+            unsigned m = 0;
+#pragma unroll
+            for (int l = 0; l < G; ++l) {
+                const float4 t = W.ltest[set + l];
+                // |a'|^2 - 2 a'.l' <= -(|l'|^2 - 100.01): three FMAs, the
+                // slot's constant on the right (invalid slots: -3e30)
+                const float q = fmaf(ax, t.x, fmaf(ay, t.y, fmaf(az, t.z, aa)));
+                m |= (q <= -t.w ? 1u : 0u) << l;
+            }
+            // lane-major append: each lane writes its hits (slot order)
+            // at the warp's exclusive prefix of the hit counts
+            const int nh = __popc(m);
+            int inc = nh;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int v = __shfl_up_sync(FULL, inc, o);
+                if (lane >= o) inc += v;
+            }
+            const int chunk_hits = __shfl_sync(FULL, inc, 31);
+            if (chunk_hits == 0) return;
+            unsigned* dst = W.hit + tail + (inc - nh);
+            const unsigned enc = (unsigned)ridx | enc_set;
+#pragma unroll
+            for (int l = 0; l < G; ++l)
+                if (m & (1u << l)) *dst++ = enc + ((unsigned)l << 26);
+            tail += chunk_hits;
+            __syncwarp();
+            // 4. full batches
+            while (tail - head >= BATCH) {
+                if (PAIR2)
+                    w_pair2<G>(c, W, W.hit[head + lane], W.hit[head + 32 + lane], true, flags, acc.elec,
+                               acc.vdw, acc.np);
+                else
+                    w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[head + lane], flags, iset, acc.elec,
+                                             acc.vdw, acc.np);
+                head += BATCH;
+            }
+            // keep the buffer linear: the < BATCH pending hits move to its front
+            if (head > 0) {
+                const int rem = tail - head;
+                const unsigned v = lane < rem ? W.hit[head + lane] : 0u;
+                const unsigned v2 = (PAIR2 && lane + 32 < rem) ? W.hit[head + 32 + lane] : 0u;
+                __syncwarp();
+                if (lane < rem) W.hit[lane] = v;
+                if (PAIR2 && lane + 32 < rem) W.hit[32 + lane] = v2;
+                __syncwarp();
+                prev_start = max(prev_start - head, 0);
+                tail = rem;
+                head = 0;
+            }
+        };
+        // a candidate farther than R from the group centre is more than 10 A
+        // from every slot atom (|l'| <= rho).  The plain and interface
+        // kernels queue only the candidates within R (the row spans' corners
+        // outside the sphere, about 40 % of the candidates with 6 A cells,
+        // then cost no slot tests); the cpydock kernel, short of shared
+        // memory and L1, tests whole chunks and skips those with none within R
+        int q_head = 0, q_tail = 0;
+        auto chunk = [&](const float4 a, const int ridx) {
+            const float ax = a.x - gx, ay = a.y - gy, az = a.z - gz;
+            const bool in = ax * ax + ay * ay + az * az <= R2;
+            if (DESOLV) {
+                if (__any_sync(FULL, in)) test_chunk(ax, ay, az, ridx);
+                return;
+            }
+            const unsigned b = __ballot_sync(FULL, in);
+            if (in)
+                Q->a[(q_tail + __popc(b & lt_mask)) & (W_CQ - 1)] = make_float4(ax, ay, az, __int_as_float(ridx));
+            q_tail += __popc(b);
+            if (q_tail - q_head >= 32) {
+                __syncwarp();
+                const float4 q = Q->a[(q_head + lane) & (W_CQ - 1)];
+                q_head += 32;
+                test_chunk(q.x, q.y, q.z, __float_as_int(q.w));
+            }
+        };
         for (int r0 = 0; r0 < nbox; r0 += 32) {
             const int r = r0 + lane;
             int st = 0, len = 0;
@@ -546,68 +638,6 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
             }
             const int total = __shfl_sync(FULL, inc, 31);
             const int excl = inc - len;
-            // 3. candidate chunks of 32: each lane tests its candidate
-            //    against the group's slots and appends its hits
-            auto chunk = [&](const float4 a, const int ridx) {
-                const float ax = a.x - gx, ay = a.y - gy, az = a.z - gz;
-                const float aa = ax * ax + ay * ay + az * az;
-                // cpydock kernel: a candidate farther than R = 10.001 + rho
-                // from the group centre is more than 10 A from every slot atom
-                // (|l'| <= rho), so a chunk with none closer is skipped (the
-                // test pays off there, not in the plain kernel)
-                if (DESOLV && !__any_sync(FULL, aa <= R2)) return;
-                // the lane's candidate against every slot: a bit per hit
-                unsigned m = 0;
-#pragma unroll
-                for (int l = 0; l < G; ++l) {
-                    const float4 t = W.ltest[set + l];
-                    // |a'|^2 - 2 a'.l' <= -(|l'|^2 - 100.01): three FMAs, the
-                    // slot's constant on the right (invalid slots: -3e30)
-                    const float q = fmaf(ax, t.x, fmaf(ay, t.y, fmaf(az, t.z, aa)));
-                    m |= (q <= -t.w ? 1u : 0u) << l;
-                }
-                // lane-major append: each lane writes its hits (slot order)
-                // at the warp's exclusive prefix of the hit counts
-                const int nh = __popc(m);
-                int inc = nh;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const int v = __shfl_up_sync(FULL, inc, o);
-                    if (lane >= o) inc += v;
-                }
-                const int chunk_hits = __shfl_sync(FULL, inc, 31);
-                if (chunk_hits == 0) return;
-                unsigned* dst = W.hit + tail + (inc - nh);
-                const unsigned enc = (unsigned)ridx | enc_set;
-#pragma unroll
-                for (int l = 0; l < G; ++l)
-                    if (m & (1u << l)) *dst++ = enc + ((unsigned)l << 26);
-                tail += chunk_hits;
-                __syncwarp();
-                // 4. full batches
-                while (tail - head >= BATCH) {
-                    if (PAIR2)
-                        w_pair2<G>(c, W, W.hit[head + lane], W.hit[head + 32 + lane], true, flags, acc.elec,
-                                   acc.vdw, acc.np);
-                    else
-                        w_pair<G, DESOLV, IFACE>(c, W, D, hash, status, W.hit[head + lane], flags, iset, acc.elec,
-                                                 acc.vdw, acc.np);
-                    head += BATCH;
-                }
-                // keep the buffer linear: the < BATCH pending hits move to its front
-                if (head > 0) {
-                    const int rem = tail - head;
-                    const unsigned v = lane < rem ? W.hit[head + lane] : 0u;
-                    const unsigned v2 = (PAIR2 && lane + 32 < rem) ? W.hit[head + 32 + lane] : 0u;
-                    __syncwarp();
-                    if (lane < rem) W.hit[lane] = v;
-                    if (PAIR2 && lane + 32 < rem) W.hit[32 + lane] = v2;
-                    __syncwarp();
-                    prev_start = max(prev_start - head, 0);
-                    tail = rem;
-                    head = 0;
-                }
-            };
             if (!STAGE) {
                 // the next chunk's receptor atoms are fetched (through L1)
                 // while the current one is tested
@@ -664,6 +694,13 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
                 }
             }
         }
+        // the queue's remainder (the lanes past it test a far candidate)
+        if (!DESOLV && q_tail > q_head) {
+            __syncwarp();
+            const int n = q_tail - q_head;
+            const float4 q = lane < n ? Q->a[(q_head + lane) & (W_CQ - 1)] : make_float4(3e30f, 3e30f, 3e30f, 0.f);
+            test_chunk(q.x, q.y, q.z, __float_as_int(q.w));
+        }
     }
     __syncwarp();
     drain_partial();
@@ -683,7 +720,9 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
     extern __shared__ __align__(16) unsigned char wk_smem[];
     const int lane = threadIdx.x & 31;
     WSlots<G>& W = reinterpret_cast<WSlots<G>*>(wk_smem)[threadIdx.x >> 5];
-    WStage* S = STAGE ? reinterpret_cast<WStage*>(wk_smem + (WK_THREADS / 32) * sizeof(WSlots<G>)) + (threadIdx.x >> 5)
+    WQueue* Q = reinterpret_cast<WQueue*>(wk_smem + (WK_THREADS / 32) * sizeof(WSlots<G>)) + (threadIdx.x >> 5);
+    WStage* S = STAGE ? reinterpret_cast<WStage*>(wk_smem + (WK_THREADS / 32) * (sizeof(WSlots<G>) + sizeof(WQueue))) +
+                            (threadIdx.x >> 5)
                       : nullptr;
     if (STAGE) {
         if (lane == 0) {
@@ -718,7 +757,7 @@ __global__ void __launch_bounds__(WK_THREADS, WOcc<G>::N) k_score_warp(LaunchPar
         const int gpt = p.tile / G;
         const int g0 = tile * gpt, g1 = min(g0 + gpt, (c.nl + G - 1) / G);
         WAcc acc;
-        w_groups<G, false, IFACE, STAGE>(c, W, nullptr, nullptr, p.status, g0, g1, 1, acc, S);
+        w_groups<G, false, IFACE, STAGE>(c, W, nullptr, nullptr, p.status, g0, g1, 1, acc, Q, S);
         if (IFACE && W.ibits) {
             w_iface_flush(W, c);
             __threadfence();   // interface bits before the unit is published
@@ -797,7 +836,7 @@ __global__ void __launch_bounds__(WD_THREADS, WD_BLOCKS) k_score_warp_desolv(Lau
         }
         __syncthreads();   // hash cleared, poses set
         WAcc acc;
-        w_groups<G, true, IFACE>(c, W, D, &hash, p.status, wid, (c.nl + G - 1) / G, NW, acc, nullptr,
+        w_groups<G, true, IFACE>(c, W, D, &hash, p.status, wid, (c.nl + G - 1) / G, NW, acc, nullptr, nullptr,
                                  p.far != nullptr);
         if (IFACE && W.ibits) w_iface_flush(W, c);   // before the block's barrier below
         __syncthreads();   // every pair has updated the hash
