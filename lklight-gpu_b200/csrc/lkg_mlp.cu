@@ -14,11 +14,12 @@
 //                K-major SW128 operands, FP32 accumulator in TMEM
 //   k_wgrad_tc   tcgen05 + TMA weight gradients: MN-major SW128 operands,
 //                reduction over the batch split across CTAs
-//   k_head       last layer (256 -> 1) dot products, FP32
-//   k_loss       MSE on the standardised target, dy, head gradients
-//   k_colsum     bias gradients
-//   k_adam_all   Adam on the FP32 master weights (one launch), refreshes both
-//                BF16 layouts of the GEMM weights
+//   k_head       last layer (256 -> 1) dot products, FP32 (prediction)
+//   k_loss_head  training: the last layer, MSE on the standardised target,
+//                dy, dH3 and the head-gradient partials
+//   k_grad_adam  every gradient summed from its partials in a fixed order,
+//                then Adam on the FP32 master weights (one launch), which
+//                also refreshes both BF16 layouts of the GEMM weights
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cudaTypedefs.h>
@@ -188,7 +189,7 @@ __global__ void __launch_bounds__(128) k_gemm(int M, int N, int K, const __nv_bf
                 } else if (EPI == EPI_BWD) {
                     const float hm = __bfloat162float(Hmask[(size_t)gm * ldc + gn]);
                     Cb[(size_t)gm * ldc + gn] = __float2bfloat16(hm > 0.f ? v : 0.f);
-                } else {   // split blockIdx.z's partial tile; k_split_sum adds the splits in order
+                } else {   // split blockIdx.z's partial tile; k_grad_adam adds the splits in order
                     Cf[(size_t)blockIdx.z * M * ldc + (size_t)gm * ldc + gn] = v;
                 }
             }
@@ -370,7 +371,7 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
 // moves the start address by 2048 B (two whole atoms).  Each CTA reduces a
 // chunk of TCW_ROWS batch rows (all its slabs resident, one expect_tx
 // barrier) and writes its FP32 partial tile to part[split][o][i]; the
-// splits are added in order afterwards (k_split_sum), so training stays
+// splits are added in order afterwards (k_grad_adam), so training stays
 // bitwise reproducible.  Waits are bounded as in k_gemm_tc.
 // ---------------------------------------------------------------------------
 constexpr int TCW_ROWS = 128;                       // batch rows per CTA (two 64-row slabs)
@@ -493,19 +494,38 @@ __global__ void k_head(const __nv_bfloat16* __restrict__ H3, int n, const float*
 // (partials per block of rows or per split, then the partials in order), so
 // training is bitwise reproducible.
 constexpr int RB = 32;   // rows per partial sum (bias gradients)
-constexpr int RL = 8;    // rows per partial sum of the loss kernel (more blocks: its rows are serial)
+constexpr int RL = 32;   // rows per partial sum of the loss kernel (each warp four rows of the head)
 
-// loss, dy = 2 (y - t) / n; dH3 = dy w3 x ReLU'(H3); per block of RL rows
-// (one thread per column) the partial head gradients sum_rows dy h (H
-// columns), sum dy and sum (y - t)^2 / n -> part[blk][H + 2]
-__global__ void k_loss(const float* __restrict__ y, const float* __restrict__ t, const __nv_bfloat16* __restrict__ H3,
-                       int n, const float* __restrict__ w3, __nv_bfloat16* __restrict__ dH3, float* __restrict__ part) {
+// training, per block of RL rows (one thread per column): the head
+// y = H3 . w3 + b3 (a warp per row, as k_head; y is also stored), the loss
+// terms d = y - t, dy = 2 d / n, dH3 = dy w3 x ReLU'(H3), and the partial
+// sums over the block's rows of dy h (the w3 gradient, H columns), of dy
+// (b3) and of d^2 / n (the loss) -> part[blk][H + 2]
+__global__ void __launch_bounds__(H) k_loss_head(const float* __restrict__ t, const __nv_bfloat16* __restrict__ H3,
+                                                int n, const float* __restrict__ w3, const float* __restrict__ b3,
+                                                float* __restrict__ y, __nv_bfloat16* __restrict__ dH3,
+                                                float* __restrict__ part) {
+    static_assert(RL % (H / 32) == 0, "whole rows per warp");
+    __shared__ float s_y[RL];
     const int k = threadIdx.x, r0 = blockIdx.x * RL, r1 = min(n, r0 + RL);
+    for (int rr = k >> 5; rr < RL; rr += H / 32) {
+        const int row = r0 + rr, lane = k & 31;
+        if (row < r1) {
+            float sy = 0.f;
+            for (int c = lane; c < H; c += 32) sy += __bfloat162float(H3[(size_t)row * H + c]) * w3[c];
+            for (int o = 16; o > 0; o >>= 1) sy += __shfl_xor_sync(0xffffffffu, sy, o);
+            if (lane == 0) {
+                s_y[rr] = sy + b3[0];
+                y[row] = sy + b3[0];
+            }
+        }
+    }
+    __syncthreads();
     float gw = 0.f, gb = 0.f, ls = 0.f;
 #pragma unroll
     for (int r = r0; r < r0 + RL; ++r) {
         if (r >= r1) break;
-        const float d = y[r] - t[r];
+        const float d = s_y[r - r0] - t[r];
         const float dy = 2.f * d / (float)n;
         const float h = __bfloat162float(H3[(size_t)r * H + k]);
         dH3[(size_t)r * H + k] = __float2bfloat16(h > 0.f ? dy * w3[k] : 0.f);
@@ -518,41 +538,18 @@ __global__ void k_loss(const float* __restrict__ y, const float* __restrict__ t,
     if (k == 0) { p[H] = gb; p[H + 1] = ls; }
 }
 
-// head gradients (w3, b3: contiguous) and the loss (added to the running
-// epoch sum) from the row-block partials, in block order
-__global__ void k_head_sum(const float* __restrict__ part, int nblk, float* __restrict__ g_w3b3,
-                           float* __restrict__ loss) {
-    const int k = threadIdx.x;
-    if (k > H + 1) return;
-    float s = 0.f;
-    for (int b = 0; b < nblk; ++b) s += part[(size_t)b * (H + 2) + k];
-    if (k <= H) g_w3b3[k] = s;
-    else *loss += s;
-}
-
-// bias gradients: column sums of dC [n x H] per block of RB rows -> part[blk][H]
-__global__ void k_colsum(const __nv_bfloat16* __restrict__ dC, int n, float* __restrict__ part) {
-    const int col = threadIdx.x, r0 = blockIdx.x * RB, r1 = min(n, r0 + RB);
+// bias-gradient partials of the three layers in one launch: column sums
+// of dC_L [n x H] per block of RB rows -> part[L][blk][H] (blockIdx.y = L)
+struct ColSums {
+    const __nv_bfloat16* dC[3];
+    float* part;
+};
+__global__ void __launch_bounds__(H) k_colsum3(ColSums a, int n) {
+    const int col = threadIdx.x, blk = blockIdx.x, L = blockIdx.y, r0 = blk * RB, r1 = min(n, r0 + RB);
+    const __nv_bfloat16* dC = a.dC[L];
     float s = 0.f;
     for (int r = r0; r < r1; ++r) s += __bfloat162float(dC[(size_t)r * H + col]);
-    part[(size_t)blockIdx.x * H + col] = s;
-}
-
-// out[i] = sum over z = 0, 1, ... of part[z * count + i], for two such
-// reductions in one launch (threads past count1 serve the second)
-struct SplitSum {
-    const float* part;
-    int nz, count;
-    float* out;
-};
-__global__ void k_split_sum(SplitSum a, SplitSum b) {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const SplitSum& r = i < a.count ? a : b;
-    if (i >= a.count) i -= a.count;
-    if (i >= r.count) return;
-    float s = 0.f;
-    for (int z = 0; z < r.nz; ++z) s += r.part[(size_t)z * r.count + i];
-    r.out[i] = s;
+    a.part[((size_t)L * gridDim.x + blk) * H + col] = s;
 }
 
 // the three GEMM layers inside the flat parameter vector
@@ -562,29 +559,70 @@ struct AdamLayers {
     __nv_bfloat16* w[3];
 };
 
-// Adam over the whole flat parameter vector in one launch; GEMM-layer
-// entries also refresh both BF16 layouts
-// The step count t (1-based) lives on the device so that training steps can
-// be replayed from a CUDA graph; the kernel's last block advances it.
-// step[0]: the step count t; step[1]: blocks done (the last block to
-// finish advances t, after every block has read it, and resets the count)
-__global__ void k_adam_all(float* __restrict__ p, const float* __restrict__ gr, float* __restrict__ m1,
-                           float* __restrict__ m2, int n, float lr, float b1, float b2, float eps,
-                           int* __restrict__ step, AdamLayers L) {
+// The whole gradient and the Adam step in one launch.  Every parameter's
+// gradient is summed in a fixed order: a weight over the weight-gradient
+// splits in split order; a bias over k_colsum3's row blocks in order; w3
+// and b3 over k_loss_head's row blocks in order.  g receives the sums, and the loss sum is added to
+// the running loss.  Nothing depends on thread timing, so training repeats
+// bit for bit.  apply = 0: gradients only (no update).  The step count t
+// (1-based) lives on the device so that training steps can be replayed from
+// a CUDA graph: step[0] is t, step[1] counts finished blocks, and the last
+// block to finish advances t (after every block has read it).
+struct GradSums {
+    const float* wpart[3];           // per layer: nz[L] partial [H x cols] tiles
+    int nz[3];
+    const float* cpart;              // k_colsum3 partials [3][nblk][H]
+    int nblk;
+    const float* lpart;              // k_loss_head partials [nlblk][H + 2]
+    int nlblk;
+    float* loss;                     // running loss sum
+};
+__global__ void k_grad_adam(float* __restrict__ p, float* __restrict__ gr, float* __restrict__ m1,
+                            float* __restrict__ m2, int n, float lr, float b1, float b2, float eps,
+                            int* __restrict__ step, AdamLayers L, GradSums G, int apply) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    const float t = (float)*reinterpret_cast<volatile int*>(step);
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        __threadfence();
-        const unsigned v = atomicAdd(reinterpret_cast<unsigned*>(step + 1), 1u);
-        if (v == gridDim.x - 1) {
-            step[0] += 1;
-            step[1] = 0;
+    float t = 0.f;
+    if (apply) {
+        t = (float)*reinterpret_cast<volatile int*>(step);
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            __threadfence();
+            const unsigned v = atomicAdd(reinterpret_cast<unsigned*>(step + 1), 1u);
+            if (v == gridDim.x - 1) {
+                step[0] += 1;
+                step[1] = 0;
+            }
         }
     }
     if (i >= n) return;
+    float gg = 0.f;
+    const int off_w3 = L.off[2] + H * L.cols[2] + H;
+    if (i >= off_w3) {   // w3 [H], b3 (and the loss, with b3)
+        const int k = i - off_w3;
+        #pragma unroll 8
+        for (int b = 0; b < G.nlblk; ++b) gg += G.lpart[(size_t)b * (H + 2) + k];
+        if (k == H) {
+            float ls = 0.f;
+            for (int b = 0; b < G.nlblk; ++b) ls += G.lpart[(size_t)b * (H + 2) + H + 1];
+            *G.loss += ls;
+        }
+    } else {
+        int l = 2;
+        while (i < L.off[l]) --l;
+        const int j = i - L.off[l], nw = H * L.cols[l];
+        if (j < nw) {
+            const float* part = G.wpart[l];
+            #pragma unroll 8
+            for (int z = 0; z < G.nz[l]; ++z) gg += part[(size_t)z * nw + j];
+        } else {   // bias o of layer l: the row blocks' column sums in order
+            const float* part = G.cpart + (size_t)l * G.nblk * H + (j - nw);
+            #pragma unroll 8
+            for (int b = 0; b < G.nblk; ++b) gg += part[(size_t)b * H];
+        }
+    }
+    gr[i] = gg;
+    if (!apply) return;
     const float bc1 = 1.f - powf(b1, t), bc2 = 1.f - powf(b2, t);
-    const float gg = gr[i];
     const float a = b1 * m1[i] + (1.f - b1) * gg, v = b2 * m2[i] + (1.f - b2) * gg * gg;
     m1[i] = a;
     m2[i] = v;
@@ -632,7 +670,12 @@ struct lkg_surrogate {
     DBuf wt[3], w[3];   // BF16 layouts per GEMM layer
     // activations for a batch
     DBuf X, H1, H2, H3, dH1, dH2, dH3, y, t, loss;
-    DBuf wpart, rpart;   // backward partial sums: per split (weight gradients), per row block
+    DBuf wpart, rpart;   // backward partial sums: per layer and split (weight gradients), per row block (loss)
+    size_t wsplits = 0;  // splits each layer's region of wpart holds
+    int wnz[3] = {0, 0, 0};   // splits the last backward wrote per layer
+    DBuf cpart;          // bias-gradient partials [3][row blocks][H]
+    DBuf Xtr, ttr;       // training: features and standardised targets of the whole training set
+    int cap_tr = 0;
     int cap = 0;     // rows of X, H1..H3, y, t (forward)
     int cap_b = 0;   // rows of dH1..dH3 (backward)
     DBuf d_step;   // Adam step count (device, 1-based) and the Adam kernel's block counter
@@ -675,8 +718,10 @@ int sur_reserve(lkg_surrogate* S, int n, bool bwd) {
         LKG_CK(S->dH2.reserve(nb * H), "surrogate alloc");
         LKG_CK(S->dH3.reserve(nb * H), "surrogate alloc");
         const size_t splits = std::max<size_t>(wgrad_splits(m), (size_t)(m + TCW_ROWS - 1) / TCW_ROWS);
-        LKG_CK(S->wpart.reserve(splits * H * H * sizeof(float)), "surrogate alloc");
+        LKG_CK(S->wpart.reserve(splits * H * (IN + 2 * H) * sizeof(float)), "surrogate alloc");
+        S->wsplits = splits;
         LKG_CK(S->rpart.reserve((size_t)((m + RL - 1) / RL) * (H + 2) * sizeof(float)), "surrogate alloc");
+        LKG_CK(S->cpart.reserve((size_t)3 * ((m + RB - 1) / RB) * H * sizeof(float)), "surrogate alloc");
         S->cap_b = m;
     }
     return 0;
@@ -696,7 +741,10 @@ cudaError_t gemm(cudaStream_t s, int M, int N, int K, const __nv_bfloat16* A, in
 }
 
 float* P(lkg_surrogate* S, int k) { return S->p.as<float>() + S->off[k]; }
-float* Gd(lkg_surrogate* S, int k) { return S->g.as<float>() + S->off[k]; }
+// layer L's region of the weight-gradient partials (layers 0, 1, 2 in turn)
+float* wpart_of(lkg_surrogate* S, int L) {
+    return S->wpart.as<float>() + S->wsplits * H * (L == 0 ? 0 : (size_t)IN + (size_t)(L - 1) * H);
+}
 
 // forward of n feature rows already in S->X; y in S->y
 // 2D tiled tensor map of a row-major [rows x K] bf16 matrix for the tcgen05
@@ -756,9 +804,11 @@ cudaError_t wgrad_tc(lkg_surrogate* S, int n, int kin, const __nv_bfloat16* dC, 
     return cudaGetLastError();
 }
 
-int forward(lkg_surrogate* S, int n) {
+// forward of n feature rows (X, default S->X): H1..H3, and with `head`
+// the output y (training fuses the head into the loss kernel instead)
+int forward(lkg_surrogate* S, int n, const __nv_bfloat16* X = nullptr, bool head = true) {
     cudaStream_t s = S->ctx->stream;
-    const __nv_bfloat16* X = S->X.as<__nv_bfloat16>();
+    if (!X) X = S->X.as<__nv_bfloat16>();
     if (S->tc) {
         LKG_CK(gemm_tc<EPI_FWD>(S, n, IN, X, S->wt[0].as<__nv_bfloat16>(), P(S, 1), nullptr,
                                 S->H1.as<__nv_bfloat16>()), "mlp fwd tc");
@@ -766,56 +816,53 @@ int forward(lkg_surrogate* S, int n) {
                                 S->H2.as<__nv_bfloat16>()), "mlp fwd tc");
         LKG_CK(gemm_tc<EPI_FWD>(S, n, H, S->H2.as<__nv_bfloat16>(), S->wt[2].as<__nv_bfloat16>(), P(S, 5), nullptr,
                                 S->H3.as<__nv_bfloat16>()), "mlp fwd tc");
+    } else {
+        LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, IN, X, IN, S->wt[0].as<__nv_bfloat16>(), IN, nullptr,
+                                            S->H1.as<__nv_bfloat16>(), H, P(S, 1), nullptr)), "mlp fwd");
+        LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, H, S->H1.as<__nv_bfloat16>(), H, S->wt[1].as<__nv_bfloat16>(), H,
+                                            nullptr, S->H2.as<__nv_bfloat16>(), H, P(S, 3), nullptr)), "mlp fwd");
+        LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, H, S->H2.as<__nv_bfloat16>(), H, S->wt[2].as<__nv_bfloat16>(), H,
+                                            nullptr, S->H3.as<__nv_bfloat16>(), H, P(S, 5), nullptr)), "mlp fwd");
+    }
+    S->ctx->launches += 3;
+    if (head) {
         k_head<<<(n + 7) / 8, 256, 0, s>>>(S->H3.as<__nv_bfloat16>(), n, P(S, 6), P(S, 7), S->y.as<float>());
         LKG_CK(cudaGetLastError(), "mlp head");
-        S->ctx->launches += 4;
-        return 0;
+        S->ctx->launches += 1;
     }
-    LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, IN, X, IN, S->wt[0].as<__nv_bfloat16>(), IN, nullptr,
-                                        S->H1.as<__nv_bfloat16>(), H, P(S, 1), nullptr)), "mlp fwd");
-    LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, H, S->H1.as<__nv_bfloat16>(), H, S->wt[1].as<__nv_bfloat16>(), H,
-                                        nullptr, S->H2.as<__nv_bfloat16>(), H, P(S, 3), nullptr)), "mlp fwd");
-    LKG_CK((gemm<false, false, EPI_FWD>(s, n, H, H, S->H2.as<__nv_bfloat16>(), H, S->wt[2].as<__nv_bfloat16>(), H,
-                                        nullptr, S->H3.as<__nv_bfloat16>(), H, P(S, 5), nullptr)), "mlp fwd");
-    k_head<<<(n + 7) / 8, 256, 0, s>>>(S->H3.as<__nv_bfloat16>(), n, P(S, 6), P(S, 7), S->y.as<float>());
-    LKG_CK(cudaGetLastError(), "mlp head");
-    S->ctx->launches += 4;
     return 0;
 }
 
-// backward into S->g (zeroed here); targets in S->t; the batch's mean loss
-// is added to S->loss (cleared here when clear_loss)
-int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
+// backward of n rows after forward(head = false): the fused head and loss
+// (y, dH3, the loss partials), then per layer the weight-gradient partials
+// (each layer into its own region of wpart) and the backward-data product,
+// then the bias partials of all three layers.
+// X, t: the rows' features and standardised targets (default S->X, S->t).
+// grad_step sums every gradient afterwards.
+int backward(lkg_surrogate* S, int n, const __nv_bfloat16* X = nullptr, const float* t = nullptr) {
     cudaStream_t s = S->ctx->stream;
-    LKG_CK(cudaMemsetAsync(S->g.p, 0, NPARAM * sizeof(float), s), "mlp grad clear");
-    if (clear_loss) LKG_CK(cudaMemsetAsync(S->loss.p, 0, sizeof(float), s), "mlp loss clear");
-    const int nblk = (n + RB - 1) / RB, nlblk = (n + RL - 1) / RL;
-    float* rpart = S->rpart.as<float>();
-    float* wpart = S->wpart.as<float>();
-    k_loss<<<nlblk, H, 0, s>>>(S->y.as<float>(), S->t.as<float>(), S->H3.as<__nv_bfloat16>(), n, P(S, 6),
-                               S->dH3.as<__nv_bfloat16>(), rpart);
-    k_head_sum<<<1, H + 2, 0, s>>>(rpart, nlblk, Gd(S, 6), S->loss.as<float>());
+    if (!X) X = S->X.as<__nv_bfloat16>();
+    if (!t) t = S->t.as<float>();
+    const int nlblk = (n + RL - 1) / RL;
+    k_loss_head<<<nlblk, H, 0, s>>>(t, S->H3.as<__nv_bfloat16>(), n, P(S, 6), P(S, 7), S->y.as<float>(),
+                                    S->dH3.as<__nv_bfloat16>(), S->rpart.as<float>());
     LKG_CK(cudaGetLastError(), "mlp loss");
     const int splits = wgrad_splits(n);
     const __nv_bfloat16* acts[3] = {S->H1.as<__nv_bfloat16>(), S->H2.as<__nv_bfloat16>(), S->H3.as<__nv_bfloat16>()};
     __nv_bfloat16* dacts[3] = {S->dH1.as<__nv_bfloat16>(), S->dH2.as<__nv_bfloat16>(), S->dH3.as<__nv_bfloat16>()};
     for (int L = 2; L >= 0; --L) {
         const int kin = L == 0 ? IN : H;
-        const __nv_bfloat16* ain = L == 0 ? S->X.as<__nv_bfloat16>() : acts[L - 1];
+        const __nv_bfloat16* ain = L == 0 ? X : acts[L - 1];
         // dW_L[o][i] = sum_n dC[n][o] * A_in[n][i]   (A = dC^T, B = A_in^T)
         int nz = 0;
         if (S->tc) {
-            LKG_CK(wgrad_tc(S, n, kin, dacts[L], ain, wpart, &nz), "mlp wgrad tc");
+            LKG_CK(wgrad_tc(S, n, kin, dacts[L], ain, wpart_of(S, L), &nz), "mlp wgrad tc");
         } else {
-            LKG_CK((gemm<true, true, EPI_WGRAD>(s, H, kin, n, dacts[L], H, ain, kin, wpart, nullptr, kin, nullptr,
-                                                nullptr, splits)), "mlp wgrad");
+            LKG_CK((gemm<true, true, EPI_WGRAD>(s, H, kin, n, dacts[L], H, ain, kin, wpart_of(S, L), nullptr, kin,
+                                                nullptr, nullptr, splits)), "mlp wgrad");
             nz = split_count(n, splits);
         }
-        k_colsum<<<nblk, H, 0, s>>>(dacts[L], n, rpart);
-        const SplitSum wsum{wpart, nz, H * kin, Gd(S, 2 * L)};
-        const SplitSum bsum{rpart, nblk, H, Gd(S, 2 * L + 1)};
-        k_split_sum<<<(H * kin + H + 255) / 256, 256, 0, s>>>(wsum, bsum);
-        LKG_CK(cudaGetLastError(), "mlp bias grad");
+        S->wnz[L] = nz;
         if (L > 0) {
             // dA_in[n][i] = (sum_o dC[n][o] W_L[o][i]) x ReLU'(A_in); w[L] is W_L^T [in x out]
             if (S->tc)
@@ -826,24 +873,40 @@ int backward(lkg_surrogate* S, int n, bool clear_loss = true) {
                                                     dacts[L - 1], H, nullptr, acts[L - 1])), "mlp bwd");
         }
     }
-    S->ctx->launches += 13;   // loss, head sums, 3 x (weight grads, column sums, split sums), 2 x backward data
+    const ColSums cs{{S->dH1.as<__nv_bfloat16>(), S->dH2.as<__nv_bfloat16>(), S->dH3.as<__nv_bfloat16>()},
+                     S->cpart.as<float>()};
+    k_colsum3<<<dim3((n + RB - 1) / RB, 3), H, 0, s>>>(cs, n);
+    LKG_CK(cudaGetLastError(), "mlp bias grad");
+    S->ctx->launches += 7;   // head and loss, 3 x weight-gradient partials, 2 x backward data, bias partials
     return 0;
 }
 
-int adam(lkg_surrogate* S, float lr) {
+// every gradient summed from the partials of backward(n rows) into S->g,
+// the batch's loss added to S->loss, and with `apply` the Adam step (one
+// launch)
+int grad_step(lkg_surrogate* S, int n, bool apply, float lr = 0.f) {
     cudaStream_t s = S->ctx->stream;
     const float b1 = 0.9f, b2 = 0.999f, eps = 1e-8f;
     AdamLayers L;
+    GradSums G;
     for (int k = 0; k < 3; ++k) {
         L.off[k] = (int)S->off[2 * k];
         L.cols[k] = k == 0 ? IN : H;
         L.wt[k] = S->wt[k].as<__nv_bfloat16>();
         L.w[k] = S->w[k].as<__nv_bfloat16>();
+        G.wpart[k] = wpart_of(S, k);
+        G.nz[k] = S->wnz[k];
     }
-    const int n = (int)NPARAM;
-    k_adam_all<<<(n + 255) / 256, 256, 0, s>>>(S->p.as<float>(), S->g.as<float>(), S->m1.as<float>(),
-                                               S->m2.as<float>(), n, lr, b1, b2, eps, S->d_step.as<int>(), L);
-    LKG_CK(cudaGetLastError(), "mlp adam");
+    G.cpart = S->cpart.as<float>();
+    G.nblk = (n + RB - 1) / RB;
+    G.lpart = S->rpart.as<float>();
+    G.nlblk = (n + RL - 1) / RL;
+    G.loss = S->loss.as<float>();
+    const int np = (int)NPARAM;
+    k_grad_adam<<<(np + 255) / 256, 256, 0, s>>>(S->p.as<float>(), S->g.as<float>(), S->m1.as<float>(),
+                                                 S->m2.as<float>(), np, lr, b1, b2, eps, S->d_step.as<int>(), L, G,
+                                                 apply ? 1 : 0);
+    LKG_CK(cudaGetLastError(), "mlp grad / adam");
     S->ctx->launches += 1;
     return 0;
 }
@@ -861,14 +924,18 @@ int refresh_bf16(lkg_surrogate* S) {
 
 // features of n device poses into S->X; with d_scores also their
 // standardised targets into S->t (training)
-int features(lkg_surrogate* S, int n, const double* d_poses, const double* d_scores = nullptr) {
-    if (sur_reserve(S, n, false)) return lkg_last_status();
+// (into X_out / t_out instead when given: the training set's buffers)
+int features(lkg_surrogate* S, int n, const double* d_poses, const double* d_scores = nullptr,
+             __nv_bfloat16* X_out = nullptr, float* t_out = nullptr) {
+    if (!X_out && sur_reserve(S, n, false)) return lkg_last_status();
     int st = sync_descriptors(S->ctx);
     if (st) return st;
+    if (!X_out) X_out = S->X.as<__nv_bfloat16>();
+    if (!t_out) t_out = S->t.as<float>();
     const int threads = 256, blocks = (int)(((size_t)n * NA + threads - 1) / threads);
-    const TargetArgs tgt{d_scores, S->e_scale, S->t_mu, S->t_sd, d_scores ? S->t.as<float>() : nullptr};
+    const TargetArgs tgt{d_scores, S->e_scale, S->t_mu, S->t_sd, d_scores ? t_out : nullptr};
     k_features<<<blocks, threads, 0, S->ctx->stream>>>(S->ctx->d_cx.as<ComplexDev>(), S->cid, d_poses, n,
-                                                       S->anchors.as<int>(), S->tscale, S->X.as<__nv_bfloat16>(), tgt);
+                                                       S->anchors.as<int>(), S->tscale, X_out, tgt);
     LKG_CK(cudaGetLastError(), "features");
     S->ctx->launches++;
     return 0;
@@ -1030,17 +1097,27 @@ int lkg_surrogate_train(lkg_surrogate* S, int n, const double* d_poses, const do
     int st;
     double last = 0.0;
     const int nb = n / batch;
-    // one epoch = launches only (the loss is summed on the device); it is
-    // captured once in a CUDA graph and replayed `epochs` times
     if ((st = sur_reserve(S, batch, true)) || (st = sync_descriptors(S->ctx))) return st ? st : lkg_last_status();
+    // the features and targets of the whole set, once (they do not change
+    // between epochs); then one epoch = per batch the forward layers, the
+    // backward and one gradient / Adam launch (the loss is summed on the
+    // device), captured once in a CUDA graph and replayed `epochs` times
+    if (n > S->cap_tr) {
+        LKG_CK(S->Xtr.reserve((size_t)n * IN * sizeof(__nv_bfloat16)), "surrogate alloc");
+        LKG_CK(S->ttr.reserve((size_t)n * sizeof(float)), "surrogate alloc");
+        S->cap_tr = n;
+    }
+    __nv_bfloat16* Xtr = S->Xtr.as<__nv_bfloat16>();
+    float* ttr = S->ttr.as<float>();
+    if ((st = features(S, n, d_poses, d_scores, Xtr, ttr))) return st;
     auto epoch = [&]() -> int {
         LKG_CK(cudaMemsetAsync(S->loss.p, 0, sizeof(float), s), "mlp loss clear");
         for (int b0 = 0; b0 + batch <= n; b0 += batch) {
+            const __nv_bfloat16* xb = Xtr + (size_t)b0 * IN;
             int r;
-            if ((r = features(S, batch, d_poses + 7 * (size_t)b0, d_scores + b0))) return r;
-            if ((r = forward(S, batch))) return r;
-            if ((r = backward(S, batch, false))) return r;
-            if ((r = adam(S, lr))) return r;
+            if ((r = forward(S, batch, xb, false))) return r;
+            if ((r = backward(S, batch, xb, ttr + b0))) return r;
+            if ((r = grad_step(S, batch, true, lr))) return r;
         }
         return 0;
     };
@@ -1121,8 +1198,9 @@ int lkg_surrogate_grad(lkg_surrogate* S, int n, const uint16_t* feats, const flo
     if (sur_reserve(S, n, true)) return lkg_last_status();
     LKG_CK(cudaMemcpy(S->X.p, feats, (size_t)n * IN * 2, cudaMemcpyHostToDevice), "grad upload");
     LKG_CK(cudaMemcpy(S->t.p, targets, (size_t)n * 4, cudaMemcpyHostToDevice), "grad upload");
+    LKG_CK(cudaMemsetAsync(S->loss.p, 0, sizeof(float), S->ctx->stream), "grad loss clear");
     int st;
-    if ((st = forward(S, n)) || (st = backward(S, n))) return st;
+    if ((st = forward(S, n, nullptr, false)) || (st = backward(S, n)) || (st = grad_step(S, n, false))) return st;
     LKG_CK(cudaStreamSynchronize(S->ctx->stream), "grad");
     if (y_out) LKG_CK(cudaMemcpy(y_out, S->y.p, (size_t)n * 4, cudaMemcpyDeviceToHost), "grad read");
     if (grad_out) LKG_CK(cudaMemcpy(grad_out, S->g.p, NPARAM * 4, cudaMemcpyDeviceToHost), "grad read");
