@@ -41,9 +41,9 @@ REPO = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, REPO)
 
 FLOPS_PER_PAIR = {"dna": 24, "pydock": 23, "vdw": 19, "cpydock": 25}
-# DRAM bytes per pose of the fast kernel (67.0 MB per 24,000-pose launch of
-# the 4-complex profiling case under ncu, at tile 256, groups of 16, cell 6 A)
-TRAFFIC_PER_POSE = 67.0e6 / 24000
+# DRAM bytes per pose of the fast kernel (56.8 MB per 24,000-pose launch of
+# the 4-complex profiling case under ncu, at tile 256, groups of 16, cell 7 A)
+TRAFFIC_PER_POSE = 56.8e6 / 24000
 FAR_FLOPS = 30
 
 
@@ -609,7 +609,7 @@ def main():
                          "frac": achieved / fp32_peak,
                          "traffic": TRAFFIC_PER_POSE * npose if args.workload == "config2" else None,
                          "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum of one ncu capture of "
-                                           "k_score_warp<16> (tile 256, cell 6 A) on the first 4 complexes "
+                                           "k_score_warp<16> (tile 256, cell 7 A) on the first 4 complexes "
                                            "(24,000 poses), scaled by poses to this launch",
                          "peak_source": "148 SMs x 128 FP32 lanes x 2 x sm_max_mhz of MEASURED_PEAKS.json",
                          "work": "near pairs x FLOPs/pair (dna 24, pydock 23, vdw 19) + 30 per charged ligand "
