@@ -361,6 +361,210 @@ k_gemm_tc(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUte
 }
 
 // ---------------------------------------------------------------------------
+// Forward layer for large predictions: a persistent, warp-specialised
+// tcgen05 GEMM.  Each CTA (one per SM) keeps the layer's weights B
+// [256 x K] resident in shared memory and walks row tiles t = blockIdx.x,
+// + gridDim.x, ...:
+//   warp 0, one lane:  TMA producer; 128-row x 64-K slabs of A into a ring
+//                      of PP_ST stages (full / empty mbarriers per stage)
+//   warp 1, one lane:  MMA issuer; per slab four tcgen05.mma (M 128, N 256,
+//                      K 16) into one of two TMEM accumulators, the slab's
+//                      stage freed by tcgen05.commit, the tile's accumulator
+//                      announced by a second commit
+//   warps 2-5:         epilogue; each warp reads its TMEM lane quarter
+//                      (warp % 4), adds the bias, applies ReLU, stores bf16,
+//                      and frees the accumulator for the tile after next
+// so the next tile's copies and MMAs run under the current tile's epilogue.
+// The MMAs are the same as k_gemm_tc's (same descriptors, same K order), so
+// the outputs are too.  Every wait is bounded: one that runs out sets status
+// bit 4 and an abort flag that ends every role's loop; the producer and the
+// MMA issuer then wait (bounded) for their copies and MMAs still in flight
+// before the accumulators are freed.
+// ---------------------------------------------------------------------------
+constexpr int PP_ST = 4;                          // A ring stages (16 KB each)
+constexpr int PP_THREADS = 192;
+constexpr size_t PP_SMEM = (size_t)TC_N * TC_KMAX * 2 + (size_t)PP_ST * TC_BM * 128 + 1024;
+
+__device__ __forceinline__ bool pp_wait(uint32_t bar, uint32_t phase, volatile int* abort) {
+    for (int it = 0; it < (1 << 22); ++it) {
+        uint32_t ok;
+        asm volatile("{\n\t.reg .pred P1;\n\t"
+                     "mbarrier.try_wait.parity.shared::cta.b64 P1, [%1], %2;\n\t"
+                     "selp.b32 %0, 1, 0, P1;\n\t}\n"
+                     : "=r"(ok) : "r"(bar), "r"(phase) : "memory");
+        if (ok) return true;
+        if ((it & 255) == 255 && abort && *abort) return false;
+    }
+    return false;
+}
+
+__global__ void __launch_bounds__(PP_THREADS, 1)
+k_gemm_tc_pp(const __grid_constant__ CUtensorMap mapA, const __grid_constant__ CUtensorMap mapB, int M, int K,
+             const float* __restrict__ bias, __nv_bfloat16* __restrict__ Y, int* __restrict__ status) {
+    extern __shared__ __align__(1024) unsigned char tc_smem[];
+    __shared__ __align__(8) unsigned long long full[PP_ST], empty[PP_ST], accf[2], acce[2], bfull;
+    __shared__ uint32_t tmem_slot;
+    __shared__ volatile int abort_flag;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int nslab = K / TC_KS, tiles = (M + TC_BM - 1) / TC_BM;
+    const uint32_t base = (smem_u32(tc_smem) + 1023u) & ~1023u;   // SW128 atoms are 1024-byte aligned
+    const uint32_t sB = base, sA = base + (uint32_t)(TC_N * TC_KMAX * 2);
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     :: "r"(smem_u32(&tmem_slot)), "r"(512));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::);
+    }
+    if (tid == 0) {
+        abort_flag = 0;
+        for (int i = 0; i < PP_ST; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&full[i])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&empty[i])), "r"(1));
+        }
+        for (int i = 0; i < 2; ++i) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&accf[i])), "r"(1));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&acce[i])), "r"(4));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&bfull)), "r"(1));
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_slot;
+    if (warp == 0) {
+        if (lane == 0) {
+            // the weights, once; then the A slabs of every tile through the ring
+            const uint32_t bb = smem_u32(&bfull);
+            asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                         :: "r"(bb), "r"((uint32_t)(nslab * TC_N * 128)) : "memory");
+            for (int sl = 0; sl < nslab; ++sl) tma_load_2d(sB + (uint32_t)(sl * TC_N * 128), &mapB, sl * TC_KS, 0, bb);
+            int it = 0;
+            for (int t = blockIdx.x; t < tiles && !abort_flag; t += gridDim.x)
+                for (int sl = 0; sl < nslab; ++sl, ++it) {
+                    const int s = it % PP_ST, round = it / PP_ST;
+                    if (round > 0 && !pp_wait(smem_u32(&empty[s]), (uint32_t)((round - 1) & 1), &abort_flag)) {
+                        atomicOr(status, 4);
+                        abort_flag = 1;
+                        break;
+                    }
+                    const uint32_t fb = smem_u32(&full[s]);
+                    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                                 :: "r"(fb), "r"((uint32_t)(TC_BM * 128)) : "memory");
+                    tma_load_2d(sA + (uint32_t)(s * TC_BM * 128), &mapA, sl * TC_KS, t * TC_BM, fb);
+                }
+            // every copy issued has landed before the CTA ends (the last
+            // round of each stage; bounded)
+            for (int s = 0; s < PP_ST && s < it; ++s) {
+                const int last = s + ((it - 1 - s) / PP_ST) * PP_ST;
+                pp_wait(smem_u32(&full[s]), (uint32_t)((last / PP_ST) & 1), nullptr);
+            }
+            pp_wait(smem_u32(&bfull), 0u, nullptr);
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_N >> 3) << 17) |
+                                   ((uint32_t)(TC_BM >> 4) << 24);
+            int it = 0, lt = 0, last_s = -1, last_round = 0;
+            bool ok = pp_wait(smem_u32(&bfull), 0u, &abort_flag);
+            for (int t = blockIdx.x; ok && t < tiles && !abort_flag; t += gridDim.x, ++lt) {
+                const int buf = lt & 1, use = lt >> 1;
+                if (use > 0 && !pp_wait(smem_u32(&acce[buf]), (uint32_t)((use - 1) & 1), &abort_flag)) {
+                    ok = false;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc_addr = tmem + (uint32_t)(buf * TC_N);
+                for (int sl = 0; sl < nslab; ++sl, ++it) {
+                    const int s = it % PP_ST, round = it / PP_ST;
+                    if (!pp_wait(smem_u32(&full[s]), (uint32_t)(round & 1), &abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    for (int ks = 0; ks < TC_KS / 16; ++ks) {
+                        const uint64_t ad = tc_desc(sA + (uint32_t)(s * TC_BM * 128 + ks * 32));
+                        const uint64_t bd = tc_desc(sB + (uint32_t)(sl * TC_N * 128 + ks * 32));
+                        const uint32_t acc = (sl | ks) ? 1u : 0u;
+                        asm volatile(
+                            "{\n\t.reg .pred p;\n\t"
+                            "setp.ne.b32 p, %4, 0;\n\t"
+                            "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %6, %7, %8}, p;\n\t}\n"
+                            :: "r"(acc_addr), "l"(ad), "l"(bd), "r"(idesc), "r"(acc), "r"(0u), "r"(0u), "r"(0u),
+                               "r"(0u));
+                    }
+                    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                                 :: "r"(smem_u32(&empty[s])) : "memory");
+                    last_s = s;
+                    last_round = round;
+                }
+                if (!ok) break;
+                asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                             :: "r"(smem_u32(&accf[buf])) : "memory");
+            }
+            if (!ok) {
+                atomicOr(status, 4);
+                abort_flag = 1;
+            }
+            // the MMAs issued have completed before the accumulators are
+            // freed (the last commit covers every earlier MMA; bounded)
+            if (last_s >= 0) pp_wait(smem_u32(&empty[last_s]), (uint32_t)(last_round & 1), nullptr);
+        }
+    } else {
+        const int q = warp & 3;   // the TMEM lane quarter this warp may read
+        int lt = 0;
+        for (int t = blockIdx.x; t < tiles; t += gridDim.x, ++lt) {
+            const int buf = lt & 1, use = lt >> 1;
+            // one decision for the whole warp (its TMEM loads are warp-wide)
+            if (!__all_sync(0xffffffffu, pp_wait(smem_u32(&accf[buf]), (uint32_t)(use & 1), &abort_flag))) {
+                if (lane == 0) {
+                    atomicOr(status, 4);
+                    abort_flag = 1;
+                }
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const int row = t * TC_BM + q * 32 + lane;
+            for (int cl = 0; cl < TC_N; cl += 32) {
+                uint32_t r[32];
+                const uint32_t taddr = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(buf * TC_N + cl);
+                asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+                             "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
+                             "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
+                             : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                               "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]),
+                               "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]),
+                               "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+                               "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]),
+                               "=r"(r[31])
+                             : "r"(taddr));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (row < M) {
+                    __align__(16) __nv_bfloat16 o[32];
+#pragma unroll
+                    for (int j = 0; j < 32; ++j) {
+                        const float v = __uint_as_float(r[j]) + bias[cl + j];
+                        o[j] = __float2bfloat16(v > 0.f ? v : 0.f);
+                    }
+                    uint4* dst = reinterpret_cast<uint4*>(Y + (size_t)row * TC_N + cl);
+#pragma unroll
+                    for (int qq = 0; qq < 4; ++qq) dst[qq] = reinterpret_cast<const uint4*>(o)[qq];
+                }
+            }
+            // this warp is done with the accumulator: the tile after next may use it
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" :: "r"(smem_u32(&acce[buf])) : "memory");
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (warp == 0) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" :: "r"(tmem), "r"(512));
+    }
+}
+
+// ---------------------------------------------------------------------------
 // Weight gradients on tcgen05: dW[o][i] = sum_r dC[r][o] * A_in[r][i] over
 // the batch rows r.  Both operands are stored row by row ([r][o], [r][i]),
 // so for the reduction over r they are MN-major: A (M = o, 128 per CTA)
@@ -774,8 +978,19 @@ template <int EPI>
 cudaError_t gemm_tc(lkg_surrogate* S, int n, int K, const __nv_bfloat16* A, const __nv_bfloat16* B, const float* b,
                     const __nv_bfloat16* Hm, __nv_bfloat16* Y) {
     if (n <= 0) return cudaSuccess;
-    // few row tiles (training batches): two CTAs of 128 columns per tile
     const int tiles = (n + TC_BM - 1) / TC_BM;
+    if (EPI == EPI_FWD && tiles > S->ctx->sm_count && K % TC_KS == 0 && K <= TC_KMAX) {
+        // more row tiles than SMs (large predictions): the persistent,
+        // pipelined kernel, one CTA per SM
+        alignas(64) CUtensorMap ma, mb;
+        if (!tc_map(&ma, A, n, K, TC_BM) || !tc_map(&mb, B, TC_N, K, TC_N)) return cudaErrorInvalidValue;
+        cudaError_t e = cudaFuncSetAttribute(k_gemm_tc_pp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PP_SMEM);
+        if (e != cudaSuccess) return e;
+        k_gemm_tc_pp<<<S->ctx->sm_count, PP_THREADS, PP_SMEM, S->ctx->stream>>>(ma, mb, n, K, b, Y,
+                                                                              S->d_status.as<int>());
+        return cudaGetLastError();
+    }
+    // few row tiles (training batches): two CTAs of 128 columns per tile
     const bool split = 2 * tiles <= S->ctx->sm_count;
     const int tn = split ? 128 : TC_N;
     alignas(64) CUtensorMap ma, mb;

@@ -142,6 +142,41 @@ def test_tcgen05_forward_matches_mma_sync_and_the_oracle(sur, n):
         assert err < 3e-2, (k, err)
 
 
+def test_pipelined_forward_equals_the_per_tile_kernel(sur):
+    # more row tiles than SMs: every forward layer runs on the persistent,
+    # pipelined tcgen05 kernel (weights resident, A slabs through a ring,
+    # two TMEM accumulators); its MMAs are the per-tile kernel's, so the
+    # predictions equal those of calls small enough for the per-tile kernel
+    ctx, cid, s = sur
+    n = 40000 + 77   # a ragged last tile
+    c0 = config0()
+    pos = synth.to_kernel_poses(synth.setup_poses(c0["rec"]["coords"], 13, n // 13 + 1, 9))[:n]
+    d = torch.tensor(pos, device="cuda")
+    big = torch.zeros(n, dtype=torch.float64, device="cuda")
+    s.predict_device(n, d.data_ptr(), big.data_ptr())
+    small = torch.zeros(n, dtype=torch.float64, device="cuda")
+    step = 4096   # 32 row tiles a call: the per-tile kernel
+    for b0 in range(0, n, step):
+        m = min(step, n - b0)
+        s.predict_device(m, d.data_ptr() + 56 * b0, small.data_ptr() + 8 * b0)
+    torch.cuda.synchronize()
+    assert s.status() == 0
+    a, b = big.cpu().numpy(), small.cpu().numpy()
+    assert np.all(np.isfinite(a))
+    print("pipelined vs per-tile predictions: max |diff| %.3g, bitwise equal %s" % (
+        np.abs(a - b).max(), bool(np.array_equal(a, b))))
+    assert np.abs(a - b).max() <= 1e-6 * (1.0 + np.abs(b).max())
+    s.set_backend(False)
+    try:
+        ref = torch.zeros(n, dtype=torch.float64, device="cuda")
+        s.predict_device(n, d.data_ptr(), ref.data_ptr())
+        torch.cuda.synchronize()
+        r = ref.cpu().numpy()
+    finally:
+        s.set_backend(True)
+    assert np.abs(a - r).max() < 1e-2 * (1.0 + np.abs(r).max())
+
+
 def test_tcgen05_predict_throughput_is_reported(sur):
     import time
     ctx, cid, s = sur
