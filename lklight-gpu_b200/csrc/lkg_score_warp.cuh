@@ -309,8 +309,10 @@ __device__ __forceinline__ F2 fma2(F2 a, F2 b, F2 c) {
 // two queued hits a lane (the plain kernel, no desolvation, no interface
 // bits): the pair terms of w_pair for hits e0 and e1 computed side by side
 // on packed f32 pairs, which halves the FP32 instructions of the pair math.
-// e1 counts only when v1 (a partial batch).  Same formulas and rounding
-// steps as w_pair, per hit.
+// e1 counts only when v1 (a partial batch).  Same formulas as w_pair, per
+// hit; d^2 is summed as (dx^2 + dy^2) + dz^2 with the squares of (x, y)
+// taken as one packed pair, a difference of a few ulps from w_pair's
+// fused chain (the f64 decision near the cutoff sees through it).
 template <int G>
 __device__ __forceinline__ void w_pair2(const ComplexDev& c, WSlots<G>& W, unsigned e0, unsigned e1, bool v1,
                                         unsigned flags, double& elec, double& vdw, int& np) {
@@ -320,12 +322,15 @@ __device__ __forceinline__ void w_pair2(const ComplexDev& c, WSlots<G>& W, unsig
     const float4 p0 = __ldg(c.rpar + k0), p1 = __ldg(c.rpar + k1);
     const float4 lp0 = W.lpos[l0], lp1 = W.lpos[l1], lr0 = W.lres[l0], lr1 = W.lres[l1];
     const float2 lq0 = W.lpar[l0], lq1 = W.lpar[l1];
-    const F2 dx = add2(sub2(f2(lp0.x, lp1.x), f2(a0.x, a1.x)), f2(lr0.x, lr1.x));
-    const F2 dy = add2(sub2(f2(lp0.y, lp1.y), f2(a0.y, a1.y)), f2(lr0.y, lr1.y));
-    const F2 dz = add2(sub2(f2(lp0.z, lp1.z), f2(a0.z, a1.z)), f2(lr0.z, lr1.z));
-    const F2 d2 = fma2(dz, dz, fma2(dy, dy, mul2(dx, dx)));
-    float d20, d21;
-    f2_get(d2, d20, d21);
+    // per hit: (x, y) as one packed pair (the float4s' aligned halves), z scalar
+    const F2 dxy0 = add2(sub2(f2(lp0.x, lp0.y), f2(a0.x, a0.y)), f2(lr0.x, lr0.y));
+    const F2 dxy1 = add2(sub2(f2(lp1.x, lp1.y), f2(a1.x, a1.y)), f2(lr1.x, lr1.y));
+    const float dz0 = (lp0.z - a0.z) + lr0.z, dz1 = (lp1.z - a1.z) + lr1.z;
+    float sx0, sy0, sx1, sy1;
+    f2_get(mul2(dxy0, dxy0), sx0, sy0);
+    f2_get(mul2(dxy1, dxy1), sx1, sy1);
+    const float d20 = fmaf(dz0, dz0, sy0 + sx0), d21 = fmaf(dz1, dz1, sy1 + sx1);
+    const F2 d2 = f2(d20, d21);
     bool ok0 = d20 <= 100.f, ok1 = v1 && d21 <= 100.f;
     // a hit within f32 rounding of the cutoff leaves this path for the
     // deferred list (w_flush_deferred decides it in f64); were the list full
