@@ -316,6 +316,11 @@ int lkg_surrogate_status(lkg_surrogate* s, int* bits);
  * (grid_dna.rs:44-149).  Query dims with phi == NULL. */
 int lkg_field_build(const double* coords, const double* charges, int32_t n,
                     double origin[3], int32_t dims[3], double* spacing, float* phi);
+/* Lower bound of the distance from each of m points (x, y, z) to the
+ * nearest of n receptor atoms, as the warp kernels use it to skip ligand
+ * groups that no receptor atom can reach (a 2 A grid over the receptor's
+ * box grown by 24 A; 24 outside it).  No counterpart in the reference. */
+int lkg_receptor_distance_bound(const double* coords, int32_t n, const double* points, int32_t m, float* out);
 /* Lee & Richards SASA, probe 1.4, 20 slices (lr_sasa.rs:277-291). */
 int lkg_lr_sasa(const double* coords, const double* radii, int32_t n, double* out);
 /* Self-avoiding random chain for synthetic receptors (see lkg_setup.cpp). */

@@ -89,6 +89,7 @@ def lib():
         "lkg_plan_capture": (I, [P, P, P, P, I]), "lkg_plan_replay": (I, [P]),
         "lkg_plan_sync": (I, [P]), "lkg_plan_destroy": (I, [P]),
         "lkg_field_build": (I, [P, P, I32, P, P, P, P]), "lkg_lr_sasa": (I, [P, P, I32, P]),
+        "lkg_receptor_distance_bound": (I, [P, I32, P, I32, P]),
         "lkg_synth_chain": (I, [U64, I32, D, D, D, I32, P, P]),
         "lkg_rng_new": (P, [U64]), "lkg_rng_f64": (D, [P]), "lkg_rng_free": (None, [P]),
         "lkg_gso_create": (I, [P, I, P, P, P, P, P, P]), "lkg_gso_run": (I, [P, I]),
@@ -518,6 +519,15 @@ def field_build(coords, charges):
     phi = np.zeros(int(np.prod(d.astype(np.int64))), np.float32)
     _check(lib().lkg_field_build(ptr(c), ptr(q), len(q), ptr(o), ptr(d), C.byref(s), ptr(phi)))
     return dict(phi=phi, dims=d, origin=o, spacing=s.value)
+
+
+def receptor_distance_bound(coords, points):
+    """Lower bound of each point's distance to the nearest receptor atom, as
+    the warp kernels use it to skip ligand groups out of reach (host)."""
+    c, q = _arr(coords, np.float64).reshape(-1, 3), _arr(points, np.float64).reshape(-1, 3)
+    out = np.zeros(len(q), np.float32)
+    _check(lib().lkg_receptor_distance_bound(ptr(c), len(c), ptr(q), len(q), ptr(out)))
+    return out
 
 
 def lr_sasa(coords, radii):

@@ -48,6 +48,12 @@ struct ComplexDev {
     const double4* lpar64;
     const double2* lsolv64;
     const int* lorig;
+    // lower bound of the distance to the nearest receptor atom on cells of
+    // rlb_s A (x fastest) over the receptor's box grown by rlb_m A; points
+    // outside are farther than rlb_m from every atom; null: no bound
+    const float* rlb;
+    int rlbx, rlby, rlbz;
+    float rlbox, rlboy, rlboz, rlb_inv, rlb_m;
     const float4* lgrp;      // per group of `group` atoms: ligand-frame centre, radius
     int group;               // ligand atoms per candidate-search group
     int ntiles;              // ceil(nl / tile)

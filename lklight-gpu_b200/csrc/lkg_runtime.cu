@@ -80,6 +80,97 @@ cudaError_t upload(DBuf& b, const std::vector<T>& v, cudaStream_t s) {
     return cudaMemcpyAsync(b.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s);
 }
 
+// Lower bound of the distance from a point to the nearest receptor atom,
+// on cells of RLB_S A over the receptor's box grown by RLB_M A (x fastest).
+// Cell A holds max(0, |c_A - c_B| - RLB_S sqrt(3) - 0.01), B the nearest
+// cell that holds an atom (cell centres c): a point lies within
+// RLB_S sqrt(3) / 2 of its cell's centre and so does every atom of its
+// cell, so no point of A is closer to an atom.  |c_A - c_B| comes from an
+// exact squared Euclidean distance transform over the cell centres (three
+// separable passes of the lower envelope of parabolas, Felzenszwalb and
+// Huttenlocher, "Distance transforms of sampled functions", 2012).  A point
+// outside the grid is farther than RLB_M from every atom.  The warp kernels
+// skip a ligand group whose centre's bound exceeds its candidate radius.
+constexpr float RLB_S = 2.0f, RLB_M = 24.0f;
+
+// one line of the squared transform: d[q] = min_p (q - p)^2 + f[p]
+void edt_line(const float* f, float* d, int n, int* v, float* z) {
+    int k = 0;
+    v[0] = 0;
+    z[0] = -INFINITY;
+    z[1] = INFINITY;
+    for (int q = 1; q < n; ++q) {
+        if (f[q] == INFINITY) continue;
+        while (true) {
+            if (f[v[k]] == INFINITY) { v[k] = q; z[k] = -INFINITY; z[k + 1] = INFINITY; break; }
+            const float sq = ((f[q] + (float)q * q) - (f[v[k]] + (float)v[k] * v[k])) / (2.0f * (q - v[k]));
+            if (sq <= z[k]) {
+                if (k == 0) { v[0] = q; z[0] = -INFINITY; z[1] = INFINITY; break; }
+                --k;
+                continue;
+            }
+            ++k;
+            v[k] = q;
+            z[k] = sq;
+            z[k + 1] = INFINITY;
+            break;
+        }
+    }
+    k = 0;
+    for (int q = 0; q < n; ++q) {
+        while (z[k + 1] < (float)q) ++k;
+        d[q] = f[v[k]] == INFINITY ? INFINITY : (float)(q - v[k]) * (q - v[k]) + f[v[k]];
+    }
+}
+
+}  // namespace
+
+// the bound grid of n receptor atoms (host); dims and origin out
+std::vector<float> receptor_distance_bound(const double* c, int n, int dims[3], float origin[3]) {
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
+    for (int i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = std::min(mn[a], (float)c[3 * i + a]);
+            mx[a] = std::max(mx[a], (float)c[3 * i + a]);
+        }
+    if (n == 0) { mn[0] = mn[1] = mn[2] = 0.f; mx[0] = mx[1] = mx[2] = 0.f; }
+    for (int a = 0; a < 3; ++a) {
+        origin[a] = std::floor(mn[a] - RLB_M);
+        dims[a] = std::max(1, (int)std::ceil((mx[a] + RLB_M - origin[a]) / RLB_S));
+    }
+    const size_t nc = (size_t)dims[0] * dims[1] * dims[2];
+    std::vector<float> g(nc, INFINITY);
+    for (int i = 0; i < n; ++i) {
+        int ci[3];
+        for (int a = 0; a < 3; ++a)
+            ci[a] = std::min(std::max((int)std::floor(((float)c[3 * i + a] - origin[a]) / RLB_S), 0), dims[a] - 1);
+        g[((size_t)ci[2] * dims[1] + ci[1]) * dims[0] + ci[0]] = 0.f;
+    }
+    const int L = std::max(dims[0], std::max(dims[1], dims[2]));
+    std::vector<float> f(L), d(L), z(L + 1);
+    std::vector<int> v(L);
+    for (int a = 0; a < 3; ++a) {   // the squared transform along x, then y, then z
+        const int n0 = dims[a];
+        const size_t stride = a == 0 ? 1 : (a == 1 ? (size_t)dims[0] : (size_t)dims[0] * dims[1]);
+        const int o1 = a == 0 ? 1 : 0, o2 = a == 2 ? 1 : 2;
+        for (int j2 = 0; j2 < dims[o2]; ++j2)
+            for (int j1 = 0; j1 < dims[o1]; ++j1) {
+                size_t base = 0;
+                const size_t st1 = o1 == 0 ? 1 : (size_t)dims[0], st2 = o2 == 1 ? (size_t)dims[0] : (size_t)dims[0] * dims[1];
+                base = (size_t)j1 * st1 + (size_t)j2 * st2;
+                for (int q = 0; q < n0; ++q) f[q] = g[base + q * stride];
+                edt_line(f.data(), d.data(), n0, v.data(), z.data());
+                for (int q = 0; q < n0; ++q) g[base + q * stride] = d[q];
+            }
+    }
+    const float slack = RLB_S * std::sqrt(3.0f) + 0.01f;
+    for (size_t i = 0; i < nc; ++i)
+        g[i] = g[i] == INFINITY ? RLB_M : std::max(0.f, std::min(RLB_M, std::sqrt(g[i]) * RLB_S - slack));
+    return g;
+}
+
+namespace {
+
 // receptor: sort by fine cell (x fastest), pack device arrays; the sort and
 // packing run on the GPU (lkg_cells.cu) unless the context asks for the
 // host build
@@ -158,6 +249,18 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     d.rorig = cr.rorig.as<int>(); d.cell_start = cr.cell_start.as<int>();
     d.ncx = nc[0]; d.ncy = nc[1]; d.ncz = nc[2];
     d.ox = o[0]; d.oy = o[1]; d.oz = o[2]; d.h = h; d.inv_h = inv_h; d.hx = hx; d.inv_hx = inv_hx;
+    {   // the distance bound the warp kernels skip far ligand groups with
+        int ld[3];
+        float lo[3];
+        const std::vector<float> lb = receptor_distance_bound(R.c.data(), n, ld, lo);
+        LKG_CK(upload(cr.rlb, lb, ctx->stream), "upload receptor bound");
+        LKG_CK(cudaStreamSynchronize(ctx->stream), "upload receptor bound");
+        d.rlb = cr.rlb.as<float>();
+        d.rlbx = ld[0]; d.rlby = ld[1]; d.rlbz = ld[2];
+        d.rlbox = lo[0]; d.rlboy = lo[1]; d.rlboz = lo[2];
+        d.rlb_inv = 1.0f / RLB_S;
+        d.rlb_m = RLB_M;
+    }
     cr.n_cells = (int)ncell;
     // desolvation hash capacity: >= 2 x receptor atoms up to 2048 slots
     // (16 KB of shared memory in the fast kernel, 24 KB in the exact one); a
@@ -1159,6 +1262,31 @@ int lkg_plan_sync(lkg_plan* P) {
     int st = wait_stream(P->ctx, 300.0);
     if (st) return st;
     return check_status_word(P->scratch.status.as<int>());
+}
+
+}  // extern "C"
+
+extern "C" {
+
+// The lower bound of the distance to the nearest of n receptor atoms that
+// the warp kernels skip far ligand groups with, at m points (host; for
+// checks of the bound).
+int lkg_receptor_distance_bound(const double* coords, int32_t n, const double* points, int32_t m, float* out) {
+    if (n < 0 || m < 0 || (n > 0 && !coords) || (m > 0 && (!points || !out)))
+        return set_error(LKG_ERR_ARG, "bad distance-bound args");
+    int dims[3];
+    float o[3];
+    const std::vector<float> g = receptor_distance_bound(coords, n, dims, o);
+    for (int i = 0; i < m; ++i) {
+        int ix[3];
+        bool inside = true;
+        for (int a = 0; a < 3; ++a) {
+            ix[a] = (int)std::floor(((float)points[3 * i + a] - o[a]) * (1.0f / RLB_S));
+            inside = inside && ix[a] >= 0 && ix[a] < dims[a];
+        }
+        out[i] = inside ? g[((size_t)ix[2] * dims[1] + ix[1]) * dims[0] + ix[0]] : RLB_M;
+    }
+    return set_ok();
 }
 
 }  // extern "C"

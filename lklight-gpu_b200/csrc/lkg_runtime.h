@@ -80,6 +80,7 @@ struct MolIn {
 struct ComplexRec {
     int family = -1;
     DBuf rpos, rpar, rsolv, rpos64, rpar64, rsolv64, rorig, cell_start;
+    DBuf rlb;   // distance lower bound of the receptor (ComplexDev::rlb)
     DBuf lpos, lpar, lsolv, lpos64, lpar64, lsolv64, lorig, lgrp;
     DBuf phi;
     DBuf rtag, ltag;   // interface tags (restraints / membrane), when set
@@ -154,6 +155,9 @@ namespace lkg {
 int complex_create(lkg_ctx* ctx, int family, unsigned flags, int lj_form, const MolIn& rec,
                    const MolIn& lig, const lkg_field* field, bool build_field, double solv_const,
                    int* out_id);
+// lower bound of the distance to the nearest of n receptor atoms on a
+// coarse grid (dims, origin out; ComplexDev::rlb)
+std::vector<float> receptor_distance_bound(const double* c, int n, int dims[3], float origin[3]);
 // the receptor's cell-sorted arrays and cell_start built on the GPU
 // (lkg_cells.cu), bit for bit the host build's
 int build_receptor_device(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr, const float o[3], const int nc[3],

@@ -409,6 +409,16 @@ __device__ __forceinline__ void w_fetch(const ComplexDev& c, int st, int excl, i
 
 constexpr unsigned long long W_NOMIN = 0x7fefffffffffffffull;   // largest finite double
 
+// lower bound of the distance from (x, y, z) to the nearest receptor atom
+// (ComplexDev::rlb; rlb_m outside its grid)
+__device__ __forceinline__ float w_receptor_bound(const ComplexDev& c, float x, float y, float z) {
+    const int ix = (int)floorf((x - c.rlbox) * c.rlb_inv);
+    const int iy = (int)floorf((y - c.rlboy) * c.rlb_inv);
+    const int iz = (int)floorf((z - c.rlboz) * c.rlb_inv);
+    if (ix < 0 || iy < 0 || iz < 0 || ix >= c.rlbx || iy >= c.rlby || iz >= c.rlbz) return c.rlb_m;
+    return __ldg(c.rlb + ((size_t)iz * c.rlby + iy) * c.rlbx + ix);
+}
+
 
 // The warp's sums over its groups.
 struct WAcc {
@@ -522,6 +532,12 @@ __device__ __forceinline__ void w_groups(const ComplexDev& c, WSlots<G>& W, WDes
         }
         __syncwarp();
         const float R = SCAN_R + gs.w, R2 = R * R;
+        // cpydock kernel: no receptor atom within R of the centre, so the
+        // group has no candidate and its rows are not enumerated (most groups
+        // of a large ligand at the interface: with a 12,000-atom ligand on a
+        // 101,000-atom receptor the step is 4.5 % faster; the plain kernel,
+        // whose ligands are smaller, measured 1 % slower with the test)
+        if (DESOLV && c.rlb && R < c.rlb_m && w_receptor_bound(c, gx, gy, gz) > R) continue;
         const int cz0 = max(0, (int)floorf((gz - R - c.oz) * c.inv_h));
         const int cz1 = min(c.ncz - 1, (int)floorf((gz + R - c.oz) * c.inv_h));
         const int cy0 = max(0, (int)floorf((gy - R - c.oy) * c.inv_h));

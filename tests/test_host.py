@@ -245,3 +245,26 @@ def test_bench_top5_overlap_rule():
     # run B's top 5 exclude its lowest-scored pose
     sc_b = np.array([1.0, 5, 4, 3, 2, 6])
     assert bench.top5_overlap(tr_a, sc_a, tr_a, sc_b) == 0.8
+
+
+def test_receptor_distance_bound_never_exceeds_the_nearest_atom():
+    # the warp kernels skip a ligand group when this bound at its centre
+    # exceeds its candidate radius: it must never exceed the true distance
+    # to the nearest receptor atom, and it should be tight enough to skip
+    # (within the grid's slack of 2 sqrt(3) cell half-diagonals + 0.01 A)
+    import numpy as np
+    from scipy.spatial import cKDTree
+    for nr, seed in ((1500, 3), (6000, 8)):
+        rec = synth.globule(nr, seed)
+        c = rec["coords"]
+        rng = np.random.default_rng(seed)
+        lo, hi = c.min(0) - 35.0, c.max(0) + 35.0
+        pts = rng.uniform(lo, hi, size=(20000, 3))
+        pts = np.vstack([pts, c[:500] + rng.normal(0, 1.0, size=(500, 3))])   # near the atoms too
+        lb = lkg.receptor_distance_bound(c, pts).astype(np.float64)
+        d, _ = cKDTree(c).query(pts)
+        assert np.all(lb <= d + 1e-9), float((lb - d).max())
+        inside = lb < 24.0
+        slack = 2.0 * np.sqrt(3.0) * 2.0 + 0.02
+        assert np.all(lb[inside] >= np.minimum(d[inside], 24.0) - slack)
+        assert (lb > 15.0).mean() > 0.2   # far points are recognised as far
