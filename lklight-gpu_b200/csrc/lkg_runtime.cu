@@ -266,10 +266,10 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
     // (16 KB of shared memory in the fast kernel, 24 KB in the exact one); a
     // pose touching more receptor atoms within 6.4 A continues in the launch
     // group's global spill tables (more slots than receptor atoms).  The
-    // small table leaves room for two 12-warp blocks per SM with groups of
-    // 16 and for L1: on the 101k-atom config-4 receptor 2048 slots score
-    // 1.3x faster than 8192 (whose larger tables spilled less) and 1.24x
-    // faster than 1024 (which spill more)
+    // small table leaves room for several blocks per SM with groups of 16
+    // and for L1: on a 101k-atom receptor with a 12k-atom ligand 2048 slots
+    // score 1.3x faster than 8192 (whose larger tables spilled less) and
+    // 1.24x faster than 1024 (which spill more)
     int cap = 64;
     while (cap < 2 * n && cap < 2048) cap <<= 1;
     d.hcap = cap;
