@@ -92,6 +92,7 @@ cudaError_t upload(DBuf& b, const std::vector<T>& v, cudaStream_t s) {
 // outside the grid is farther than RLB_M from every atom.  The warp kernels
 // skip a ligand group whose centre's bound exceeds its candidate radius.
 constexpr float RLB_S = 2.0f, RLB_M = 24.0f;
+constexpr size_t RLB_MAX_CELLS = (size_t)1 << 26;   // 256 MB of bound at most
 
 // one line of the squared transform: d[q] = min_p (q - p)^2 + f[p]
 void edt_line(const float* f, float* d, int n, int* v, float* z) {
@@ -125,7 +126,8 @@ void edt_line(const float* f, float* d, int n, int* v, float* z) {
 
 }  // namespace
 
-// the bound grid of n receptor atoms (host); dims and origin out
+// the bound grid of n receptor atoms (host); dims and origin out; empty
+// when the grid would exceed RLB_MAX_CELLS
 std::vector<float> receptor_distance_bound(const double* c, int n, int dims[3], float origin[3]) {
     float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
     for (int i = 0; i < n; ++i)
@@ -134,10 +136,16 @@ std::vector<float> receptor_distance_bound(const double* c, int n, int dims[3], 
             mx[a] = std::max(mx[a], (float)c[3 * i + a]);
         }
     if (n == 0) { mn[0] = mn[1] = mn[2] = 0.f; mx[0] = mx[1] = mx[2] = 0.f; }
+    double cells = 1.0;
     for (int a = 0; a < 3; ++a) {
         origin[a] = std::floor(mn[a] - RLB_M);
-        dims[a] = std::max(1, (int)std::ceil((mx[a] + RLB_M - origin[a]) / RLB_S));
+        const double w = std::ceil(((double)mx[a] + RLB_M - origin[a]) / RLB_S);
+        cells *= std::max(1.0, w);
+        dims[a] = (int)std::min(std::max(1.0, w), 1e9);
     }
+    // an implausibly spread receptor (or non-finite coordinates) gets no
+    // bound: the kernels then enumerate every group's rows
+    if (!(cells <= (double)RLB_MAX_CELLS)) return {};
     const size_t nc = (size_t)dims[0] * dims[1] * dims[2];
     std::vector<float> g(nc, INFINITY);
     for (int i = 0; i < n; ++i) {
@@ -253,9 +261,11 @@ int build_receptor(lkg_ctx* ctx, const MolIn& R, ComplexRec& cr) {
         int ld[3];
         float lo[3];
         const std::vector<float> lb = receptor_distance_bound(R.c.data(), n, ld, lo);
-        LKG_CK(upload(cr.rlb, lb, ctx->stream), "upload receptor bound");
-        LKG_CK(cudaStreamSynchronize(ctx->stream), "upload receptor bound");
-        d.rlb = cr.rlb.as<float>();
+        if (!lb.empty()) {
+            LKG_CK(upload(cr.rlb, lb, ctx->stream), "upload receptor bound");
+            LKG_CK(cudaStreamSynchronize(ctx->stream), "upload receptor bound");
+        }
+        d.rlb = lb.empty() ? nullptr : cr.rlb.as<float>();
         d.rlbx = ld[0]; d.rlby = ld[1]; d.rlbz = ld[2];
         d.rlbox = lo[0]; d.rlboy = lo[1]; d.rlboz = lo[2];
         d.rlb_inv = 1.0f / RLB_S;
@@ -1277,7 +1287,8 @@ int lkg_receptor_distance_bound(const double* coords, int32_t n, const double* p
     int dims[3];
     float o[3];
     const std::vector<float> g = receptor_distance_bound(coords, n, dims, o);
-    for (int i = 0; i < m; ++i) {
+    for (int i = 0; i < m && g.empty(); ++i) out[i] = 0.f;   // no bound: 0 bounds every distance
+    for (int i = 0; i < m && !g.empty(); ++i) {
         int ix[3];
         bool inside = true;
         for (int a = 0; a < 3; ++a) {

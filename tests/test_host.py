@@ -268,3 +268,13 @@ def test_receptor_distance_bound_never_exceeds_the_nearest_atom():
         slack = 2.0 * np.sqrt(3.0) * 2.0 + 0.02
         assert np.all(lb[inside] >= np.minimum(d[inside], 24.0) - slack)
         assert (lb > 15.0).mean() > 0.2   # far points are recognised as far
+
+
+def test_receptor_distance_bound_gives_up_on_a_spread_receptor():
+    # a receptor spread over kilometres would need a huge bound grid: the
+    # library builds none (the kernels then enumerate every group) and the
+    # bound is 0, still a lower bound
+    import numpy as np
+    c = np.array([[0.0, 0.0, 0.0], [1.0, 2.0, 3.0], [4.0e5, 0.0, 0.0]])
+    lb = lkg.receptor_distance_bound(c, np.array([[50.0, 50.0, 50.0], [0.0, 0.0, 0.0]]))
+    assert np.array_equal(lb, np.zeros(2, np.float32))
